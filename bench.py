@@ -1,0 +1,315 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 respond() path (InsPIRe keyword PIR, rkdud007/inspire-rs).
+
+Workload: 1,000,000 ML-KEM-768 records (32-byte IDs + 1184-byte keys), cuckoo
+buckets 2^21 (the reference default for 1M records; 262,144 is rejected by the
+reference because buckets < records), dim0 = 2048 -> DB 2048 x 720,896 u16,
+352 packing outputs, interpolation degree 32, 11 fold groups.  One step = one
+respond() of one KeywordQueryPayload (2 cuckoo sub-queries), batch 1, u64
+modular arithmetic.  Server state is seeded synthetic data of the reference's
+shapes (the reference's own timing mode, engine.rs:693-729); queries are
+seeded synthetic payloads.
+
+  value : payloads/s with queries resident in HBM (ipr_server_respond_device)
+  e2e   : payloads/s through ipr_server_respond with host buffers (H2D query,
+          D2H response inside the timed region)
+
+--impl reference times the CPU restatement of the reference's respond() on the
+host cores (the reference's Rust CPU path cannot be built here).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+
+RECORDS, KEY, VALUE, BUCKETS, DIM0 = 1_000_000, 32, 1184, 2_097_152, 2048
+N = 2048
+METRIC = "queries/s at 1M ML-KEM-768 keys (batch-1 u64 respond, bit-exact)"
+UNIT = "payloads/s"
+
+
+def load_package():
+    import importlib.util
+    if "inspire_rs_b200" in sys.modules:
+        return sys.modules["inspire_rs_b200"]
+    d = os.path.join(ROOT, "inspire-rs_b200")
+    spec = importlib.util.spec_from_file_location("inspire_rs_b200", os.path.join(d, "__init__.py"),
+                                                  submodule_search_locations=[d])
+    m = importlib.util.module_from_spec(spec)
+    sys.modules["inspire_rs_b200"] = m
+    spec.loader.exec_module(m)
+    return m
+
+
+def load_oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    return oracle
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def read_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def read_traffic():
+    """dram bytes per k_pack launch from the committed ncu summary (scaled to the full launch), or None"""
+    path = os.path.join(ROOT, "profiles", "k_pack_1M_dram.md")
+    try:
+        for ln in open(path):
+            if ln.startswith("traffic_bytes_per_full_launch:"):
+                return float(ln.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_sample(orc, threads_note=""):
+    """Oracle respond() on one fold group of the 1M workload (32 of 352 packing
+    outputs, 65,536 DB columns), scaled by the 11 groups to a full payload."""
+    plan = orc.plan_from_shape(RECORDS, KEY, VALUE, BUCKETS, DIM0)
+    groups = plan["c"]
+    sdb = orc.SynthDB(plan["db_rows"], plan["interp"], plan["interp"], 1, seed=7)
+    q = orc.synth_query(2026, plan["db_rows"], 2)
+    orc.respond(sdb, q)  # warm
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        orc.respond(sdb, q)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el > 8 or reps >= 3:
+            break
+    per_group = el / reps
+    per_payload = per_group * groups
+    return {"value": 1.0 / per_payload, "unit": UNIT, "cores": int(orc.threads()), "kind": "port",
+            "sample": f"oracle respond() of 1 of {groups} fold groups (32 packing outputs, db 2048x65536, "
+                      f"2 queries) x{reps}, scaled x{groups}; {per_payload:.2f} s/payload"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        orc = load_oracle()
+        vals = []
+        for _ in range(args.warmup):
+            cpu_sample(orc)
+        for _ in range(args.steps):
+            vals.append(cpu_sample(orc))
+        v = statistics.median([x["value"] for x in vals])
+        cb = dict(vals[-1])
+        cb["value"] = v
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": "1M ML-KEM-768 respond(), buckets 2^21, dim0 2048, 2 queries/payload",
+                       "records": RECORDS, "buckets": BUCKETS, "dim0": DIM0, "batch": 1},
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }))
+        return 0
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+
+    pkg = load_package()
+    plan = pkg.plan_from_shape(RECORDS, KEY, VALUE, BUCKETS, DIM0)
+    srv = pkg.KeywordServer.synthetic(plan, seed=7 + rank, device=dev)
+    qbytes = srv.query_bytes(2)
+    rbytes = srv.response_bytes(2)
+
+    # distinct seeded payloads, resident in HBM for the device-timed loop
+    nq_distinct = 4
+    import numpy as np
+
+    def synth_payload(seed):
+        # a structurally valid payload: uniform 28-bit residues below each prime
+        rng = np.random.default_rng(seed)
+        nvals = 3 * N * 2 + 2 * (plan.db_rows + 6 * N)
+        lo = rng.integers(0, 268369921, nvals, dtype=np.uint64)
+        hi = rng.integers(0, 249561089, nvals, dtype=np.uint64)
+        v = (lo | (hi << np.uint64(28))).astype("<u8")
+        return bytes([2]) + v.view(np.uint8).reshape(-1, 8)[:, :7].tobytes()
+
+    payloads = [synth_payload(1000 * rank + i) for i in range(nq_distinct)]
+    assert len(payloads[0]) == qbytes
+    d_q = [torch.frombuffer(bytearray(p), dtype=torch.uint8).to(dev) for p in payloads]
+    d_out = torch.empty(rbytes, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.ExternalStream(srv.stream_handle(), device=dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # warmup (device path and host path)
+    for i in range(args.warmup):
+        srv.respond_device(d_q[i % nq_distinct].data_ptr(), qbytes, d_out.data_ptr(), rbytes)
+        srv.respond_to_serialized_query(payloads[i % nq_distinct])
+    srv.sync()
+
+    # ---- device-resident timed region -------------------------------------------------
+    clocks = ClockSampler(dev if world == 1 else local)
+    clocks.start()
+    srv.set_profiling(True)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(args.steps):
+        srv.respond_device(d_q[i % nq_distinct].data_ptr(), qbytes, d_out.data_ptr(), rbytes)
+    e1.record(stream)
+    srv.sync()
+    barrier()
+    dev_ms = e0.elapsed_time(e1)
+    stage_ms, calls = srv.stage_times()
+    srv.set_profiling(False)
+    clk = clocks.stop()
+
+    # ---- end-to-end through the host API (pinned staging, H2D + D2H per step) ----------
+    barrier()
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    h0.record(stream)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        srv.respond_to_serialized_query(payloads[i % nq_distinct])
+    h1.record(stream)
+    srv.sync()
+    wall_ms = (time.perf_counter() - t0) * 1000
+    barrier()
+    e2e_ms = max(h0.elapsed_time(h1), 0.0)
+    e2e_ms = max(e2e_ms, wall_ms)
+
+    t = torch.tensor([dev_ms, e2e_ms], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev_ms, e2e_ms = float(t[0]), float(t[1])
+    total = args.steps * world
+    value = total / (dev_ms / 1000.0)
+    e2e = total / (e2e_ms / 1000.0)
+
+    pack_ms = stage_ms["pack"] / max(calls, 1)
+    pack_bytes = plan.instances * (2 * 3069 + 3) * N * 8  # bold_t + bold_t_bar + bold_t_hat per launch
+    peak, peak_kind = read_peaks()
+    achieved = pack_bytes / (pack_ms / 1000.0) / 1e9
+
+    out = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            try:
+                cpu = cpu_sample(load_oracle())
+            except Exception as ex:  # reported, never fatal to the GPU number
+                cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "port", "sample": f"failed: {ex}"}
+        stage_avg = {k: round(v / max(calls, 1), 4) for k, v in stage_ms.items()}
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": "1M ML-KEM-768 respond(), buckets 2^21, dim0 2048, 2 queries/payload, batch 1",
+                       "records": RECORDS, "buckets": BUCKETS, "dim0": DIM0, "db_rows": plan.db_rows,
+                       "db_cols": plan.db_cols, "instances": plan.instances, "interp": plan.interp, "c": plan.c,
+                       "parallelism": f"replica x{world}",
+                       "l2": "inputs larger than L2 (35.4 GB packing stream + 2.95 GB DB per step)"},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": qbytes, "d2h_bytes_per_step": rbytes},
+            "roofline": {"bound": "hbm", "kernel": "k_pack", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                         "traffic": read_traffic(), "algorithmic_bytes": pack_bytes, "avg_launch_ms": pack_ms},
+            "stage_ms": stage_avg,
+            "gpu_launches": 6 * args.steps,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(out))
+    srv.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

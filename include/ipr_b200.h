@@ -1,0 +1,142 @@
+/*
+ * ipr_b200.h — C ABI of the B200-native InsPIRe keyword-PIR respond() path.
+ *
+ * Drop-in boundary for rkdud007/inspire-rs: the Rust KeywordServer
+ * (src/pir/server/keyword.rs) keeps setup / public_params / respond and the
+ * client wire format; the device work behind respond() is this library.
+ * Plain pointers and sizes only; every call returns an int status
+ * (IPR_OK = 0, negative on error) and never aborts; ipr_last_error() gives the
+ * message of the calling thread's last failure.
+ *
+ * The reference-named entry points the Rust crate already declares
+ * (src/pir/gpu/gemv.rs:5-25, encode.rs:3-32, packing_online.rs:11-92) are in
+ * ipr_b200_compat.h.
+ */
+#ifndef IPR_B200_H
+#define IPR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IPR_OK 0
+#define IPR_E_ARGS -1     /* bad argument or shape */
+#define IPR_E_OOM -2      /* device or host allocation failed, or HBM budget exceeded */
+#define IPR_E_CUDA -3     /* CUDA runtime error (message in ipr_last_error) */
+#define IPR_E_TIMEOUT -4  /* a bounded wait ran out */
+#define IPR_E_FORMAT -5   /* malformed query bytes */
+#define IPR_E_SPACE -6    /* output buffer too small (required size reported) */
+#define IPR_E_STATE -7    /* call made in the wrong state */
+
+#define IPR_POLY_LEN 2048
+#define IPR_RESULT_BYTES 12288 /* one switched RLWE result: 2048x28 + 2048x20 bits */
+
+/* Shape plan of a keyword server.
+ * Replaces KeywordServerSetupPlan::from_shape (src/pir/server/keyword.rs:145-233)
+ * and KeywordServerGpuMemoryEstimate::from_plan (keyword.rs:105-141);
+ * buckets = 0 / dim0 = 0 select the reference defaults (keyword.rs:29-31, 191-200). */
+typedef struct ipr_plan {
+    uint64_t num_items;      /* cuckoo buckets */
+    uint64_t entry_size;     /* key + value bytes */
+    uint64_t item_size_bits;
+    uint64_t dim0;
+    uint64_t db_rows;        /* first dimension (query row length) */
+    uint64_t db_cols;        /* instances * 2048 */
+    uint64_t instances;      /* packing outputs per query */
+    uint64_t interp;         /* interpolation degree (fold depth) */
+    uint64_t c;              /* fold groups = result polys per query */
+    uint64_t peak_bytes;     /* the reference's setup peak estimate */
+} ipr_plan;
+
+int ipr_plan_from_shape(uint64_t record_count, uint64_t key_size, uint64_t value_size, uint64_t buckets,
+                        uint64_t dim0, ipr_plan *out);
+
+/* Serialized sizes: deserialize_keyword_query (src/protocol/wire.rs:618-705) and
+ * serialize_keyword_response (wire.rs:708-726). */
+uint64_t ipr_query_bytes(uint64_t db_rows, unsigned num_queries);
+
+typedef struct ipr_server ipr_server;
+
+/* Host copies of the server state produced by setup (encode + offline
+ * precomputation).  Layouts follow the reference:
+ *   db          [db_cols][db_rows] u16, column-major (native/cuda/gemv_kernel.cu:63)
+ *   a_hat       [instances][2048] u64 mod q           (PrecompInsPIR::a_hat, packing.rs:1718-1723)
+ *   bold_t      [instances][3069][2048] u64 condensed (lo32 = mod q0, hi32 = mod q1)
+ *   bold_t_bar  same layout
+ *   bold_t_hat  [instances][3][2048] u64 condensed
+ *   stash       stash_count entries of stash_entry_bytes (echoed in every response)
+ * The public-parameter fields feed ipr_server_public_params_json. */
+typedef struct ipr_server_data {
+    const uint16_t *db;
+    const uint64_t *a_hat;
+    const uint64_t *bold_t;
+    const uint64_t *bold_t_bar;
+    const uint64_t *bold_t_hat;
+    const uint8_t *stash;
+    uint64_t stash_count;
+    uint64_t stash_entry_bytes;
+    uint64_t key_size, value_size, num_records;
+    uint8_t cuckoo_seed[16];
+} ipr_server_data;
+
+/* Upload server state to device `device` and build the per-request pipeline.
+ * Replaces gpu_gemv_upload_db + gpu_packing_online_upload_precomp +
+ * gpu_rotation_upload_tables (gemv_kernel.cu:116-141, packing_online_kernel.cu:110-142,
+ * rotation_kernel.cu:71-94).  Fails with IPR_E_OOM if it does not fit. */
+int ipr_server_create(int device, const ipr_plan *plan, const ipr_server_data *data, ipr_server **out);
+
+/* Same, with seeded synthetic DB / precomputation generated on the device
+ * (uniform u16 < 65535, uniform residues), the timing mode the reference
+ * itself uses (online_only, src/pir/server/engine.rs:693-729). */
+int ipr_server_create_synthetic(int device, const ipr_plan *plan, uint64_t seed, ipr_server **out);
+
+void ipr_server_destroy(ipr_server *srv);
+
+/* KeywordServer::public_params (keyword.rs:511-532), serde JSON form of PublicParams. */
+int ipr_server_public_params_json(const ipr_server *srv, char *out, size_t cap, size_t *out_len);
+
+uint64_t ipr_server_query_bytes(const ipr_server *srv, unsigned num_queries);
+uint64_t ipr_server_response_bytes(const ipr_server *srv, unsigned num_queries);
+int ipr_server_hbm_bytes(const ipr_server *srv, uint64_t *out);
+int ipr_server_plan(const ipr_server *srv, ipr_plan *out);
+
+/* KeywordServer::respond_to_serialized_query (keyword.rs:636-640): serialized
+ * KeywordQueryPayload in, serialized KeywordResponsePayload out, host buffers.
+ * On IPR_E_SPACE *out_len holds the required size.  Thread safe (serialised
+ * per server). */
+int ipr_server_respond(ipr_server *srv, const uint8_t *query, size_t len, uint8_t *out, size_t cap,
+                       size_t *out_len);
+
+/* n payloads; statuses[i] receives each payload's status. */
+int ipr_server_respond_batch(ipr_server *srv, int n, const uint8_t *const *queries, const size_t *lens,
+                             uint8_t *const *outs, const size_t *caps, size_t *out_lens, int *statuses);
+
+/* Device-resident variant: query and response already in device memory of
+ * the server's device.  Enqueued on the server stream and returns without
+ * waiting; `len` must be the exact query size for the payload's query count. */
+int ipr_server_respond_device(ipr_server *srv, const uint8_t *d_query, size_t len, uint8_t *d_out, size_t cap,
+                              size_t *out_len);
+int ipr_server_stream(ipr_server *srv, void **cuda_stream);
+int ipr_server_sync(ipr_server *srv);
+
+/* Per-stage CUDA-event timing on the server stream (stages below), summed
+ * over the calls since profiling was enabled. */
+#define IPR_STAGE_PARSE 0
+#define IPR_STAGE_GEMV 1
+#define IPR_STAGE_PACK 2
+#define IPR_STAGE_INTT 3
+#define IPR_STAGE_FOLD 4
+#define IPR_NSTAGES 5
+int ipr_server_set_profiling(ipr_server *srv, int on);
+int ipr_server_stage_times(ipr_server *srv, double *ms_sum, uint64_t *calls);
+
+const char *ipr_last_error(void);
+const char *ipr_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,332 @@
+"""inspire-rs_b200 — B200-native respond() path of the InsPIRe keyword-PIR server.
+
+Python mirror of the reference's server interface (rkdud007/inspire-rs,
+src/pir/server/keyword.rs): ``KeywordServer`` with ``public_params()``,
+``respond(payload)`` and ``respond_to_serialized_query(bytes)``, plus the shape
+plan of ``KeywordServerSetupPlan::from_shape`` (keyword.rs:145-233).  All work
+runs in ``libipr_b200.so`` (sm_100a CUDA behind the C ABI in
+``include/ipr_b200.h``); there is no CPU fallback.  Importing the package on a
+machine without the built library raises ``ImportError``.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+from dataclasses import dataclass
+from typing import List, Optional, Sequence
+
+__all__ = [
+    "IprError", "Plan", "KeywordServer", "plan_from_shape", "query_bytes", "lib",
+    "KeywordQueryPayload", "KeywordResponsePayload", "serialize_keyword_query",
+    "deserialize_keyword_response", "POLY_LEN", "RESULT_BYTES",
+]
+
+POLY_LEN = 2048
+RESULT_BYTES = 12288
+STAGES = ("parse", "gemv", "pack", "intt", "fold")
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libipr_b200.so")
+
+if not os.path.exists(_LIB_PATH):
+    raise ImportError(
+        f"libipr_b200.so not built at {_LIB_PATH}; run `make -C inspire-rs_b200` "
+        "(the respond() path has no CPU fallback)")
+lib = ctypes.CDLL(_LIB_PATH)
+
+_u64, _i32, _sz = ctypes.c_uint64, ctypes.c_int, ctypes.c_size_t
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_vp = ctypes.c_void_p
+
+
+class _Plan(ctypes.Structure):
+    _fields_ = [(n, _u64) for n in (
+        "num_items", "entry_size", "item_size_bits", "dim0", "db_rows", "db_cols",
+        "instances", "interp", "c", "peak_bytes")]
+
+
+class _ServerData(ctypes.Structure):
+    _fields_ = [("db", _vp), ("a_hat", _vp), ("bold_t", _vp), ("bold_t_bar", _vp),
+                ("bold_t_hat", _vp), ("stash", _vp), ("stash_count", _u64),
+                ("stash_entry_bytes", _u64), ("key_size", _u64), ("value_size", _u64),
+                ("num_records", _u64), ("cuckoo_seed", ctypes.c_uint8 * 16)]
+
+
+def _sig(name, restype, *argtypes):
+    f = getattr(lib, name)
+    f.restype = restype
+    f.argtypes = list(argtypes)
+    return f
+
+
+_plan_from_shape = _sig("ipr_plan_from_shape", _i32, _u64, _u64, _u64, _u64, _u64, ctypes.POINTER(_Plan))
+_query_bytes = _sig("ipr_query_bytes", _u64, _u64, ctypes.c_uint)
+_create = _sig("ipr_server_create", _i32, _i32, ctypes.POINTER(_Plan), ctypes.POINTER(_ServerData), ctypes.POINTER(_vp))
+_create_synth = _sig("ipr_server_create_synthetic", _i32, _i32, ctypes.POINTER(_Plan), _u64, ctypes.POINTER(_vp))
+_destroy = _sig("ipr_server_destroy", None, _vp)
+_pp_json = _sig("ipr_server_public_params_json", _i32, _vp, ctypes.c_char_p, _sz, ctypes.POINTER(_sz))
+_srv_qbytes = _sig("ipr_server_query_bytes", _u64, _vp, ctypes.c_uint)
+_srv_rbytes = _sig("ipr_server_response_bytes", _u64, _vp, ctypes.c_uint)
+_hbm = _sig("ipr_server_hbm_bytes", _i32, _vp, ctypes.POINTER(_u64))
+_respond = _sig("ipr_server_respond", _i32, _vp, _u8p, _sz, _u8p, _sz, ctypes.POINTER(_sz))
+_respond_dev = _sig("ipr_server_respond_device", _i32, _vp, _vp, _sz, _vp, _sz, ctypes.POINTER(_sz))
+_stream = _sig("ipr_server_stream", _i32, _vp, ctypes.POINTER(_vp))
+_sync = _sig("ipr_server_sync", _i32, _vp)
+_set_prof = _sig("ipr_server_set_profiling", _i32, _vp, _i32)
+_stage_times = _sig("ipr_server_stage_times", _i32, _vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_u64))
+_last_error = _sig("ipr_last_error", ctypes.c_char_p)
+_version = _sig("ipr_version", ctypes.c_char_p)
+
+STATUS = {0: "IPR_OK", -1: "IPR_E_ARGS", -2: "IPR_E_OOM", -3: "IPR_E_CUDA", -4: "IPR_E_TIMEOUT",
+          -5: "IPR_E_FORMAT", -6: "IPR_E_SPACE", -7: "IPR_E_STATE"}
+
+
+class IprError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        msg = (_last_error() or b"").decode(errors="replace")
+        super().__init__(f"{where}: {STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+def _check(st: int, where: str):
+    if st != 0:
+        raise IprError(st, where)
+
+
+@dataclass(frozen=True)
+class Plan:
+    """KeywordServerSetupPlan (keyword.rs:91-102) plus the GPU memory estimate."""
+    num_items: int
+    entry_size: int
+    item_size_bits: int
+    dim0: int
+    db_rows: int
+    db_cols: int
+    instances: int
+    interp: int
+    c: int
+    peak_bytes: int
+
+    def _c(self) -> _Plan:
+        return _Plan(*[getattr(self, f) for f, _ in _Plan._fields_])
+
+    @property
+    def query_bytes(self) -> int:
+        return query_bytes(self.db_rows, 2)
+
+
+def plan_from_shape(record_count: int, key_size: int, value_size: int,
+                    buckets: Optional[int] = None, dim0: Optional[int] = None) -> Plan:
+    """KeywordServerSetupPlan::from_shape (keyword.rs:145-233); raises on the
+    shapes the reference rejects (e.g. buckets < records, keyword.rs:171-180)."""
+    p = _Plan()
+    _check(_plan_from_shape(record_count, key_size, value_size, buckets or 0, dim0 or 0, ctypes.byref(p)),
+           "plan_from_shape")
+    return Plan(*[getattr(p, f) for f, _ in _Plan._fields_])
+
+
+def query_bytes(db_rows: int, num_queries: int = 2) -> int:
+    return int(_query_bytes(db_rows, num_queries))
+
+
+# ---------------------------------------------------------------------------
+# wire payloads (src/protocol/wire.rs:522-538, 542-615, 708-759)
+# ---------------------------------------------------------------------------
+@dataclass
+class KeywordQueryPayload:
+    """Decoded form of a keyword query.  y_body/z_body: 3 x 2048 condensed u64
+    (lo32 = mod q0, hi32 = mod q1); queries: list of (packed_query_row
+    [db_rows] condensed, ct_gsw_body 6 x (2 x 2048) limb-major residues)."""
+    y_body: Sequence[Sequence[int]]
+    z_body: Sequence[Sequence[int]]
+    queries: List[tuple]
+
+
+@dataclass
+class KeywordResponsePayload:
+    responses: List[bytes]
+    stash_entries: List[bytes]
+
+
+def serialize_keyword_query(p: KeywordQueryPayload) -> bytes:
+    """serialize_keyword_query (wire.rs:542-615): 1 count byte, then 56-bit
+    fields (crt0 | crt1 << 28) LSB-first from bit 8."""
+    import numpy as np
+    m28 = (1 << 28) - 1
+    vals = []
+    for i in range(3):
+        yz = np.empty(2 * POLY_LEN, dtype=np.uint64)
+        yz[0::2] = np.asarray(p.y_body[i], dtype=np.uint64)
+        yz[1::2] = np.asarray(p.z_body[i], dtype=np.uint64)
+        vals.append((yz & np.uint64(m28)) | ((yz >> np.uint64(32)) << np.uint64(28)))
+    for row, gsw in p.queries:
+        r = np.asarray(row, dtype=np.uint64)
+        vals.append((r & np.uint64(m28)) | ((r >> np.uint64(32)) << np.uint64(28)))
+        g = np.asarray(gsw, dtype=np.uint64).reshape(6, 2, POLY_LEN)
+        vals.append(((g[:, 0, :] & np.uint64(m28)) | (g[:, 1, :] << np.uint64(28))).reshape(-1))
+    allv = np.concatenate(vals).astype("<u8")
+    by = allv.view(np.uint8).reshape(-1, 8)[:, :7].reshape(-1)
+    return bytes([len(p.queries)]) + by.tobytes()
+
+
+def deserialize_keyword_response(data: bytes) -> KeywordResponsePayload:
+    """deserialize_keyword_response (wire.rs:729-759)."""
+    off = 0
+
+    def u32():
+        nonlocal off
+        v = int.from_bytes(data[off:off + 4], "little")
+        off += 4
+        return v
+    responses = []
+    for _ in range(u32()):
+        n = u32()
+        responses.append(bytes(data[off:off + n]))
+        off += n
+    stash = []
+    for _ in range(u32()):
+        n = u32()
+        stash.append(bytes(data[off:off + n]))
+        off += n
+    return KeywordResponsePayload(responses, stash)
+
+
+# ---------------------------------------------------------------------------
+# server
+# ---------------------------------------------------------------------------
+class KeywordServer:
+    """Device-resident keyword server (KeywordServer<u16>, keyword.rs:49-63).
+
+    Build with ``KeywordServer.from_encoded`` (encoded DB + InspiRING
+    precomputation arrays, the state the reference's setup leaves on the GPU)
+    or ``KeywordServer.synthetic`` (seeded synthetic state of the same shapes).
+    """
+
+    def __init__(self, handle: int, plan: Plan, device: int):
+        self._h = _vp(handle)
+        self.plan = plan
+        self.device = device
+
+    @classmethod
+    def from_encoded(cls, plan: Plan, db, a_hat, bold_t, bold_t_bar, bold_t_hat, stash=(),
+                     key_size: int = 32, value_size: Optional[int] = None, num_records: int = 0,
+                     cuckoo_seed: bytes = bytes(16), device: int = 0) -> "KeywordServer":
+        import numpy as np
+        arrs = {
+            "db": np.ascontiguousarray(db, dtype=np.uint16),
+            "a_hat": np.ascontiguousarray(a_hat, dtype=np.uint64),
+            "bold_t": np.ascontiguousarray(bold_t, dtype=np.uint64),
+            "bold_t_bar": np.ascontiguousarray(bold_t_bar, dtype=np.uint64),
+            "bold_t_hat": np.ascontiguousarray(bold_t_hat, dtype=np.uint64),
+        }
+        n, ninner = plan.instances, 3069
+        want = {"db": plan.db_rows * plan.db_cols, "a_hat": n * POLY_LEN, "bold_t": n * ninner * POLY_LEN,
+                "bold_t_bar": n * ninner * POLY_LEN, "bold_t_hat": n * 3 * POLY_LEN}
+        for k, v in arrs.items():
+            if v.size != want[k]:
+                raise ValueError(f"{k} has {v.size} elements, plan needs {want[k]}")
+        stash = [bytes(s) for s in stash]
+        entry = len(stash[0]) if stash else 0
+        if any(len(s) != entry for s in stash):
+            raise ValueError("stash entries must have equal length")
+        stash_buf = np.frombuffer(b"".join(stash), dtype=np.uint8) if stash else None
+        d = _ServerData()
+        for k, v in arrs.items():
+            setattr(d, k, v.ctypes.data)
+        d.stash = stash_buf.ctypes.data if stash_buf is not None else None
+        d.stash_count, d.stash_entry_bytes = len(stash), entry
+        d.key_size = key_size
+        d.value_size = plan.entry_size - key_size if value_size is None else value_size
+        d.num_records = num_records
+        d.cuckoo_seed[:] = list(cuckoo_seed[:16].ljust(16, b"\0"))
+        h = _vp()
+        pc = plan._c()
+        _check(_create(device, ctypes.byref(pc), ctypes.byref(d), ctypes.byref(h)), "ipr_server_create")
+        return cls(h.value, plan, device)
+
+    @classmethod
+    def synthetic(cls, plan: Plan, seed: int = 7, device: int = 0) -> "KeywordServer":
+        h = _vp()
+        pc = plan._c()
+        _check(_create_synth(device, ctypes.byref(pc), seed, ctypes.byref(h)), "ipr_server_create_synthetic")
+        return cls(h.value, plan, device)
+
+    def close(self):
+        if self._h and self._h.value:
+            _destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # --- reference API -------------------------------------------------
+    def public_params(self) -> dict:
+        """KeywordServer::public_params (keyword.rs:511-532) as the serde JSON dict."""
+        n = _sz()
+        _pp_json(self._h, None, 0, ctypes.byref(n))
+        buf = ctypes.create_string_buffer(n.value + 1)
+        _check(_pp_json(self._h, buf, n.value + 1, ctypes.byref(n)), "public_params")
+        return json.loads(buf.value.decode())
+
+    def respond_to_serialized_query(self, query: bytes) -> bytes:
+        """keyword.rs:636-640: serialized query payload -> serialized response."""
+        q = (ctypes.c_uint8 * len(query)).from_buffer_copy(query)
+        nq = query[0] if query else 0
+        cap = int(_srv_rbytes(self._h, nq))
+        out = (ctypes.c_uint8 * cap)()
+        n = _sz()
+        _check(_respond(self._h, q, len(query), out, cap, ctypes.byref(n)), "respond")
+        return bytes(out)[:n.value]
+
+    def respond(self, payload: KeywordQueryPayload) -> KeywordResponsePayload:
+        """KeywordServer::respond (keyword.rs:534-628)."""
+        return deserialize_keyword_response(self.respond_to_serialized_query(serialize_keyword_query(payload)))
+
+    # --- device-level helpers (bench / serving) ---------------------------
+    def respond_device(self, d_query_ptr: int, length: int, d_out_ptr: int, cap: int) -> int:
+        n = _sz()
+        _check(_respond_dev(self._h, _vp(d_query_ptr), length, _vp(d_out_ptr), cap, ctypes.byref(n)),
+               "respond_device")
+        return n.value
+
+    def stream_handle(self) -> int:
+        s = _vp()
+        _check(_stream(self._h, ctypes.byref(s)), "stream")
+        return s.value or 0
+
+    def sync(self):
+        _check(_sync(self._h), "sync")
+
+    def set_profiling(self, on: bool):
+        _check(_set_prof(self._h, 1 if on else 0), "set_profiling")
+
+    def stage_times(self):
+        arr = (ctypes.c_double * len(STAGES))()
+        calls = _u64()
+        _check(_stage_times(self._h, arr, ctypes.byref(calls)), "stage_times")
+        return dict(zip(STAGES, list(arr))), calls.value
+
+    def query_bytes(self, num_queries: int = 2) -> int:
+        return int(_srv_qbytes(self._h, num_queries))
+
+    def response_bytes(self, num_queries: int = 2) -> int:
+        return int(_srv_rbytes(self._h, num_queries))
+
+    def hbm_bytes(self) -> int:
+        v = _u64()
+        _check(_hbm(self._h, ctypes.byref(v)), "hbm_bytes")
+        return v.value
+
+
+def version() -> str:
+    return _version().decode()

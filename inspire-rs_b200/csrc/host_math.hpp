@@ -1,0 +1,40 @@
+// host_math.hpp — host-side parameter derivation for the respond() path:
+// moduli constants, NTT twiddle tables, the RGSW mask row, and the keyword
+// server shape plan.  Restates (rkdud007/inspire-rs):
+//   Params::init                    src/core/params.rs:225-301
+//   build_ntt_tables                src/core/ntt.rs:74-108
+//   get_minimal_primitive_root      src/core/number_theory.rs:41-55
+//   ChaCha20Rng + random_rng        rand_chacha 0.10 / src/core/poly.rs:211-231
+//   params_rgswpir_given_input_size_and_dim0  src/protocol/wire.rs:386-477
+//   KeywordServerSetupPlan::from_shape        src/pir/server/keyword.rs:145-233
+#pragma once
+#include <cstdint>
+#include <vector>
+
+namespace ipr {
+
+struct HostParams {
+    uint64_t q[2];
+    uint64_t modulus;
+    uint64_t barrett[2];      // floor(2^64 / q_l)
+    uint32_t q0_inv_mod_q1;
+    // [limb][N] u32 twiddle tables: forward psi powers (bit-reversed order) and
+    // their Shoup companions; inverse powers pre-halved and companions
+    std::vector<uint32_t> fw, fwp, iw, iwp;
+    std::vector<uint32_t> row0;  // [2][N] NTT(-a), a from ChaCha20Rng([7;32])
+};
+
+void host_params_init(HostParams& p);
+
+struct Plan {
+    uint64_t num_items, entry_size, item_size_bits, dim0;
+    uint64_t db_rows, db_cols, instances, interp, c;
+    uint64_t peak_bytes;
+};
+// returns 0 or a negative IPR_E_* status
+int plan_from_shape(uint64_t record_count, uint64_t key_size, uint64_t value_size, uint64_t buckets,
+                    uint64_t dim0, Plan& out);
+
+uint64_t query_bytes(uint64_t db_rows, unsigned nq);
+
+}  // namespace ipr

@@ -1,0 +1,152 @@
+// ipr_device.cuh — device-side modular arithmetic and negacyclic NTTs for the
+// InsPIRe respond() path on sm_100a.
+//
+// Arithmetic domain (src/pir/params.rs:8-9 of rkdud007/inspire-rs): two NTT
+// primes q0 = 268369921, q1 = 249561089 (both < 2^28), q = q0*q1 < 2^56,
+// ring dimension N = 2048.  Every value that leaves a kernel is canonical, so
+// any correct reduction strategy reproduces the reference's outputs exactly.
+#pragma once
+#include <cstdint>
+
+namespace ipr {
+
+constexpr int N = 2048;
+constexpr int LOGN = 11;
+constexpr int T_EXP = 3;                 // t_exp_left = t_gsw (wire.rs:424)
+constexpr int NROT = N / 2 - 1;          // 1023 rotations (packing.rs:1766)
+constexpr int NINNER = NROT * T_EXP;     // 3069 key-switch rows per output
+constexpr uint32_t Q0 = 268369921u;
+constexpr uint32_t Q1 = 249561089u;
+constexpr uint64_t QQ = (uint64_t)Q0 * (uint64_t)Q1;
+constexpr uint32_t PT = 65535u;          // plaintext modulus (wire.rs:421)
+constexpr uint64_t QP1 = 1ull << 20;     // q'_1 (params.rs:346-348)
+constexpr uint64_t QP2 = 268369921ull;   // q'_2 = Q2_VALUES[28] (core/params.rs:37)
+constexpr int RESULT_BYTES = 12288;      // (28 + 20) * 2048 / 8 (modulus_switch.rs:45-73)
+constexpr int GADGET_BITS = 19;          // floor(56/3)+1 (gadget.rs:3-9)
+
+// Per-limb constants kept in __constant__ memory (filled by the host).
+struct LimbConst {
+    uint32_t q[2];
+    uint64_t barrett[2];     // floor(2^64 / q_l)
+    uint32_t q0_inv_mod_q1;  // Garner CRT coefficient
+};
+
+// exact x mod q for any 64-bit x (Barrett with floor(2^64/q), one correction)
+__device__ __forceinline__ uint32_t mod64(uint64_t x, uint32_t q, uint64_t br) {
+    uint64_t t = __umul64hi(x, br);
+    uint64_t r = x - t * q;
+    return (uint32_t)(r >= q ? r - q : r);
+}
+
+// Shoup multiply: y * w mod q in [0, 2q), wp = floor(w * 2^32 / q)
+__device__ __forceinline__ uint32_t shoup_lazy(uint32_t y, uint32_t w, uint32_t wp, uint32_t q) {
+    uint32_t qt = __umulhi(y, wp);
+    return y * w - qt * q;
+}
+
+// CRT compose of canonical residues (x mod q0, y mod q1) -> value mod q0*q1 in
+// [0, q): Garner form v = x + q0 * ((y - x) * q0^-1 mod q1).  Same canonical
+// result as crt_compose_2 (core/params.rs:203-215), which is a unique CRT lift.
+__device__ __forceinline__ uint64_t crt2(uint32_t x, uint32_t y, uint32_t q0inv, uint64_t br1) {
+    uint32_t xm = x >= Q1 ? x - Q1 : x;            // x < q0 < 2*q1
+    uint32_t d = y >= xm ? y - xm : y + Q1 - xm;   // (y - x) mod q1
+    uint32_t k = mod64((uint64_t)d * q0inv, Q1, br1);
+    return (uint64_t)x + (uint64_t)Q0 * k;
+}
+
+// ---------------------------------------------------------------------------
+// Shared-memory negacyclic NTTs over u32 residues, executed cooperatively by
+// all threads of a CTA on `npoly` independent polynomials laid out at
+// smem + p * N.  Twiddles: w/wp for forward (bit-reversed psi powers) and the
+// pre-halved inverse tables, exactly the tables of build_ntt_tables
+// (src/core/ntt.rs:74-108).  Butterflies are the Harvey forms of
+// ntt_forward (ntt.rs:111-160) and ntt_inverse (ntt.rs:731-780); outputs are
+// reduced to [0, q).  limb_of(p) selects the prime of polynomial p.
+// ---------------------------------------------------------------------------
+template <int NPOLY, typename LimbOf>
+__device__ __forceinline__ void ntt_forward_smem(uint32_t* smem, const uint32_t* __restrict__ fw,
+                                                 const uint32_t* __restrict__ fwp, LimbOf limb_of) {
+#pragma unroll 1
+    for (int mm = 0; mm < LOGN; mm++) {
+        const int m = 1 << mm, t = N >> (mm + 1);
+        for (int idx = threadIdx.x; idx < NPOLY * (N / 2); idx += blockDim.x) {
+            const int p = idx >> (LOGN - 1);
+            const int b = idx & (N / 2 - 1);
+            const int i = b >> (LOGN - 1 - mm);        // b / t
+            const int j = b & (t - 1);
+            const int l = limb_of(p);
+            const uint32_t q = l ? Q1 : Q0, two_q = 2 * q;
+            const uint32_t w = __ldg(fw + l * N + m + i), wp = __ldg(fwp + l * N + m + i);
+            uint32_t* o = smem + p * N + 2 * t * i + j;
+            uint32_t x = o[0], y = o[t];
+            x -= (x >= two_q) ? two_q : 0;
+            uint32_t qn = shoup_lazy(y, w, wp, q);
+            o[0] = x + qn;
+            o[t] = x + two_q - qn;
+        }
+        __syncthreads();
+    }
+    for (int idx = threadIdx.x; idx < NPOLY * N; idx += blockDim.x) {
+        const int l = limb_of(idx >> LOGN);
+        const uint32_t q = l ? Q1 : Q0;
+        uint32_t v = smem[idx];
+        v -= (v >= 2 * q) ? 2 * q : 0;
+        v -= (v >= q) ? q : 0;
+        smem[idx] = v;
+    }
+    __syncthreads();
+}
+
+template <int NPOLY, typename LimbOf>
+__device__ __forceinline__ void ntt_inverse_smem(uint32_t* smem, const uint32_t* __restrict__ iw,
+                                                 const uint32_t* __restrict__ iwp, LimbOf limb_of) {
+#pragma unroll 1
+    for (int mm = LOGN - 1; mm >= 0; mm--) {
+        const int h = 1 << mm, t = N >> (mm + 1);
+        for (int idx = threadIdx.x; idx < NPOLY * (N / 2); idx += blockDim.x) {
+            const int p = idx >> (LOGN - 1);
+            const int b = idx & (N / 2 - 1);
+            const int i = b >> (LOGN - 1 - mm);
+            const int j = b & (t - 1);
+            const int l = limb_of(p);
+            const uint32_t q = l ? Q1 : Q0, two_q = 2 * q;
+            const uint32_t w = __ldg(iw + l * N + h + i), wp = __ldg(iwp + l * N + h + i);
+            uint32_t* o = smem + p * N + 2 * t * i + j;
+            uint32_t x = o[0], y = o[t];
+            uint32_t tt = two_q - y + x;
+            uint32_t cx = x + y - ((2 * x >= tt) ? two_q : 0);
+            uint32_t ht = __umulhi(tt, wp);
+            o[0] = (cx + ((tt & 1) ? q : 0)) >> 1;
+            o[t] = w * tt - ht * q;
+        }
+        __syncthreads();
+    }
+    for (int idx = threadIdx.x; idx < NPOLY * N; idx += blockDim.x) {
+        const int l = limb_of(idx >> LOGN);
+        const uint32_t q = l ? Q1 : Q0;
+        uint32_t v = smem[idx];
+        v -= (v >= 2 * q) ? 2 * q : 0;
+        v -= (v >= q) ? q : 0;
+        smem[idx] = v;
+    }
+    __syncthreads();
+}
+
+// slot of the forward NTT output that evaluates at psi^e (e odd):  the
+// Cooley-Tukey order with bit-reversed twiddles leaves slot s holding the
+// evaluation at psi^(2*brv(s)+1).
+__device__ __forceinline__ uint32_t slot_of_exponent(uint32_t e) {
+    return __brev((e - 1) >> 1) >> (32 - LOGN);
+}
+__device__ __forceinline__ uint32_t exponent_of_slot(uint32_t s) {
+    return 2 * (__brev(s) >> (32 - LOGN)) + 1;
+}
+
+// NTT-domain Galois automorphism x -> x^t as a slot permutation:
+// NTT(a(x^t))[s] = NTT(a)[auto_src(t, s)]  (closed form of
+// generate_automorph_tables_brute_force, src/pir/packing.rs:1423-1468)
+__device__ __forceinline__ uint32_t auto_src(uint32_t t, uint32_t s) {
+    return slot_of_exponent((t * exponent_of_slot(s)) & (2 * N - 1));
+}
+
+}  // namespace ipr

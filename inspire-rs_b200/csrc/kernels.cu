@@ -1,0 +1,583 @@
+// kernels.cu — sm_100a kernels of the InsPIRe keyword-PIR respond() path.
+//
+// Step map (rkdud007/inspire-rs, src/pir/server/keyword.rs:534-628):
+//   k_parse_query    deserialize_keyword_query (src/protocol/wire.rs:618-705)
+//   k_gemv           first-dimension GEMV (native/cuda/gemv_kernel.cu:46-103),
+//                    both queries of a payload in one pass over the DB
+//   k_pack           InspiRING key-switch inner product with the Galois
+//                    rotations of the client key fused in (rotation_kernel.cu:21-59
+//                    + packing_online_kernel.cu:18-92), once per payload
+//   k_intt_crt       from_ntt of the packing sums (src/pir/gpu/packing_online.rs:359-375)
+//   k_fold_switch    RGSW interpolation fold (keyword.rs:543-574) fused with
+//                    switch_and_keep (src/pir/modulus_switch.rs:45-73)
+//   k_response_frame serialize_keyword_response framing (wire.rs:708-726)
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "ipr_device.cuh"
+#include "kernels.cuh"
+
+namespace ipr {
+
+__constant__ uint64_t c_br[2];      // floor(2^64 / q_l)
+__constant__ uint32_t c_q0inv;      // q0^-1 mod q1
+
+__host__ cudaError_t set_constants(const uint64_t br[2], uint32_t q0inv) {
+    cudaError_t e = cudaMemcpyToSymbol(c_br, br, sizeof(uint64_t) * 2);
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyToSymbol(c_q0inv, &q0inv, sizeof(uint32_t));
+}
+
+__device__ __forceinline__ uint32_t modq(uint64_t x, int l) {
+    return mod64(x, l ? Q1 : Q0, c_br[l]);
+}
+
+// ---------------------------------------------------------------------------
+// query parse: 56-bit fields start at bit 8 (byte 1) and are byte aligned
+// (7 bytes each), little-endian.  Field layout (serialize_keyword_query,
+// wire.rs:542-615): keys y/z interleaved per (i<3, k<N); then per query the
+// db_rows packed query row values followed by 6 raw-CRT RGSW body polys.
+// ---------------------------------------------------------------------------
+__global__ void k_parse_query(const uint8_t* __restrict__ qb, int nq, int db_rows,
+                              uint64_t* __restrict__ y_body, uint64_t* __restrict__ z_body,
+                              uint32_t* __restrict__ a_il, uint32_t* __restrict__ gsw) {
+    const int64_t keys = 2LL * T_EXP * N;
+    const int64_t per_q = (int64_t)db_rows + 2LL * T_EXP * N;
+    const int64_t total = keys + (int64_t)nq * per_q;
+    const uint64_t m28 = (1ull << 28) - 1;
+    for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f < total;
+         f += (int64_t)gridDim.x * blockDim.x) {
+        const uint8_t* p = qb + 1 + 7 * f;
+        uint64_t v = 0;
+#pragma unroll
+        for (int b = 0; b < 7; b++) v |= (uint64_t)p[b] << (8 * b);
+        const uint32_t lo = (uint32_t)(v & m28), hi = (uint32_t)((v >> 28) & m28);
+        if (f < keys) {
+            const int64_t ik = f >> 1;
+            const uint64_t cond = (uint64_t)lo | ((uint64_t)hi << 32);
+            if (f & 1) z_body[ik] = cond;
+            else y_body[ik] = cond;
+        } else {
+            const int64_t g = f - keys;
+            const int q = (int)(g / per_q);
+            const int64_t r = g - (int64_t)q * per_q;
+            if (r < db_rows) {
+                // GEMV operand, queries grouped in pairs: a_il[g][k][qq][l], g = q/2
+                const int g2 = q >> 1, qq = q & 1, ng = (nq - 2 * g2) < 2 ? (nq - 2 * g2) : 2;
+                uint32_t* dst = a_il + (int64_t)g2 * db_rows * 4 + (r * ng + qq) * 2;
+                dst[0] = lo;
+                dst[1] = hi;
+            } else {
+                const int64_t rr = r - db_rows;  // poly c = rr / N, coeff z = rr % N
+                const int c = (int)(rr >> LOGN), z = (int)(rr & (N - 1));
+                uint32_t* poly = gsw + ((int64_t)q * 2 * T_EXP + c) * 2 * N;
+                poly[z] = lo;
+                poly[N + z] = hi;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// First-dimension GEMV for NQ queries in one pass over the DB:
+//   c[q][j] = CRT( sum_k a_q,0[k] D[j][k] mod q0 , sum_k a_q,1[k] D[j][k] mod q1 )
+// D is column-major [db_cols][db_rows] u16 (the reference layout).  A warp owns
+// COLS consecutive columns; lane l reads 16 B (8 rows) of each column per
+// 256-row stripe, so every load instruction covers 512 contiguous bytes.
+// Per-lane u64 partial sums are combined by a 31-shuffle transpose-reduce.
+// ---------------------------------------------------------------------------
+template <int NQ, int COLS>
+__global__ void __launch_bounds__(256) k_gemv(const uint16_t* __restrict__ db, int db_rows,
+                                              int64_t db_cols, const uint32_t* __restrict__ a_il,
+                                              uint64_t* __restrict__ c) {
+    constexpr int NV = COLS * NQ * 2;  // values reduced per warp task (must be 32)
+    static_assert(NV == 32, "transpose-reduce expects 32 values per lane");
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t ntasks = db_cols / COLS;
+    const int stripes = db_rows >> 8;
+    for (int64_t task = warp; task < ntasks; task += nwarps) {
+        const int64_t col0 = task * COLS;
+        uint64_t acc[NV];
+#pragma unroll
+        for (int v = 0; v < NV; v++) acc[v] = 0;
+        for (int it = 0; it < stripes; it++) {
+            const int k0 = it * 256 + lane * 8;
+            uint4 d[COLS];
+#pragma unroll
+            for (int cc = 0; cc < COLS; cc++) {
+                const uint4* src =
+                    reinterpret_cast<const uint4*>(db + (col0 + cc) * (int64_t)db_rows + k0);
+                asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"
+                             : "=r"(d[cc].x), "=r"(d[cc].y), "=r"(d[cc].z), "=r"(d[cc].w)
+                             : "l"(src));
+            }
+#pragma unroll
+            for (int kk = 0; kk < 8; kk++) {
+                uint32_t av[NQ * 2];
+                if constexpr (NQ == 2) {
+                    uint4 t = __ldg(reinterpret_cast<const uint4*>(a_il) + (k0 + kk));
+                    av[0] = t.x; av[1] = t.y; av[2] = t.z; av[3] = t.w;
+                } else {
+                    uint2 t = __ldg(reinterpret_cast<const uint2*>(a_il) + (k0 + kk));
+                    av[0] = t.x; av[1] = t.y;
+                }
+#pragma unroll
+                for (int cc = 0; cc < COLS; cc++) {
+                    const uint32_t w = (&d[cc].x)[kk >> 1];
+                    const uint32_t dv = (kk & 1) ? (w >> 16) : (w & 0xffffu);
+#pragma unroll
+                    for (int v = 0; v < NQ * 2; v++)
+                        acc[cc * NQ * 2 + v] += (uint64_t)av[v] * dv;
+                }
+            }
+        }
+        // transpose-reduce: lane v ends with the warp-wide sum of value v
+#pragma unroll
+        for (int s = 16; s >= 1; s >>= 1) {
+            const bool upper = lane & s;
+#pragma unroll
+            for (int i = 0; i < s; i++) {
+                const uint64_t send = upper ? acc[i] : acc[i + s];
+                const uint64_t keep = upper ? acc[i + s] : acc[i];
+                acc[i] = keep + __shfl_xor_sync(0xffffffffu, send, s);
+            }
+        }
+        // value v = cc*(NQ*2) + q*2 + l ; limb partner is lane ^ 1
+        const int l = lane & 1;
+        const uint32_t r = modq(acc[0], l);
+        const uint32_t other = __shfl_xor_sync(0xffffffffu, r, 1);
+        if (l == 0) {
+            const int q = (lane >> 1) % NQ, cc = lane / (NQ * 2);
+            c[(int64_t)q * db_cols + col0 + cc] = crt2(r, other, c_q0inv, c_br[1]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Packing inner product, rotations fused.  For output j, NTT slot z, limb l:
+//   S[j][l][z] = sum_{i<1023,k<3} y_l[k][rot_i(z)] T_l[j][i,k][z]
+//              + y_l[k][rotbar_i(z)] Tbar_l[j][i,k][z] + sum_k z_l[k][z] That_l[j][k][z]
+// with rot_i = auto_src(5^i mod 2N, .), rotbar_i = auto_src(2N - 5^i, .).
+// The client key y_body stays in shared memory; the precomputed bold_t stream
+// (the dominant HBM traffic) is read once per payload with 16-byte
+// non-allocating loads, two adjacent slots per thread.  Slots z and z+1 (z even)
+// rotate to the slot pair {s, s^1}, so each gather is one 16-byte smem load.
+// ---------------------------------------------------------------------------
+constexpr int PACK_THREADS = 128;
+constexpr int PACK_ZB = 2 * PACK_THREADS;  // slots per CTA
+
+__device__ __forceinline__ void ldg_nc_v2(const uint64_t* p, uint64_t& a, uint64_t& b) {
+    asm volatile("ld.global.nc.L1::no_allocate.v2.u64 {%0,%1}, [%2];" : "=l"(a), "=l"(b) : "l"(p));
+}
+
+__global__ void __launch_bounds__(PACK_THREADS) k_pack(const uint64_t* __restrict__ bt,
+                                                       const uint64_t* __restrict__ btb,
+                                                       const uint64_t* __restrict__ bth,
+                                                       const uint64_t* __restrict__ y_body,
+                                                       const uint64_t* __restrict__ z_body,
+                                                       uint32_t* __restrict__ S) {
+    extern __shared__ uint64_t ys[];  // [3][N] condensed
+    for (int i = threadIdx.x; i < T_EXP * N; i += blockDim.x) ys[i] = y_body[i];
+    __syncthreads();
+    const int j = blockIdx.y;
+    const int z = blockIdx.x * PACK_ZB + 2 * threadIdx.x;
+    const uint32_t ez = exponent_of_slot(z);
+    const uint64_t* T = bt + (int64_t)j * NINNER * N + z;
+    const uint64_t* Tb = btb + (int64_t)j * NINNER * N + z;
+    uint64_t a00 = 0, a01 = 0, a10 = 0, a11 = 0;  // a{limb}{slot}
+    uint32_t g = 1;                               // 5^i mod 2N
+    for (int i0 = 0; i0 < NROT; i0 += 32) {
+        const int iend = i0 + 32 < NROT ? i0 + 32 : NROT;
+#pragma unroll 2
+        for (int i = i0; i < iend; i++) {
+            const uint32_t s1 = slot_of_exponent((g * ez) & (2 * N - 1));
+            const uint32_t s2 = slot_of_exponent(((2 * N - g) * ez) & (2 * N - 1));
+            uint64_t tv[3][2], tbv[3][2];
+#pragma unroll
+            for (int k = 0; k < T_EXP; k++) {
+                ldg_nc_v2(T + (int64_t)(i * T_EXP + k) * N, tv[k][0], tv[k][1]);
+                ldg_nc_v2(Tb + (int64_t)(i * T_EXP + k) * N, tbv[k][0], tbv[k][1]);
+            }
+#pragma unroll
+            for (int k = 0; k < T_EXP; k++) {
+                const ulonglong2 yp = *reinterpret_cast<const ulonglong2*>(ys + k * N + (s1 & ~1u));
+                const ulonglong2 bp = *reinterpret_cast<const ulonglong2*>(ys + k * N + (s2 & ~1u));
+                const uint64_t y0 = (s1 & 1) ? yp.y : yp.x, y1 = (s1 & 1) ? yp.x : yp.y;
+                const uint64_t b0 = (s2 & 1) ? bp.y : bp.x, b1 = (s2 & 1) ? bp.x : bp.y;
+                a00 += (uint64_t)(uint32_t)y0 * (uint32_t)tv[k][0] + (uint64_t)(uint32_t)b0 * (uint32_t)tbv[k][0];
+                a01 += (uint64_t)(uint32_t)y1 * (uint32_t)tv[k][1] + (uint64_t)(uint32_t)b1 * (uint32_t)tbv[k][1];
+                a10 += (y0 >> 32) * (tv[k][0] >> 32) + (b0 >> 32) * (tbv[k][0] >> 32);
+                a11 += (y1 >> 32) * (tv[k][1] >> 32) + (b1 >> 32) * (tbv[k][1] >> 32);
+            }
+            g = (g * 5) & (2 * N - 1);
+        }
+        // <= 192 products of two 28-bit values plus a residue: no overflow
+        a00 = modq(a00, 0); a01 = modq(a01, 0);
+        a10 = modq(a10, 1); a11 = modq(a11, 1);
+    }
+    const uint64_t* Th = bth + (int64_t)j * T_EXP * N + z;
+#pragma unroll
+    for (int k = 0; k < T_EXP; k++) {
+        const uint64_t t0 = Th[k * N], t1 = Th[k * N + 1];
+        const uint64_t z0 = z_body[k * N + z], z1 = z_body[k * N + z + 1];
+        a00 += (uint64_t)(uint32_t)z0 * (uint32_t)t0;
+        a01 += (uint64_t)(uint32_t)z1 * (uint32_t)t1;
+        a10 += (z0 >> 32) * (t0 >> 32);
+        a11 += (z1 >> 32) * (t1 >> 32);
+    }
+    uint32_t* Sj = S + (int64_t)j * 2 * N;
+    *reinterpret_cast<uint2*>(Sj + z) = make_uint2(modq(a00, 0), modq(a01, 0));
+    *reinterpret_cast<uint2*>(Sj + N + z) = make_uint2(modq(a10, 1), modq(a11, 1));
+}
+
+// ---------------------------------------------------------------------------
+// R[j] = from_ntt(S[j]) : inverse NTT per limb + CRT compose (one CTA per output)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(512) k_intt_crt(const uint32_t* __restrict__ S,
+                                                  const uint32_t* __restrict__ iw,
+                                                  const uint32_t* __restrict__ iwp,
+                                                  uint64_t* __restrict__ R) {
+    __shared__ uint32_t sm[2 * N];
+    const int j = blockIdx.x;
+    for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) sm[i] = S[(int64_t)j * 2 * N + i];
+    __syncthreads();
+    ntt_inverse_smem<2>(sm, iw, iwp, [](int p) { return p; });
+    for (int z = threadIdx.x; z < N; z += blockDim.x)
+        R[(int64_t)j * N + z] = crt2(sm[z], sm[N + z], c_q0inv, c_br[1]);
+}
+
+// ---------------------------------------------------------------------------
+// RGSW fold + modulus switch.  One CTA per (query, fold group wp):
+//   s = 0; for i = interp-1 .. 0:
+//     s = from_ntt(CT * to_ntt(G^-1(s))) + packed[wp*interp + i]  (mod q)
+// packed[j] = (a_hat[j], c[j*N + z] + R[j][z]) (packing_online.rs:376-396).
+// CT row 0 = NTT(-a) in every column (RGSW_SEEDS are all equal, wire.rs:88-113),
+// CT row 1 = the query's 6 RGSW body polys.  The first step has s = 0, so
+// G^-1(s) = 0 and the product vanishes: it reduces to s = packed[.] mod q.
+// The final s is rescaled to (q'2, q'1) and bit-packed LSB-first into the
+// response: 2048 x 28 bits then 2048 x 20 bits (12288 bytes).
+// ---------------------------------------------------------------------------
+constexpr int FOLD_THREADS = 1024;
+
+__device__ __forceinline__ uint64_t rescale_dev(uint64_t v, uint64_t out_mod) {
+    // rescale (src/core/arith.rs:436-452) of a canonical v in [0, q)
+    const uint64_t half = QQ / 2;
+    const bool neg = v >= half;
+    const uint64_t u = neg ? QQ - v : v;
+    const unsigned __int128 num = (unsigned __int128)u * out_mod + half;
+    const uint64_t r = (uint64_t)(num / QQ);
+    const uint64_t rm = r % out_mod;
+    return neg ? (rm ? out_mod - rm : 0) : rm;
+}
+
+__global__ void __launch_bounds__(FOLD_THREADS) k_fold_switch(
+    const uint32_t* __restrict__ row0,    // [2][N] NTT(-a)
+    const uint32_t* __restrict__ gsw,     // [nq][6][2][N]
+    const uint64_t* __restrict__ a_hat,   // [outputs][N]
+    const uint64_t* __restrict__ R,       // [outputs][N]
+    const uint64_t* __restrict__ cvec,    // [nq][db_cols]
+    const uint32_t* __restrict__ fw, const uint32_t* __restrict__ fwp,
+    const uint32_t* __restrict__ iw, const uint32_t* __restrict__ iwp,
+    int interp, int c_groups, int64_t db_cols, uint8_t* __restrict__ resp, int64_t resp_query_stride) {
+    extern __shared__ uint32_t G[];  // [6][2][N] digits in NTT form; reused for products
+    const int wp = blockIdx.x, q = blockIdx.y;
+    const uint32_t* body = gsw + (int64_t)q * 2 * T_EXP * 2 * N;
+    const uint64_t* cq = cvec + (int64_t)q * db_cols;
+    uint64_t s[2][2];  // [row][which of my two slots]
+    const int z0 = threadIdx.x, z1 = threadIdx.x + FOLD_THREADS;
+    const uint64_t mask = (1ull << GADGET_BITS) - 1;
+    for (int step = interp - 1; step >= 0; step--) {
+        const int j = wp * interp + step;
+        uint64_t pk[2][2];
+        pk[0][0] = a_hat[(int64_t)j * N + z0];
+        pk[0][1] = a_hat[(int64_t)j * N + z1];
+        pk[1][0] = cq[(int64_t)j * N + z0] + R[(int64_t)j * N + z0];
+        pk[1][1] = cq[(int64_t)j * N + z1] + R[(int64_t)j * N + z1];
+        if (step == interp - 1) {
+#pragma unroll
+            for (int r = 0; r < 2; r++)
+#pragma unroll
+                for (int h = 0; h < 2; h++) s[r][h] = pk[r][h] % QQ;
+            continue;
+        }
+        // gadget_invert (gadget.rs:35-61): row j + k*2 holds digit k of input row j
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int z = h ? z1 : z0;
+#pragma unroll
+            for (int r = 0; r < 2; r++)
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    const uint32_t d = (uint32_t)((s[r][h] >> (k * GADGET_BITS)) & mask);
+                    const int p = r + 2 * k;
+                    G[(p * 2 + 0) * N + z] = d;
+                    G[(p * 2 + 1) * N + z] = d;
+                }
+        }
+        __syncthreads();
+        ntt_forward_smem<12>(G, fw, fwp, [](int p) { return p & 1; });
+        // pointwise 2x6 . 6x1 product; results overwrite polys 0..3 at the same slot
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int z = h ? z1 : z0;
+#pragma unroll
+            for (int l = 0; l < 2; l++) {
+                uint64_t sg = 0, acc = 0;
+#pragma unroll
+                for (int p = 0; p < 6; p++) {
+                    const uint32_t gv = G[(p * 2 + l) * N + z];
+                    sg += gv;
+                    acc += (uint64_t)body[(p * 2 + l) * N + z] * gv;
+                }
+                const uint32_t p0 = modq((uint64_t)row0[l * N + z] * modq(sg, l), l);
+                const uint32_t p1 = modq(acc, l);
+                G[(0 * 2 + l) * N + z] = p0;
+                G[(1 * 2 + l) * N + z] = p1;
+            }
+        }
+        __syncthreads();
+        ntt_inverse_smem<4>(G, iw, iwp, [](int p) { return p & 1; });
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int z = h ? z1 : z0;
+#pragma unroll
+            for (int r = 0; r < 2; r++) {
+                uint64_t v = crt2(G[(r * 2 + 0) * N + z], G[(r * 2 + 1) * N + z], c_q0inv, c_br[1]);
+                v += pk[r][h];                      // < q + 2q
+                v = v >= QQ ? v - QQ : v;
+                v = v >= QQ ? v - QQ : v;
+                s[r][h] = v;
+            }
+        }
+        __syncthreads();
+    }
+    // switch_and_keep: stage s in smem as u64 then emit 7-byte (2 x 28 bit) and
+    // 5-byte (2 x 20 bit) little-endian groups
+    uint64_t* S64 = reinterpret_cast<uint64_t*>(G);
+    S64[z0] = s[0][0]; S64[z1] = s[0][1];
+    S64[N + z0] = s[1][0]; S64[N + z1] = s[1][1];
+    __syncthreads();
+    uint8_t* out = resp + (int64_t)q * resp_query_stride + (int64_t)wp * RESULT_BYTES;
+    {
+        const int t = threadIdx.x;  // fields 2t, 2t+1 of row 0 -> bytes [7t, 7t+7)
+        const uint64_t v = rescale_dev(S64[2 * t], QP2) | (rescale_dev(S64[2 * t + 1], QP2) << 28);
+#pragma unroll
+        for (int b = 0; b < 7; b++) out[7 * t + b] = (uint8_t)(v >> (8 * b));
+        const uint64_t w = rescale_dev(S64[N + 2 * t], QP1) | (rescale_dev(S64[N + 2 * t + 1], QP1) << 20);
+#pragma unroll
+        for (int b = 0; b < 5; b++) out[7 * N / 2 + 5 * t + b] = (uint8_t)(w >> (8 * b));
+    }
+}
+
+// serialize_keyword_response framing: [u32 nq] { [u32 len] bytes }* [u32 nstash] { [u32 len] entry }*
+__global__ void k_response_frame(uint8_t* __restrict__ resp, int nq, int64_t per_query_bytes,
+                                 const uint8_t* __restrict__ stash, int64_t stash_count,
+                                 int64_t stash_entry) {
+    auto put = [](uint8_t* p, uint32_t v) {
+        p[0] = (uint8_t)v; p[1] = (uint8_t)(v >> 8); p[2] = (uint8_t)(v >> 16); p[3] = (uint8_t)(v >> 24);
+    };
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t tail = 4 + (int64_t)nq * (4 + per_query_bytes);
+    if (tid == 0) {
+        put(resp, (uint32_t)nq);
+        for (int q = 0; q < nq; q++) put(resp + 4 + q * (4 + per_query_bytes), (uint32_t)per_query_bytes);
+        put(resp + tail, (uint32_t)stash_count);
+    }
+    const int64_t rec = 4 + stash_entry;
+    for (int64_t i = tid; i < stash_count * rec; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e = i / rec, o = i % rec;
+        uint8_t* dst = resp + tail + 4 + e * rec;
+        if (o < 4) dst[o] = (uint8_t)((uint32_t)stash_entry >> (8 * o));
+        else dst[o] = stash[e * stash_entry + (o - 4)];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Standalone Galois expansion of a key body (the reference's
+// gpu_rotation_expand_keys, rotation_kernel.cu:21-59), for the compatibility
+// entry points and the automorphism microbenchmark.  Table-free.
+// ---------------------------------------------------------------------------
+__global__ void k_rotations(const uint64_t* __restrict__ y_body, uint64_t* __restrict__ y_all,
+                            uint64_t* __restrict__ y_bar_all, int num_rotations) {
+    const int i = blockIdx.x, k = blockIdx.y;
+    uint32_t g = 1;
+    for (int e = 0; e < i; e++) g = (g * 5) & (2 * N - 1);
+    for (int z = threadIdx.x; z < N; z += blockDim.x) {
+        const int64_t o = ((int64_t)i * T_EXP + k) * N + z;
+        y_all[o] = y_body[k * N + auto_src(g, z)];
+        y_bar_all[o] = y_body[k * N + auto_src(2 * N - g, z)];
+    }
+}
+
+// packing from materialised y_all / y_bar_all (compat path of gpu_packing_online_compute)
+__global__ void __launch_bounds__(256) k_pack_materialized(
+    const uint64_t* __restrict__ bt, const uint64_t* __restrict__ btb, const uint64_t* __restrict__ bth,
+    const uint64_t* __restrict__ y_all, const uint64_t* __restrict__ y_bar_all,
+    const uint64_t* __restrict__ z_body, int num_outputs, int n_rot, uint64_t* __restrict__ out) {
+    const int j = blockIdx.x;
+    const int z = blockIdx.y * blockDim.x + threadIdx.x;
+    if (j >= num_outputs || z >= N) return;
+    const int n_inner = n_rot * T_EXP;
+    const uint64_t* T = bt + (int64_t)j * n_inner * N;
+    const uint64_t* Tb = btb + (int64_t)j * n_inner * N;
+    uint64_t lo = 0, hi = 0;
+    for (int r0 = 0; r0 < n_inner; r0 += 96) {
+        const int r1 = r0 + 96 < n_inner ? r0 + 96 : n_inner;
+        for (int r = r0; r < r1; r++) {
+            const uint64_t y = y_all[(int64_t)r * N + z], t = T[(int64_t)r * N + z];
+            const uint64_t yb = y_bar_all[(int64_t)r * N + z], tb = Tb[(int64_t)r * N + z];
+            lo += (uint64_t)(uint32_t)y * (uint32_t)t + (uint64_t)(uint32_t)yb * (uint32_t)tb;
+            hi += (y >> 32) * (t >> 32) + (yb >> 32) * (tb >> 32);
+        }
+        lo = modq(lo, 0);
+        hi = modq(hi, 1);
+    }
+    for (int k = 0; k < T_EXP; k++) {
+        const uint64_t zv = z_body[k * N + z], tv = bth[((int64_t)j * T_EXP + k) * N + z];
+        lo += (uint64_t)(uint32_t)zv * (uint32_t)tv;
+        hi += (zv >> 32) * (tv >> 32);
+    }
+    out[(int64_t)j * 2 * N + z] = modq(lo, 0);
+    out[(int64_t)j * 2 * N + N + z] = modq(hi, 1);
+}
+
+// standalone negacyclic NTT / INTT over a batch of limb-major polynomial pairs
+// ([poly][limb][N] u64 canonical), one CTA per pair (config: kernel microbench)
+__global__ void __launch_bounds__(512) k_ntt_batch(uint64_t* __restrict__ data, int forward,
+                                                   const uint32_t* __restrict__ w, const uint32_t* __restrict__ wp) {
+    __shared__ uint32_t sm[2 * N];
+    uint64_t* d = data + (int64_t)blockIdx.x * 2 * N;
+    for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) sm[i] = (uint32_t)d[i];
+    __syncthreads();
+    if (forward) ntt_forward_smem<2>(sm, w, wp, [](int p) { return p; });
+    else ntt_inverse_smem<2>(sm, w, wp, [](int p) { return p; });
+    for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) d[i] = sm[i];
+}
+
+// ---------------------------------------------------------------------------
+// seeded synthetic data (identical definition to the oracle's ipr_synth)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t synth(uint64_t seed, uint64_t stream, uint64_t idx) {
+    uint64_t x = seed ^ (stream * 0x9E3779B97F4A7C15ull) ^ (idx * 0xD1B54A32D192ED03ull);
+    x ^= x >> 30; x *= 0xBF58476D1CE4E5B9ull;
+    x ^= x >> 27; x *= 0x94D049BB133111EBull;
+    x ^= x >> 31;
+    x += 0x9E3779B97F4A7C15ull;
+    x ^= x >> 29; x *= 0xBF58476D1CE4E5B9ull;
+    x ^= x >> 32;
+    return x;
+}
+
+__global__ void k_synth_db(uint16_t* db, int64_t n, uint64_t seed) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        db[i] = (uint16_t)(synth(seed, 1, (uint64_t)i) % PT);
+}
+
+__global__ void k_synth_condensed(uint64_t* out, int64_t n, uint64_t seed, uint64_t stream) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t x = synth(seed, stream, (uint64_t)i);
+        out[i] = ((x & 0xffffffffull) % Q0) | (((x >> 32) % Q1) << 32);
+    }
+}
+
+__global__ void k_synth_modq(uint64_t* out, int64_t n, uint64_t seed, uint64_t stream) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = synth(seed, stream, (uint64_t)i) % QQ;
+}
+
+// ---------------------------------------------------------------------------
+// host launch wrappers
+// ---------------------------------------------------------------------------
+// per-device kernel attributes (dynamic shared memory above 48 KB); call once
+// with the target device current
+cudaError_t init_device_kernels() {
+    cudaError_t e = cudaFuncSetAttribute(k_pack, cudaFuncAttributeMaxDynamicSharedMemorySize, T_EXP * N * 8);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_fold_switch, cudaFuncAttributeMaxDynamicSharedMemorySize, 12 * N * 4);
+}
+
+cudaError_t launch_parse_query(const uint8_t* qb, int nq, int db_rows, uint64_t* y, uint64_t* z,
+                               uint32_t* a_il, uint32_t* gsw, cudaStream_t st) {
+    k_parse_query<<<2 * 148, 256, 0, st>>>(qb, nq, db_rows, y, z, a_il, gsw);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gemv(const uint16_t* db, int db_rows, int64_t db_cols, int nq, const uint32_t* a_il,
+                        uint64_t* c, int sm_count, cudaStream_t st) {
+    const int blocks = sm_count * 4;
+    if (nq == 2) k_gemv<2, 8><<<blocks, 256, 0, st>>>(db, db_rows, db_cols, a_il, c);
+    else if (nq == 1) k_gemv<1, 16><<<blocks, 256, 0, st>>>(db, db_rows, db_cols, a_il, c);
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack(const uint64_t* bt, const uint64_t* btb, const uint64_t* bth, const uint64_t* y,
+                        const uint64_t* z, uint32_t* S, int num_outputs, cudaStream_t st) {
+    const int smem = T_EXP * N * 8;
+    dim3 grid(N / PACK_ZB, num_outputs);
+    k_pack<<<grid, PACK_THREADS, smem, st>>>(bt, btb, bth, y, z, S);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_intt_crt(const uint32_t* S, const uint32_t* iw, const uint32_t* iwp, uint64_t* R,
+                            int num_outputs, cudaStream_t st) {
+    k_intt_crt<<<num_outputs, 512, 0, st>>>(S, iw, iwp, R);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fold_switch(const uint32_t* row0, const uint32_t* gsw, const uint64_t* a_hat,
+                               const uint64_t* R, const uint64_t* cvec, const uint32_t* fw,
+                               const uint32_t* fwp, const uint32_t* iw, const uint32_t* iwp, int interp,
+                               int c_groups, int nq, int64_t db_cols, uint8_t* resp,
+                               int64_t resp_query_stride, cudaStream_t st) {
+    const int smem = 12 * N * 4;
+    dim3 grid(c_groups, nq);
+    k_fold_switch<<<grid, FOLD_THREADS, smem, st>>>(row0, gsw, a_hat, R, cvec, fw, fwp, iw, iwp, interp,
+                                                    c_groups, db_cols, resp, resp_query_stride);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_response_frame(uint8_t* resp, int nq, int64_t per_query, const uint8_t* stash,
+                                  int64_t stash_count, int64_t stash_entry, cudaStream_t st) {
+    k_response_frame<<<8, 256, 0, st>>>(resp, nq, per_query, stash, stash_count, stash_entry);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rotations(const uint64_t* y_body, uint64_t* y_all, uint64_t* y_bar_all, int num_rotations,
+                             cudaStream_t st) {
+    dim3 grid(num_rotations, T_EXP);
+    k_rotations<<<grid, 256, 0, st>>>(y_body, y_all, y_bar_all, num_rotations);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack_materialized(const uint64_t* bt, const uint64_t* btb, const uint64_t* bth,
+                                     const uint64_t* y_all, const uint64_t* y_bar_all, const uint64_t* z,
+                                     int num_outputs, int n_rot, uint64_t* out, cudaStream_t st) {
+    dim3 grid(num_outputs, N / 256);
+    k_pack_materialized<<<grid, 256, 0, st>>>(bt, btb, bth, y_all, y_bar_all, z, num_outputs, n_rot, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ntt_batch(uint64_t* data, int npairs, int forward, const uint32_t* w, const uint32_t* wp,
+                             cudaStream_t st) {
+    k_ntt_batch<<<npairs, 512, 0, st>>>(data, forward, w, wp);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_synth_db(uint16_t* db, int64_t n, uint64_t seed, cudaStream_t st) {
+    k_synth_db<<<148 * 8, 256, 0, st>>>(db, n, seed);
+    return cudaGetLastError();
+}
+cudaError_t launch_synth_condensed(uint64_t* out, int64_t n, uint64_t seed, uint64_t stream, cudaStream_t st) {
+    k_synth_condensed<<<148 * 8, 256, 0, st>>>(out, n, seed, stream);
+    return cudaGetLastError();
+}
+cudaError_t launch_synth_modq(uint64_t* out, int64_t n, uint64_t seed, uint64_t stream, cudaStream_t st) {
+    k_synth_modq<<<148 * 8, 256, 0, st>>>(out, n, seed, stream);
+    return cudaGetLastError();
+}
+
+}  // namespace ipr

@@ -1,0 +1,39 @@
+// kernels.cuh — host-side launch wrappers for the respond() kernels (kernels.cu)
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace ipr {
+
+cudaError_t set_constants(const uint64_t br[2], uint32_t q0inv);
+cudaError_t init_device_kernels();
+
+cudaError_t launch_parse_query(const uint8_t* qb, int nq, int db_rows, uint64_t* y, uint64_t* z,
+                               uint32_t* a_il, uint32_t* gsw, cudaStream_t st);
+// nq must be 1 or 2; a_il points at the pair group, c at [nq][db_cols]
+cudaError_t launch_gemv(const uint16_t* db, int db_rows, int64_t db_cols, int nq, const uint32_t* a_il,
+                        uint64_t* c, int sm_count, cudaStream_t st);
+cudaError_t launch_pack(const uint64_t* bt, const uint64_t* btb, const uint64_t* bth, const uint64_t* y,
+                        const uint64_t* z, uint32_t* S, int num_outputs, cudaStream_t st);
+cudaError_t launch_intt_crt(const uint32_t* S, const uint32_t* iw, const uint32_t* iwp, uint64_t* R,
+                            int num_outputs, cudaStream_t st);
+cudaError_t launch_fold_switch(const uint32_t* row0, const uint32_t* gsw, const uint64_t* a_hat,
+                               const uint64_t* R, const uint64_t* cvec, const uint32_t* fw,
+                               const uint32_t* fwp, const uint32_t* iw, const uint32_t* iwp, int interp,
+                               int c_groups, int nq, int64_t db_cols, uint8_t* resp,
+                               int64_t resp_query_stride, cudaStream_t st);
+cudaError_t launch_response_frame(uint8_t* resp, int nq, int64_t per_query, const uint8_t* stash,
+                                  int64_t stash_count, int64_t stash_entry, cudaStream_t st);
+cudaError_t launch_rotations(const uint64_t* y_body, uint64_t* y_all, uint64_t* y_bar_all, int num_rotations,
+                             cudaStream_t st);
+cudaError_t launch_pack_materialized(const uint64_t* bt, const uint64_t* btb, const uint64_t* bth,
+                                     const uint64_t* y_all, const uint64_t* y_bar_all, const uint64_t* z,
+                                     int num_outputs, int n_rot, uint64_t* out, cudaStream_t st);
+cudaError_t launch_ntt_batch(uint64_t* data, int npairs, int forward, const uint32_t* w, const uint32_t* wp,
+                             cudaStream_t st);
+cudaError_t launch_synth_db(uint16_t* db, int64_t n, uint64_t seed, cudaStream_t st);
+cudaError_t launch_synth_condensed(uint64_t* out, int64_t n, uint64_t seed, uint64_t stream, cudaStream_t st);
+cudaError_t launch_synth_modq(uint64_t* out, int64_t n, uint64_t seed, uint64_t stream, cudaStream_t st);
+
+}  // namespace ipr

@@ -1,0 +1,547 @@
+// server.cu — keyword server handle and the C ABI of include/ipr_b200.h.
+//
+// One ipr_server owns the device-resident state of one database (encoded DB,
+// packing precomputation, NTT tables, RGSW mask row) plus the per-request
+// scratch, a stream, and one CUDA graph per query count.  respond() runs
+// (rkdud007/inspire-rs src/pir/server/keyword.rs:534-640):
+//   H2D query bytes -> parse -> GEMV (both queries, one DB pass) -> packing
+//   (once per payload) -> INTT/CRT -> fold + modulus switch -> framing -> D2H.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "host_math.hpp"
+#include "ipr_b200.h"
+#include "kernels.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define CU(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return fail(e_ == cudaErrorMemoryAllocation ? IPR_E_OOM : IPR_E_CUDA, "%s: %s (%s:%d)", \
+                        #call, cudaGetErrorString(e_), __FILE__, __LINE__);                   \
+    } while (0)
+
+constexpr int kN = 2048;
+constexpr int kNInner = 3069;
+constexpr int kMaxProfileSlots = 8192;
+
+}  // namespace
+
+struct ipr_server {
+    int device = 0;
+    int sm_count = 148;
+    ipr::Plan plan{};
+    ipr::HostParams hp;
+    cudaStream_t stream = nullptr;
+    // resident state
+    uint16_t* d_db = nullptr;
+    uint64_t *d_ahat = nullptr, *d_bt = nullptr, *d_btb = nullptr, *d_bth = nullptr;
+    uint8_t* d_stash = nullptr;
+    uint64_t stash_count = 0, stash_entry = 0;
+    uint32_t *d_fw = nullptr, *d_fwp = nullptr, *d_iw = nullptr, *d_iwp = nullptr, *d_row0 = nullptr;
+    // per-request scratch
+    unsigned cap_q = 0;
+    uint8_t* d_query = nullptr;
+    uint64_t *d_y = nullptr, *d_z = nullptr;
+    uint32_t *d_ail = nullptr, *d_gsw = nullptr, *d_S = nullptr;
+    uint64_t *d_R = nullptr, *d_c = nullptr;
+    uint8_t* d_resp = nullptr;
+    uint8_t *h_query = nullptr, *h_resp = nullptr;
+    std::map<unsigned, cudaGraphExec_t> graphs;
+    std::mutex mu;
+    // profiling
+    bool profiling = false;
+    std::vector<cudaEvent_t> events;  // kMaxProfileSlots * (IPR_NSTAGES + 1)
+    int slots_used = 0;
+    double stage_ms[IPR_NSTAGES] = {0};
+    uint64_t calls = 0;
+    // public parameters
+    uint64_t key_size = 0, value_size = 0, num_records = 0;
+    uint8_t cuckoo_seed[16] = {0};
+    uint64_t hbm = 0;
+    std::vector<void*> allocs;
+
+    template <typename T>
+    int alloc(T** p, size_t bytes) {
+        void* v = nullptr;
+        cudaError_t e = cudaMalloc(&v, bytes ? bytes : 16);
+        if (e != cudaSuccess)
+            return fail(IPR_E_OOM, "cudaMalloc(%zu bytes) failed on device %d: %s", bytes, device,
+                        cudaGetErrorString(e));
+        allocs.push_back(v);
+        hbm += bytes;
+        *p = static_cast<T*>(v);
+        return IPR_OK;
+    }
+    void free_ptr(void* p) {
+        for (size_t i = 0; i < allocs.size(); i++)
+            if (allocs[i] == p) {
+                cudaFree(p);
+                allocs.erase(allocs.begin() + i);
+                return;
+            }
+    }
+    uint64_t per_query_bytes() const { return plan.c * IPR_RESULT_BYTES; }
+    uint64_t response_bytes(unsigned nq) const {
+        return 4 + (uint64_t)nq * (4 + per_query_bytes()) + 4 + stash_count * (4 + stash_entry);
+    }
+};
+
+namespace {
+
+void destroy_graphs(ipr_server* s) {
+    for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
+    s->graphs.clear();
+}
+
+int ensure_scratch(ipr_server* s, unsigned nq) {
+    const unsigned want = nq < 2 ? 2 : nq;
+    if (want <= s->cap_q) return IPR_OK;
+    destroy_graphs(s);
+    for (void* p : {(void*)s->d_query, (void*)s->d_ail, (void*)s->d_gsw, (void*)s->d_c, (void*)s->d_resp})
+        if (p) s->free_ptr(p);
+    if (s->h_query) cudaFreeHost(s->h_query);
+    if (s->h_resp) cudaFreeHost(s->h_resp);
+    s->h_query = s->h_resp = nullptr;
+    const uint64_t rows = s->plan.db_rows, cols = s->plan.db_cols;
+    const unsigned groups = (want + 1) / 2;
+    int st;
+    if ((st = s->alloc(&s->d_query, ipr::query_bytes(rows, want) + 16))) return st;
+    if ((st = s->alloc(&s->d_ail, (size_t)groups * rows * 4 * 4))) return st;
+    if ((st = s->alloc(&s->d_gsw, (size_t)want * 12 * kN * 4))) return st;
+    if ((st = s->alloc(&s->d_c, (size_t)want * cols * 8))) return st;
+    if ((st = s->alloc(&s->d_resp, s->response_bytes(want)))) return st;
+    CU(cudaMallocHost(&s->h_query, ipr::query_bytes(rows, want) + 16));
+    CU(cudaMallocHost(&s->h_resp, s->response_bytes(want)));
+    s->cap_q = want;
+    return IPR_OK;
+}
+
+// enqueue the device pipeline for one payload; `prof` = event slot base or -1
+int enqueue(ipr_server* s, unsigned nq, const uint8_t* d_query, uint8_t* d_resp, int prof) {
+    cudaStream_t st = s->stream;
+    const ipr::Plan& p = s->plan;
+    auto rec = [&](int stage) {
+        if (prof >= 0) cudaEventRecord(s->events[(size_t)prof * (IPR_NSTAGES + 1) + stage], st);
+    };
+    rec(0);
+    if (nq > 0) {
+        CU(ipr::launch_parse_query(d_query, (int)nq, (int)p.db_rows, s->d_y, s->d_z, s->d_ail, s->d_gsw, st));
+        rec(1);
+        for (unsigned g = 0; 2 * g < nq; g++) {
+            const int ng = nq - 2 * g >= 2 ? 2 : 1;
+            CU(ipr::launch_gemv(s->d_db, (int)p.db_rows, (int64_t)p.db_cols, ng,
+                                s->d_ail + (size_t)g * p.db_rows * 4, s->d_c + (size_t)2 * g * p.db_cols,
+                                s->sm_count, st));
+        }
+        rec(2);
+        CU(ipr::launch_pack(s->d_bt, s->d_btb, s->d_bth, s->d_y, s->d_z, s->d_S, (int)p.instances, st));
+        rec(3);
+        CU(ipr::launch_intt_crt(s->d_S, s->d_iw, s->d_iwp, s->d_R, (int)p.instances, st));
+        rec(4);
+        CU(ipr::launch_fold_switch(s->d_row0, s->d_gsw, s->d_ahat, s->d_R, s->d_c, s->d_fw, s->d_fwp, s->d_iw,
+                                   s->d_iwp, (int)p.interp, (int)p.c, (int)nq, (int64_t)p.db_cols, d_resp + 8,
+                                   (int64_t)(4 + s->per_query_bytes()), st));
+    } else {
+        rec(1); rec(2); rec(3); rec(4);
+    }
+    CU(ipr::launch_response_frame(d_resp, (int)nq, (int64_t)s->per_query_bytes(), s->d_stash,
+                                  (int64_t)s->stash_count, (int64_t)s->stash_entry, st));
+    rec(5);
+    return IPR_OK;
+}
+
+int harvest_profile(ipr_server* s) {
+    if (!s->slots_used) return IPR_OK;
+    CU(cudaStreamSynchronize(s->stream));
+    for (int slot = 0; slot < s->slots_used; slot++) {
+        for (int k = 0; k < IPR_NSTAGES; k++) {
+            float ms = 0;
+            cudaEvent_t a = s->events[(size_t)slot * (IPR_NSTAGES + 1) + k];
+            cudaEvent_t b = s->events[(size_t)slot * (IPR_NSTAGES + 1) + k + 1];
+            CU(cudaEventElapsedTime(&ms, a, b));
+            s->stage_ms[k] += ms;
+        }
+        s->calls++;
+    }
+    s->slots_used = 0;
+    return IPR_OK;
+}
+
+int next_profile_slot(ipr_server* s) {
+    if (!s->profiling) return -1;
+    if (s->slots_used == kMaxProfileSlots && harvest_profile(s)) return -1;
+    return s->slots_used++;
+}
+
+int get_graph(ipr_server* s, unsigned nq, cudaGraphExec_t* out) {
+    auto it = s->graphs.find(nq);
+    if (it != s->graphs.end()) {
+        *out = it->second;
+        return IPR_OK;
+    }
+    const size_t qb = ipr::query_bytes(s->plan.db_rows, nq), rb = s->response_bytes(nq);
+    cudaGraph_t g;
+    CU(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    cudaMemcpyAsync(s->d_query, s->h_query, qb, cudaMemcpyHostToDevice, s->stream);
+    int st = enqueue(s, nq, s->d_query, s->d_resp, -1);
+    cudaMemcpyAsync(s->h_resp, s->d_resp, rb, cudaMemcpyDeviceToHost, s->stream);
+    cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    if (st) return st;
+    CU(e);
+    cudaGraphExec_t ex;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    CU(e);
+    s->graphs[nq] = ex;
+    *out = ex;
+    return IPR_OK;
+}
+
+int init_common(ipr_server* s, int device, const ipr_plan* plan) {
+    if (!plan || plan->db_rows < (uint64_t)kN || (plan->db_rows & 255) || plan->instances == 0 ||
+        plan->interp == 0 || plan->c == 0 || plan->c * plan->interp > plan->instances ||
+        plan->db_cols != plan->instances * kN)
+        return fail(IPR_E_ARGS, "invalid plan");
+    s->device = device;
+    CU(cudaSetDevice(device));
+    CU(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, device));
+    s->plan.num_items = plan->num_items;
+    s->plan.entry_size = plan->entry_size;
+    s->plan.item_size_bits = plan->item_size_bits;
+    s->plan.dim0 = plan->dim0;
+    s->plan.db_rows = plan->db_rows;
+    s->plan.db_cols = plan->db_cols;
+    s->plan.instances = plan->instances;
+    s->plan.interp = plan->interp;
+    s->plan.c = plan->c;
+    s->plan.peak_bytes = plan->peak_bytes;
+    // HBM preflight (the reference's check, keyword.rs:368-387, on the resident footprint)
+    const uint64_t resident = plan->db_rows * plan->db_cols * 2 + plan->instances * kN * 8 +
+                              2 * plan->instances * (uint64_t)kNInner * kN * 8 + plan->instances * 3ull * kN * 8;
+    size_t free_b = 0, total_b = 0;
+    CU(cudaMemGetInfo(&free_b, &total_b));
+    if (resident > free_b)
+        return fail(IPR_E_OOM,
+                    "insufficient GPU memory: requires %llu bytes, only %zu bytes available (db_rows=%llu, "
+                    "db_cols=%llu, instances=%llu)",
+                    (unsigned long long)resident, free_b, (unsigned long long)plan->db_rows,
+                    (unsigned long long)plan->db_cols, (unsigned long long)plan->instances);
+    int lo, hi;
+    CU(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    CU(cudaStreamCreateWithPriority(&s->stream, cudaStreamNonBlocking, hi));
+    CU(ipr::init_device_kernels());
+    ipr::host_params_init(s->hp);
+    CU(ipr::set_constants(s->hp.barrett, s->hp.q0_inv_mod_q1));
+    int st;
+    const size_t tb = 2 * kN * 4;
+    if ((st = s->alloc(&s->d_fw, tb)) || (st = s->alloc(&s->d_fwp, tb)) || (st = s->alloc(&s->d_iw, tb)) ||
+        (st = s->alloc(&s->d_iwp, tb)) || (st = s->alloc(&s->d_row0, tb)))
+        return st;
+    CU(cudaMemcpy(s->d_fw, s->hp.fw.data(), tb, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(s->d_fwp, s->hp.fwp.data(), tb, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(s->d_iw, s->hp.iw.data(), tb, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(s->d_iwp, s->hp.iwp.data(), tb, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(s->d_row0, s->hp.row0.data(), tb, cudaMemcpyHostToDevice));
+    const uint64_t no = plan->instances;
+    if ((st = s->alloc(&s->d_db, plan->db_rows * plan->db_cols * 2)) || (st = s->alloc(&s->d_ahat, no * kN * 8)) ||
+        (st = s->alloc(&s->d_bt, no * (uint64_t)kNInner * kN * 8)) ||
+        (st = s->alloc(&s->d_btb, no * (uint64_t)kNInner * kN * 8)) || (st = s->alloc(&s->d_bth, no * 3 * kN * 8)) ||
+        (st = s->alloc(&s->d_y, 3 * kN * 8)) || (st = s->alloc(&s->d_z, 3 * kN * 8)) ||
+        (st = s->alloc(&s->d_S, no * 2 * kN * 4)) || (st = s->alloc(&s->d_R, no * kN * 8)))
+        return st;
+    s->events.resize((size_t)kMaxProfileSlots * (IPR_NSTAGES + 1), nullptr);
+    return ensure_scratch(s, 2);
+}
+
+int check_payload(ipr_server* s, const uint8_t* query, size_t len, unsigned* nq) {
+    if (!query || len < 1) return fail(IPR_E_FORMAT, "empty query");
+    *nq = query[0];
+    const uint64_t need = ipr::query_bytes(s->plan.db_rows, *nq);
+    if (len < need)
+        return fail(IPR_E_FORMAT, "query has %zu bytes, %u queries need %llu", len, *nq, (unsigned long long)need);
+    return IPR_OK;
+}
+
+int respond_locked(ipr_server* s, const uint8_t* query, size_t len, uint8_t* out, size_t cap, size_t* out_len) {
+    unsigned nq;
+    int st = check_payload(s, query, len, &nq);
+    if (st) return st;
+    const uint64_t rb = s->response_bytes(nq);
+    if (out_len) *out_len = rb;
+    if (!out || cap < rb) return fail(IPR_E_SPACE, "response needs %llu bytes", (unsigned long long)rb);
+    CU(cudaSetDevice(s->device));
+    if ((st = ensure_scratch(s, nq))) return st;
+    const uint64_t qb = ipr::query_bytes(s->plan.db_rows, nq);
+    std::memcpy(s->h_query, query, qb);
+    if (s->profiling) {
+        CU(cudaMemcpyAsync(s->d_query, s->h_query, qb, cudaMemcpyHostToDevice, s->stream));
+        if ((st = enqueue(s, nq, s->d_query, s->d_resp, next_profile_slot(s)))) return st;
+        CU(cudaMemcpyAsync(s->h_resp, s->d_resp, rb, cudaMemcpyDeviceToHost, s->stream));
+    } else {
+        cudaGraphExec_t g;
+        if ((st = get_graph(s, nq, &g))) return st;
+        CU(cudaGraphLaunch(g, s->stream));
+    }
+    CU(cudaStreamSynchronize(s->stream));
+    std::memcpy(out, s->h_resp, rb);
+    return IPR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ipr_plan_from_shape(uint64_t record_count, uint64_t key_size, uint64_t value_size, uint64_t buckets,
+                        uint64_t dim0, ipr_plan* out) {
+    if (!out) return fail(IPR_E_ARGS, "null output");
+    ipr::Plan p;
+    int st = ipr::plan_from_shape(record_count, key_size, value_size, buckets, dim0, p);
+    if (st) return fail(st, "invalid keyword server shape (records=%llu, buckets=%llu, dim0=%llu)",
+                        (unsigned long long)record_count, (unsigned long long)buckets, (unsigned long long)dim0);
+    out->num_items = p.num_items;
+    out->entry_size = p.entry_size;
+    out->item_size_bits = p.item_size_bits;
+    out->dim0 = p.dim0;
+    out->db_rows = p.db_rows;
+    out->db_cols = p.db_cols;
+    out->instances = p.instances;
+    out->interp = p.interp;
+    out->c = p.c;
+    out->peak_bytes = p.peak_bytes;
+    return IPR_OK;
+}
+
+uint64_t ipr_query_bytes(uint64_t db_rows, unsigned num_queries) { return ipr::query_bytes(db_rows, num_queries); }
+
+int ipr_server_create(int device, const ipr_plan* plan, const ipr_server_data* data, ipr_server** out) {
+    if (!out || !data || !data->db || !data->a_hat || !data->bold_t || !data->bold_t_bar || !data->bold_t_hat)
+        return fail(IPR_E_ARGS, "null argument");
+    if (data->stash_count && (!data->stash || !data->stash_entry_bytes)) return fail(IPR_E_ARGS, "bad stash");
+    *out = nullptr;
+    auto* s = new ipr_server();
+    int st = init_common(s, device, plan);
+    if (st) {
+        ipr_server_destroy(s);
+        return st;
+    }
+    const uint64_t no = plan->instances;
+    auto up = [&](void* dst, const void* src, size_t bytes) -> int {
+        CU(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+        return IPR_OK;
+    };
+    if ((st = up(s->d_db, data->db, plan->db_rows * plan->db_cols * 2)) || (st = up(s->d_ahat, data->a_hat, no * kN * 8)) ||
+        (st = up(s->d_bt, data->bold_t, no * (uint64_t)kNInner * kN * 8)) ||
+        (st = up(s->d_btb, data->bold_t_bar, no * (uint64_t)kNInner * kN * 8)) ||
+        (st = up(s->d_bth, data->bold_t_hat, no * 3 * kN * 8))) {
+        ipr_server_destroy(s);
+        return st;
+    }
+    s->stash_count = data->stash_count;
+    s->stash_entry = data->stash_entry_bytes;
+    if (s->stash_count) {
+        if ((st = s->alloc(&s->d_stash, s->stash_count * s->stash_entry)) ||
+            (st = up(s->d_stash, data->stash, s->stash_count * s->stash_entry))) {
+            ipr_server_destroy(s);
+            return st;
+        }
+    }
+    s->key_size = data->key_size;
+    s->value_size = data->value_size;
+    s->num_records = data->num_records;
+    std::memcpy(s->cuckoo_seed, data->cuckoo_seed, 16);
+    // response buffers depend on the stash size: rebuild scratch
+    s->cap_q = 0;
+    if ((st = ensure_scratch(s, 2))) {
+        ipr_server_destroy(s);
+        return st;
+    }
+    *out = s;
+    return IPR_OK;
+}
+
+int ipr_server_create_synthetic(int device, const ipr_plan* plan, uint64_t seed, ipr_server** out) {
+    if (!out) return fail(IPR_E_ARGS, "null output");
+    *out = nullptr;
+    auto* s = new ipr_server();
+    int st = init_common(s, device, plan);
+    if (st) {
+        ipr_server_destroy(s);
+        return st;
+    }
+    const int64_t no = (int64_t)plan->instances;
+    cudaStream_t t = s->stream;
+    auto chk = [&](cudaError_t e) -> int {
+        if (e != cudaSuccess) return fail(IPR_E_CUDA, "synthetic fill: %s", cudaGetErrorString(e));
+        return IPR_OK;
+    };
+    if ((st = chk(ipr::launch_synth_db(s->d_db, (int64_t)(plan->db_rows * plan->db_cols), seed, t))) ||
+        (st = chk(ipr::launch_synth_modq(s->d_ahat, no * kN, seed, 2, t))) ||
+        (st = chk(ipr::launch_synth_condensed(s->d_bt, no * kNInner * kN, seed, 3, t))) ||
+        (st = chk(ipr::launch_synth_condensed(s->d_btb, no * kNInner * kN, seed, 4, t))) ||
+        (st = chk(ipr::launch_synth_condensed(s->d_bth, no * 3 * kN, seed, 5, t))) ||
+        (st = chk(cudaStreamSynchronize(t)))) {
+        ipr_server_destroy(s);
+        return st;
+    }
+    s->key_size = 32;
+    s->value_size = plan->entry_size > 32 ? plan->entry_size - 32 : 0;
+    *out = s;
+    return IPR_OK;
+}
+
+void ipr_server_destroy(ipr_server* s) {
+    if (!s) return;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    destroy_graphs(s);
+    for (auto e : s->events)
+        if (e) cudaEventDestroy(e);
+    for (void* p : s->allocs) cudaFree(p);
+    if (s->h_query) cudaFreeHost(s->h_query);
+    if (s->h_resp) cudaFreeHost(s->h_resp);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+int ipr_server_public_params_json(const ipr_server* s, char* out, size_t cap, size_t* out_len) {
+    if (!s) return fail(IPR_E_ARGS, "null server");
+    std::string j = "{\"num_items\":" + std::to_string(s->plan.num_items) +
+                    ",\"item_size_bits\":" + std::to_string(s->plan.entry_size * 8) +
+                    ",\"dim0\":" + std::to_string(s->plan.dim0) + ",\"keyword_pir\":{\"cuckoo_seed\":[";
+    for (int i = 0; i < 16; i++) j += (i ? "," : "") + std::to_string((int)s->cuckoo_seed[i]);
+    j += "],\"num_hashes\":2,\"key_size\":" + std::to_string(s->key_size) +
+         ",\"value_size\":" + std::to_string(s->value_size) + ",\"entry_size\":" + std::to_string(s->plan.entry_size) +
+         ",\"num_records\":" + std::to_string(s->num_records) + "}}";
+    if (out_len) *out_len = j.size();
+    if (!out || cap < j.size() + 1) return fail(IPR_E_SPACE, "public params need %zu bytes", j.size() + 1);
+    std::memcpy(out, j.c_str(), j.size() + 1);
+    return IPR_OK;
+}
+
+uint64_t ipr_server_query_bytes(const ipr_server* s, unsigned nq) {
+    return s ? ipr::query_bytes(s->plan.db_rows, nq) : 0;
+}
+uint64_t ipr_server_response_bytes(const ipr_server* s, unsigned nq) { return s ? s->response_bytes(nq) : 0; }
+
+int ipr_server_hbm_bytes(const ipr_server* s, uint64_t* out) {
+    if (!s || !out) return fail(IPR_E_ARGS, "null argument");
+    *out = s->hbm;
+    return IPR_OK;
+}
+
+int ipr_server_plan(const ipr_server* s, ipr_plan* out) {
+    if (!s || !out) return fail(IPR_E_ARGS, "null argument");
+    out->num_items = s->plan.num_items;
+    out->entry_size = s->plan.entry_size;
+    out->item_size_bits = s->plan.item_size_bits;
+    out->dim0 = s->plan.dim0;
+    out->db_rows = s->plan.db_rows;
+    out->db_cols = s->plan.db_cols;
+    out->instances = s->plan.instances;
+    out->interp = s->plan.interp;
+    out->c = s->plan.c;
+    out->peak_bytes = s->plan.peak_bytes;
+    return IPR_OK;
+}
+
+int ipr_server_respond(ipr_server* s, const uint8_t* query, size_t len, uint8_t* out, size_t cap, size_t* out_len) {
+    if (!s) return fail(IPR_E_ARGS, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    return respond_locked(s, query, len, out, cap, out_len);
+}
+
+int ipr_server_respond_batch(ipr_server* s, int n, const uint8_t* const* queries, const size_t* lens,
+                             uint8_t* const* outs, const size_t* caps, size_t* out_lens, int* statuses) {
+    if (!s || n < 0 || (n && (!queries || !lens || !outs || !caps))) return fail(IPR_E_ARGS, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    int worst = IPR_OK;
+    for (int i = 0; i < n; i++) {
+        size_t ol = 0;
+        int st = respond_locked(s, queries[i], lens[i], outs[i], caps[i], &ol);
+        if (out_lens) out_lens[i] = ol;
+        if (statuses) statuses[i] = st;
+        if (st && !worst) worst = st;
+    }
+    return worst;
+}
+
+int ipr_server_respond_device(ipr_server* s, const uint8_t* d_query, size_t len, uint8_t* d_out, size_t cap,
+                              size_t* out_len) {
+    if (!s || !d_query || !d_out) return fail(IPR_E_ARGS, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    CU(cudaSetDevice(s->device));
+    // the query count follows from the exact length (the count byte stays on the device)
+    const uint64_t base = ipr::query_bytes(s->plan.db_rows, 0), per = ipr::query_bytes(s->plan.db_rows, 1) - base;
+    if (len < base || (len - base) % per || (len - base) / per > 255)
+        return fail(IPR_E_FORMAT, "device query length %zu is not an exact payload size", len);
+    const unsigned nq = (unsigned)((len - base) / per);
+    const uint64_t rb = s->response_bytes(nq);
+    if (out_len) *out_len = rb;
+    if (cap < rb) return fail(IPR_E_SPACE, "response needs %llu bytes", (unsigned long long)rb);
+    int st = ensure_scratch(s, nq);
+    if (st) return st;
+    return enqueue(s, nq, d_query, d_out, next_profile_slot(s));
+}
+
+int ipr_server_stream(ipr_server* s, void** stream) {
+    if (!s || !stream) return fail(IPR_E_ARGS, "null argument");
+    *stream = (void*)s->stream;
+    return IPR_OK;
+}
+
+int ipr_server_sync(ipr_server* s) {
+    if (!s) return fail(IPR_E_ARGS, "null server");
+    CU(cudaStreamSynchronize(s->stream));
+    return IPR_OK;
+}
+
+int ipr_server_set_profiling(ipr_server* s, int on) {
+    if (!s) return fail(IPR_E_ARGS, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    CU(cudaSetDevice(s->device));
+    if (on && !s->events[0])
+        for (auto& e : s->events) CU(cudaEventCreate(&e));
+    int st = harvest_profile(s);
+    if (st) return st;
+    s->profiling = on != 0;
+    for (double& v : s->stage_ms) v = 0;
+    s->calls = 0;
+    return IPR_OK;
+}
+
+int ipr_server_stage_times(ipr_server* s, double* ms_sum, uint64_t* calls) {
+    if (!s || !ms_sum) return fail(IPR_E_ARGS, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    int st = harvest_profile(s);
+    if (st) return st;
+    for (int k = 0; k < IPR_NSTAGES; k++) ms_sum[k] = s->stage_ms[k];
+    if (calls) *calls = s->calls;
+    return IPR_OK;
+}
+
+const char* ipr_last_error(void) { return g_last_error.c_str(); }
+const char* ipr_version(void) { return "inspire-rs_b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

@@ -270,6 +270,24 @@ void ipr_gadget_invert_2(const ipr_params *p, const uint64_t *in2, uint64_t *out
         }
 }
 
+/* gadget_invert_rdim (gadget.rs:35-61) for any mx = rows * num_elems:
+ * out row j + k*rows holds bits [k*bits_per, (k+1)*bits_per) of input row j */
+void ipr_gadget_invert_general(const ipr_params *p, const uint64_t *in, unsigned rows, unsigned num_elems,
+                               uint64_t *out) {
+    unsigned bits_per = (num_elems == p->modulus_log2)
+                            ? 1
+                            : (unsigned)floor((double)p->modulus_log2 / (double)num_elems) + 1;
+    uint64_t mask = (1ULL << bits_per) - 1;
+    for (unsigned j = 0; j < rows; j++)
+        for (int z = 0; z < IPR_N; z++) {
+            uint64_t v = in[(size_t)j * IPR_N + z];
+            for (unsigned k = 0; k < num_elems; k++) {
+                unsigned off = k * bits_per;
+                out[((size_t)j + (size_t)k * rows) * IPR_N + z] = off >= 64 ? 0 : (v >> off) & mask;
+            }
+        }
+}
+
 /* ------------------------------------------------------------------ */
 /* automorphisms                                                        */
 /* ------------------------------------------------------------------ */

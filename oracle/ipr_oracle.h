@@ -77,6 +77,8 @@ void ipr_from_ntt(const ipr_params *p, const uint64_t *ntt_in, uint64_t *raw_out
 
 /* ---- gadget (gadget.rs:35-65): 2x1 raw -> 6x1 raw, row j + k*2 ---- */
 void ipr_gadget_invert_2(const ipr_params *p, const uint64_t *in2, uint64_t *out6);
+void ipr_gadget_invert_general(const ipr_params *p, const uint64_t *in, unsigned rows, unsigned num_elems,
+                               uint64_t *out);
 
 /* ---- automorphisms (poly.rs:531-543, packing.rs:1423-1516) ---- */
 void ipr_automorph_poly(const ipr_params *p, const uint64_t *a, uint64_t *res, uint64_t t);

@@ -1,0 +1,336 @@
+"""ctypes bindings of the CPU oracle (liboracle.so).  TEST INFRASTRUCTURE ONLY.
+
+Imported by tests/, __graft_entry__.smoke() and bench.py's cpu_baseline /
+reference legs as the checker; the product package never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libinspire_ref_kernels.so")
+
+N = 2048
+NINNER = 3069
+Q0, Q1 = 268369921, 249561089
+Q = Q0 * Q1
+RESULT_BYTES = 12288
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+if not os.path.exists(LIB):
+    build()
+_lib = ctypes.CDLL(LIB)
+
+_u64 = ctypes.c_uint64
+_p = ctypes.c_void_p
+_sz = ctypes.c_size_t
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("q", _u64 * 2), ("modulus", _u64), ("barrett_cr0", _u64 * 2), ("barrett_cr1", _u64 * 2),
+                ("cr0_mod", _u64), ("cr1_mod", _u64), ("mod0_inv_mod1", _u64), ("mod1_inv_mod0", _u64),
+                ("modulus_log2", _u64), ("root", _u64 * 2), ("ntt", ((_u64 * N) * 4) * 2)]
+
+
+class CPlan(ctypes.Structure):
+    _fields_ = [(n, _u64) for n in ("num_items", "entry_size", "item_size_bits", "dim0", "db_rows", "db_cols",
+                                   "instances", "interp", "c", "peak_bytes")]
+
+
+class OracleDB(ctypes.Structure):
+    _fields_ = [("db_rows", _u64), ("db_cols", _u64), ("num_outputs", _u64), ("interp", _u64), ("c", _u64),
+                ("db", _p), ("a_hat", _p), ("bold_t", _p), ("bold_t_bar", _p), ("bold_t_hat", _p),
+                ("stash", _p), ("stash_count", _u64), ("stash_entry_bytes", _u64)]
+
+
+def _sig(name, res, *args):
+    f = getattr(_lib, name)
+    f.restype = res
+    f.argtypes = list(args)
+    return f
+
+
+_params_init = _sig("ipr_params_init", None, ctypes.POINTER(Params))
+get_barrett_crs_c = _sig("ipr_get_barrett_crs", None, _u64, ctypes.POINTER(_u64), ctypes.POINTER(_u64))
+barrett_raw_u64 = _sig("ipr_barrett_raw_u64", _u64, _u64, _u64, _u64)
+barrett_reduction_u128_raw = _sig("ipr_barrett_reduction_u128_raw", _u64, _u64, _u64, _u64, _u64, _u64)
+div2_uint_mod = _sig("ipr_div2_uint_mod", _u64, _u64, _u64)
+invert_uint_mod = _sig("ipr_invert_uint_mod", _u64, _u64, _u64)
+rescale = _sig("ipr_rescale", _u64, _u64, _u64, _u64)
+_crt = _sig("ipr_crt_compose", _u64, ctypes.POINTER(Params), _u64, _u64)
+_ntt_f = _sig("ipr_ntt_forward", None, ctypes.POINTER(Params), _p)
+_ntt_i = _sig("ipr_ntt_inverse", None, ctypes.POINTER(Params), _p)
+_to_ntt = _sig("ipr_to_ntt", None, ctypes.POINTER(Params), _p, _p)
+_from_ntt = _sig("ipr_from_ntt", None, ctypes.POINTER(Params), _p, _p)
+_gadget = _sig("ipr_gadget_invert_2", None, ctypes.POINTER(Params), _p, _p)
+_gadget_g = _sig("ipr_gadget_invert_general", None, ctypes.POINTER(Params), _p, ctypes.c_uint, ctypes.c_uint, _p)
+_auto_poly = _sig("ipr_automorph_poly", None, ctypes.POINTER(Params), _p, _p, _u64)
+_auto_table = _sig("ipr_automorph_table", None, _u64, _p)
+_auto_bf = _sig("ipr_automorph_table_bruteforce", ctypes.c_int, ctypes.POINTER(Params), _u64, _p, _u64)
+gen_pow = _sig("ipr_gen_pow", _u64, ctypes.c_uint)
+_read_bits = _sig("ipr_read_bits", _u64, _p, _sz, ctypes.c_uint)
+_write_bits = _sig("ipr_write_bits", None, _p, _u64, _sz, ctypes.c_uint)
+_chacha_rfc = _sig("ipr_chacha20_rfc8439_block", None, _p, ctypes.c_uint32, _p, _p)
+_rgsw_row0 = _sig("ipr_rgsw_row0", None, ctypes.POINTER(Params), _p)
+_plan = _sig("ipr_plan_from_shape", ctypes.c_int, _u64, _u64, _u64, _u64, _u64, ctypes.POINTER(CPlan))
+_gemv = _sig("ipr_oracle_gemv", None, ctypes.POINTER(Params), ctypes.POINTER(OracleDB), _p, _p)
+_rot = _sig("ipr_oracle_rotations", None, _p, _p, _p)
+_pack = _sig("ipr_oracle_packing_sum", None, ctypes.POINTER(Params), ctypes.POINTER(OracleDB), _p, _p, _p)
+_post = _sig("ipr_oracle_postprocess", None, ctypes.POINTER(Params), ctypes.POINTER(OracleDB), _p, _p, _p)
+_fold = _sig("ipr_oracle_fold", None, ctypes.POINTER(Params), ctypes.POINTER(OracleDB), _p, _p, _p, _p)
+_switch = _sig("ipr_oracle_switch", None, ctypes.POINTER(Params), _p, _p)
+query_bytes = _sig("ipr_query_bytes", _sz, _u64, ctypes.c_uint)
+_parse = _sig("ipr_oracle_parse_query", ctypes.c_int, _p, _sz, _u64, ctypes.POINTER(ctypes.c_uint), _p, _p, _p, _p,
+              ctypes.c_uint)
+_resp_bytes = _sig("ipr_response_bytes", _sz, ctypes.POINTER(OracleDB), ctypes.c_uint)
+_respond = _sig("ipr_oracle_respond", ctypes.c_int, ctypes.POINTER(Params), ctypes.POINTER(OracleDB), _p, _sz, _p, _sz,
+                ctypes.POINTER(_sz))
+synth = _sig("ipr_synth", _u64, _u64, _u64, _u64)
+_synth_db = _sig("ipr_synth_db", None, _u64, _u64, _u64, _p)
+_synth_pre = _sig("ipr_synth_precomp", None, _u64, _u64, _p, _p, _p, _p)
+_synth_q = _sig("ipr_synth_query", ctypes.c_int, _u64, _u64, ctypes.c_uint, _p, _sz, ctypes.POINTER(_sz))
+threads = _sig("ipr_oracle_threads", ctypes.c_int)
+
+_PARAMS = None
+
+
+def params() -> Params:
+    global _PARAMS
+    if _PARAMS is None:
+        _PARAMS = Params()
+        _params_init(ctypes.byref(_PARAMS))
+    return _PARAMS
+
+
+def _ptr(a: np.ndarray) -> int:
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data
+
+
+def get_barrett_crs(m: int):
+    a, b = _u64(), _u64()
+    get_barrett_crs_c(m, ctypes.byref(a), ctypes.byref(b))
+    return a.value, b.value
+
+
+def ntt_tables() -> np.ndarray:
+    return np.ctypeslib.as_array(params().ntt).reshape(2, 4, N).copy()
+
+
+def crt_compose(x: int, y: int) -> int:
+    return _crt(ctypes.byref(params()), x, y)
+
+
+def ntt_forward(limbs: np.ndarray) -> np.ndarray:
+    a = np.ascontiguousarray(limbs, dtype=np.uint64).copy()
+    _ntt_f(ctypes.byref(params()), _ptr(a))
+    return a
+
+
+def ntt_inverse(limbs: np.ndarray) -> np.ndarray:
+    a = np.ascontiguousarray(limbs, dtype=np.uint64).copy()
+    _ntt_i(ctypes.byref(params()), _ptr(a))
+    return a
+
+
+def to_ntt(raw: np.ndarray) -> np.ndarray:
+    r = np.ascontiguousarray(raw, dtype=np.uint64)
+    out = np.zeros(2 * N, dtype=np.uint64)
+    _to_ntt(ctypes.byref(params()), _ptr(r), _ptr(out))
+    return out
+
+
+def from_ntt(ntt: np.ndarray) -> np.ndarray:
+    a = np.ascontiguousarray(ntt, dtype=np.uint64)
+    out = np.zeros(N, dtype=np.uint64)
+    _from_ntt(ctypes.byref(params()), _ptr(a), _ptr(out))
+    return out
+
+
+def gadget_invert_2(rows2: np.ndarray) -> np.ndarray:
+    a = np.ascontiguousarray(rows2, dtype=np.uint64).reshape(2 * N)
+    out = np.zeros(6 * N, dtype=np.uint64)
+    _gadget(ctypes.byref(params()), _ptr(a), _ptr(out))
+    return out.reshape(6, N)
+
+
+def gadget_invert_general(rows: np.ndarray, num_elems: int) -> np.ndarray:
+    a = np.ascontiguousarray(rows, dtype=np.uint64)
+    r = a.size // N
+    out = np.zeros(r * num_elems * N, dtype=np.uint64)
+    _gadget_g(ctypes.byref(params()), _ptr(a), r, num_elems, _ptr(out))
+    return out.reshape(r * num_elems, N)
+
+
+def automorph_poly(a: np.ndarray, t: int) -> np.ndarray:
+    x = np.ascontiguousarray(a, dtype=np.uint64)
+    out = np.zeros(N, dtype=np.uint64)
+    _auto_poly(ctypes.byref(params()), _ptr(x), _ptr(out), t)
+    return out
+
+
+def automorph_table(t: int) -> np.ndarray:
+    out = np.zeros(N, dtype=np.uint32)
+    _auto_table(t, _ptr(out))
+    return out
+
+
+def automorph_table_bruteforce(t: int, seed: int = 1):
+    out = np.zeros(N, dtype=np.uint32)
+    bad = _auto_bf(ctypes.byref(params()), t, _ptr(out), seed)
+    return None if bad else out
+
+
+def read_bits(buf: np.ndarray, off: int, n: int) -> int:
+    return _read_bits(_ptr(buf), off, n)
+
+
+def write_bits(buf: np.ndarray, val: int, off: int, n: int):
+    _write_bits(_ptr(buf), val, off, n)
+
+
+def chacha20_rfc8439_block(key: bytes, counter: int, nonce: bytes) -> bytes:
+    k = np.frombuffer(key, dtype="<u4").copy()
+    n = np.frombuffer(nonce, dtype="<u4").copy()
+    out = np.zeros(16, dtype=np.uint32)
+    _chacha_rfc(_ptr(k), counter, _ptr(n), _ptr(out))
+    return out.astype("<u4").tobytes()
+
+
+def rgsw_row0() -> np.ndarray:
+    out = np.zeros(2 * N, dtype=np.uint64)
+    _rgsw_row0(ctypes.byref(params()), _ptr(out))
+    return out
+
+
+def plan_from_shape(records, key_size, value_size, buckets=0, dim0=0):
+    p = CPlan()
+    st = _plan(records, key_size, value_size, buckets or 0, dim0 or 0, ctypes.byref(p))
+    if st:
+        return None
+    return {f: getattr(p, f) for f, _ in CPlan._fields_}
+
+
+class SynthDB:
+    """Seeded synthetic server state (same generator as the device's
+    ipr_server_create_synthetic) held in host memory for the oracle."""
+
+    def __init__(self, db_rows, instances, interp, c, seed, stash=()):
+        self.db_rows, self.instances, self.interp, self.c, self.seed = db_rows, instances, interp, c, seed
+        self.db_cols = instances * N
+        self.db = np.zeros(self.db_cols * db_rows, dtype=np.uint16)
+        _synth_db(seed, db_rows, self.db_cols, _ptr(self.db))
+        self.a_hat = np.zeros(instances * N, dtype=np.uint64)
+        self.bold_t = np.zeros(instances * NINNER * N, dtype=np.uint64)
+        self.bold_t_bar = np.zeros(instances * NINNER * N, dtype=np.uint64)
+        self.bold_t_hat = np.zeros(instances * 3 * N, dtype=np.uint64)
+        _synth_pre(seed, instances, _ptr(self.a_hat), _ptr(self.bold_t), _ptr(self.bold_t_bar),
+                   _ptr(self.bold_t_hat))
+        self.stash = [bytes(s) for s in stash]
+        self._stash_buf = np.frombuffer(b"".join(self.stash) or b"\0", dtype=np.uint8).copy()
+
+    def c_struct(self) -> OracleDB:
+        d = OracleDB()
+        d.db_rows, d.db_cols, d.num_outputs, d.interp, d.c = (self.db_rows, self.db_cols, self.instances,
+                                                              self.interp, self.c)
+        d.db, d.a_hat = _ptr(self.db), _ptr(self.a_hat)
+        d.bold_t, d.bold_t_bar, d.bold_t_hat = _ptr(self.bold_t), _ptr(self.bold_t_bar), _ptr(self.bold_t_hat)
+        d.stash = _ptr(self._stash_buf)
+        d.stash_count = len(self.stash)
+        d.stash_entry_bytes = len(self.stash[0]) if self.stash else 0
+        return d
+
+
+def synth_query(seed: int, db_rows: int, nq: int = 2) -> bytes:
+    cap = query_bytes(db_rows, nq)
+    buf = np.zeros(cap, dtype=np.uint8)
+    n = _sz()
+    assert _synth_q(seed, db_rows, nq, _ptr(buf), cap, ctypes.byref(n)) == 0
+    return buf[:n.value].tobytes()
+
+
+def respond(sdb: SynthDB, query: bytes) -> bytes:
+    d = sdb.c_struct()
+    q = np.frombuffer(query, dtype=np.uint8).copy()
+    nq = query[0]
+    cap = _resp_bytes(ctypes.byref(d), nq)
+    out = np.zeros(cap, dtype=np.uint8)
+    n = _sz()
+    st = _respond(ctypes.byref(params()), ctypes.byref(d), _ptr(q), len(query), _ptr(out), cap, ctypes.byref(n))
+    if st:
+        raise ValueError(f"oracle respond status {st}")
+    return out[:n.value].tobytes()
+
+
+def parse_query(query: bytes, db_rows: int):
+    q = np.frombuffer(query, dtype=np.uint8).copy()
+    nq = query[0]
+    y = np.zeros(3 * N, dtype=np.uint64)
+    z = np.zeros(3 * N, dtype=np.uint64)
+    rows = np.zeros(max(nq, 1) * db_rows, dtype=np.uint64)
+    gsw = np.zeros(max(nq, 1) * 12 * N, dtype=np.uint64)
+    got = ctypes.c_uint()
+    st = _parse(_ptr(q), len(query), db_rows, ctypes.byref(got), _ptr(y), _ptr(z), _ptr(rows), _ptr(gsw), 255)
+    if st:
+        raise ValueError(f"parse status {st}")
+    return y, z, rows.reshape(max(nq, 1), db_rows), gsw.reshape(max(nq, 1), 6, 2, N)
+
+
+def gemv(sdb: SynthDB, a: np.ndarray) -> np.ndarray:
+    d = sdb.c_struct()
+    av = np.ascontiguousarray(a, dtype=np.uint64)
+    c = np.zeros(sdb.db_cols, dtype=np.uint64)
+    _gemv(ctypes.byref(params()), ctypes.byref(d), _ptr(av), _ptr(c))
+    return c
+
+
+def rotations(y_body: np.ndarray):
+    y = np.ascontiguousarray(y_body, dtype=np.uint64)
+    ya = np.zeros(NINNER * N, dtype=np.uint64)
+    yb = np.zeros(NINNER * N, dtype=np.uint64)
+    _rot(_ptr(y), _ptr(ya), _ptr(yb))
+    return ya, yb
+
+
+def packing_sum(sdb: SynthDB, y_body, z_body) -> np.ndarray:
+    d = sdb.c_struct()
+    y = np.ascontiguousarray(y_body, dtype=np.uint64)
+    z = np.ascontiguousarray(z_body, dtype=np.uint64)
+    S = np.zeros(sdb.instances * 2 * N, dtype=np.uint64)
+    _pack(ctypes.byref(params()), ctypes.byref(d), _ptr(y), _ptr(z), _ptr(S))
+    return S.reshape(sdb.instances, 2, N)
+
+
+def postprocess(sdb: SynthDB, S, b_values) -> np.ndarray:
+    d = sdb.c_struct()
+    s = np.ascontiguousarray(S, dtype=np.uint64)
+    b = np.ascontiguousarray(b_values, dtype=np.uint64)
+    out = np.zeros(sdb.instances * 2 * N, dtype=np.uint64)
+    _post(ctypes.byref(params()), ctypes.byref(d), _ptr(s), _ptr(b), _ptr(out))
+    return out.reshape(sdb.instances, 2, N)
+
+
+def fold(sdb: SynthDB, gsw_body, packed) -> np.ndarray:
+    d = sdb.c_struct()
+    row0 = rgsw_row0()
+    g = np.ascontiguousarray(gsw_body, dtype=np.uint64)
+    p = np.ascontiguousarray(packed, dtype=np.uint64)
+    out = np.zeros(sdb.c * 2 * N, dtype=np.uint64)
+    _fold(ctypes.byref(params()), ctypes.byref(d), _ptr(row0), _ptr(g), _ptr(p), _ptr(out))
+    return out.reshape(sdb.c, 2, N)
+
+
+def switch(result) -> bytes:
+    r = np.ascontiguousarray(result, dtype=np.uint64)
+    out = np.zeros(RESULT_BYTES, dtype=np.uint8)
+    _switch(ctypes.byref(params()), _ptr(r), _ptr(out))
+    return out.tobytes()

@@ -1,0 +1,116 @@
+"""Host-side checks that need no GPU: the C-ABI library loads and exports every
+symbol the headers declare; the product's shape plan and wire helpers agree
+with the oracle (and so with the reference's derivation)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared(header):
+    txt = open(os.path.join(ROOT, "include", header)).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b((?:ipr|gpu)_[a-z0-9_]+)\s*\(", txt)))
+
+
+@pytest.mark.parametrize("header", ["ipr_b200.h", "ipr_b200_compat.h"])
+def test_library_exports_every_declared_symbol(pkg, header):
+    names = _declared(header)
+    assert len(names) > 10
+    for n in names:
+        assert hasattr(pkg.lib, n), n
+    out = subprocess.run(["nm", "-D", "--defined-only", pkg._LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (\S+)", out))
+    missing = [n for n in names if n not in exported]
+    assert not missing, missing
+
+
+def test_library_is_sm100a(pkg):
+    out = subprocess.run(["cuobjdump", "--list-elf", pkg._LIB_PATH], capture_output=True, text=True)
+    if out.returncode != 0:
+        pytest.skip("cuobjdump unavailable")
+    assert "sm_100a" in out.stdout
+
+
+SHAPES = [
+    (10_000, 32, 1184, None, None),
+    (1_000_000, 32, 1184, 2_097_152, 2048),
+    (4_000_000, 32, 800, 8_388_608, 8192),
+    (1_000_000, 32, 1184, 2_097_152, 8192),
+    (2_000_000, 32, 1568, 4_194_304, 8192),
+    (5_000_000, 32, 1184, 8_388_608, 65_536),
+    (5_000_000, 32, 1184, None, None),
+    (3000, 16, 16, None, None),
+    (700, 32, 1184, None, None),
+]
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_plan_matches_oracle(pkg, orc, shape):
+    p = pkg.plan_from_shape(*shape)
+    o = orc.plan_from_shape(*[s or 0 for s in shape])
+    assert o is not None
+    for k, v in o.items():
+        assert getattr(p, k) == v, k
+
+
+def test_plan_rejections(pkg):
+    with pytest.raises(pkg.IprError) as e:
+        pkg.plan_from_shape(1_000_000, 32, 1184, 262_144, 2048)  # buckets < records
+    assert e.value.status == -1
+    with pytest.raises(pkg.IprError):
+        pkg.plan_from_shape(10, 3, 0)
+    with pytest.raises(pkg.IprError):
+        pkg.plan_from_shape(0, 32, 1184)
+
+
+def test_query_bytes(pkg, orc):
+    for rows in (2048, 8192, 65536):
+        for nq in (0, 1, 2, 5):
+            assert pkg.query_bytes(rows, nq) == orc.query_bytes(rows, nq)
+    assert pkg.query_bytes(2048, 2) == 286_721
+
+
+def test_serialize_query_roundtrip(pkg, orc):
+    rows = 2048
+    q = orc.synth_query(5, rows, 2)
+    y, z, qrows, gsw = orc.parse_query(q, rows)
+    payload = pkg.KeywordQueryPayload(
+        y_body=y.reshape(3, 2048), z_body=z.reshape(3, 2048),
+        queries=[(qrows[i], gsw[i]) for i in range(2)])
+    assert pkg.serialize_keyword_query(payload) == q
+
+
+def test_response_framing_roundtrip(pkg):
+    body = [bytes(range(7)) * 3, b"xyz"]
+    stash = [b"k" * 5]
+    buf = len(body).to_bytes(4, "little")
+    for b in body:
+        buf += len(b).to_bytes(4, "little") + b
+    buf += len(stash).to_bytes(4, "little") + len(stash[0]).to_bytes(4, "little") + stash[0]
+    r = pkg.deserialize_keyword_response(buf)
+    assert r.responses == body and r.stash_entries == stash
+
+
+def test_server_create_without_gpu_fails_loudly(pkg):
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("GPU present")
+    except ImportError:
+        pass
+    plan = pkg.plan_from_shape(10_000, 32, 1184)
+    with pytest.raises(pkg.IprError) as e:
+        pkg.KeywordServer.synthetic(plan, seed=1)
+    assert e.value.status in (-2, -3)
+
+
+def test_error_string_reports_status(pkg):
+    with pytest.raises(pkg.IprError) as e:
+        pkg.plan_from_shape(1_000_000, 32, 1184, 262_144, 2048)
+    assert "IPR_E_ARGS" in str(e.value) and "buckets" in str(e.value)
