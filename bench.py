@@ -126,26 +126,34 @@ def read_traffic():
     return None
 
 
-def cpu_sample(orc, threads_note=""):
+class CpuSample:
     """Oracle respond() on one fold group of the 1M workload (32 of 352 packing
-    outputs, 65,536 DB columns), scaled by the 11 groups to a full payload."""
-    plan = orc.plan_from_shape(RECORDS, KEY, VALUE, BUCKETS, DIM0)
-    groups = plan["c"]
-    sdb = orc.SynthDB(plan["db_rows"], plan["interp"], plan["interp"], 1, seed=7)
-    q = orc.synth_query(2026, plan["db_rows"], 2)
-    orc.respond(sdb, q)  # warm
-    reps, t0 = 0, time.perf_counter()
-    while True:
-        orc.respond(sdb, q)
-        reps += 1
-        el = time.perf_counter() - t0
-        if el > 8 or reps >= 3:
-            break
-    per_group = el / reps
-    per_payload = per_group * groups
-    return {"value": 1.0 / per_payload, "unit": UNIT, "cores": int(orc.threads()), "kind": "port",
-            "sample": f"oracle respond() of 1 of {groups} fold groups (32 packing outputs, db 2048x65536, "
-                      f"2 queries) x{reps}, scaled x{groups}; {per_payload:.2f} s/payload"}
+    outputs, 65,536 DB columns, both queries), scaled by the 11 groups to one
+    full payload.  The sample's state is generated once."""
+
+    def __init__(self, orc):
+        self.orc = orc
+        plan = orc.plan_from_shape(RECORDS, KEY, VALUE, BUCKETS, DIM0)
+        self.groups = plan["c"]
+        self.sdb = orc.SynthDB(plan["db_rows"], plan["interp"], plan["interp"], 1, seed=7)
+        self.q = orc.synth_query(2026, plan["db_rows"], 2)
+
+    def step(self):
+        t0 = time.perf_counter()
+        self.orc.respond(self.sdb, self.q)
+        return (time.perf_counter() - t0) * self.groups  # seconds per full payload
+
+    def describe(self, per_payload, reps):
+        return {"value": 1.0 / per_payload, "unit": UNIT, "cores": int(self.orc.threads()), "kind": "port",
+                "sample": f"oracle respond() of 1 of {self.groups} fold groups (32 packing outputs, db 2048x65536,"
+                          f" 2 queries) x{reps}, scaled x{self.groups}; {per_payload:.2f} s/payload"}
+
+
+def cpu_sample(orc, reps=3):
+    s = CpuSample(orc)
+    s.step()  # warm
+    t = statistics.median([s.step() for _ in range(reps)])
+    return s.describe(t, reps)
 
 
 def main():
@@ -155,7 +163,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--records", type=int, default=RECORDS, help="workload override (profiling small cases)")
+    ap.add_argument("--buckets", type=int, default=None)
+    ap.add_argument("--dim0", type=int, default=None)
     args = ap.parse_args()
+    small = args.records != RECORDS
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -164,15 +176,12 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        orc = load_oracle()
-        vals = []
+        s = CpuSample(load_oracle())
         for _ in range(args.warmup):
-            cpu_sample(orc)
-        for _ in range(args.steps):
-            vals.append(cpu_sample(orc))
-        v = statistics.median([x["value"] for x in vals])
-        cb = dict(vals[-1])
-        cb["value"] = v
+            s.step()
+        times = [s.step() for _ in range(args.steps)]
+        v = args.steps / sum(times)
+        cb = s.describe(sum(times) / args.steps, args.steps)
         print(json.dumps({
             "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
@@ -197,7 +206,10 @@ def main():
     dev = torch.cuda.current_device()
 
     pkg = load_package()
-    plan = pkg.plan_from_shape(RECORDS, KEY, VALUE, BUCKETS, DIM0)
+    if small:
+        plan = pkg.plan_from_shape(args.records, KEY, VALUE, args.buckets, args.dim0)
+    else:
+        plan = pkg.plan_from_shape(RECORDS, KEY, VALUE, BUCKETS, DIM0)
     srv = pkg.KeywordServer.synthetic(plan, seed=7 + rank, device=dev)
     qbytes = srv.query_bytes(2)
     rbytes = srv.response_bytes(2)
@@ -279,7 +291,7 @@ def main():
     out = None
     if rank == 0:
         cpu = None
-        if not args.no_cpu_baseline and world == 1:
+        if not args.no_cpu_baseline and world == 1 and not small:
             try:
                 cpu = cpu_sample(load_oracle())
             except Exception as ex:  # reported, never fatal to the GPU number
@@ -289,11 +301,13 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": "1M ML-KEM-768 respond(), buckets 2^21, dim0 2048, 2 queries/payload, batch 1",
-                       "records": RECORDS, "buckets": BUCKETS, "dim0": DIM0, "db_rows": plan.db_rows,
+            "config": {"workload": ("1M ML-KEM-768 respond(), buckets 2^21, dim0 2048, 2 queries/payload, batch 1"
+                                    if not small else f"{args.records} ML-KEM-768 records (profiling case)"),
+                       "records": args.records, "buckets": plan.num_items, "dim0": plan.dim0, "db_rows": plan.db_rows,
                        "db_cols": plan.db_cols, "instances": plan.instances, "interp": plan.interp, "c": plan.c,
                        "parallelism": f"replica x{world}",
-                       "l2": "inputs larger than L2 (35.4 GB packing stream + 2.95 GB DB per step)"},
+                       "l2": "inputs larger than L2 (packing stream of %.1f GB + DB of %.2f GB per step)" % (
+                           plan.instances * 6141 * N * 8 / 1e9, plan.db_rows * plan.db_cols * 2 / 1e9)},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": qbytes, "d2h_bytes_per_step": rbytes},
             "roofline": {"bound": "hbm", "kernel": "k_pack", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
