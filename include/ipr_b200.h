@@ -136,6 +136,22 @@ int ipr_server_stage_times(ipr_server *srv, double *ms_sum, uint64_t *calls);
 const char *ipr_last_error(void);
 const char *ipr_version(void);
 
+/* First-dimension GEMV query that allocates no device memory.  No counterpart
+ * in the reference: it is gpu_gemv_query (ipr_b200_compat.h) for callers that
+ * cannot call cudaMalloc, e.g. a process whose framework has reserved all free
+ * HBM for its own pool, or a request path that cannot take cudaMalloc's
+ * device-wide synchronisation.  Same arguments and result as gpu_gemv_query
+ * (h_a: db_rows condensed query values; h_c: b_cols results mod q; d_db: the
+ * column-major u16 DB on the current device), but the query row and result
+ * are staged in a fixed 8.5 MiB device array inside this library (at most
+ * 65,536 rows and 1,048,576 columns; larger shapes return IPR_E_ARGS).  Every
+ * GPU that loads the library holds that array until the process exits.  All
+ * calls share it, so calls that overlap on the GPU race; issue them one at a
+ * time.  The first call on a device resolves the array's address and loads
+ * constants for that device; make it before any stream capture there.
+ * Returns IPR_OK or a negative status (message in ipr_last_error()). */
+int ipr_gemv_query_noalloc(uint64_t *h_c, const uint64_t *h_a, const uint16_t *d_db, int db_rows, int b_cols);
+
 #ifdef __cplusplus
 }
 #endif

@@ -224,6 +224,13 @@ void host_params_init(HostParams& p) {
     for (int i = 0; i < 2 * kN; i++) p.row0[i] = (uint32_t)a[i];
 }
 
+void host_moduli_constants(uint64_t barrett[2], uint32_t* q0_inv_mod_q1) {
+    const uint64_t q0 = 268369921ull, q1 = 249561089ull;
+    barrett[0] = (uint64_t)((((u128)1) << 64) / q0);
+    barrett[1] = (uint64_t)((((u128)1) << 64) / q1);
+    *q0_inv_mod_q1 = (uint32_t)inverse(q0 % q1, q1);
+}
+
 int plan_from_shape(uint64_t record_count, uint64_t key_size, uint64_t value_size, uint64_t buckets,
                     uint64_t dim0, Plan& out) {
     if (!record_count || !key_size || !value_size) return IPR_E_ARGS;

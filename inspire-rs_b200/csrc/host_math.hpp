@@ -26,6 +26,10 @@ struct HostParams {
 
 void host_params_init(HostParams& p);
 
+// Only the two reduction constants the kernels keep in constant memory
+// (floor(2^64 / q_l) and q0^-1 mod q1); computes them without touching the heap.
+void host_moduli_constants(uint64_t barrett[2], uint32_t* q0_inv_mod_q1);
+
 struct Plan {
     uint64_t num_items, entry_size, item_size_bits, dim0;
     uint64_t db_rows, db_cols, instances, interp, c;

@@ -48,6 +48,11 @@ constexpr int kMaxProfileSlots = 8192;
 
 }  // namespace
 
+namespace ipr {
+// lets other translation units of the library report through ipr_last_error()
+void set_last_error(const char* msg) { g_last_error = msg; }
+}  // namespace ipr
+
 struct ipr_server {
     int device = 0;
     int sm_count = 148;
