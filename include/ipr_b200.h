@@ -131,6 +131,12 @@ int ipr_server_sync(ipr_server *srv);
 #define IPR_STAGE_FOLD 4
 #define IPR_NSTAGES 5
 int ipr_server_set_profiling(ipr_server *srv, int on);
+
+/* Execution options.  IPR_OPT_TENSOR_GEMV: 1 = first-dimension GEMV on the
+ * tensor cores over DB byte planes (default where db_rows <= 32768), 0 = the
+ * CUDA-core kernel on the u16 DB.  Both give identical results. */
+#define IPR_OPT_TENSOR_GEMV 1
+int ipr_server_set_option(ipr_server *srv, int option, int64_t value);
 int ipr_server_stage_times(ipr_server *srv, double *ms_sum, uint64_t *calls);
 
 const char *ipr_last_error(void);

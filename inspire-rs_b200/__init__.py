@@ -74,6 +74,7 @@ _respond_dev = _sig("ipr_server_respond_device", _i32, _vp, _vp, _sz, _vp, _sz, 
 _stream = _sig("ipr_server_stream", _i32, _vp, ctypes.POINTER(_vp))
 _sync = _sig("ipr_server_sync", _i32, _vp)
 _set_prof = _sig("ipr_server_set_profiling", _i32, _vp, _i32)
+_set_opt = _sig("ipr_server_set_option", _i32, _vp, _i32, ctypes.c_int64)
 _stage_times = _sig("ipr_server_stage_times", _i32, _vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_u64))
 _last_error = _sig("ipr_last_error", ctypes.c_char_p)
 _version = _sig("ipr_version", ctypes.c_char_p)
@@ -306,6 +307,13 @@ class KeywordServer:
 
     def sync(self):
         _check(_sync(self._h), "sync")
+
+    OPT_TENSOR_GEMV = 1
+
+    def set_option(self, option: int, value: int):
+        """ipr_server_set_option: e.g. OPT_TENSOR_GEMV 0/1 selects the CUDA-core or
+        tensor-core first-dimension GEMV (identical results)."""
+        _check(_set_opt(self._h, option, value), "set_option")
 
     def set_profiling(self, on: bool):
         _check(_set_prof(self._h, 1 if on else 0), "set_profiling")

@@ -1,0 +1,296 @@
+// gemm_tc.cu — first-dimension GEMM on the 5th-generation tensor cores.
+//
+// c[q][j] = CRT( sum_k a_q,0[k] D[j][k] mod q0 , sum_k a_q,1[k] D[j][k] mod q1 )
+// (native/cuda/gemv_kernel.cu:46-103 of rkdud007/inspire-rs, for many queries).
+// Exact split precision: the DB is kept as two byte planes D = D_0 + 256 D_1
+// ([plane][db_cols][db_rows] u8) and every 28-bit query residue as four bytes
+// a = sum_b 256^b a_b, so the dot products are sums of u8 x u8 products:
+//   sum_k D[j][k] a[k] = sum_{p,b} 256^(p+b) P_pb[j],  P_pb[j] = sum_k D_p[j][k] a_b[k]
+// Each P_pb is one column of a u8 x u8 -> 32-bit tcgen05.mma (kind::i8) GEMM;
+// P_pb < 255^2 * db_rows < 2^31 for db_rows <= 32768, so accumulation is exact,
+// and the recombination sum_{p,b} 256^(p+b) P_pb < 2^63 fits a u64.
+//
+// Kernel shape: persistent CTAs of 6 warps.  Warp 0 issues TMA loads of
+// [128 rows x 128 bytes] DB tiles and [NT x 128 bytes] query-byte tiles into a
+// multi-stage shared-memory ring (128-byte swizzle); warp 1 issues the MMAs
+// (M = 128 DB columns, N = NT query-byte columns, K = 32 bytes each) into
+// TMEM accumulators, one per plane, double buffered when they fit; warps 2-5
+// read the accumulators, recombine, reduce mod q0 / q1 and CRT-compose.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "ipr_device.cuh"
+#include "kernels.cuh"
+#include "umma.cuh"
+
+namespace ipr {
+
+namespace {
+
+constexpr int G1_THREADS = 192;
+constexpr int TILE_M = 128;
+constexpr int TILE_K = 128;  // bytes per stage along K (one 128-byte swizzle row)
+constexpr int A_STAGE_BYTES = TILE_M * TILE_K;
+constexpr int MAX_STAGES = 8;
+
+struct G1Smem {
+    uint64_t full[MAX_STAGES], empty[MAX_STAGES], acc_full[2], acc_empty[2];
+    uint32_t tmem_base;
+    int err;
+};
+
+}  // namespace
+
+__global__ void __launch_bounds__(G1_THREADS, 1)
+    k_gemm1(const __grid_constant__ CUtensorMap tm_db, const __grid_constant__ CUtensorMap tm_qb, int db_rows,
+            int64_t db_cols, int nt, int n_tiles, int num_queries, int stages, uint64_t* __restrict__ c,
+            int* __restrict__ err_flag) {
+    extern __shared__ uint8_t smem_raw[];
+    // 1024-byte aligned tile area (128-byte swizzle atoms)
+    uint8_t* base = smem_raw + ((1024 - (umma::smem_addr(smem_raw) & 1023)) & 1023);
+    G1Smem* sh = reinterpret_cast<G1Smem*>(base);
+    volatile int* err = &sh->err;
+    uint8_t* tiles = base + 1024;
+    const int b_stage_bytes = nt * TILE_K;
+    uint8_t* a_tiles = tiles;
+    uint8_t* b_tiles = tiles + stages * A_STAGE_BYTES;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nbuf = (4 * nt <= 512) ? 2 : 1;
+    uint32_t ncols = 32;
+    while (ncols < (uint32_t)(nbuf * 2 * nt)) ncols <<= 1;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < stages; s++) {
+            umma::mbar_init(&sh->full[s], 1);
+            umma::mbar_init(&sh->empty[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            umma::mbar_init(&sh->acc_full[b], 1);
+            umma::mbar_init(&sh->acc_empty[b], 4);
+        }
+        *err = 0;
+        umma::fence_mbar_init();
+    }
+    if (warp == 1) umma::tmem_alloc(&sh->tmem_base, ncols);
+    umma::fence_before();
+    __syncthreads();
+    umma::fence_after();
+    const uint32_t tmem = sh->tmem_base;
+
+    const int kpp = db_rows / TILE_K;  // stages per plane
+    const int ks_total = 2 * kpp;
+    const int64_t m_tiles = db_cols / TILE_M;
+    const int64_t total = m_tiles * n_tiles;
+
+    if (warp == 0) {
+        if (lane == 0) {  // TMA producer
+            int stage = 0;
+            uint32_t phase = 0;
+            int last_phase[MAX_STAGES];
+            for (int s = 0; s < MAX_STAGES; s++) last_phase[s] = -1;
+            for (int64_t t = blockIdx.x; t < total && !*err; t += gridDim.x) {
+                const int64_t m = t / n_tiles;
+                const int n = (int)(t % n_tiles);
+                for (int ks = 0; ks < ks_total; ks++) {
+                    if (!umma::mbar_wait(&sh->empty[stage], phase ^ 1)) {
+                        *err = 1;
+                        break;
+                    }
+                    umma::mbar_expect_tx(&sh->full[stage], A_STAGE_BYTES + b_stage_bytes);
+                    const int p = ks / kpp, kk = ks % kpp;
+                    umma::tma_load_2d(a_tiles + stage * A_STAGE_BYTES, &tm_db, kk * TILE_K,
+                                      (int)(p * db_cols + m * TILE_M), &sh->full[stage]);
+                    umma::tma_load_2d(b_tiles + stage * b_stage_bytes, &tm_qb, kk * TILE_K, n * nt, &sh->full[stage]);
+                    last_phase[stage] = (int)phase;
+                    if (++stage == stages) {
+                        stage = 0;
+                        phase ^= 1;
+                    }
+                }
+            }
+            // every tile load issued has landed before the CTA may exit
+            for (int s = 0; s < stages; s++)
+                if (last_phase[s] >= 0) umma::mbar_wait(&sh->full[s], (uint32_t)last_phase[s], 1u << 22);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {  // MMA issuer
+            const uint32_t idesc = umma::idesc_u8(TILE_M, nt);
+            int stage = 0, buf = 0, last_stage = -1;
+            uint32_t phase = 0, acc_phase = 0, last_parity = 0;
+            for (int64_t t = blockIdx.x; t < total && !*err; t += gridDim.x) {
+                if (!umma::mbar_wait(&sh->acc_empty[buf], acc_phase ^ 1)) {
+                    *err = 2;
+                    break;
+                }
+                umma::fence_after();
+                bool ok = true;
+                for (int ks = 0; ks < ks_total; ks++) {
+                    if (!umma::mbar_wait(&sh->full[stage], phase)) {
+                        *err = 3;
+                        ok = false;
+                        break;
+                    }
+                    umma::fence_after();
+                    const int p = ks / kpp;
+                    const bool first = (ks % kpp) == 0;
+                    const uint32_t d = tmem + (uint32_t)((buf * 2 + p) * nt);
+                    const uint32_t sa = umma::smem_addr(a_tiles + stage * A_STAGE_BYTES);
+                    const uint32_t sb = umma::smem_addr(b_tiles + stage * b_stage_bytes);
+#pragma unroll
+                    for (int k4 = 0; k4 < TILE_K / 32; k4++)
+                        umma::mma_u8(d, umma::desc_sw128(sa + 32 * k4), umma::desc_sw128(sb + 32 * k4), idesc,
+                                     (first && k4 == 0) ? 0u : 1u);
+                    umma::commit(&sh->empty[stage]);  // frees the smem stage when these MMAs finish
+                    last_stage = stage;
+                    last_parity = phase;
+                    if (++stage == stages) {
+                        stage = 0;
+                        phase ^= 1;
+                    }
+                }
+                if (!ok) break;
+                umma::commit(&sh->acc_full[buf]);
+                if (nbuf == 2) {
+                    buf ^= 1;
+                    if (buf == 0) acc_phase ^= 1;
+                } else {
+                    acc_phase ^= 1;
+                }
+            }
+            // the last MMAs have completed before TMEM can be released
+            if (last_stage >= 0) umma::mbar_wait(&sh->empty[last_stage], last_parity, 1u << 22);
+        }
+    } else {
+        // epilogue: warps 2..5 -> TMEM lane quarters 2,3,0,1
+        const int quarter = warp & 3;
+        const int row = quarter * 32 + lane;
+        int buf = 0;
+        uint32_t acc_phase = 0;
+        for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
+            if (!umma::mbar_wait(&sh->acc_full[buf], acc_phase)) {
+                if (lane == 0) *err = 4;
+                break;
+            }
+            umma::fence_after();
+            const int64_t m = t / n_tiles;
+            const int n_tile = (int)(t % n_tiles);
+            const int64_t j = m * TILE_M + row;
+            const uint32_t lane_off = (uint32_t)(quarter * 32) << 16;
+            for (int g = 0; g < nt / 16; g++) {
+                uint32_t p0[16], p1[16];
+                umma::tmem_ld16(tmem + lane_off + (uint32_t)((buf * 2 + 0) * nt + g * 16), p0);
+                umma::tmem_ld16(tmem + lane_off + (uint32_t)((buf * 2 + 1) * nt + g * 16), p1);
+                umma::tmem_wait_ld();
+                // 16 columns = 2 queries x 2 limbs x 4 bytes: column (q*2 + l)*4 + b
+#pragma unroll
+                for (int qq = 0; qq < 2; qq++) {
+                    const int q = (n_tile * nt + g * 16) / 8 + qq;
+                    uint32_t r[2];
+#pragma unroll
+                    for (int l = 0; l < 2; l++) {
+                        uint64_t v = 0;
+#pragma unroll
+                        for (int b = 0; b < 4; b++) {
+                            const int i = (qq * 2 + l) * 4 + b;
+                            v += ((uint64_t)p0[i] + ((uint64_t)p1[i] << 8)) << (8 * b);
+                        }
+                        r[l] = l ? mod64(v, Q1, BR1) : mod64(v, Q0, BR0);
+                    }
+                    if (q < num_queries) c[(int64_t)q * db_cols + j] = crt2(r[0], r[1], Q0INV, BR1);
+                }
+            }
+            umma::fence_before();
+            __syncwarp();
+            if (lane == 0) umma::mbar_arrive(&sh->acc_empty[buf]);
+            if (nbuf == 2) {
+                buf ^= 1;
+                if (buf == 0) acc_phase ^= 1;
+            } else {
+                acc_phase ^= 1;
+            }
+        }
+    }
+    umma::fence_before();
+    __syncthreads();
+    if (warp == 1) umma::tmem_dealloc(tmem, ncols);
+    if (threadIdx.x == 0 && *err) atomicExch(err_flag, *err);
+}
+
+// [plane][db_cols][db_rows] byte planes of the column-major u16 DB
+__global__ void k_db_to_planes(const uint16_t* __restrict__ db, uint8_t* __restrict__ planes, int64_t n) {
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) * 8; i < n;
+         i += (int64_t)gridDim.x * blockDim.x * 8) {
+        const uint4 v = *reinterpret_cast<const uint4*>(db + i);  // 8 values, 2 per word
+        uint2 lo, hi;
+        lo.x = __byte_perm(v.x, v.y, 0x6420);
+        lo.y = __byte_perm(v.z, v.w, 0x6420);
+        hi.x = __byte_perm(v.x, v.y, 0x7531);
+        hi.y = __byte_perm(v.z, v.w, 0x7531);
+        *reinterpret_cast<uint2*>(planes + i) = lo;
+        *reinterpret_cast<uint2*>(planes + n + i) = hi;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+namespace {
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn g_encode = nullptr;
+}  // namespace
+
+cudaError_t make_u8_tile_map(CUtensorMap* map, const void* base, uint64_t row_bytes, uint64_t rows, uint32_t box_rows) {
+    if (!g_encode) {
+        cudaDriverEntryPointQueryResult q;
+        cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", (void**)&g_encode, cudaEnableDefault, &q);
+        if (e != cudaSuccess) return e;
+        if (!g_encode || q != cudaDriverEntryPointSuccess) return cudaErrorNotSupported;
+    }
+    if ((reinterpret_cast<uintptr_t>(base) & 15) || (row_bytes & 15) || box_rows == 0 || box_rows > 256)
+        return cudaErrorInvalidValue;
+    cuuint64_t dims[2] = {row_bytes, rows};
+    cuuint64_t strides[1] = {row_bytes};
+    cuuint32_t box[2] = {128, box_rows};
+    cuuint32_t elem[2] = {1, 1};
+    CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base), dims, strides, box, elem,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+int gemm1_stages(int nt) {
+    const int per = A_STAGE_BYTES + nt * TILE_K;
+    int s = (200 * 1024) / per;
+    return s > 8 ? 8 : (s < 2 ? 2 : s);
+}
+
+size_t gemm1_smem_bytes(int nt) { return 2048 + (size_t)gemm1_stages(nt) * (A_STAGE_BYTES + nt * TILE_K); }
+
+cudaError_t init_gemm1_kernel() {
+    return cudaFuncSetAttribute(k_gemm1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm1_smem_bytes(256));
+}
+
+cudaError_t launch_db_to_planes(const uint16_t* db, uint8_t* planes, int64_t n, cudaStream_t st) {
+    if (n % 8) return cudaErrorInvalidValue;
+    k_db_to_planes<<<148 * 8, 256, 0, st>>>(db, planes, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gemm1(const CUtensorMap* tm_db, const CUtensorMap* tm_qb, int db_rows, int64_t db_cols, int nt,
+                         int n_tiles, int num_queries, uint64_t* c, int* err_flag, int sm_count, cudaStream_t st) {
+    if (nt < 16 || nt > 256 || (nt & 15) || (db_rows % TILE_K) || db_rows > 32768 || (db_cols % TILE_M))
+        return cudaErrorInvalidValue;
+    const int stages = gemm1_stages(nt);
+    const int64_t total = (db_cols / TILE_M) * n_tiles;
+    const int grid = (int)(total < sm_count ? total : sm_count);
+    k_gemm1<<<grid, G1_THREADS, gemm1_smem_bytes(nt), st>>>(*tm_db, *tm_qb, db_rows, db_cols, nt, n_tiles,
+                                                            num_queries, stages, c, err_flag);
+    return cudaGetLastError();
+}
+
+}  // namespace ipr

@@ -23,6 +23,9 @@ constexpr uint64_t QP1 = 1ull << 20;     // q'_1 (params.rs:346-348)
 constexpr uint64_t QP2 = 268369921ull;   // q'_2 = Q2_VALUES[28] (core/params.rs:37)
 constexpr int RESULT_BYTES = 12288;      // (28 + 20) * 2048 / 8 (modulus_switch.rs:45-73)
 constexpr int GADGET_BITS = 19;          // floor(56/3)+1 (gadget.rs:3-9)
+constexpr uint64_t BR0 = 68736257792ull;  // floor(2^64 / q0)
+constexpr uint64_t BR1 = 73916747789ull;  // floor(2^64 / q1)
+constexpr uint32_t Q0INV = 97389680u;     // q0^-1 mod q1
 
 // Per-limb constants kept in __constant__ memory (filled by the host).
 struct LimbConst {

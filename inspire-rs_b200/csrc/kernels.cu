@@ -41,7 +41,8 @@ __device__ __forceinline__ uint32_t modq(uint64_t x, int l) {
 // ---------------------------------------------------------------------------
 __global__ void k_parse_query(const uint8_t* __restrict__ qb, int nq, int db_rows,
                               uint64_t* __restrict__ y_body, uint64_t* __restrict__ z_body,
-                              uint32_t* __restrict__ a_il, uint32_t* __restrict__ gsw) {
+                              uint32_t* __restrict__ a_il, uint32_t* __restrict__ gsw,
+                              uint8_t* __restrict__ qbytes, int qbase) {
     const int64_t keys = 2LL * T_EXP * N;
     const int64_t per_q = (int64_t)db_rows + 2LL * T_EXP * N;
     const int64_t total = keys + (int64_t)nq * per_q;
@@ -68,6 +69,14 @@ __global__ void k_parse_query(const uint8_t* __restrict__ qb, int nq, int db_row
                 uint32_t* dst = a_il + (int64_t)g2 * db_rows * 4 + (r * ng + qq) * 2;
                 dst[0] = lo;
                 dst[1] = hi;
+                if (qbytes) {  // tensor-core operand: row (query*2 + limb)*4 + byte, column r
+                    uint8_t* qrow = qbytes + (int64_t)(qbase + q) * 8 * db_rows + r;
+#pragma unroll
+                    for (int b = 0; b < 4; b++) {
+                        qrow[(int64_t)b * db_rows] = (uint8_t)(lo >> (8 * b));
+                        qrow[(int64_t)(4 + b) * db_rows] = (uint8_t)(hi >> (8 * b));
+                    }
+                }
             } else {
                 const int64_t rr = r - db_rows;  // poly c = rr / N, coeff z = rr % N
                 const int c = (int)(rr >> LOGN), z = (int)(rr & (N - 1));
@@ -500,8 +509,8 @@ cudaError_t init_device_kernels() {
 }
 
 cudaError_t launch_parse_query(const uint8_t* qb, int nq, int db_rows, uint64_t* y, uint64_t* z,
-                               uint32_t* a_il, uint32_t* gsw, cudaStream_t st) {
-    k_parse_query<<<2 * 148, 256, 0, st>>>(qb, nq, db_rows, y, z, a_il, gsw);
+                               uint32_t* a_il, uint32_t* gsw, uint8_t* qbytes, int qbase, cudaStream_t st) {
+    k_parse_query<<<2 * 148, 256, 0, st>>>(qb, nq, db_rows, y, z, a_il, gsw, qbytes, qbase);
     return cudaGetLastError();
 }
 

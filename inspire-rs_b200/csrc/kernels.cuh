@@ -1,5 +1,6 @@
 // kernels.cuh — host-side launch wrappers for the respond() kernels (kernels.cu)
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -9,8 +10,10 @@ namespace ipr {
 cudaError_t set_constants(const uint64_t br[2], uint32_t q0inv);
 cudaError_t init_device_kernels();
 
+// qbytes (optional): tensor-core GEMM operand [(query*2 + limb)*4 + byte][db_rows] u8,
+// this payload's queries starting at global query index qbase
 cudaError_t launch_parse_query(const uint8_t* qb, int nq, int db_rows, uint64_t* y, uint64_t* z,
-                               uint32_t* a_il, uint32_t* gsw, cudaStream_t st);
+                               uint32_t* a_il, uint32_t* gsw, uint8_t* qbytes, int qbase, cudaStream_t st);
 // nq must be 1 or 2; a_il points at the pair group, c at [nq][db_cols]
 cudaError_t launch_gemv(const uint16_t* db, int db_rows, int64_t db_cols, int nq, const uint32_t* a_il,
                         uint64_t* c, int sm_count, cudaStream_t st);
@@ -35,5 +38,13 @@ cudaError_t launch_ntt_batch(uint64_t* data, int npairs, int forward, const uint
 cudaError_t launch_synth_db(uint16_t* db, int64_t n, uint64_t seed, cudaStream_t st);
 cudaError_t launch_synth_condensed(uint64_t* out, int64_t n, uint64_t seed, uint64_t stream, cudaStream_t st);
 cudaError_t launch_synth_modq(uint64_t* out, int64_t n, uint64_t seed, uint64_t stream, cudaStream_t st);
+
+// tensor-core first-dimension GEMM (gemm_tc.cu)
+cudaError_t make_u8_tile_map(CUtensorMap* map, const void* base, uint64_t row_bytes, uint64_t rows, uint32_t box_rows);
+cudaError_t init_gemm1_kernel();
+cudaError_t launch_db_to_planes(const uint16_t* db, uint8_t* planes, int64_t n, cudaStream_t st);
+// nt: query-byte columns per tile (16..256, multiple of 16); db_rows <= 32768
+cudaError_t launch_gemm1(const CUtensorMap* tm_db, const CUtensorMap* tm_qb, int db_rows, int64_t db_cols, int nt,
+                         int n_tiles, int num_queries, uint64_t* c, int* err_flag, int sm_count, cudaStream_t st);
 
 }  // namespace ipr

@@ -61,6 +61,10 @@ struct ipr_server {
     cudaStream_t stream = nullptr;
     // resident state
     uint16_t* d_db = nullptr;
+    uint8_t* d_db8 = nullptr;  // [2][db_cols][db_rows] byte planes for the tensor-core GEMM
+    CUtensorMap tm_db;
+    bool gemv_tc = false;      // first dimension on tcgen05 (db_rows <= 32768)
+    std::map<int, CUtensorMap> tm_qb;  // per query-byte tile height
     uint64_t *d_ahat = nullptr, *d_bt = nullptr, *d_btb = nullptr, *d_bth = nullptr;
     uint8_t* d_stash = nullptr;
     uint64_t stash_count = 0, stash_entry = 0;
@@ -72,7 +76,10 @@ struct ipr_server {
     uint32_t *d_ail = nullptr, *d_gsw = nullptr, *d_S = nullptr;
     uint64_t *d_R = nullptr, *d_c = nullptr;
     uint8_t* d_resp = nullptr;
+    uint8_t* d_qb = nullptr;  // query bytes [(q*2 + limb)*4 + byte][db_rows]
+    int* d_err = nullptr;     // device-side wait failures (bounded waits)
     uint8_t *h_query = nullptr, *h_resp = nullptr;
+    int* h_err = nullptr;
     std::map<unsigned, cudaGraphExec_t> graphs;
     std::mutex mu;
     // profiling
@@ -120,12 +127,35 @@ void destroy_graphs(ipr_server* s) {
     s->graphs.clear();
 }
 
+// query-byte tile height for nq queries (8 byte-rows per query) and the padded row count
+int qb_tile(unsigned nq) {
+    int n = (int)(8 * nq + 15) / 16 * 16;
+    return n > 256 ? 256 : n;
+}
+unsigned qb_rows(unsigned nq) {
+    const unsigned nt = (unsigned)qb_tile(nq);
+    return (8 * nq + nt - 1) / nt * nt;
+}
+
+int qb_map(ipr_server* s, int nt, const CUtensorMap** out) {
+    auto it = s->tm_qb.find(nt);
+    if (it == s->tm_qb.end()) {
+        CUtensorMap m;
+        CU(ipr::make_u8_tile_map(&m, s->d_qb, s->plan.db_rows, qb_rows(s->cap_q), (uint32_t)nt));
+        it = s->tm_qb.emplace(nt, m).first;
+    }
+    *out = &it->second;
+    return IPR_OK;
+}
+
 int ensure_scratch(ipr_server* s, unsigned nq) {
     const unsigned want = nq < 2 ? 2 : nq;
     if (want <= s->cap_q) return IPR_OK;
     destroy_graphs(s);
-    for (void* p : {(void*)s->d_query, (void*)s->d_ail, (void*)s->d_gsw, (void*)s->d_c, (void*)s->d_resp})
+    for (void* p : {(void*)s->d_query, (void*)s->d_ail, (void*)s->d_gsw, (void*)s->d_c, (void*)s->d_resp,
+                    (void*)s->d_qb})
         if (p) s->free_ptr(p);
+    s->tm_qb.clear();
     if (s->h_query) cudaFreeHost(s->h_query);
     if (s->h_resp) cudaFreeHost(s->h_resp);
     s->h_query = s->h_resp = nullptr;
@@ -137,6 +167,7 @@ int ensure_scratch(ipr_server* s, unsigned nq) {
     if ((st = s->alloc(&s->d_gsw, (size_t)want * 12 * kN * 4))) return st;
     if ((st = s->alloc(&s->d_c, (size_t)want * cols * 8))) return st;
     if ((st = s->alloc(&s->d_resp, s->response_bytes(want)))) return st;
+    if ((st = s->alloc(&s->d_qb, (size_t)qb_rows(want) * rows))) return st;
     CU(cudaMallocHost(&s->h_query, ipr::query_bytes(rows, want) + 16));
     CU(cudaMallocHost(&s->h_resp, s->response_bytes(want)));
     s->cap_q = want;
@@ -152,13 +183,23 @@ int enqueue(ipr_server* s, unsigned nq, const uint8_t* d_query, uint8_t* d_resp,
     };
     rec(0);
     if (nq > 0) {
-        CU(ipr::launch_parse_query(d_query, (int)nq, (int)p.db_rows, s->d_y, s->d_z, s->d_ail, s->d_gsw, st));
+        CU(ipr::launch_parse_query(d_query, (int)nq, (int)p.db_rows, s->d_y, s->d_z, s->d_ail, s->d_gsw,
+                                   s->gemv_tc ? s->d_qb : nullptr, 0, st));
         rec(1);
-        for (unsigned g = 0; 2 * g < nq; g++) {
-            const int ng = nq - 2 * g >= 2 ? 2 : 1;
-            CU(ipr::launch_gemv(s->d_db, (int)p.db_rows, (int64_t)p.db_cols, ng,
-                                s->d_ail + (size_t)g * p.db_rows * 4, s->d_c + (size_t)2 * g * p.db_cols,
-                                s->sm_count, st));
+        if (s->gemv_tc) {
+            const int nt = qb_tile(nq);
+            const CUtensorMap* tq;
+            int e = qb_map(s, nt, &tq);
+            if (e) return e;
+            CU(ipr::launch_gemm1(&s->tm_db, tq, (int)p.db_rows, (int64_t)p.db_cols, nt, (int)(qb_rows(nq) / nt),
+                                 (int)nq, s->d_c, s->d_err, s->sm_count, st));
+        } else {
+            for (unsigned g = 0; 2 * g < nq; g++) {
+                const int ng = nq - 2 * g >= 2 ? 2 : 1;
+                CU(ipr::launch_gemv(s->d_db, (int)p.db_rows, (int64_t)p.db_cols, ng,
+                                    s->d_ail + (size_t)g * p.db_rows * 4, s->d_c + (size_t)2 * g * p.db_cols,
+                                    s->sm_count, st));
+            }
         }
         rec(2);
         CU(ipr::launch_pack(s->d_bt, s->d_btb, s->d_bth, s->d_y, s->d_z, s->d_S, (int)p.instances, st));
@@ -209,9 +250,11 @@ int get_graph(ipr_server* s, unsigned nq, cudaGraphExec_t* out) {
     const size_t qb = ipr::query_bytes(s->plan.db_rows, nq), rb = s->response_bytes(nq);
     cudaGraph_t g;
     CU(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    cudaMemsetAsync(s->d_err, 0, sizeof(int), s->stream);
     cudaMemcpyAsync(s->d_query, s->h_query, qb, cudaMemcpyHostToDevice, s->stream);
     int st = enqueue(s, nq, s->d_query, s->d_resp, -1);
     cudaMemcpyAsync(s->h_resp, s->d_resp, rb, cudaMemcpyDeviceToHost, s->stream);
+    cudaMemcpyAsync(s->h_err, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
     cudaError_t e = cudaStreamEndCapture(s->stream, &g);
     if (st) return st;
     CU(e);
@@ -257,6 +300,7 @@ int init_common(ipr_server* s, int device, const ipr_plan* plan) {
     CU(cudaDeviceGetStreamPriorityRange(&lo, &hi));
     CU(cudaStreamCreateWithPriority(&s->stream, cudaStreamNonBlocking, hi));
     CU(ipr::init_device_kernels());
+    CU(ipr::init_gemm1_kernel());
     ipr::host_params_init(s->hp);
     CU(ipr::set_constants(s->hp.barrett, s->hp.q0_inv_mod_q1));
     int st;
@@ -276,6 +320,13 @@ int init_common(ipr_server* s, int device, const ipr_plan* plan) {
         (st = s->alloc(&s->d_y, 3 * kN * 8)) || (st = s->alloc(&s->d_z, 3 * kN * 8)) ||
         (st = s->alloc(&s->d_S, no * 2 * kN * 4)) || (st = s->alloc(&s->d_R, no * kN * 8)))
         return st;
+    s->gemv_tc = plan->db_rows <= 32768 && plan->db_rows % 128 == 0 && plan->db_cols % 128 == 0;
+    if ((st = s->alloc(&s->d_db8, plan->db_rows * plan->db_cols * 2)) || (st = s->alloc(&s->d_err, sizeof(int))))
+        return st;
+    CU(cudaMemset(s->d_err, 0, sizeof(int)));
+    CU(cudaMallocHost(&s->h_err, sizeof(int)));
+    *s->h_err = 0;
+    CU(ipr::make_u8_tile_map(&s->tm_db, s->d_db8, plan->db_rows, 2 * plan->db_cols, 128));
     s->events.resize((size_t)kMaxProfileSlots * (IPR_NSTAGES + 1), nullptr);
     return ensure_scratch(s, 2);
 }
@@ -301,15 +352,18 @@ int respond_locked(ipr_server* s, const uint8_t* query, size_t len, uint8_t* out
     const uint64_t qb = ipr::query_bytes(s->plan.db_rows, nq);
     std::memcpy(s->h_query, query, qb);
     if (s->profiling) {
+        CU(cudaMemsetAsync(s->d_err, 0, sizeof(int), s->stream));
         CU(cudaMemcpyAsync(s->d_query, s->h_query, qb, cudaMemcpyHostToDevice, s->stream));
         if ((st = enqueue(s, nq, s->d_query, s->d_resp, next_profile_slot(s)))) return st;
         CU(cudaMemcpyAsync(s->h_resp, s->d_resp, rb, cudaMemcpyDeviceToHost, s->stream));
+        CU(cudaMemcpyAsync(s->h_err, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
     } else {
         cudaGraphExec_t g;
         if ((st = get_graph(s, nq, &g))) return st;
         CU(cudaGraphLaunch(g, s->stream));
     }
     CU(cudaStreamSynchronize(s->stream));
+    if (*s->h_err) return fail(IPR_E_TIMEOUT, "a device-side wait ran out (code %d)", *s->h_err);
     std::memcpy(out, s->h_resp, rb);
     return IPR_OK;
 }
@@ -359,7 +413,11 @@ int ipr_server_create(int device, const ipr_plan* plan, const ipr_server_data* d
     if ((st = up(s->d_db, data->db, plan->db_rows * plan->db_cols * 2)) || (st = up(s->d_ahat, data->a_hat, no * kN * 8)) ||
         (st = up(s->d_bt, data->bold_t, no * (uint64_t)kNInner * kN * 8)) ||
         (st = up(s->d_btb, data->bold_t_bar, no * (uint64_t)kNInner * kN * 8)) ||
-        (st = up(s->d_bth, data->bold_t_hat, no * 3 * kN * 8))) {
+        (st = up(s->d_bth, data->bold_t_hat, no * 3 * kN * 8)) ||
+        (st = (ipr::launch_db_to_planes(s->d_db, s->d_db8, (int64_t)(plan->db_rows * plan->db_cols), s->stream) ==
+                       cudaSuccess && cudaStreamSynchronize(s->stream) == cudaSuccess
+                   ? IPR_OK
+                   : fail(IPR_E_CUDA, "DB byte planes: %s", cudaGetErrorString(cudaGetLastError()))))) {
         ipr_server_destroy(s);
         return st;
     }
@@ -406,6 +464,7 @@ int ipr_server_create_synthetic(int device, const ipr_plan* plan, uint64_t seed,
         (st = chk(ipr::launch_synth_condensed(s->d_bt, no * kNInner * kN, seed, 3, t))) ||
         (st = chk(ipr::launch_synth_condensed(s->d_btb, no * kNInner * kN, seed, 4, t))) ||
         (st = chk(ipr::launch_synth_condensed(s->d_bth, no * 3 * kN, seed, 5, t))) ||
+        (st = chk(ipr::launch_db_to_planes(s->d_db, s->d_db8, (int64_t)(plan->db_rows * plan->db_cols), t))) ||
         (st = chk(cudaStreamSynchronize(t)))) {
         ipr_server_destroy(s);
         return st;
@@ -426,6 +485,7 @@ void ipr_server_destroy(ipr_server* s) {
     for (void* p : s->allocs) cudaFree(p);
     if (s->h_query) cudaFreeHost(s->h_query);
     if (s->h_resp) cudaFreeHost(s->h_resp);
+    if (s->h_err) cudaFreeHost(s->h_err);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -507,6 +567,7 @@ int ipr_server_respond_device(ipr_server* s, const uint8_t* d_query, size_t len,
     if (cap < rb) return fail(IPR_E_SPACE, "response needs %llu bytes", (unsigned long long)rb);
     int st = ensure_scratch(s, nq);
     if (st) return st;
+    CU(cudaMemsetAsync(s->d_err, 0, sizeof(int), s->stream));
     return enqueue(s, nq, d_query, d_out, next_profile_slot(s));
 }
 
@@ -519,7 +580,25 @@ int ipr_server_stream(ipr_server* s, void** stream) {
 int ipr_server_sync(ipr_server* s) {
     if (!s) return fail(IPR_E_ARGS, "null server");
     CU(cudaStreamSynchronize(s->stream));
+    int flag = 0;
+    CU(cudaMemcpy(&flag, s->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) return fail(IPR_E_TIMEOUT, "a device-side wait ran out (code %d)", flag);
     return IPR_OK;
+}
+
+int ipr_server_set_option(ipr_server* s, int option, int64_t value) {
+    if (!s) return fail(IPR_E_ARGS, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    switch (option) {
+        case IPR_OPT_TENSOR_GEMV:
+            if (value && !(s->plan.db_rows <= 32768 && s->plan.db_rows % 128 == 0))
+                return fail(IPR_E_ARGS, "tensor-core first dimension needs db_rows <= 32768, a multiple of 128");
+            s->gemv_tc = value != 0;
+            destroy_graphs(s);
+            return IPR_OK;
+        default:
+            return fail(IPR_E_ARGS, "unknown option %d", option);
+    }
 }
 
 int ipr_server_set_profiling(ipr_server* s, int on) {

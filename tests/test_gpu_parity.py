@@ -76,6 +76,30 @@ def test_respond_wider_first_dimension(pkg, orc):
         assert srv.respond_to_serialized_query(q) == orc.respond(sdb, q)
 
 
+@pytest.mark.parametrize("tensor", [0, 1])
+@pytest.mark.parametrize("nq", [1, 2, 3])
+def test_first_dimension_paths(cfg0, pkg, orc, tensor, nq):
+    """tcgen05 byte-plane GEMM and the CUDA-core GEMV give the oracle's bytes"""
+    plan, srv, sdb = cfg0
+    srv.set_option(pkg.KeywordServer.OPT_TENSOR_GEMV, tensor)
+    try:
+        q = orc.synth_query(40 + nq, plan.db_rows, nq)
+        assert srv.respond_to_serialized_query(q) == orc.respond(sdb, q)
+    finally:
+        srv.set_option(pkg.KeywordServer.OPT_TENSOR_GEMV, 1)
+
+
+def test_first_dimension_tensor_wide_rows(pkg, orc):
+    plan = _plan(pkg, 2, 2, db_rows=16384)
+    with pkg.KeywordServer.synthetic(plan, seed=21) as srv:
+        sdb = orc.SynthDB(plan.db_rows, 2, 2, 1, seed=21)
+        q = orc.synth_query(4, plan.db_rows, 2)
+        want = orc.respond(sdb, q)
+        assert srv.respond_to_serialized_query(q) == want
+        srv.set_option(pkg.KeywordServer.OPT_TENSOR_GEMV, 0)
+        assert srv.respond_to_serialized_query(q) == want
+
+
 def test_from_encoded_with_stash(pkg, orc):
     plan = _plan(pkg, 4, 2)
     stash = [bytes([i]) * 1216 for i in range(3)]
