@@ -110,9 +110,24 @@ int ipr_server_plan(const ipr_server *srv, ipr_plan *out);
 int ipr_server_respond(ipr_server *srv, const uint8_t *query, size_t len, uint8_t *out, size_t cap,
                        size_t *out_len);
 
-/* n payloads; statuses[i] receives each payload's status. */
+/* n payloads; statuses[i] receives each payload's status.  Payloads carrying
+ * the usual two cuckoo queries are answered together, up to 64 per pass, on
+ * the tensor-core batch path (byte-split INT8 tcgen05 GEMMs for the first
+ * dimension and for the InspiRING packing of all clients at once); results
+ * are identical to answering them one at a time. */
 int ipr_server_respond_batch(ipr_server *srv, int n, const uint8_t *const *queries, const size_t *lens,
                              uint8_t *const *outs, const size_t *caps, size_t *out_lens, int *statuses);
+
+/* Build the batch-path state ahead of the first batch (the slot-indexed
+ * packing precomputation, instances x 2 x 2048 x 128 x 6144 / 32 bytes, and
+ * scratch for max_payloads <= 64 payloads). */
+int ipr_server_prepare_batch(ipr_server *srv, int max_payloads);
+
+/* Device-resident batch: n (1..64) two-query payloads packed back to back in
+ * device memory (stride ipr_server_query_bytes(srv, 2)), responses written back
+ * to back (stride ipr_server_response_bytes(srv, 2)).  Enqueued on the server
+ * stream; returns without waiting. */
+int ipr_server_respond_batch_device(ipr_server *srv, int n, const uint8_t *d_queries, uint8_t *d_out);
 
 /* Device-resident variant: query and response already in device memory of
  * the server's device.  Enqueued on the server stream and returns without
@@ -136,6 +151,9 @@ int ipr_server_set_profiling(ipr_server *srv, int on);
  * tensor cores over DB byte planes (default where db_rows <= 32768), 0 = the
  * CUDA-core kernel on the u16 DB.  Both give identical results. */
 #define IPR_OPT_TENSOR_GEMV 1
+/* IPR_OPT_FOLD_REGISTER_NTT: 1 = RGSW fold with register-resident NTTs and
+ * warp-shuffle butterflies (default), 0 = shared-memory NTTs.  Identical results. */
+#define IPR_OPT_FOLD_REGISTER_NTT 2
 int ipr_server_set_option(ipr_server *srv, int option, int64_t value);
 int ipr_server_stage_times(ipr_server *srv, double *ms_sum, uint64_t *calls);
 

@@ -72,6 +72,10 @@ _hbm = _sig("ipr_server_hbm_bytes", _i32, _vp, ctypes.POINTER(_u64))
 _respond = _sig("ipr_server_respond", _i32, _vp, _u8p, _sz, _u8p, _sz, ctypes.POINTER(_sz))
 _respond_dev = _sig("ipr_server_respond_device", _i32, _vp, _vp, _sz, _vp, _sz, ctypes.POINTER(_sz))
 _stream = _sig("ipr_server_stream", _i32, _vp, ctypes.POINTER(_vp))
+_respond_batch = _sig("ipr_server_respond_batch", _i32, _vp, _i32, ctypes.POINTER(_u8p), ctypes.POINTER(_sz),
+                      ctypes.POINTER(_u8p), ctypes.POINTER(_sz), ctypes.POINTER(_sz), ctypes.POINTER(_i32))
+_prepare_batch = _sig("ipr_server_prepare_batch", _i32, _vp, _i32)
+_respond_batch_dev = _sig("ipr_server_respond_batch_device", _i32, _vp, _i32, _vp, _vp)
 _sync = _sig("ipr_server_sync", _i32, _vp)
 _set_prof = _sig("ipr_server_set_profiling", _i32, _vp, _i32)
 _set_opt = _sig("ipr_server_set_option", _i32, _vp, _i32, ctypes.c_int64)
@@ -293,6 +297,36 @@ class KeywordServer:
         """KeywordServer::respond (keyword.rs:534-628)."""
         return deserialize_keyword_response(self.respond_to_serialized_query(serialize_keyword_query(payload)))
 
+    def respond_batch(self, queries: Sequence[bytes]) -> List[bytes]:
+        """Answer many serialized payloads in one call (ipr_server_respond_batch);
+        two-query payloads share the tensor-core batch path.  Raises on the
+        first failing payload."""
+        n = len(queries)
+        if n == 0:
+            return []
+        qbufs = [(ctypes.c_uint8 * len(q)).from_buffer_copy(q) for q in queries]
+        caps = [int(_srv_rbytes(self._h, q[0] if q else 0)) for q in queries]
+        obufs = [(ctypes.c_uint8 * c)() for c in caps]
+        qp = (_u8p * n)(*[ctypes.cast(b, _u8p) for b in qbufs])
+        op = (_u8p * n)(*[ctypes.cast(b, _u8p) for b in obufs])
+        lens = (_sz * n)(*[len(q) for q in queries])
+        capa = (_sz * n)(*caps)
+        olen = (_sz * n)()
+        sts = (_i32 * n)()
+        st = _respond_batch(self._h, n, qp, lens, op, capa, olen, sts)
+        for i in range(n):
+            if sts[i]:
+                raise IprError(sts[i], f"respond_batch[{i}]")
+        _check(st, "respond_batch")
+        return [bytes(obufs[i])[:olen[i]] for i in range(n)]
+
+    def prepare_batch(self, max_payloads: int = 64):
+        _check(_prepare_batch(self._h, max_payloads), "prepare_batch")
+
+    def respond_batch_device(self, n: int, d_queries_ptr: int, d_out_ptr: int):
+        """n two-query payloads back to back in device memory -> responses back to back (async)."""
+        _check(_respond_batch_dev(self._h, n, _vp(d_queries_ptr), _vp(d_out_ptr)), "respond_batch_device")
+
     # --- device-level helpers (bench / serving) ---------------------------
     def respond_device(self, d_query_ptr: int, length: int, d_out_ptr: int, cap: int) -> int:
         n = _sz()
@@ -309,6 +343,7 @@ class KeywordServer:
         _check(_sync(self._h), "sync")
 
     OPT_TENSOR_GEMV = 1
+    OPT_FOLD_REGISTER_NTT = 2
 
     def set_option(self, option: int, value: int):
         """ipr_server_set_option: e.g. OPT_TENSOR_GEMV 0/1 selects the CUDA-core or

@@ -39,16 +39,28 @@ __device__ __forceinline__ uint32_t modq(uint64_t x, int l) {
 // wire.rs:542-615): keys y/z interleaved per (i<3, k<N); then per query the
 // db_rows packed query row values followed by 6 raw-CRT RGSW body polys.
 // ---------------------------------------------------------------------------
-__global__ void k_parse_query(const uint8_t* __restrict__ qb, int nq, int db_rows,
-                              uint64_t* __restrict__ y_body, uint64_t* __restrict__ z_body,
-                              uint32_t* __restrict__ a_il, uint32_t* __restrict__ gsw,
-                              uint8_t* __restrict__ qbytes, int qbase) {
+// npay payloads of nq queries each, `pstride` bytes apart; payload p writes its
+// keys at y_body/z_body + p*3N, its RGSW bodies at gsw + p*nq*12N and its
+// query bytes at global query index qbase + p*nq.  a_il is the CUDA-core GEMV
+// operand (single payload only; may be null).
+__global__ void k_parse_query(const uint8_t* __restrict__ qb_all, int nq, int db_rows,
+                              uint64_t* __restrict__ y_all, uint64_t* __restrict__ z_all,
+                              uint32_t* __restrict__ a_il, uint32_t* __restrict__ gsw_all,
+                              uint8_t* __restrict__ qbytes, int qbase0, int npay, int64_t pstride) {
     const int64_t keys = 2LL * T_EXP * N;
     const int64_t per_q = (int64_t)db_rows + 2LL * T_EXP * N;
-    const int64_t total = keys + (int64_t)nq * per_q;
+    const int64_t fpp = keys + (int64_t)nq * per_q;  // fields per payload
+    const int64_t total_all = fpp * npay;
     const uint64_t m28 = (1ull << 28) - 1;
-    for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f < total;
-         f += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t fa = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; fa < total_all;
+         fa += (int64_t)gridDim.x * blockDim.x) {
+        const int pay = (int)(fa / fpp);
+        const int64_t f = fa - (int64_t)pay * fpp;
+        const uint8_t* qb = qb_all + (int64_t)pay * pstride;
+        uint64_t* y_body = y_all + (int64_t)pay * T_EXP * N;
+        uint64_t* z_body = z_all + (int64_t)pay * T_EXP * N;
+        uint32_t* gsw = gsw_all + (int64_t)pay * nq * 12 * N;
+        const int qbase = qbase0 + pay * nq;
         const uint8_t* p = qb + 1 + 7 * f;
         uint64_t v = 0;
 #pragma unroll
@@ -66,9 +78,11 @@ __global__ void k_parse_query(const uint8_t* __restrict__ qb, int nq, int db_row
             if (r < db_rows) {
                 // GEMV operand, queries grouped in pairs: a_il[g][k][qq][l], g = q/2
                 const int g2 = q >> 1, qq = q & 1, ng = (nq - 2 * g2) < 2 ? (nq - 2 * g2) : 2;
-                uint32_t* dst = a_il + (int64_t)g2 * db_rows * 4 + (r * ng + qq) * 2;
-                dst[0] = lo;
-                dst[1] = hi;
+                if (a_il) {
+                    uint32_t* dst = a_il + (int64_t)g2 * db_rows * 4 + (r * ng + qq) * 2;
+                    dst[0] = lo;
+                    dst[1] = hi;
+                }
                 if (qbytes) {  // tensor-core operand: row (query*2 + limb)*4 + byte, column r
                     uint8_t* qrow = qbytes + (int64_t)(qbase + q) * 8 * db_rows + r;
 #pragma unroll
@@ -382,9 +396,10 @@ __global__ void __launch_bounds__(FOLD_THREADS) k_fold_switch(
 }
 
 // serialize_keyword_response framing: [u32 nq] { [u32 len] bytes }* [u32 nstash] { [u32 len] entry }*
-__global__ void k_response_frame(uint8_t* __restrict__ resp, int nq, int64_t per_query_bytes,
+__global__ void k_response_frame(uint8_t* __restrict__ resp_all, int nq, int64_t per_query_bytes,
                                  const uint8_t* __restrict__ stash, int64_t stash_count,
-                                 int64_t stash_entry) {
+                                 int64_t stash_entry, int64_t pstride) {
+    uint8_t* resp = resp_all + (int64_t)blockIdx.y * pstride;  // one payload per grid row
     auto put = [](uint8_t* p, uint32_t v) {
         p[0] = (uint8_t)v; p[1] = (uint8_t)(v >> 8); p[2] = (uint8_t)(v >> 16); p[3] = (uint8_t)(v >> 24);
     };
@@ -510,7 +525,13 @@ cudaError_t init_device_kernels() {
 
 cudaError_t launch_parse_query(const uint8_t* qb, int nq, int db_rows, uint64_t* y, uint64_t* z,
                                uint32_t* a_il, uint32_t* gsw, uint8_t* qbytes, int qbase, cudaStream_t st) {
-    k_parse_query<<<2 * 148, 256, 0, st>>>(qb, nq, db_rows, y, z, a_il, gsw, qbytes, qbase);
+    k_parse_query<<<2 * 148, 256, 0, st>>>(qb, nq, db_rows, y, z, a_il, gsw, qbytes, qbase, 1, 0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_parse_batch(const uint8_t* qb, int npay, int64_t pstride, int nq, int db_rows, uint64_t* y,
+                               uint64_t* z, uint32_t* gsw, uint8_t* qbytes, cudaStream_t st) {
+    k_parse_query<<<8 * 148, 256, 0, st>>>(qb, nq, db_rows, y, z, nullptr, gsw, qbytes, 0, npay, pstride);
     return cudaGetLastError();
 }
 
@@ -550,8 +571,9 @@ cudaError_t launch_fold_switch(const uint32_t* row0, const uint32_t* gsw, const 
 }
 
 cudaError_t launch_response_frame(uint8_t* resp, int nq, int64_t per_query, const uint8_t* stash,
-                                  int64_t stash_count, int64_t stash_entry, cudaStream_t st) {
-    k_response_frame<<<8, 256, 0, st>>>(resp, nq, per_query, stash, stash_count, stash_entry);
+                                  int64_t stash_count, int64_t stash_entry, cudaStream_t st, int npay,
+                                  int64_t pstride) {
+    k_response_frame<<<dim3(8, npay), 256, 0, st>>>(resp, nq, per_query, stash, stash_count, stash_entry, pstride);
     return cudaGetLastError();
 }
 

@@ -27,7 +27,21 @@ cudaError_t launch_fold_switch(const uint32_t* row0, const uint32_t* gsw, const 
                                int c_groups, int nq, int64_t db_cols, uint8_t* resp,
                                int64_t resp_query_stride, cudaStream_t st);
 cudaError_t launch_response_frame(uint8_t* resp, int nq, int64_t per_query, const uint8_t* stash,
-                                  int64_t stash_count, int64_t stash_entry, cudaStream_t st);
+                                  int64_t stash_count, int64_t stash_entry, cudaStream_t st, int npay = 1,
+                                  int64_t pstride = 0);
+// npay payloads of nq queries each, pstride bytes apart, into per-payload key / body slots
+cudaError_t launch_parse_batch(const uint8_t* qb, int npay, int64_t pstride, int nq, int db_rows, uint64_t* y,
+                               uint64_t* z, uint32_t* gsw, uint8_t* qbytes, cudaStream_t st);
+// batched packing on tcgen05 (pack_tc.cu)
+int pack_mma_nt(int clients);
+uint64_t tpp_bytes(int instances);
+cudaError_t init_pack_mma_kernel();
+cudaError_t launch_relayout_tpp(const uint64_t* bt, const uint64_t* btb, uint8_t* tpp, int instances,
+                                cudaStream_t st);
+cudaError_t launch_build_y8(const uint64_t* y_bodies, uint8_t* y8, int clients, int np, cudaStream_t st);
+cudaError_t launch_pack_mma(const CUtensorMap* tm_t, const CUtensorMap* tm_y, int instances, int clients, int np,
+                            const uint64_t* z_bodies, const uint64_t* bth, uint32_t* S, int* err_flag, int sm_count,
+                            cudaStream_t st);
 cudaError_t launch_rotations(const uint64_t* y_body, uint64_t* y_all, uint64_t* y_bar_all, int num_rotations,
                              cudaStream_t st);
 cudaError_t launch_pack_materialized(const uint64_t* bt, const uint64_t* btb, const uint64_t* bth,
@@ -46,5 +60,13 @@ cudaError_t launch_db_to_planes(const uint16_t* db, uint8_t* planes, int64_t n, 
 // nt: query-byte columns per tile (16..256, multiple of 16); db_rows <= 32768
 cudaError_t launch_gemm1(const CUtensorMap* tm_db, const CUtensorMap* tm_qb, int db_rows, int64_t db_cols, int nt,
                          int n_tiles, int num_queries, uint64_t* c, int* err_flag, int sm_count, cudaStream_t st);
+
+// register-resident-NTT fold + switch (fold.cu); queries grouped qpp per payload
+cudaError_t init_fold2_kernel();
+cudaError_t launch_fold2(const uint32_t* row0, const uint32_t* gsw, const uint64_t* a_hat, const uint64_t* R,
+                         int64_t r_payload_stride, const uint64_t* cvec, const uint32_t* fw, const uint32_t* fwp,
+                         const uint32_t* iw, const uint32_t* iwp, int interp, int c_groups, int num_queries,
+                         int64_t db_cols, int qpp, uint8_t* resp, int64_t resp_payload_stride,
+                         int64_t resp_query_stride, cudaStream_t st);
 
 }  // namespace ipr

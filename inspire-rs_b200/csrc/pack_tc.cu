@@ -1,0 +1,350 @@
+// pack_tc.cu — the InspiRING packing inner product for a batch of clients on
+// the 5th-generation tensor cores.
+//
+// For output j, NTT slot z, limb l (packing_online_kernel.cu:18-92 /
+// full_packing_with_preprocessing_online, src/pir/packing.rs:2941-3012):
+//   S[c][j][l][z] = sum_{i<1023,k<3} y_c[k][rot_i(z)] T[j][i,k][z] + y_c[k][rotbar_i(z)] Tbar[j][i,k][z]
+//                 + sum_k z_c[k][z] That[j][k][z]                          (mod q_l)
+// The rotated slots rot_i(z) = auto_src(5^i, z) and rotbar_i(z) = auto_src(2N - 5^i, z)
+// are distinct for every (i, kind) at a fixed z (5 generates a subgroup of the
+// odd residues mod 2N that excludes -1), so re-indexing the precomputation by
+// the slot it multiplies turns the client side into a z-independent matrix:
+//   S[c][j][l][z] = sum_{k, s} Y_l[c][k*N + s] * Tpp_{z,l}[j][k*N + s]   (+ the z_body term)
+//   Y_l[c][k*N + s]      = y_c[k][s] (limb l)
+//   Tpp_{z,l}[j][k*N+s]  = T[j][i,k][z] if s = rot_i(z), Tbar[j][i,k][z] if s = rotbar_i(z), else 0
+// Tpp is built once at setup.  Both operands are split into bytes (28-bit
+// residues = 4 bytes) so every term is a u8 x u8 product:
+//   S = sum_{a,b} 256^(a+b) P_ab,  P_ab = sum_K Y_l,a[c][K] * Tpp_{z,l},b[j][K]
+// with P_ab < 255^2 * 6144 < 2^29 exact in a 32-bit accumulator.
+//
+// GEMM per (z, l, tile of 32 outputs): M = 128 rows = 4 bytes b x 32 outputs,
+// N = 4 bytes a x clients (<= 256), K = 6144.  Persistent CTAs of 6 warps:
+// TMA producer, MMA issuer, 4 epilogue warps (the same pipeline as gemm_tc.cu).
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "ipr_device.cuh"
+#include "kernels.cuh"
+#include "umma.cuh"
+
+namespace ipr {
+
+namespace {
+
+constexpr int P_THREADS = 192;
+constexpr int P_TILE_M = 128;
+constexpr int P_TILE_K = 128;
+constexpr int P_K = 3 * N;  // 6144
+constexpr int P_A_STAGE = P_TILE_M * P_TILE_K;
+constexpr int P_MAX_STAGES = 8;
+
+struct PSmem {
+    uint64_t full[P_MAX_STAGES], empty[P_MAX_STAGES], acc_full[2], acc_empty[2];
+    uint32_t tmem_base;
+    int err;
+    int ep_fail;  // written only by the epilogue warps, read after their named barrier
+};
+
+__device__ __forceinline__ uint32_t pow5(uint32_t i) {  // 5^i mod 2N
+    uint32_t r = 1, b = 5;
+    while (i) {
+        if (i & 1) r = (r * b) & (2 * N - 1);
+        b = (b * b) & (2 * N - 1);
+        i >>= 1;
+    }
+    return r;
+}
+
+}  // namespace
+
+// Tpp rows ((z*2 + l)*mt_count + mt)*128 + b*32 + jl, columns k*N + s (zeroed beforehand)
+__global__ void k_relayout_tpp(const uint64_t* __restrict__ bt, const uint64_t* __restrict__ btb, uint8_t* __restrict__ tpp,
+                               int instances, int mt_count) {
+    const int64_t total = (int64_t)instances * 2 * NINNER * N;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int z = (int)(idx & (N - 1));
+        int64_t rest = idx >> LOGN;
+        const int rr = (int)(rest % NINNER);
+        rest /= NINNER;
+        const int kind = (int)(rest & 1);
+        const int j = (int)(rest >> 1);
+        const int i = rr / T_EXP, k = rr % T_EXP;
+        const uint32_t g = pow5((uint32_t)i);
+        const uint32_t s = auto_src(kind ? 2 * N - g : g, (uint32_t)z);
+        const uint64_t v = (kind ? btb : bt)[((int64_t)j * NINNER + rr) * N + z];
+        const int mt = j >> 5, jl = j & 31;
+#pragma unroll
+        for (int l = 0; l < 2; l++) {
+            const uint32_t limb = (uint32_t)(l ? (v >> 32) : v);
+            const int64_t row0 = (((int64_t)z * 2 + l) * mt_count + mt) * P_TILE_M + jl;
+#pragma unroll
+            for (int b = 0; b < 4; b++)
+                tpp[(row0 + b * 32) * P_K + k * N + s] = (uint8_t)(limb >> (8 * b));
+        }
+    }
+}
+
+// Y8[l][c*4 + a][k*N + s] = byte a of y_c[k][s] (limb l); rows c >= clients stay as zeroed
+__global__ void k_build_y8(const uint64_t* __restrict__ y_bodies, uint8_t* __restrict__ y8, int clients, int np) {
+    const int64_t total = (int64_t)clients * T_EXP * N;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int c = (int)(idx / (T_EXP * N));
+        const int ks = (int)(idx % (T_EXP * N));  // k*N + s
+        const uint64_t v = y_bodies[idx];
+#pragma unroll
+        for (int l = 0; l < 2; l++) {
+            const uint32_t limb = (uint32_t)(l ? (v >> 32) : v);
+#pragma unroll
+            for (int a = 0; a < 4; a++) y8[((int64_t)l * np + c * 4 + a) * P_K + ks] = (uint8_t)(limb >> (8 * a));
+        }
+    }
+}
+
+__global__ void __launch_bounds__(P_THREADS, 1)
+    k_pack_mma(const __grid_constant__ CUtensorMap tm_t, const __grid_constant__ CUtensorMap tm_y, int instances,
+               int mt_count, int clients, int np, int nt, int stages, const uint64_t* __restrict__ z_bodies,
+               const uint64_t* __restrict__ bth, uint32_t* __restrict__ S, int* __restrict__ err_flag) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* base = smem_raw + ((1024 - (umma::smem_addr(smem_raw) & 1023)) & 1023);
+    PSmem* sh = reinterpret_cast<PSmem*>(base);
+    volatile int* err = &sh->err;
+    uint8_t* a_tiles = base + 1024;
+    const int b_stage = nt * P_TILE_K;
+    uint8_t* b_tiles = a_tiles + stages * P_A_STAGE;
+    uint32_t* xch = reinterpret_cast<uint32_t*>(b_tiles + stages * b_stage);  // [clients][4][32]
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nbuf = (2 * nt <= 512) ? 2 : 1;
+    uint32_t ncols = 32;
+    while (ncols < (uint32_t)(nbuf * nt)) ncols <<= 1;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < stages; s++) {
+            umma::mbar_init(&sh->full[s], 1);
+            umma::mbar_init(&sh->empty[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            umma::mbar_init(&sh->acc_full[b], 1);
+            umma::mbar_init(&sh->acc_empty[b], 4);
+        }
+        *err = 0;
+        sh->ep_fail = 0;
+        umma::fence_mbar_init();
+    }
+    if (warp == 1) umma::tmem_alloc(&sh->tmem_base, ncols);
+    umma::fence_before();
+    __syncthreads();
+    umma::fence_after();
+    const uint32_t tmem = sh->tmem_base;
+    volatile int* ep_fail = &sh->ep_fail;
+
+    const int ks_total = P_K / P_TILE_K;  // 48
+    const int64_t total = (int64_t)2 * mt_count * N;  // units (l, mt, z), z fastest
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            int last_phase[P_MAX_STAGES];
+            for (int s = 0; s < P_MAX_STAGES; s++) last_phase[s] = -1;
+            for (int64_t u = blockIdx.x; u < total && !*err; u += gridDim.x) {
+                const int z = (int)(u & (N - 1));
+                const int lm = (int)(u >> LOGN);
+                const int l = lm / mt_count, mt = lm % mt_count;
+                const int arow = (int)(((int64_t)(z * 2 + l) * mt_count + mt) * P_TILE_M);
+                for (int ks = 0; ks < ks_total; ks++) {
+                    if (!umma::mbar_wait(&sh->empty[stage], phase ^ 1)) {
+                        *err = 11;
+                        break;
+                    }
+                    umma::mbar_expect_tx(&sh->full[stage], P_A_STAGE + b_stage);
+                    umma::tma_load_2d(a_tiles + stage * P_A_STAGE, &tm_t, ks * P_TILE_K, arow, &sh->full[stage]);
+                    umma::tma_load_2d(b_tiles + stage * b_stage, &tm_y, ks * P_TILE_K, l * np, &sh->full[stage]);
+                    last_phase[stage] = (int)phase;
+                    if (++stage == stages) {
+                        stage = 0;
+                        phase ^= 1;
+                    }
+                }
+            }
+            for (int s = 0; s < stages; s++)
+                if (last_phase[s] >= 0) umma::mbar_wait(&sh->full[s], (uint32_t)last_phase[s], 1u << 22);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = umma::idesc_u8(P_TILE_M, nt);
+            int stage = 0, buf = 0, last_stage = -1;
+            uint32_t phase = 0, acc_phase = 0, last_parity = 0;
+            for (int64_t u = blockIdx.x; u < total && !*err; u += gridDim.x) {
+                if (!umma::mbar_wait(&sh->acc_empty[buf], acc_phase ^ 1)) {
+                    *err = 12;
+                    break;
+                }
+                umma::fence_after();
+                bool ok = true;
+                const uint32_t d = tmem + (uint32_t)(buf * nt);
+                for (int ks = 0; ks < ks_total; ks++) {
+                    if (!umma::mbar_wait(&sh->full[stage], phase)) {
+                        *err = 13;
+                        ok = false;
+                        break;
+                    }
+                    umma::fence_after();
+                    const uint32_t sa = umma::smem_addr(a_tiles + stage * P_A_STAGE);
+                    const uint32_t sb = umma::smem_addr(b_tiles + stage * b_stage);
+#pragma unroll
+                    for (int k4 = 0; k4 < P_TILE_K / 32; k4++)
+                        umma::mma_u8(d, umma::desc_sw128(sa + 32 * k4), umma::desc_sw128(sb + 32 * k4), idesc,
+                                     (ks == 0 && k4 == 0) ? 0u : 1u);
+                    umma::commit(&sh->empty[stage]);
+                    last_stage = stage;
+                    last_parity = phase;
+                    if (++stage == stages) {
+                        stage = 0;
+                        phase ^= 1;
+                    }
+                }
+                if (!ok) break;
+                umma::commit(&sh->acc_full[buf]);
+                if (nbuf == 2) {
+                    buf ^= 1;
+                    if (buf == 0) acc_phase ^= 1;
+                } else {
+                    acc_phase ^= 1;
+                }
+            }
+            if (last_stage >= 0) umma::mbar_wait(&sh->empty[last_stage], last_parity, 1u << 22);
+        }
+    } else {
+        // epilogue: warp quarter b holds TMEM rows b*32 .. b*32+31 = byte b of outputs mt*32 + lane
+        const int b = warp & 3;
+        int buf = 0;
+        uint32_t acc_phase = 0;
+        for (int64_t u = blockIdx.x; u < total; u += gridDim.x) {
+            // the four epilogue warps leave together: the decision uses a flag only they write
+            if (!umma::mbar_wait(&sh->acc_full[buf], acc_phase) && lane == 0) *ep_fail = 1;
+            umma::named_bar(1, 128);
+            if (*ep_fail) {
+                if (threadIdx.x == 64) *err = 14;
+                break;
+            }
+            umma::fence_after();
+            const int z = (int)(u & (N - 1));
+            const int lm = (int)(u >> LOGN);
+            const int l = lm / mt_count, mt = lm % mt_count;
+            const uint32_t q = l ? Q1 : Q0;
+            const uint64_t br = l ? BR1 : BR0;
+            const uint32_t lane_off = (uint32_t)(b * 32) << 16;
+            for (int g = 0; g < nt / 16; g++) {
+                uint32_t d[16];
+                umma::tmem_ld16(tmem + lane_off + (uint32_t)(buf * nt + g * 16), d);
+                umma::tmem_wait_ld();
+#pragma unroll
+                for (int ci = 0; ci < 4; ci++) {
+                    const int c = g * 4 + ci;
+                    uint64_t v = 0;
+#pragma unroll
+                    for (int a = 0; a < 4; a++) v += (uint64_t)d[ci * 4 + a] << (8 * a);
+                    const uint32_t r = mod64(v, q, br);
+                    if (c < clients) xch[(c * 4 + b) * 32 + lane] = mod64((uint64_t)r << (8 * b), q, br);
+                }
+            }
+            umma::fence_before();
+            __syncwarp();
+            if (lane == 0) umma::mbar_arrive(&sh->acc_empty[buf]);  // TMEM buffer free for the next unit
+            umma::named_bar(1, 128);
+            // combine the 4 byte rows and add the z_body x That term; thread (b, lane) owns clients c = b mod 4
+            const int j = mt * 32 + lane;
+            if (j < instances) {
+                uint32_t th[T_EXP];
+#pragma unroll
+                for (int k = 0; k < T_EXP; k++) {
+                    const uint64_t tv = bth[((int64_t)j * T_EXP + k) * N + z];
+                    th[k] = (uint32_t)(l ? (tv >> 32) : tv);
+                }
+                for (int c = b; c < clients; c += 4) {
+                    uint64_t tot = (uint64_t)xch[(c * 4 + 0) * 32 + lane] + xch[(c * 4 + 1) * 32 + lane] +
+                                   xch[(c * 4 + 2) * 32 + lane] + xch[(c * 4 + 3) * 32 + lane];
+#pragma unroll
+                    for (int k = 0; k < T_EXP; k++) {
+                        const uint64_t zv = z_bodies[((int64_t)c * T_EXP + k) * N + z];
+                        tot += (uint64_t)(uint32_t)(l ? (zv >> 32) : zv) * th[k];
+                    }
+                    S[(((int64_t)c * instances + j) * 2 + l) * N + z] = mod64(tot, q, br);
+                }
+            }
+            umma::named_bar(1, 128);
+            if (nbuf == 2) {
+                buf ^= 1;
+                if (buf == 0) acc_phase ^= 1;
+            } else {
+                acc_phase ^= 1;
+            }
+        }
+    }
+    umma::fence_before();
+    __syncthreads();
+    if (warp == 1) umma::tmem_dealloc(tmem, ncols);
+    if (threadIdx.x == 0 && *err) atomicExch(err_flag, *err);
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+int pack_mma_nt(int clients) {
+    int n = (4 * clients + 15) / 16 * 16;
+    return n < 16 ? 16 : n;
+}
+
+int pack_mma_stages(int nt) {
+    const int per = P_A_STAGE + nt * P_TILE_K;
+    const int xch = 64 * 4 * 32 * 4;
+    int s = (200 * 1024 - xch) / per;
+    return s > P_MAX_STAGES ? P_MAX_STAGES : (s < 2 ? 2 : s);
+}
+
+size_t pack_mma_smem(int nt) {
+    return 2048 + (size_t)pack_mma_stages(nt) * (P_A_STAGE + nt * P_TILE_K) + (size_t)(nt / 4) * 4 * 32 * 4;
+}
+
+cudaError_t init_pack_mma_kernel() {
+    return cudaFuncSetAttribute(k_pack_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pack_mma_smem(256));
+}
+
+uint64_t tpp_bytes(int instances) {
+    const uint64_t mt = (uint64_t)(instances + 31) / 32;
+    return (uint64_t)N * 2 * mt * P_TILE_M * P_K;
+}
+
+cudaError_t launch_relayout_tpp(const uint64_t* bt, const uint64_t* btb, uint8_t* tpp, int instances,
+                                cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(tpp, 0, tpp_bytes(instances), st);
+    if (e != cudaSuccess) return e;
+    k_relayout_tpp<<<148 * 16, 256, 0, st>>>(bt, btb, tpp, instances, (instances + 31) / 32);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_build_y8(const uint64_t* y_bodies, uint8_t* y8, int clients, int np, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(y8, 0, (size_t)2 * np * P_K, st);
+    if (e != cudaSuccess) return e;
+    k_build_y8<<<148 * 4, 256, 0, st>>>(y_bodies, y8, clients, np);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack_mma(const CUtensorMap* tm_t, const CUtensorMap* tm_y, int instances, int clients, int np,
+                            const uint64_t* z_bodies, const uint64_t* bth, uint32_t* S, int* err_flag, int sm_count,
+                            cudaStream_t st) {
+    const int nt = pack_mma_nt(clients);
+    if (clients < 1 || clients > 64 || np < nt) return cudaErrorInvalidValue;
+    const int mt_count = (instances + 31) / 32;
+    const int stages = pack_mma_stages(nt);
+    k_pack_mma<<<sm_count, P_THREADS, pack_mma_smem(nt), st>>>(*tm_t, *tm_y, instances, mt_count, clients, np, nt,
+                                                                stages, z_bodies, bth, S, err_flag);
+    return cudaGetLastError();
+}
+
+}  // namespace ipr

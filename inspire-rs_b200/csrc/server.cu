@@ -10,6 +10,7 @@
 
 #include <cstdarg>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -64,6 +65,7 @@ struct ipr_server {
     uint8_t* d_db8 = nullptr;  // [2][db_cols][db_rows] byte planes for the tensor-core GEMM
     CUtensorMap tm_db;
     bool gemv_tc = false;      // first dimension on tcgen05 (db_rows <= 32768)
+    bool fold_regs = true;     // fold with register-resident NTTs (k_fold2) vs shared-memory NTTs
     std::map<int, CUtensorMap> tm_qb;  // per query-byte tile height
     uint64_t *d_ahat = nullptr, *d_bt = nullptr, *d_btb = nullptr, *d_bth = nullptr;
     uint8_t* d_stash = nullptr;
@@ -82,6 +84,18 @@ struct ipr_server {
     int* h_err = nullptr;
     std::map<unsigned, cudaGraphExec_t> graphs;
     std::mutex mu;
+    // batched path: precomputation re-indexed by slot (Tpp), batch scratch
+    uint8_t* d_tpp = nullptr;
+    CUtensorMap tm_tpp;
+    int bcap = 0, y8_np = 0;
+    uint8_t* d_bq = nullptr;
+    uint64_t *d_ybs = nullptr, *d_zbs = nullptr;
+    uint8_t* d_y8 = nullptr;
+    std::map<int, CUtensorMap> tm_y8;
+    uint32_t* d_bS = nullptr;
+    uint64_t* d_bR = nullptr;
+    uint8_t* d_bresp = nullptr;
+    uint8_t *h_bq = nullptr, *h_bresp = nullptr;
     // profiling
     bool profiling = false;
     std::vector<cudaEvent_t> events;  // kMaxProfileSlots * (IPR_NSTAGES + 1)
@@ -206,9 +220,15 @@ int enqueue(ipr_server* s, unsigned nq, const uint8_t* d_query, uint8_t* d_resp,
         rec(3);
         CU(ipr::launch_intt_crt(s->d_S, s->d_iw, s->d_iwp, s->d_R, (int)p.instances, st));
         rec(4);
-        CU(ipr::launch_fold_switch(s->d_row0, s->d_gsw, s->d_ahat, s->d_R, s->d_c, s->d_fw, s->d_fwp, s->d_iw,
-                                   s->d_iwp, (int)p.interp, (int)p.c, (int)nq, (int64_t)p.db_cols, d_resp + 8,
-                                   (int64_t)(4 + s->per_query_bytes()), st));
+        if (s->fold_regs) {
+            CU(ipr::launch_fold2(s->d_row0, s->d_gsw, s->d_ahat, s->d_R, 0, s->d_c, s->d_fw, s->d_fwp, s->d_iw,
+                                 s->d_iwp, (int)p.interp, (int)p.c, (int)nq, (int64_t)p.db_cols, (int)nq, d_resp, 0,
+                                 (int64_t)(4 + s->per_query_bytes()), st));
+        } else {
+            CU(ipr::launch_fold_switch(s->d_row0, s->d_gsw, s->d_ahat, s->d_R, s->d_c, s->d_fw, s->d_fwp, s->d_iw,
+                                       s->d_iwp, (int)p.interp, (int)p.c, (int)nq, (int64_t)p.db_cols, d_resp + 8,
+                                       (int64_t)(4 + s->per_query_bytes()), st));
+        }
     } else {
         rec(1); rec(2); rec(3); rec(4);
     }
@@ -239,6 +259,105 @@ int next_profile_slot(ipr_server* s) {
     if (!s->profiling) return -1;
     if (s->slots_used == kMaxProfileSlots && harvest_profile(s)) return -1;
     return s->slots_used++;
+}
+
+constexpr int kMaxBatch = 64;  // clients per tensor-core packing launch (N = 4 bytes x clients <= 256)
+
+// build the slot-indexed precomputation once (35.4 GB at 1M records)
+int ensure_tpp(ipr_server* s) {
+    if (s->d_tpp) return IPR_OK;
+    if (!s->gemv_tc) return fail(IPR_E_STATE, "batched respond needs the tensor-core first dimension (db_rows <= 32768)");
+    const uint64_t bytes = ipr::tpp_bytes((int)s->plan.instances);
+    size_t free_b = 0, total_b = 0;
+    CU(cudaMemGetInfo(&free_b, &total_b));
+    if (bytes + (1ull << 30) > free_b)
+        return fail(IPR_E_OOM, "batched packing needs %llu more bytes of HBM, %zu free", (unsigned long long)bytes, free_b);
+    int st = s->alloc(&s->d_tpp, bytes);
+    if (st) return st;
+    CU(ipr::launch_relayout_tpp(s->d_bt, s->d_btb, s->d_tpp, (int)s->plan.instances, s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    const uint64_t rows = bytes / (3 * kN);
+    CU(ipr::make_u8_tile_map(&s->tm_tpp, s->d_tpp, 3 * kN, rows, 128));
+    return IPR_OK;
+}
+
+int ensure_batch(ipr_server* s, int B) {
+    if (B <= s->bcap) return IPR_OK;
+    int st = ensure_tpp(s);
+    if (st) return st;
+    if ((st = ensure_scratch(s, 2 * (unsigned)B))) return st;
+    for (void* p : {(void*)s->d_bq, (void*)s->d_ybs, (void*)s->d_zbs, (void*)s->d_y8, (void*)s->d_bS, (void*)s->d_bR,
+                    (void*)s->d_bresp})
+        if (p) s->free_ptr(p);
+    if (s->h_bq) cudaFreeHost(s->h_bq);
+    if (s->h_bresp) cudaFreeHost(s->h_bresp);
+    s->h_bq = s->h_bresp = nullptr;
+    s->tm_y8.clear();
+    const uint64_t qb = ipr::query_bytes(s->plan.db_rows, 2), rb = s->response_bytes(2);
+    const uint64_t no = s->plan.instances;
+    s->y8_np = ipr::pack_mma_nt(B);
+    if ((st = s->alloc(&s->d_bq, (size_t)B * qb)) || (st = s->alloc(&s->d_ybs, (size_t)B * 3 * kN * 8)) ||
+        (st = s->alloc(&s->d_zbs, (size_t)B * 3 * kN * 8)) || (st = s->alloc(&s->d_y8, (size_t)2 * s->y8_np * 3 * kN)) ||
+        (st = s->alloc(&s->d_bS, (size_t)B * no * 2 * kN * 4)) || (st = s->alloc(&s->d_bR, (size_t)B * no * kN * 8)) ||
+        (st = s->alloc(&s->d_bresp, (size_t)B * rb)))
+        return st;
+    CU(cudaMallocHost(&s->h_bq, (size_t)B * qb));
+    CU(cudaMallocHost(&s->h_bresp, (size_t)B * rb));
+    s->bcap = B;
+    return IPR_OK;
+}
+
+int y8_map(ipr_server* s, int nt, const CUtensorMap** out) {
+    auto it = s->tm_y8.find(nt);
+    if (it == s->tm_y8.end()) {
+        CUtensorMap m;
+        CU(ipr::make_u8_tile_map(&m, s->d_y8, 3 * kN, 2 * (uint64_t)s->y8_np, (uint32_t)nt));
+        it = s->tm_y8.emplace(nt, m).first;
+    }
+    *out = &it->second;
+    return IPR_OK;
+}
+
+// B payloads of 2 queries each: queries at d_queries + p*qbytes, responses at d_resps + p*rbytes
+int enqueue_batch(ipr_server* s, int B, const uint8_t* d_queries, uint8_t* d_resps, int prof) {
+    cudaStream_t st = s->stream;
+    const ipr::Plan& p = s->plan;
+    auto rec = [&](int stage) {
+        if (prof >= 0) cudaEventRecord(s->events[(size_t)prof * (IPR_NSTAGES + 1) + stage], st);
+    };
+    const int64_t qb = (int64_t)ipr::query_bytes(p.db_rows, 2), rb = (int64_t)s->response_bytes(2);
+    const int nqt = 2 * B;
+    rec(0);
+    CU(ipr::launch_parse_batch(d_queries, B, qb, 2, (int)p.db_rows, s->d_ybs, s->d_zbs, s->d_gsw, s->d_qb, st));
+    rec(1);
+    {
+        const int nt = qb_tile((unsigned)nqt);
+        const CUtensorMap* tq;
+        int e = qb_map(s, nt, &tq);
+        if (e) return e;
+        CU(ipr::launch_gemm1(&s->tm_db, tq, (int)p.db_rows, (int64_t)p.db_cols, nt, (int)(qb_rows((unsigned)nqt) / nt),
+                             nqt, s->d_c, s->d_err, s->sm_count, st));
+    }
+    rec(2);
+    {
+        const int nt = ipr::pack_mma_nt(B);
+        const CUtensorMap* ty;
+        int e = y8_map(s, nt, &ty);
+        if (e) return e;
+        CU(ipr::launch_build_y8(s->d_ybs, s->d_y8, B, s->y8_np, st));
+        CU(ipr::launch_pack_mma(&s->tm_tpp, ty, (int)p.instances, B, s->y8_np, s->d_zbs, s->d_bth, s->d_bS, s->d_err,
+                                s->sm_count, st));
+    }
+    rec(3);
+    CU(ipr::launch_intt_crt(s->d_bS, s->d_iw, s->d_iwp, s->d_bR, (int)(B * p.instances), st));
+    rec(4);
+    CU(ipr::launch_fold2(s->d_row0, s->d_gsw, s->d_ahat, s->d_bR, (int64_t)(p.instances * kN), s->d_c, s->d_fw,
+                         s->d_fwp, s->d_iw, s->d_iwp, (int)p.interp, (int)p.c, nqt, (int64_t)p.db_cols, 2, d_resps, rb,
+                         (int64_t)(4 + s->per_query_bytes()), st));
+    CU(ipr::launch_response_frame(d_resps, 2, (int64_t)s->per_query_bytes(), s->d_stash, (int64_t)s->stash_count,
+                                  (int64_t)s->stash_entry, st, B, rb));
+    rec(5);
+    return IPR_OK;
 }
 
 int get_graph(ipr_server* s, unsigned nq, cudaGraphExec_t* out) {
@@ -301,6 +420,8 @@ int init_common(ipr_server* s, int device, const ipr_plan* plan) {
     CU(cudaStreamCreateWithPriority(&s->stream, cudaStreamNonBlocking, hi));
     CU(ipr::init_device_kernels());
     CU(ipr::init_gemm1_kernel());
+    CU(ipr::init_fold2_kernel());
+    CU(ipr::init_pack_mma_kernel());
     ipr::host_params_init(s->hp);
     CU(ipr::set_constants(s->hp.barrett, s->hp.q0_inv_mod_q1));
     int st;
@@ -486,6 +607,8 @@ void ipr_server_destroy(ipr_server* s) {
     if (s->h_query) cudaFreeHost(s->h_query);
     if (s->h_resp) cudaFreeHost(s->h_resp);
     if (s->h_err) cudaFreeHost(s->h_err);
+    if (s->h_bq) cudaFreeHost(s->h_bq);
+    if (s->h_bresp) cudaFreeHost(s->h_bresp);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -541,15 +664,65 @@ int ipr_server_respond_batch(ipr_server* s, int n, const uint8_t* const* queries
                              uint8_t* const* outs, const size_t* caps, size_t* out_lens, int* statuses) {
     if (!s || n < 0 || (n && (!queries || !lens || !outs || !caps))) return fail(IPR_E_ARGS, "null argument");
     std::lock_guard<std::mutex> lk(s->mu);
-    int worst = IPR_OK;
+    const uint64_t qb = ipr::query_bytes(s->plan.db_rows, 2), rb = s->response_bytes(2);
+    // payloads with the usual two cuckoo queries go through the tensor-core batch
+    // path, up to 64 at a time; anything else is answered one by one
+    std::vector<int> batchable, single;
     for (int i = 0; i < n; i++) {
-        size_t ol = 0;
-        int st = respond_locked(s, queries[i], lens[i], outs[i], caps[i], &ol);
+        const bool ok2 = queries[i] && lens[i] >= qb && queries[i][0] == 2 && outs[i] && caps[i] >= rb;
+        (ok2 && n >= 2 && s->gemv_tc ? batchable : single).push_back(i);
+    }
+    int worst = IPR_OK;
+    auto note = [&](int i, int st, size_t ol) {
         if (out_lens) out_lens[i] = ol;
         if (statuses) statuses[i] = st;
         if (st && !worst) worst = st;
+    };
+    for (size_t c0 = 0; c0 < batchable.size(); c0 += kMaxBatch) {
+        const int B = (int)std::min<size_t>(kMaxBatch, batchable.size() - c0);
+        int st = ensure_batch(s, B);
+        if (st == IPR_OK) {
+            CU(cudaSetDevice(s->device));
+            for (int b = 0; b < B; b++) std::memcpy(s->h_bq + (size_t)b * qb, queries[batchable[c0 + b]], qb);
+            CU(cudaMemsetAsync(s->d_err, 0, sizeof(int), s->stream));
+            CU(cudaMemcpyAsync(s->d_bq, s->h_bq, (size_t)B * qb, cudaMemcpyHostToDevice, s->stream));
+            st = enqueue_batch(s, B, s->d_bq, s->d_bresp, next_profile_slot(s));
+            if (st == IPR_OK) {
+                CU(cudaMemcpyAsync(s->h_bresp, s->d_bresp, (size_t)B * rb, cudaMemcpyDeviceToHost, s->stream));
+                CU(cudaMemcpyAsync(s->h_err, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+                CU(cudaStreamSynchronize(s->stream));
+                if (*s->h_err) st = fail(IPR_E_TIMEOUT, "a device-side wait ran out (code %d)", *s->h_err);
+            }
+        }
+        for (int b = 0; b < B; b++) {
+            const int i = batchable[c0 + b];
+            if (st == IPR_OK) std::memcpy(outs[i], s->h_bresp + (size_t)b * rb, rb);
+            note(i, st, rb);
+        }
+    }
+    for (int i : single) {
+        size_t ol = 0;
+        int st = respond_locked(s, queries[i], lens[i], outs[i], caps[i], &ol);
+        note(i, st, ol);
     }
     return worst;
+}
+
+int ipr_server_prepare_batch(ipr_server* s, int max_payloads) {
+    if (!s || max_payloads < 1) return fail(IPR_E_ARGS, "bad argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    CU(cudaSetDevice(s->device));
+    return ensure_batch(s, max_payloads < kMaxBatch ? max_payloads : kMaxBatch);
+}
+
+int ipr_server_respond_batch_device(ipr_server* s, int n, const uint8_t* d_queries, uint8_t* d_out) {
+    if (!s || !d_queries || !d_out || n < 1 || n > kMaxBatch) return fail(IPR_E_ARGS, "bad argument (1 <= n <= 64)");
+    std::lock_guard<std::mutex> lk(s->mu);
+    CU(cudaSetDevice(s->device));
+    int st = ensure_batch(s, n);
+    if (st) return st;
+    CU(cudaMemsetAsync(s->d_err, 0, sizeof(int), s->stream));
+    return enqueue_batch(s, n, d_queries, d_out, next_profile_slot(s));
 }
 
 int ipr_server_respond_device(ipr_server* s, const uint8_t* d_query, size_t len, uint8_t* d_out, size_t cap,
@@ -594,6 +767,10 @@ int ipr_server_set_option(ipr_server* s, int option, int64_t value) {
             if (value && !(s->plan.db_rows <= 32768 && s->plan.db_rows % 128 == 0))
                 return fail(IPR_E_ARGS, "tensor-core first dimension needs db_rows <= 32768, a multiple of 128");
             s->gemv_tc = value != 0;
+            destroy_graphs(s);
+            return IPR_OK;
+        case IPR_OPT_FOLD_REGISTER_NTT:
+            s->fold_regs = value != 0;
             destroy_graphs(s);
             return IPR_OK;
         default:

@@ -89,6 +89,19 @@ def test_first_dimension_paths(cfg0, pkg, orc, tensor, nq):
         srv.set_option(pkg.KeywordServer.OPT_TENSOR_GEMV, 1)
 
 
+@pytest.mark.parametrize("regs", [0, 1])
+@pytest.mark.parametrize("instances,interp", [(8, 8), (8, 1), (6, 2)])
+def test_fold_kernels(pkg, orc, regs, instances, interp):
+    """register-resident-NTT fold and shared-memory fold give the oracle's bytes"""
+    plan = _plan(pkg, instances, interp)
+    with pkg.KeywordServer.synthetic(plan, seed=50 + instances + interp) as srv:
+        srv.set_option(pkg.KeywordServer.OPT_FOLD_REGISTER_NTT, regs)
+        sdb = orc.SynthDB(plan.db_rows, instances, interp, plan.c, seed=50 + instances + interp)
+        for nq in (1, 2, 3):
+            q = orc.synth_query(60 + nq, plan.db_rows, nq)
+            assert srv.respond_to_serialized_query(q) == orc.respond(sdb, q)
+
+
 def test_first_dimension_tensor_wide_rows(pkg, orc):
     plan = _plan(pkg, 2, 2, db_rows=16384)
     with pkg.KeywordServer.synthetic(plan, seed=21) as srv:
@@ -224,3 +237,59 @@ def test_compat_rotation_and_packing(cfg0, orc):
     assert np.array_equal(out.reshape(sdb.instances, 2, N), orc.packing_sum(sdb, y, z))
     lib.gpu_packing_online_free()
     lib.gpu_rotation_free()
+
+
+# ---------------------------------------------------------------------------
+# batched respond: tensor-core packing of many clients at once
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("B", [2, 3, 8, 17])
+def test_respond_batch_bit_exact(cfg0, orc, B):
+    plan, srv, sdb = cfg0
+    qs = [orc.synth_query(1000 + 7 * B + i, plan.db_rows, 2) for i in range(B)]
+    got = srv.respond_batch(qs)
+    assert len(got) == B
+    for q, g in zip(qs, got):
+        assert g == orc.respond(sdb, q)
+
+
+def test_respond_batch_matches_single(cfg0, orc):
+    plan, srv, sdb = cfg0
+    qs = [orc.synth_query(2000 + i, plan.db_rows, 2) for i in range(5)]
+    single = [srv.respond_to_serialized_query(q) for q in qs]
+    assert srv.respond_batch(qs) == single
+
+
+def test_respond_batch_mixed_query_counts(cfg0, orc):
+    plan, srv, sdb = cfg0
+    qs = [orc.synth_query(3000, plan.db_rows, 2), orc.synth_query(3001, plan.db_rows, 1),
+          orc.synth_query(3002, plan.db_rows, 2), orc.synth_query(3003, plan.db_rows, 3)]
+    got = srv.respond_batch(qs)
+    for q, g in zip(qs, got):
+        assert g == orc.respond(sdb, q)
+
+
+@pytest.mark.parametrize("instances,interp", [(8, 2), (40, 8)])
+def test_respond_batch_other_shapes(pkg, orc, instances, interp):
+    plan = _plan(pkg, instances, interp)
+    stash = [b"\x07" * 100, b"\x09" * 100]
+    sdb = orc.SynthDB(plan.db_rows, instances, interp, plan.c, seed=90 + instances, stash=stash)
+    with pkg.KeywordServer.from_encoded(plan, sdb.db, sdb.a_hat, sdb.bold_t, sdb.bold_t_bar, sdb.bold_t_hat,
+                                        stash=stash) as srv:
+        qs = [orc.synth_query(4000 + i, plan.db_rows, 2) for i in range(6)]
+        got = srv.respond_batch(qs)
+        for q, g in zip(qs, got):
+            assert g == orc.respond(sdb, q)
+
+
+def test_respond_batch_device_entry(cfg0, orc):
+    import torch
+    plan, srv, sdb = cfg0
+    qs = [orc.synth_query(5000 + i, plan.db_rows, 2) for i in range(4)]
+    dq = torch.frombuffer(bytearray(b"".join(qs)), dtype=torch.uint8).cuda()
+    rb = srv.response_bytes(2)
+    dout = torch.zeros(4 * rb, dtype=torch.uint8, device="cuda")
+    srv.respond_batch_device(4, dq.data_ptr(), dout.data_ptr())
+    srv.sync()
+    host = bytes(dout.cpu().numpy())
+    for i, q in enumerate(qs):
+        assert host[i * rb:(i + 1) * rb] == orc.respond(sdb, q)
