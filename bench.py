@@ -5,14 +5,16 @@ Workload: 1,000,000 ML-KEM-768 records (32-byte IDs + 1184-byte keys), cuckoo
 buckets 2^21 (the reference default for 1M records; 262,144 is rejected by the
 reference because buckets < records), dim0 = 2048 -> DB 2048 x 720,896 u16,
 352 packing outputs, interpolation degree 32, 11 fold groups.  One step = one
-respond() of one KeywordQueryPayload (2 cuckoo sub-queries), batch 1, u64
-modular arithmetic.  Server state is seeded synthetic data of the reference's
+batch of B (default 64) KeywordQueryPayloads (2 cuckoo sub-queries each) from
+B distinct clients, answered together on the INT8-limb tensor-core path;
+`--batch 1` times the batch-1 path.  The same run also times the plain batch-1
+u64 path (CUDA-core GEMV and packing) on the same GPU.  Server state is seeded synthetic data of the reference's
 shapes (the reference's own timing mode, engine.rs:693-729); queries are
 seeded synthetic payloads.
 
-  value : payloads/s with queries resident in HBM (ipr_server_respond_device)
-  e2e   : payloads/s through ipr_server_respond with host buffers (H2D query,
-          D2H response inside the timed region)
+  value : payloads/s with queries resident in HBM (ipr_server_respond_batch_device)
+  e2e   : payloads/s through ipr_server_respond_batch with host buffers (H2D
+          queries, D2H responses inside the timed region)
 
 --impl reference times the CPU restatement of the reference's respond() on the
 host cores (the reference's Rust CPU path cannot be built here).
@@ -30,7 +32,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 
 RECORDS, KEY, VALUE, BUCKETS, DIM0 = 1_000_000, 32, 1184, 2_097_152, 2048
 N = 2048
-METRIC = "queries/s at 1M ML-KEM-768 keys (batch-1 u64 respond, bit-exact)"
+METRIC = "queries/s at 1M ML-KEM-768 keys, batch-64 INT8-limb vs batch-1 u64, bit-exact"
 UNIT = "payloads/s"
 
 
@@ -114,9 +116,9 @@ def read_peaks():
         return 6650.0, "fallback"
 
 
-def read_traffic():
-    """dram bytes per k_pack launch from the committed ncu summary (scaled to the full launch), or None"""
-    path = os.path.join(ROOT, "profiles", "k_pack_1M_dram.md")
+def read_traffic(kernel="k_pack"):
+    """dram bytes per launch of `kernel` from its committed ncu summary (scaled to the full launch), or None"""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_1M_dram.md")
     try:
         for ln in open(path):
             if ln.startswith("traffic_bytes_per_full_launch:"):
@@ -166,6 +168,8 @@ def main():
     ap.add_argument("--records", type=int, default=RECORDS, help="workload override (profiling small cases)")
     ap.add_argument("--buckets", type=int, default=None)
     ap.add_argument("--dim0", type=int, default=None)
+    ap.add_argument("--batch", type=int, default=64, help="payloads per step (1 = batch-1 u64 packing path)")
+    ap.add_argument("--no-batch1", action="store_true", help="skip the batch-1 comparison measurement")
     args = ap.parse_args()
     small = args.records != RECORDS
 
@@ -214,8 +218,6 @@ def main():
     qbytes = srv.query_bytes(2)
     rbytes = srv.response_bytes(2)
 
-    # distinct seeded payloads, resident in HBM for the device-timed loop
-    nq_distinct = 4
     import numpy as np
 
     def synth_payload(seed):
@@ -227,21 +229,40 @@ def main():
         v = (lo | (hi << np.uint64(28))).astype("<u8")
         return bytes([2]) + v.view(np.uint8).reshape(-1, 8)[:, :7].tobytes()
 
-    payloads = [synth_payload(1000 * rank + i) for i in range(nq_distinct)]
+    B = max(1, args.batch)
+    npay = max(2 * B, 4)
+    payloads = [synth_payload(1000 * rank + i) for i in range(npay)]
     assert len(payloads[0]) == qbytes
-    d_q = [torch.frombuffer(bytearray(p), dtype=torch.uint8).to(dev) for p in payloads]
-    d_out = torch.empty(rbytes, dtype=torch.uint8, device=dev)
     stream = torch.cuda.ExternalStream(srv.stream_handle(), device=dev)
+    # HBM-resident inputs: two distinct batches of B payloads, alternated
+    d_batches = [torch.frombuffer(bytearray(b"".join(payloads[k * B:(k + 1) * B])), dtype=torch.uint8).to(dev)
+                 for k in range(2)]
+    d_out = torch.empty(B * rbytes, dtype=torch.uint8, device=dev)
+    if B > 1:
+        srv.prepare_batch(B)
+
+    def run_device(i):
+        d = d_batches[i % 2]
+        if B > 1:
+            srv.respond_batch_device(B, d.data_ptr(), d_out.data_ptr())
+        else:
+            srv.respond_device(d.data_ptr(), qbytes, d_out.data_ptr(), rbytes)
+
+    def run_host(i):
+        batch = payloads[(i % 2) * B:(i % 2 + 1) * B]
+        if B > 1:
+            srv.respond_batch(batch)
+        else:
+            srv.respond_to_serialized_query(batch[0])
 
     def barrier():
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
 
-    # warmup (device path and host path)
     for i in range(args.warmup):
-        srv.respond_device(d_q[i % nq_distinct].data_ptr(), qbytes, d_out.data_ptr(), rbytes)
-        srv.respond_to_serialized_query(payloads[i % nq_distinct])
+        run_device(i)
+        run_host(i)
     srv.sync()
 
     # ---- device-resident timed region -------------------------------------------------
@@ -252,7 +273,7 @@ def main():
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for i in range(args.steps):
-        srv.respond_device(d_q[i % nq_distinct].data_ptr(), qbytes, d_out.data_ptr(), rbytes)
+        run_device(i)
     e1.record(stream)
     srv.sync()
     barrier()
@@ -267,25 +288,49 @@ def main():
     h0.record(stream)
     t0 = time.perf_counter()
     for i in range(args.steps):
-        srv.respond_to_serialized_query(payloads[i % nq_distinct])
+        run_host(i)
     h1.record(stream)
     srv.sync()
     wall_ms = (time.perf_counter() - t0) * 1000
     barrier()
-    e2e_ms = max(h0.elapsed_time(h1), 0.0)
-    e2e_ms = max(e2e_ms, wall_ms)
+    e2e_ms = max(h0.elapsed_time(h1), wall_ms)
+
+    # ---- the plain batch-1 u64 path on the same GPU (CUDA-core GEMV + packing) ----------
+    b1 = {}
+    if B > 1 and not args.no_batch1:
+        d1 = torch.frombuffer(bytearray(payloads[0]), dtype=torch.uint8).to(dev)
+        d1o = torch.empty(rbytes, dtype=torch.uint8, device=dev)
+        for mode, tc in (("u64", 0), ("tensor_gemv", 1)):
+            srv.set_option(pkg.KeywordServer.OPT_TENSOR_GEMV, tc)
+            for _ in range(2):
+                srv.respond_device(d1.data_ptr(), qbytes, d1o.data_ptr(), rbytes)
+            srv.sync()
+            k1 = max(5, min(args.steps, 20))
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            for _ in range(k1):
+                srv.respond_device(d1.data_ptr(), qbytes, d1o.data_ptr(), rbytes)
+            a1.record(stream)
+            srv.sync()
+            b1[mode] = k1 / (a0.elapsed_time(a1) / 1000.0)
+        srv.set_option(pkg.KeywordServer.OPT_TENSOR_GEMV, 1)
 
     t = torch.tensor([dev_ms, e2e_ms], dtype=torch.float64, device=dev)
     if dist is not None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     dev_ms, e2e_ms = float(t[0]), float(t[1])
-    total = args.steps * world
+    total = args.steps * B * world
     value = total / (dev_ms / 1000.0)
     e2e = total / (e2e_ms / 1000.0)
 
-    pack_ms = stage_ms["pack"] / max(calls, 1)
-    pack_bytes = plan.instances * (2 * 3069 + 3) * N * 8  # bold_t + bold_t_bar + bold_t_hat per launch
     peak, peak_kind = read_peaks()
+    pack_ms = stage_ms["pack"] / max(calls, 1)
+    if B > 1:  # k_pack_mma streams the slot-indexed precomputation once per batch
+        pack_bytes = N * 2 * ((plan.instances + 31) // 32) * 128 * 3 * N  # [slot][limb][tile][128 rows][6144]
+        kname = "k_pack_mma"
+    else:
+        pack_bytes = plan.instances * (2 * 3069 + 3) * N * 8  # bold_t + bold_t_bar + bold_t_hat per launch
+        kname = "k_pack"
     achieved = pack_bytes / (pack_ms / 1000.0) / 1e9
 
     out = None
@@ -297,23 +342,27 @@ def main():
             except Exception as ex:  # reported, never fatal to the GPU number
                 cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "port", "sample": f"failed: {ex}"}
         stage_avg = {k: round(v / max(calls, 1), 4) for k, v in stage_ms.items()}
+        wl = (f"1M ML-KEM-768 respond(), buckets 2^21, dim0 2048, 2 queries/payload, batch {B}"
+              + (" (INT8-limb tcgen05 GEMMs)" if B > 1 else " (u64 packing)"))
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": ("1M ML-KEM-768 respond(), buckets 2^21, dim0 2048, 2 queries/payload, batch 1"
-                                    if not small else f"{args.records} ML-KEM-768 records (profiling case)"),
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8 limbs -> s32 / u64" if B > 1 else "u64",
+            "data": "synthetic",
+            "config": {"workload": wl if not small else f"{args.records} ML-KEM-768 records (profiling case)",
                        "records": args.records, "buckets": plan.num_items, "dim0": plan.dim0, "db_rows": plan.db_rows,
                        "db_cols": plan.db_cols, "instances": plan.instances, "interp": plan.interp, "c": plan.c,
-                       "parallelism": f"replica x{world}",
+                       "batch_payloads": B, "parallelism": f"replica x{world}",
                        "l2": "inputs larger than L2 (packing stream of %.1f GB + DB of %.2f GB per step)" % (
-                           plan.instances * 6141 * N * 8 / 1e9, plan.db_rows * plan.db_cols * 2 / 1e9)},
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": qbytes, "d2h_bytes_per_step": rbytes},
-            "roofline": {"bound": "hbm", "kernel": "k_pack", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                           pack_bytes / 1e9, plan.db_rows * plan.db_cols * 2 / 1e9)},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": B * qbytes, "d2h_bytes_per_step": B * rbytes},
+            "batch1": ({"u64_payloads_per_s": b1["u64"], "tensor_gemv_payloads_per_s": b1["tensor_gemv"],
+                        "speedup_vs_batch1_u64": value / world / b1["u64"]} if b1 else None),
+            "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                         "traffic": read_traffic(), "algorithmic_bytes": pack_bytes, "avg_launch_ms": pack_ms},
+                         "traffic": read_traffic(kname), "algorithmic_bytes": pack_bytes, "avg_launch_ms": pack_ms},
             "stage_ms": stage_avg,
-            "gpu_launches": 6 * args.steps,
+            "gpu_launches": (7 if B > 1 else 6) * args.steps,
             "clocks": clk,
             "cpu_baseline": cpu,
         }

@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(F_THREADS, 1)
 #pragma unroll
             for (int m = 0; m < EPT; m++) {
                 acc0[m] += v[m];  // < 6q
-                acc1[m] += (uint64_t)__ldg(bp + eB(t, m)) * v[m];
+                acc1[m] += (uint64_t)__ldg(bp + eB(t, m)) * v[m];  // 6 terms < 2^59
             }
         }
         uint32_t p0[EPT], p1[EPT];

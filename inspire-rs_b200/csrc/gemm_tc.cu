@@ -272,7 +272,9 @@ int gemm1_stages(int nt) {
 size_t gemm1_smem_bytes(int nt) { return 2048 + (size_t)gemm1_stages(nt) * (A_STAGE_BYTES + nt * TILE_K); }
 
 cudaError_t init_gemm1_kernel() {
-    return cudaFuncSetAttribute(k_gemm1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm1_smem_bytes(256));
+    size_t mx = 0;  // the largest footprint over every tile height the launcher can pick
+    for (int nt = 16; nt <= 256; nt += 16) mx = gemm1_smem_bytes(nt) > mx ? gemm1_smem_bytes(nt) : mx;
+    return cudaFuncSetAttribute(k_gemm1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
 }
 
 cudaError_t launch_db_to_planes(const uint16_t* db, uint8_t* planes, int64_t n, cudaStream_t st) {

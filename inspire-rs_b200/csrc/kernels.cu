@@ -262,10 +262,27 @@ __global__ void __launch_bounds__(PACK_THREADS) k_pack(const uint64_t* __restric
 __global__ void __launch_bounds__(512) k_intt_crt(const uint32_t* __restrict__ S,
                                                   const uint32_t* __restrict__ iw,
                                                   const uint32_t* __restrict__ iwp,
-                                                  uint64_t* __restrict__ R) {
+                                                  uint64_t* __restrict__ R,
+                                                  const uint64_t* __restrict__ z_bodies,
+                                                  const uint64_t* __restrict__ bth, int instances) {
     __shared__ uint32_t sm[2 * N];
     const int j = blockIdx.x;
-    for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) sm[i] = S[(int64_t)j * 2 * N + i];
+    if (z_bodies) {  // + sum_k z_c[k][z] That[j'][k][z] per limb (packing_online_kernel.cu:76-83)
+        const int c = j / instances, jj = j % instances;
+        for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) {
+            const int l = i >> LOGN, z = i & (N - 1);
+            uint64_t acc = S[(int64_t)j * 2 * N + i];
+#pragma unroll
+            for (int k = 0; k < T_EXP; k++) {
+                const uint64_t zv = z_bodies[((int64_t)c * T_EXP + k) * N + z];
+                const uint64_t tv = bth[((int64_t)jj * T_EXP + k) * N + z];
+                acc += (uint64_t)(uint32_t)(l ? zv >> 32 : zv) * (uint32_t)(l ? tv >> 32 : tv);
+            }
+            sm[i] = modq(acc, l);
+        }
+    } else {
+        for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) sm[i] = S[(int64_t)j * 2 * N + i];
+    }
     __syncthreads();
     ntt_inverse_smem<2>(sm, iw, iwp, [](int p) { return p; });
     for (int z = threadIdx.x; z < N; z += blockDim.x)
@@ -553,8 +570,9 @@ cudaError_t launch_pack(const uint64_t* bt, const uint64_t* btb, const uint64_t*
 }
 
 cudaError_t launch_intt_crt(const uint32_t* S, const uint32_t* iw, const uint32_t* iwp, uint64_t* R,
-                            int num_outputs, cudaStream_t st) {
-    k_intt_crt<<<num_outputs, 512, 0, st>>>(S, iw, iwp, R);
+                            int num_outputs, cudaStream_t st, const uint64_t* z_bodies, const uint64_t* bth,
+                            int instances) {
+    k_intt_crt<<<num_outputs, 512, 0, st>>>(S, iw, iwp, R, z_bodies, bth, instances);
     return cudaGetLastError();
 }
 

@@ -19,8 +19,11 @@ cudaError_t launch_gemv(const uint16_t* db, int db_rows, int64_t db_cols, int nq
                         uint64_t* c, int sm_count, cudaStream_t st);
 cudaError_t launch_pack(const uint64_t* bt, const uint64_t* btb, const uint64_t* bth, const uint64_t* y,
                         const uint64_t* z, uint32_t* S, int num_outputs, cudaStream_t st);
+// R = from_ntt(S) per (client, output) polynomial pair; with z_bodies non-null the
+// z_body x That term of client f / instances is added to S first
 cudaError_t launch_intt_crt(const uint32_t* S, const uint32_t* iw, const uint32_t* iwp, uint64_t* R,
-                            int num_outputs, cudaStream_t st);
+                            int num_outputs, cudaStream_t st, const uint64_t* z_bodies = nullptr,
+                            const uint64_t* bth = nullptr, int instances = 1);
 cudaError_t launch_fold_switch(const uint32_t* row0, const uint32_t* gsw, const uint64_t* a_hat,
                                const uint64_t* R, const uint64_t* cvec, const uint32_t* fw,
                                const uint32_t* fwp, const uint32_t* iw, const uint32_t* iwp, int interp,
@@ -39,9 +42,9 @@ cudaError_t init_pack_mma_kernel();
 cudaError_t launch_relayout_tpp(const uint64_t* bt, const uint64_t* btb, uint8_t* tpp, int instances,
                                 cudaStream_t st);
 cudaError_t launch_build_y8(const uint64_t* y_bodies, uint8_t* y8, int clients, int np, cudaStream_t st);
+// S[c][j][l][z] without the z_body x That term (added by launch_intt_crt when given z_bodies)
 cudaError_t launch_pack_mma(const CUtensorMap* tm_t, const CUtensorMap* tm_y, int instances, int clients, int np,
-                            const uint64_t* z_bodies, const uint64_t* bth, uint32_t* S, int* err_flag, int sm_count,
-                            cudaStream_t st);
+                            uint32_t* S, int* err_flag, int sm_count, cudaStream_t st);
 cudaError_t launch_rotations(const uint64_t* y_body, uint64_t* y_all, uint64_t* y_bar_all, int num_rotations,
                              cudaStream_t st);
 cudaError_t launch_pack_materialized(const uint64_t* bt, const uint64_t* btb, const uint64_t* bth,

@@ -9,7 +9,8 @@
 // are distinct for every (i, kind) at a fixed z (5 generates a subgroup of the
 // odd residues mod 2N that excludes -1), so re-indexing the precomputation by
 // the slot it multiplies turns the client side into a z-independent matrix:
-//   S[c][j][l][z] = sum_{k, s} Y_l[c][k*N + s] * Tpp_{z,l}[j][k*N + s]   (+ the z_body term)
+//   S[c][j][l][z] = sum_{k, s} Y_l[c][k*N + s] * Tpp_{z,l}[j][k*N + s]   (+ the z_body term,
+//                   which k_intt_crt adds before its inverse NTT)
 //   Y_l[c][k*N + s]      = y_c[k][s] (limb l)
 //   Tpp_{z,l}[j][k*N+s]  = T[j][i,k][z] if s = rot_i(z), Tbar[j][i,k][z] if s = rotbar_i(z), else 0
 // Tpp is built once at setup.  Both operands are split into bytes (28-bit
@@ -106,8 +107,8 @@ __global__ void k_build_y8(const uint64_t* __restrict__ y_bodies, uint8_t* __res
 
 __global__ void __launch_bounds__(P_THREADS, 1)
     k_pack_mma(const __grid_constant__ CUtensorMap tm_t, const __grid_constant__ CUtensorMap tm_y, int instances,
-               int mt_count, int clients, int np, int nt, int stages, const uint64_t* __restrict__ z_bodies,
-               const uint64_t* __restrict__ bth, uint32_t* __restrict__ S, int* __restrict__ err_flag) {
+               int mt_count, int clients, int np, int nt, int stages, uint32_t* __restrict__ S,
+               int* __restrict__ err_flag) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* base = smem_raw + ((1024 - (umma::smem_addr(smem_raw) & 1023)) & 1023);
     PSmem* sh = reinterpret_cast<PSmem*>(base);
@@ -257,23 +258,13 @@ __global__ void __launch_bounds__(P_THREADS, 1)
             __syncwarp();
             if (lane == 0) umma::mbar_arrive(&sh->acc_empty[buf]);  // TMEM buffer free for the next unit
             umma::named_bar(1, 128);
-            // combine the 4 byte rows and add the z_body x That term; thread (b, lane) owns clients c = b mod 4
+            // combine the 4 byte rows; thread (b, lane) owns clients c = b mod 4.  The z_body x That
+            // term is added by the inverse-NTT kernel that consumes S.
             const int j = mt * 32 + lane;
             if (j < instances) {
-                uint32_t th[T_EXP];
-#pragma unroll
-                for (int k = 0; k < T_EXP; k++) {
-                    const uint64_t tv = bth[((int64_t)j * T_EXP + k) * N + z];
-                    th[k] = (uint32_t)(l ? (tv >> 32) : tv);
-                }
                 for (int c = b; c < clients; c += 4) {
-                    uint64_t tot = (uint64_t)xch[(c * 4 + 0) * 32 + lane] + xch[(c * 4 + 1) * 32 + lane] +
-                                   xch[(c * 4 + 2) * 32 + lane] + xch[(c * 4 + 3) * 32 + lane];
-#pragma unroll
-                    for (int k = 0; k < T_EXP; k++) {
-                        const uint64_t zv = z_bodies[((int64_t)c * T_EXP + k) * N + z];
-                        tot += (uint64_t)(uint32_t)(l ? (zv >> 32) : zv) * th[k];
-                    }
+                    const uint64_t tot = (uint64_t)xch[(c * 4 + 0) * 32 + lane] + xch[(c * 4 + 1) * 32 + lane] +
+                                         xch[(c * 4 + 2) * 32 + lane] + xch[(c * 4 + 3) * 32 + lane];
                     S[(((int64_t)c * instances + j) * 2 + l) * N + z] = mod64(tot, q, br);
                 }
             }
@@ -312,7 +303,9 @@ size_t pack_mma_smem(int nt) {
 }
 
 cudaError_t init_pack_mma_kernel() {
-    return cudaFuncSetAttribute(k_pack_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pack_mma_smem(256));
+    size_t mx = 0;  // the largest footprint over every client count the launcher can pick
+    for (int nt = 16; nt <= 256; nt += 16) mx = pack_mma_smem(nt) > mx ? pack_mma_smem(nt) : mx;
+    return cudaFuncSetAttribute(k_pack_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
 }
 
 uint64_t tpp_bytes(int instances) {
@@ -336,14 +329,13 @@ cudaError_t launch_build_y8(const uint64_t* y_bodies, uint8_t* y8, int clients, 
 }
 
 cudaError_t launch_pack_mma(const CUtensorMap* tm_t, const CUtensorMap* tm_y, int instances, int clients, int np,
-                            const uint64_t* z_bodies, const uint64_t* bth, uint32_t* S, int* err_flag, int sm_count,
-                            cudaStream_t st) {
+                            uint32_t* S, int* err_flag, int sm_count, cudaStream_t st) {
     const int nt = pack_mma_nt(clients);
     if (clients < 1 || clients > 64 || np < nt) return cudaErrorInvalidValue;
     const int mt_count = (instances + 31) / 32;
     const int stages = pack_mma_stages(nt);
     k_pack_mma<<<sm_count, P_THREADS, pack_mma_smem(nt), st>>>(*tm_t, *tm_y, instances, mt_count, clients, np, nt,
-                                                                stages, z_bodies, bth, S, err_flag);
+                                                                stages, S, err_flag);
     return cudaGetLastError();
 }
 

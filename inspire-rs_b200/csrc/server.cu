@@ -345,11 +345,11 @@ int enqueue_batch(ipr_server* s, int B, const uint8_t* d_queries, uint8_t* d_res
         int e = y8_map(s, nt, &ty);
         if (e) return e;
         CU(ipr::launch_build_y8(s->d_ybs, s->d_y8, B, s->y8_np, st));
-        CU(ipr::launch_pack_mma(&s->tm_tpp, ty, (int)p.instances, B, s->y8_np, s->d_zbs, s->d_bth, s->d_bS, s->d_err,
-                                s->sm_count, st));
+        CU(ipr::launch_pack_mma(&s->tm_tpp, ty, (int)p.instances, B, s->y8_np, s->d_bS, s->d_err, s->sm_count, st));
     }
     rec(3);
-    CU(ipr::launch_intt_crt(s->d_bS, s->d_iw, s->d_iwp, s->d_bR, (int)(B * p.instances), st));
+    CU(ipr::launch_intt_crt(s->d_bS, s->d_iw, s->d_iwp, s->d_bR, (int)(B * p.instances), st, s->d_zbs, s->d_bth,
+                            (int)p.instances));
     rec(4);
     CU(ipr::launch_fold2(s->d_row0, s->d_gsw, s->d_ahat, s->d_bR, (int64_t)(p.instances * kN), s->d_c, s->d_fw,
                          s->d_fwp, s->d_iw, s->d_iwp, (int)p.interp, (int)p.c, nqt, (int64_t)p.db_cols, 2, d_resps, rb,
