@@ -17,6 +17,7 @@
 
 #include "ipr_device.cuh"
 #include "kernels.cuh"
+#include "ntt_regs.cuh"
 
 namespace ipr {
 
@@ -259,6 +260,8 @@ __global__ void __launch_bounds__(PACK_THREADS) k_pack(const uint64_t* __restric
 // ---------------------------------------------------------------------------
 // R[j] = from_ntt(S[j]) : inverse NTT per limb + CRT compose (one CTA per output)
 // ---------------------------------------------------------------------------
+// One CTA of 512 threads per output j: group g (256 threads) runs the inverse
+// NTT of limb g in registers (ntt_regs.cuh), the limbs meet at the CRT compose.
 __global__ void __launch_bounds__(512) k_intt_crt(const uint32_t* __restrict__ S,
                                                   const uint32_t* __restrict__ iw,
                                                   const uint32_t* __restrict__ iwp,
@@ -267,26 +270,34 @@ __global__ void __launch_bounds__(512) k_intt_crt(const uint32_t* __restrict__ S
                                                   const uint64_t* __restrict__ bth, int instances) {
     __shared__ uint32_t sm[2 * N];
     const int j = blockIdx.x;
+    const int g = threadIdx.x >> 8, t = threadIdx.x & 255;
+    const uint32_t q = g ? Q1 : Q0;
+    uint32_t v[1][nttr::EPT];
+    const uint32_t* Sj = S + ((int64_t)j * 2 + g) * N;
     if (z_bodies) {  // + sum_k z_c[k][z] That[j'][k][z] per limb (packing_online_kernel.cu:76-83)
         const int c = j / instances, jj = j % instances;
-        for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) {
-            const int l = i >> LOGN, z = i & (N - 1);
-            uint64_t acc = S[(int64_t)j * 2 * N + i];
+        const uint64_t* zc = z_bodies + (int64_t)c * T_EXP * N;
+        const uint64_t* th = bth + (int64_t)jj * T_EXP * N;
+        const int sh = 32 * g;
 #pragma unroll
-            for (int k = 0; k < T_EXP; k++) {
-                const uint64_t zv = z_bodies[((int64_t)c * T_EXP + k) * N + z];
-                const uint64_t tv = bth[((int64_t)jj * T_EXP + k) * N + z];
-                acc += (uint64_t)(uint32_t)(l ? zv >> 32 : zv) * (uint32_t)(l ? tv >> 32 : tv);
-            }
-            sm[i] = modq(acc, l);
+        for (int m = 0; m < nttr::EPT; m++) {
+            const int z = nttr::eB(t, m);
+            uint64_t acc = __ldg(Sj + z);
+#pragma unroll
+            for (int k = 0; k < T_EXP; k++)
+                acc += (uint64_t)(uint32_t)(__ldg(zc + k * N + z) >> sh) * (uint32_t)(__ldg(th + k * N + z) >> sh);
+            v[0][m] = mod64(acc, q, g ? BR1 : BR0);
         }
     } else {
-        for (int i = threadIdx.x; i < 2 * N; i += blockDim.x) sm[i] = S[(int64_t)j * 2 * N + i];
+#pragma unroll
+        for (int m = 0; m < nttr::EPT; m++) v[0][m] = __ldg(Sj + nttr::eB(t, m));
     }
+    nttr::inverse<1>(v, t, sm + g * N, 1 + g, iw + g * N, iwp + g * N, q);
+#pragma unroll
+    for (int m = 0; m < nttr::EPT; m++) sm[g * N + nttr::eA(t, m)] = v[0][m];
     __syncthreads();
-    ntt_inverse_smem<2>(sm, iw, iwp, [](int p) { return p; });
     for (int z = threadIdx.x; z < N; z += blockDim.x)
-        R[(int64_t)j * N + z] = crt2(sm[z], sm[N + z], c_q0inv, c_br[1]);
+        R[(int64_t)j * N + z] = crt2(sm[z], sm[N + z], Q0INV, BR1);
 }
 
 // ---------------------------------------------------------------------------
