@@ -19,8 +19,9 @@
 // with P_ab < 255^2 * 6144 < 2^29 exact in a 32-bit accumulator.
 //
 // GEMM per (z, l, tile of 32 outputs): M = 128 rows = 4 bytes b x 32 outputs,
-// N = 4 bytes a x clients (<= 256), K = 6144.  Persistent CTAs of 6 warps:
-// TMA producer, MMA issuer, 4 epilogue warps (the same pipeline as gemm_tc.cu).
+// N = 4 bytes a x clients (<= 256), K = 6144.  Persistent CTAs of 10 warps:
+// TMA producer, MMA issuer, 2 x 4 epilogue warps; each unit is two slots that
+// share the client operand.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -34,7 +35,7 @@ namespace ipr {
 
 namespace {
 
-constexpr int P_THREADS = 192;
+constexpr int P_THREADS = 320;
 constexpr int P_TILE_M = 128;
 constexpr int P_TILE_K = 128;
 constexpr int P_K = 3 * N;  // 6144
@@ -45,7 +46,7 @@ struct PSmem {
     uint64_t full[P_MAX_STAGES], empty[P_MAX_STAGES], acc_full[2], acc_empty[2];
     uint32_t tmem_base;
     int err;
-    int ep_fail;  // written only by the epilogue warps, read after their named barrier
+    int ep_fail[2];  // written only by epilogue group t's warps, read after their named barrier
 };
 
 __device__ __forceinline__ uint32_t pow5(uint32_t i) {  // 5^i mod 2N
@@ -105,6 +106,11 @@ __global__ void k_build_y8(const uint64_t* __restrict__ y_bodies, uint8_t* __res
     }
 }
 
+// Each unit is a pair of slots (z0 = 2 zp, z1 = z0 + 1) of one (limb, output tile):
+// both M tiles multiply the same Y_l K-slice, so every B stage feeds two MMAs
+// and the client operand crosses L2 once per slot pair instead of once per slot.
+// Accumulators: tile t at TMEM columns [buf * 2 nt + t nt, + nt).
+// Warps: 0 TMA producer, 1 MMA issuer, 2..5 epilogue of tile 0, 6..9 epilogue of tile 1.
 __global__ void __launch_bounds__(P_THREADS, 1)
     k_pack_mma(const __grid_constant__ CUtensorMap tm_t, const __grid_constant__ CUtensorMap tm_y, int instances,
                int mt_count, int clients, int np, int nt, int stages, uint32_t* __restrict__ S,
@@ -113,15 +119,15 @@ __global__ void __launch_bounds__(P_THREADS, 1)
     uint8_t* base = smem_raw + ((1024 - (umma::smem_addr(smem_raw) & 1023)) & 1023);
     PSmem* sh = reinterpret_cast<PSmem*>(base);
     volatile int* err = &sh->err;
-    uint8_t* a_tiles = base + 1024;
+    uint8_t* a_tiles = base + 1024;  // [stage][tile][128 x 128]
     const int b_stage = nt * P_TILE_K;
-    uint8_t* b_tiles = a_tiles + stages * P_A_STAGE;
-    uint32_t* xch = reinterpret_cast<uint32_t*>(b_tiles + stages * b_stage);  // [clients][4][32]
+    uint8_t* b_tiles = a_tiles + stages * 2 * P_A_STAGE;
+    uint32_t* xch_all = reinterpret_cast<uint32_t*>(b_tiles + stages * b_stage);  // [tile][16 clients][4][32]
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nbuf = (2 * nt <= 512) ? 2 : 1;
+    const int nbuf = (4 * nt <= 512) ? 2 : 1;
     uint32_t ncols = 32;
-    while (ncols < (uint32_t)(nbuf * nt)) ncols <<= 1;
+    while (ncols < (uint32_t)(nbuf * 2 * nt)) ncols <<= 1;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < stages; s++) {
@@ -130,10 +136,10 @@ __global__ void __launch_bounds__(P_THREADS, 1)
         }
         for (int b = 0; b < 2; b++) {
             umma::mbar_init(&sh->acc_full[b], 1);
-            umma::mbar_init(&sh->acc_empty[b], 4);
+            umma::mbar_init(&sh->acc_empty[b], 8);
         }
         *err = 0;
-        sh->ep_fail = 0;
+        sh->ep_fail[0] = sh->ep_fail[1] = 0;
         umma::fence_mbar_init();
     }
     if (warp == 1) umma::tmem_alloc(&sh->tmem_base, ncols);
@@ -141,10 +147,9 @@ __global__ void __launch_bounds__(P_THREADS, 1)
     __syncthreads();
     umma::fence_after();
     const uint32_t tmem = sh->tmem_base;
-    volatile int* ep_fail = &sh->ep_fail;
 
-    const int ks_total = P_K / P_TILE_K;  // 48
-    const int64_t total = (int64_t)2 * mt_count * N;  // units (l, mt, z), z fastest
+    const int ks_total = P_K / P_TILE_K;              // 48
+    const int64_t total = (int64_t)2 * mt_count * (N / 2);  // units (l, mt, zp), zp fastest
 
     if (warp == 0) {
         if (lane == 0) {
@@ -153,17 +158,20 @@ __global__ void __launch_bounds__(P_THREADS, 1)
             int last_phase[P_MAX_STAGES];
             for (int s = 0; s < P_MAX_STAGES; s++) last_phase[s] = -1;
             for (int64_t u = blockIdx.x; u < total && !*err; u += gridDim.x) {
-                const int z = (int)(u & (N - 1));
-                const int lm = (int)(u >> LOGN);
+                const int z0 = (int)(u & (N / 2 - 1)) * 2;
+                const int lm = (int)(u >> (LOGN - 1));
                 const int l = lm / mt_count, mt = lm % mt_count;
-                const int arow = (int)(((int64_t)(z * 2 + l) * mt_count + mt) * P_TILE_M);
+                const int arow0 = (int)(((int64_t)(z0 * 2 + l) * mt_count + mt) * P_TILE_M);
+                const int arow1 = arow0 + 2 * mt_count * P_TILE_M;  // slot z0 + 1
                 for (int ks = 0; ks < ks_total; ks++) {
                     if (!umma::mbar_wait(&sh->empty[stage], phase ^ 1)) {
                         *err = 11;
                         break;
                     }
-                    umma::mbar_expect_tx(&sh->full[stage], P_A_STAGE + b_stage);
-                    umma::tma_load_2d(a_tiles + stage * P_A_STAGE, &tm_t, ks * P_TILE_K, arow, &sh->full[stage]);
+                    uint8_t* at = a_tiles + stage * 2 * P_A_STAGE;
+                    umma::mbar_expect_tx(&sh->full[stage], 2 * P_A_STAGE + b_stage);
+                    umma::tma_load_2d(at, &tm_t, ks * P_TILE_K, arow0, &sh->full[stage]);
+                    umma::tma_load_2d(at + P_A_STAGE, &tm_t, ks * P_TILE_K, arow1, &sh->full[stage]);
                     umma::tma_load_2d(b_tiles + stage * b_stage, &tm_y, ks * P_TILE_K, l * np, &sh->full[stage]);
                     last_phase[stage] = (int)phase;
                     if (++stage == stages) {
@@ -187,7 +195,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
                 }
                 umma::fence_after();
                 bool ok = true;
-                const uint32_t d = tmem + (uint32_t)(buf * nt);
+                const uint32_t d0 = tmem + (uint32_t)(buf * 2 * nt), d1 = d0 + (uint32_t)nt;
                 for (int ks = 0; ks < ks_total; ks++) {
                     if (!umma::mbar_wait(&sh->full[stage], phase)) {
                         *err = 13;
@@ -195,12 +203,15 @@ __global__ void __launch_bounds__(P_THREADS, 1)
                         break;
                     }
                     umma::fence_after();
-                    const uint32_t sa = umma::smem_addr(a_tiles + stage * P_A_STAGE);
+                    const uint32_t sa = umma::smem_addr(a_tiles + stage * 2 * P_A_STAGE);
                     const uint32_t sb = umma::smem_addr(b_tiles + stage * b_stage);
 #pragma unroll
-                    for (int k4 = 0; k4 < P_TILE_K / 32; k4++)
-                        umma::mma_u8(d, umma::desc_sw128(sa + 32 * k4), umma::desc_sw128(sb + 32 * k4), idesc,
-                                     (ks == 0 && k4 == 0) ? 0u : 1u);
+                    for (int k4 = 0; k4 < P_TILE_K / 32; k4++) {
+                        const uint64_t db = umma::desc_sw128(sb + 32 * k4);
+                        const uint32_t acc = (ks == 0 && k4 == 0) ? 0u : 1u;
+                        umma::mma_u8(d0, umma::desc_sw128(sa + 32 * k4), db, idesc, acc);
+                        umma::mma_u8(d1, umma::desc_sw128(sa + P_A_STAGE + 32 * k4), db, idesc, acc);
+                    }
                     umma::commit(&sh->empty[stage]);
                     last_stage = stage;
                     last_parity = phase;
@@ -221,54 +232,66 @@ __global__ void __launch_bounds__(P_THREADS, 1)
             if (last_stage >= 0) umma::mbar_wait(&sh->empty[last_stage], last_parity, 1u << 22);
         }
     } else {
-        // epilogue: warp quarter b holds TMEM rows b*32 .. b*32+31 = byte b of outputs mt*32 + lane
+        // epilogue group t (warps 2+4t .. 5+4t) drains tile t (slot z0 + t).  Warp w reads TMEM
+        // lanes 32 (w % 4) .. +31 = byte b = w % 4 of outputs mt*32 + lane.
+        const int t = (warp - 2) >> 2;
         const int b = warp & 3;
+        const int gbar = 1 + t;
+        uint32_t* xch = xch_all + t * (16 * 4 * 32);
+        volatile int* ep_fail = &sh->ep_fail[t];
         int buf = 0;
         uint32_t acc_phase = 0;
+        const int chunks = (clients + 15) / 16;
         for (int64_t u = blockIdx.x; u < total; u += gridDim.x) {
-            // the four epilogue warps leave together: the decision uses a flag only they write
+            // the group's four warps leave together: the decision uses a flag only they write
             if (!umma::mbar_wait(&sh->acc_full[buf], acc_phase) && lane == 0) *ep_fail = 1;
-            umma::named_bar(1, 128);
+            umma::named_bar(gbar, 128);
             if (*ep_fail) {
-                if (threadIdx.x == 64) *err = 14;
+                if (b == 0 && lane == 0) *err = 14;
                 break;
             }
             umma::fence_after();
-            const int z = (int)(u & (N - 1));
-            const int lm = (int)(u >> LOGN);
+            const int z = (int)(u & (N / 2 - 1)) * 2 + t;
+            const int lm = (int)(u >> (LOGN - 1));
             const int l = lm / mt_count, mt = lm % mt_count;
             const uint32_t q = l ? Q1 : Q0;
             const uint64_t br = l ? BR1 : BR0;
             const uint32_t lane_off = (uint32_t)(b * 32) << 16;
-            for (int g = 0; g < nt / 16; g++) {
-                uint32_t d[16];
-                umma::tmem_ld16(tmem + lane_off + (uint32_t)(buf * nt + g * 16), d);
-                umma::tmem_wait_ld();
-#pragma unroll
-                for (int ci = 0; ci < 4; ci++) {
-                    const int c = g * 4 + ci;
-                    uint64_t v = 0;
-#pragma unroll
-                    for (int a = 0; a < 4; a++) v += (uint64_t)d[ci * 4 + a] << (8 * a);
-                    const uint32_t r = mod64(v, q, br);
-                    if (c < clients) xch[(c * 4 + b) * 32 + lane] = mod64((uint64_t)r << (8 * b), q, br);
-                }
-            }
-            umma::fence_before();
-            __syncwarp();
-            if (lane == 0) umma::mbar_arrive(&sh->acc_empty[buf]);  // TMEM buffer free for the next unit
-            umma::named_bar(1, 128);
-            // combine the 4 byte rows; thread (b, lane) owns clients c = b mod 4.  The z_body x That
-            // term is added by the inverse-NTT kernel that consumes S.
+            const uint32_t col0 = (uint32_t)(buf * 2 * nt + t * nt);
             const int j = mt * 32 + lane;
-            if (j < instances) {
-                for (int c = b; c < clients; c += 4) {
-                    const uint64_t tot = (uint64_t)xch[(c * 4 + 0) * 32 + lane] + xch[(c * 4 + 1) * 32 + lane] +
-                                         xch[(c * 4 + 2) * 32 + lane] + xch[(c * 4 + 3) * 32 + lane];
-                    S[(((int64_t)c * instances + j) * 2 + l) * N + z] = mod64(tot, q, br);
+            for (int ch = 0; ch < chunks; ch++) {
+                for (int g = ch * 4; g < ch * 4 + 4 && g < nt / 16; g++) {
+                    uint32_t d[16];
+                    umma::tmem_ld16(tmem + lane_off + col0 + (uint32_t)(g * 16), d);
+                    umma::tmem_wait_ld();
+#pragma unroll
+                    for (int ci = 0; ci < 4; ci++) {
+                        uint64_t v = 0;
+#pragma unroll
+                        for (int a = 0; a < 4; a++) v += (uint64_t)d[ci * 4 + a] << (8 * a);
+                        const uint32_t r = mod64(v, q, br);
+                        xch[(((g - ch * 4) * 4 + ci) * 4 + b) * 32 + lane] = mod64((uint64_t)r << (8 * b), q, br);
+                    }
                 }
+                if (ch == chunks - 1) {  // every TMEM read of this unit is done: free the buffer
+                    umma::fence_before();
+                    __syncwarp();
+                    if (lane == 0) umma::mbar_arrive(&sh->acc_empty[buf]);
+                }
+                umma::named_bar(gbar, 128);
+                // combine the 4 byte rows; thread (b, lane) owns clients c = b mod 4 of the chunk.
+                // The z_body x That term is added by the inverse-NTT kernel that consumes S.
+                if (j < instances) {
+                    for (int cl = b; cl < 16; cl += 4) {
+                        const int c = ch * 16 + cl;
+                        if (c >= clients) break;
+                        const uint64_t tot = (uint64_t)xch[(cl * 4 + 0) * 32 + lane] + xch[(cl * 4 + 1) * 32 + lane] +
+                                             xch[(cl * 4 + 2) * 32 + lane] + xch[(cl * 4 + 3) * 32 + lane];
+                        S[(((int64_t)c * instances + j) * 2 + l) * N + z] = mod64(tot, q, br);
+                    }
+                }
+                umma::named_bar(gbar, 128);
             }
-            umma::named_bar(1, 128);
             if (nbuf == 2) {
                 buf ^= 1;
                 if (buf == 0) acc_phase ^= 1;
@@ -291,15 +314,16 @@ int pack_mma_nt(int clients) {
     return n < 16 ? 16 : n;
 }
 
+constexpr int P_XCH_BYTES = 2 * 16 * 4 * 32 * 4;  // two epilogue groups x 16 clients x 4 bytes x 32 outputs
+
 int pack_mma_stages(int nt) {
-    const int per = P_A_STAGE + nt * P_TILE_K;
-    const int xch = 64 * 4 * 32 * 4;
-    int s = (200 * 1024 - xch) / per;
+    const int per = 2 * P_A_STAGE + nt * P_TILE_K;
+    int s = (210 * 1024 - P_XCH_BYTES) / per;
     return s > P_MAX_STAGES ? P_MAX_STAGES : (s < 2 ? 2 : s);
 }
 
 size_t pack_mma_smem(int nt) {
-    return 2048 + (size_t)pack_mma_stages(nt) * (P_A_STAGE + nt * P_TILE_K) + (size_t)(nt / 4) * 4 * 32 * 4;
+    return 2048 + (size_t)pack_mma_stages(nt) * (2 * P_A_STAGE + nt * P_TILE_K) + P_XCH_BYTES;
 }
 
 cudaError_t init_pack_mma_kernel() {
