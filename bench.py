@@ -13,8 +13,11 @@ shapes (the reference's own timing mode, engine.rs:693-729); queries are
 seeded synthetic payloads.
 
   value : payloads/s with queries resident in HBM (ipr_server_respond_batch_device)
-  e2e   : payloads/s through ipr_server_respond_batch with host buffers (H2D
-          queries, D2H responses inside the timed region)
+  e2e   : payloads/s through the serving API (KeywordService: submit host
+          bytes, wait for host bytes; H2D queries and D2H responses of every
+          batch inside the timed region)
+  serving: p50/p99 latency and throughput under Poisson arrivals at stated
+          loads (default 1000 and 2500 payloads/s, 3 s each)
 
 --impl reference times the CPU restatement of the reference's respond() on the
 host cores (the reference's Rust CPU path cannot be built here).
@@ -158,6 +161,45 @@ def cpu_sample(orc, reps=3):
     return s.describe(t, reps)
 
 
+def poisson_load(svc, payloads, rate, seconds):
+    """Poisson arrivals at `rate` payloads/s for `seconds`; latency = submit -> response ready
+    inside the service (p50/p99 over all requests), throughput = completions / elapsed."""
+    import queue
+    import random
+    svc.reset_stats()
+    rng = random.Random(int(rate))
+    n = max(1, int(rate * seconds))
+    q = queue.Queue()
+    done = []
+
+    def collector():
+        while True:
+            t = q.get()
+            if t is None:
+                return
+            svc.wait(t)
+            done.append(time.perf_counter())
+
+    th = threading.Thread(target=collector)
+    th.start()
+    t_start = time.perf_counter()
+    t_next = t_start
+    for i in range(n):
+        t_next += rng.expovariate(rate)
+        d = t_next - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        q.put(svc.submit(0, payloads[i % len(payloads)]))
+    offered_s = time.perf_counter() - t_start
+    q.put(None)
+    th.join()
+    st = svc.stats()
+    return {"offered_payloads_per_s": rate, "arrived_payloads_per_s": n / offered_s, "payloads": n,
+            "completed_payloads_per_s": n / (done[-1] - t_start), "p50_ms": st.p50_us / 1e3,
+            "p99_ms": st.p99_us / 1e3, "mean_ms": st.mean_us / 1e3, "max_ms": st.max_us / 1e3,
+            "mean_batch": st.batched_payloads / max(st.batches, 1), "failed": st.failed}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -170,6 +212,10 @@ def main():
     ap.add_argument("--dim0", type=int, default=None)
     ap.add_argument("--batch", type=int, default=64, help="payloads per step (1 = batch-1 u64 packing path)")
     ap.add_argument("--no-batch1", action="store_true", help="skip the batch-1 comparison measurement")
+    ap.add_argument("--no-serving", action="store_true", help="skip the Poisson serving measurement")
+    ap.add_argument("--serve-rates", type=float, nargs="*", default=[1000.0, 2500.0],
+                    help="offered Poisson loads (payloads/s) for the serving measurement")
+    ap.add_argument("--serve-seconds", type=float, default=3.0)
     args = ap.parse_args()
     small = args.records != RECORDS
 
@@ -282,18 +328,34 @@ def main():
     srv.set_profiling(False)
     clk = clocks.stop()
 
-    # ---- end-to-end through the host API (pinned staging, H2D + D2H per step) ----------
+    # ---- end-to-end through the serving API: host buffers, H2D + D2H of every batch ---------
+    # (KeywordService: continuous batching, pinned staging, copies overlapped with compute)
+    svc = pkg.KeywordService([srv], max_batch=B) if B > 1 else None
     barrier()
-    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    h0.record(stream)
+    # the blocking call (ipr_server_respond_batch / ipr_server_respond), for comparison
     t0 = time.perf_counter()
     for i in range(args.steps):
         run_host(i)
-    h1.record(stream)
-    srv.sync()
-    wall_ms = (time.perf_counter() - t0) * 1000
+    blocking_ms = (time.perf_counter() - t0) * 1000
+    e2e_ms = blocking_ms
+    if svc is not None:
+        for t in [svc.submit(0, payloads[i % npay]) for i in range(2 * B)]:
+            svc.wait(t)
+        barrier()
+        t0 = time.perf_counter()
+        tickets = [svc.submit(0, payloads[i % npay]) for i in range(args.steps * B)]
+        for t in tickets:
+            svc.wait(t)
+        e2e_ms = (time.perf_counter() - t0) * 1000
     barrier()
-    e2e_ms = max(h0.elapsed_time(h1), wall_ms)
+
+    # ---- serving at stated Poisson loads (1-GPU runs) -----------------------------------
+    serving = []
+    if svc is not None and world == 1 and not args.no_serving:
+        for rate in args.serve_rates:
+            serving.append(poisson_load(svc, payloads, rate, args.serve_seconds))
+    if svc is not None:
+        svc.close()
 
     # ---- the plain batch-1 u64 path on the same GPU (CUDA-core GEMV + packing) ----------
     b1 = {}
@@ -355,7 +417,11 @@ def main():
                        "batch_payloads": B, "parallelism": f"replica x{world}",
                        "l2": "inputs larger than L2 (packing stream of %.1f GB + DB of %.2f GB per step)" % (
                            pack_bytes / 1e9, plan.db_rows * plan.db_cols * 2 / 1e9)},
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": B * qbytes, "d2h_bytes_per_step": B * rbytes},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": B * qbytes, "d2h_bytes_per_step": B * rbytes,
+                    "api": ("KeywordService (ipr_service_submit / ipr_service_wait)" if B > 1
+                            else "ipr_server_respond"),
+                    "blocking_batch_call_payloads_per_s": args.steps * B / (blocking_ms / 1000.0)},
+            "serving": serving or None,
             "batch1": ({"u64_payloads_per_s": b1["u64"], "tensor_gemv_payloads_per_s": b1["tensor_gemv"],
                         "speedup_vs_batch1_u64": value / world / b1["u64"]} if b1 else None),
             "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",

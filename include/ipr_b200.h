@@ -30,6 +30,8 @@ extern "C" {
 #define IPR_E_FORMAT -5   /* malformed query bytes */
 #define IPR_E_SPACE -6    /* output buffer too small (required size reported) */
 #define IPR_E_STATE -7    /* call made in the wrong state */
+#define IPR_E_BUSY -8     /* request queue full (serving loop admission) */
+#define IPR_PENDING 1     /* request accepted, result not ready yet */
 
 #define IPR_POLY_LEN 2048
 #define IPR_RESULT_BYTES 12288 /* one switched RLWE result: 2048x28 + 2048x20 bits */
@@ -57,6 +59,20 @@ int ipr_plan_from_shape(uint64_t record_count, uint64_t key_size, uint64_t value
 /* Serialized sizes: deserialize_keyword_query (src/protocol/wire.rs:618-705) and
  * serialize_keyword_response (wire.rs:708-726). */
 uint64_t ipr_query_bytes(uint64_t db_rows, unsigned num_queries);
+
+/* Fold-group sharding over several GPUs (no reference counterpart; the
+ * partition follows the independence of the fold groups in
+ * KeywordServer::respond, keyword.rs:558-574).  Shard k of S gets a
+ * contiguous run of the plan's c fold groups (c / S, the first c % S shards
+ * one more): instances [first_instance, first_instance + out->instances),
+ * i.e. DB columns first_instance*2048 .. and the matching precomputation
+ * rows.  Each shard's server answers the same query bytes with its groups'
+ * results; ipr_response_merge concatenates the parts' results per query in
+ * shard order and keeps the first part's stash block, which gives exactly the
+ * unsharded server's response. */
+int ipr_plan_shard(const ipr_plan *full, int num_shards, int shard, ipr_plan *out, uint64_t *first_instance);
+int ipr_response_merge(const uint8_t *const *parts, const size_t *lens, int num_parts, uint8_t *out, size_t cap,
+                       size_t *out_len);
 
 typedef struct ipr_server ipr_server;
 
@@ -175,6 +191,56 @@ const char *ipr_version(void);
  * constants for that device; make it before any stream capture there.
  * Returns IPR_OK or a negative status (message in ipr_last_error()). */
 int ipr_gemv_query_noalloc(uint64_t *h_c, const uint64_t *h_a, const uint16_t *d_db, int db_rows, int b_cols);
+
+/* ---------------------------------------------------------------------------
+ * Serving loop with continuous batching (no reference counterpart: the
+ * reference answers one payload at a time, keyword.rs:534-640).  One
+ * scheduler thread per service; requests are queued per database (index into
+ * `servers`); whenever a device slot of a database frees, everything pending
+ * for it (up to the admitted batch size) is launched as one tensor-core batch,
+ * so batches grow with the load.  Two-query payloads take the batch path;
+ * other query counts are answered alone, in arrival order.  Responses are
+ * byte-identical to ipr_server_respond.
+ *
+ * Admission: the batch size is the largest B <= max_batch (<= 64) whose
+ * batch-path device memory over all databases fits hbm_budget_bytes (0 = the
+ * free HBM at creation minus 2 GiB); creation fails with IPR_E_OOM if even
+ * B = 1 does not fit.  At most max_pending requests wait (0 = 4096); beyond
+ * that ipr_service_submit returns IPR_E_BUSY.  The servers must outlive the
+ * service; direct calls on them stay legal and are serialised with it.
+ * -------------------------------------------------------------------------- */
+typedef struct ipr_service ipr_service;
+
+typedef struct ipr_service_config {
+    int max_batch;
+    int max_pending;
+    uint64_t hbm_budget_bytes;
+} ipr_service_config;
+
+typedef struct ipr_service_stats {
+    uint64_t submitted, completed, rejected, failed;
+    uint64_t batches, batched_payloads; /* device batch passes and the payloads they carried */
+    uint64_t pending, in_flight;        /* queued / submitted but not yet collected */
+    int max_batch;                      /* admitted batch size */
+    uint64_t hbm_bytes;                 /* device bytes the batch path and the I/O slots hold */
+    double p50_us, p99_us, mean_us, max_us; /* submit -> completion, completed requests since the last reset */
+    uint64_t latency_samples;
+} ipr_service_stats;
+
+int ipr_service_create(ipr_server *const *servers, int num_servers, const ipr_service_config *cfg,
+                       ipr_service **out);
+/* Queue one serialized KeywordQueryPayload for database `db`; *ticket names it. */
+int ipr_service_submit(ipr_service *svc, int db, const uint8_t *query, size_t len, uint64_t *ticket);
+/* IPR_PENDING while running; otherwise the request's status, with the serialized
+ * response copied to out (IPR_E_SPACE and *out_len = size if cap is short; the
+ * result is kept for a retry).  A collected ticket is released. */
+int ipr_service_poll(ipr_service *svc, uint64_t ticket, uint8_t *out, size_t cap, size_t *out_len);
+/* As poll, blocking up to timeout_ms (< 0: no limit); IPR_PENDING on timeout. */
+int ipr_service_wait(ipr_service *svc, uint64_t ticket, int timeout_ms, uint8_t *out, size_t cap, size_t *out_len);
+int ipr_service_get_stats(ipr_service *svc, ipr_service_stats *out);
+int ipr_service_reset_stats(ipr_service *svc);
+/* Finishes the batches in flight, drops queued and uncollected requests. */
+void ipr_service_destroy(ipr_service *svc);
 
 #ifdef __cplusplus
 }

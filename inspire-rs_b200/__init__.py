@@ -19,7 +19,8 @@ from typing import List, Optional, Sequence
 __all__ = [
     "IprError", "Plan", "KeywordServer", "plan_from_shape", "query_bytes", "lib",
     "KeywordQueryPayload", "KeywordResponsePayload", "serialize_keyword_query",
-    "deserialize_keyword_response", "POLY_LEN", "RESULT_BYTES",
+    "deserialize_keyword_response", "POLY_LEN", "RESULT_BYTES", "KeywordService", "ServiceStats",
+    "shard_plan", "merge_responses", "ShardedKeywordServer",
 ]
 
 POLY_LEN = 2048
@@ -81,10 +82,38 @@ _set_prof = _sig("ipr_server_set_profiling", _i32, _vp, _i32)
 _set_opt = _sig("ipr_server_set_option", _i32, _vp, _i32, ctypes.c_int64)
 _stage_times = _sig("ipr_server_stage_times", _i32, _vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_u64))
 _last_error = _sig("ipr_last_error", ctypes.c_char_p)
+
+
+class _ServiceConfig(ctypes.Structure):
+    _fields_ = [("max_batch", _i32), ("max_pending", _i32), ("hbm_budget_bytes", _u64)]
+
+
+class _ServiceStats(ctypes.Structure):
+    _fields_ = [("submitted", _u64), ("completed", _u64), ("rejected", _u64), ("failed", _u64),
+                ("batches", _u64), ("batched_payloads", _u64), ("pending", _u64), ("in_flight", _u64),
+                ("max_batch", _i32), ("hbm_bytes", _u64), ("p50_us", ctypes.c_double),
+                ("p99_us", ctypes.c_double), ("mean_us", ctypes.c_double), ("max_us", ctypes.c_double),
+                ("latency_samples", _u64)]
+
+
+_plan_shard = _sig("ipr_plan_shard", _i32, ctypes.POINTER(_Plan), _i32, _i32, ctypes.POINTER(_Plan),
+                   ctypes.POINTER(_u64))
+_merge = _sig("ipr_response_merge", _i32, ctypes.POINTER(_u8p), ctypes.POINTER(_sz), _i32, _u8p, _sz,
+              ctypes.POINTER(_sz))
+_svc_create = _sig("ipr_service_create", _i32, ctypes.POINTER(_vp), _i32, ctypes.POINTER(_ServiceConfig),
+                   ctypes.POINTER(_vp))
+_svc_submit = _sig("ipr_service_submit", _i32, _vp, _i32, _u8p, _sz, ctypes.POINTER(_u64))
+_svc_poll = _sig("ipr_service_poll", _i32, _vp, _u64, _u8p, _sz, ctypes.POINTER(_sz))
+_svc_wait = _sig("ipr_service_wait", _i32, _vp, _u64, _i32, _u8p, _sz, ctypes.POINTER(_sz))
+_svc_stats = _sig("ipr_service_get_stats", _i32, _vp, ctypes.POINTER(_ServiceStats))
+_svc_reset = _sig("ipr_service_reset_stats", _i32, _vp)
+_svc_destroy = _sig("ipr_service_destroy", None, _vp)
 _version = _sig("ipr_version", ctypes.c_char_p)
 
-STATUS = {0: "IPR_OK", -1: "IPR_E_ARGS", -2: "IPR_E_OOM", -3: "IPR_E_CUDA", -4: "IPR_E_TIMEOUT",
-          -5: "IPR_E_FORMAT", -6: "IPR_E_SPACE", -7: "IPR_E_STATE"}
+STATUS = {0: "IPR_OK", 1: "IPR_PENDING", -1: "IPR_E_ARGS", -2: "IPR_E_OOM", -3: "IPR_E_CUDA",
+          -4: "IPR_E_TIMEOUT", -5: "IPR_E_FORMAT", -6: "IPR_E_SPACE", -7: "IPR_E_STATE", -8: "IPR_E_BUSY"}
+IPR_PENDING = 1
+IPR_E_BUSY = -8
 
 
 class IprError(RuntimeError):
@@ -373,3 +402,184 @@ class KeywordServer:
 
 def version() -> str:
     return _version().decode()
+
+
+@dataclass(frozen=True)
+class ServiceStats:
+    submitted: int
+    completed: int
+    rejected: int
+    failed: int
+    batches: int
+    batched_payloads: int
+    pending: int
+    in_flight: int
+    max_batch: int
+    hbm_bytes: int
+    p50_us: float
+    p99_us: float
+    mean_us: float
+    max_us: float
+    latency_samples: int
+
+
+class KeywordService:
+    """Continuous-batching serving loop over one or more KeywordServers
+    (ipr_service_*): ``submit`` queues a serialized payload for database
+    ``db`` and returns a ticket; ``wait`` / ``poll`` return the serialized
+    response, byte-identical to ``KeywordServer.respond_to_serialized_query``.
+    The servers must stay open while the service runs."""
+
+    def __init__(self, servers: Sequence["KeywordServer"], max_batch: int = 64, max_pending: int = 0,
+                 hbm_budget_bytes: int = 0):
+        self._servers = list(servers)
+        arr = (_vp * len(self._servers))(*[s._h.value for s in self._servers])
+        cfg = _ServiceConfig(max_batch, max_pending, hbm_budget_bytes)
+        self._h = _vp()
+        _check(_svc_create(arr, len(self._servers), ctypes.byref(cfg), ctypes.byref(self._h)), "service_create")
+        self._cap = max(s.response_bytes(2) for s in self._servers)
+
+    def submit(self, db: int, query: bytes) -> int:
+        t = _u64()
+        query = bytes(query)
+        ptr = ctypes.cast(ctypes.c_char_p(query), _u8p)  # no copy: the service copies on submit
+        _check(_svc_submit(self._h, db, ptr, len(query), ctypes.byref(t)), "service_submit")
+        return t.value
+
+    def _collect(self, fn, ticket, *extra):
+        cap = self._cap
+        out = (ctypes.c_uint8 * cap)()
+        n = _sz()
+        st = fn(self._h, ticket, *extra, ctypes.cast(out, _u8p), cap, ctypes.byref(n))
+        if st == IPR_PENDING:
+            return None
+        if st == -6 and n.value > cap:  # a larger payload: the result is kept for the retry
+            cap = n.value
+            out = (ctypes.c_uint8 * cap)()
+            st = _svc_poll(self._h, ticket, ctypes.cast(out, _u8p), cap, ctypes.byref(n))
+        _check(st, "service_result")
+        return ctypes.string_at(out, n.value)
+
+    def poll(self, ticket: int) -> Optional[bytes]:
+        """the response, or None while the request runs"""
+        return self._collect(_svc_poll, ticket)
+
+    def wait(self, ticket: int, timeout_ms: int = -1) -> Optional[bytes]:
+        """the response (None if timeout_ms ran out first)"""
+        return self._collect(_svc_wait, ticket, timeout_ms)
+
+    def stats(self) -> ServiceStats:
+        st = _ServiceStats()
+        _check(_svc_stats(self._h, ctypes.byref(st)), "service_stats")
+        return ServiceStats(*[getattr(st, f) for f, _ in _ServiceStats._fields_])
+
+    def reset_stats(self):
+        _check(_svc_reset(self._h), "service_reset_stats")
+
+    def close(self):
+        if self._h and self._h.value:
+            _svc_destroy(self._h)
+            self._h = _vp()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# fold-group sharding across GPUs (one process per GPU)
+# ---------------------------------------------------------------------------
+def shard_plan(plan: Plan, num_shards: int, shard: int):
+    """(sub-plan, first instance) of shard `shard` (ipr_plan_shard): a contiguous run of fold groups."""
+    out = _Plan()
+    first = _u64()
+    _check(_plan_shard(ctypes.byref(plan._c()), num_shards, shard, ctypes.byref(out), ctypes.byref(first)),
+           "plan_shard")
+    return Plan(**{f: getattr(out, f) for f, _ in _Plan._fields_}), first.value
+
+
+def shard_slices(plan: Plan, num_shards: int, shard: int):
+    """element ranges of the shard's slice in each host array of ipr_server_data"""
+    sub, first = shard_plan(plan, num_shards, shard)
+    n, rows = sub.instances, plan.db_rows
+    return sub, {
+        "db": (first * POLY_LEN * rows, (first + n) * POLY_LEN * rows),
+        "a_hat": (first * POLY_LEN, (first + n) * POLY_LEN),
+        "bold_t": (first * 3069 * POLY_LEN, (first + n) * 3069 * POLY_LEN),
+        "bold_t_bar": (first * 3069 * POLY_LEN, (first + n) * 3069 * POLY_LEN),
+        "bold_t_hat": (first * 3 * POLY_LEN, (first + n) * 3 * POLY_LEN),
+    }
+
+
+def merge_responses(parts: Sequence[bytes]) -> bytes:
+    """ipr_response_merge: the unsharded response from the shards' responses (in shard order)."""
+    k = len(parts)
+    bufs = [(ctypes.c_uint8 * max(len(p), 1)).from_buffer_copy(p if p else b"\0") for p in parts]
+    arr = (_u8p * k)(*[ctypes.cast(b, _u8p) for b in bufs])
+    lens = (_sz * k)(*[len(p) for p in parts])
+    need = _sz()
+    st = _merge(arr, lens, k, None, 0, ctypes.byref(need))
+    if st not in (0, -6):
+        _check(st, "response_merge")
+    out = (ctypes.c_uint8 * need.value)()
+    _check(_merge(arr, lens, k, ctypes.cast(out, _u8p), need.value, ctypes.byref(need)), "response_merge")
+    return bytes(out)
+
+
+class ShardedKeywordServer:
+    """One fold-group shard per process (torch.distributed rank); the ranks
+    together answer like one KeywordServer.  ``respond_to_serialized_query``
+    is collective: rank 0's query bytes are broadcast, every rank answers its
+    groups, and the parts are gathered to rank 0, which returns the merged
+    response (other ranks return None).  ``answer`` is the per-rank step:
+    any callable bytes -> bytes (a KeywordServer built from the shard's
+    slices, or a test stand-in)."""
+
+    def __init__(self, answer, group=None, device=None):
+        import torch.distributed as dist
+        self._dist = dist
+        self._answer = answer
+        self._group = group
+        self._device = device  # tensors for the collectives live here (a CUDA device under NCCL)
+        self.rank = dist.get_rank(group)
+        self.world = dist.get_world_size(group)
+
+    def _bcast_bytes(self, data: Optional[bytes]) -> bytes:
+        import torch
+        dist = self._dist
+        n = torch.tensor([len(data) if self.rank == 0 else 0], dtype=torch.int64, device=self._device)
+        dist.broadcast(n, 0, group=self._group)
+        buf = (torch.frombuffer(bytearray(data), dtype=torch.uint8).to(self._device) if self.rank == 0
+               else torch.empty(int(n.item()), dtype=torch.uint8, device=self._device))
+        dist.broadcast(buf, 0, group=self._group)
+        return bytes(buf.cpu().numpy().tobytes())
+
+    def _gather_bytes(self, data: bytes) -> Optional[List[bytes]]:
+        import torch
+        dist = self._dist
+        n = torch.tensor([len(data)], dtype=torch.int64, device=self._device)
+        ns = [torch.zeros(1, dtype=torch.int64, device=self._device) for _ in range(self.world)]
+        dist.all_gather(ns, n, group=self._group)
+        mx = max(int(x.item()) for x in ns)
+        mine = torch.zeros(mx, dtype=torch.uint8, device=self._device)
+        if data:
+            mine[:len(data)] = torch.frombuffer(bytearray(data), dtype=torch.uint8).to(self._device)
+        parts = [torch.empty(mx, dtype=torch.uint8, device=self._device) for _ in range(self.world)]
+        dist.all_gather(parts, mine, group=self._group)
+        if self.rank != 0:
+            return None
+        return [bytes(p.cpu().numpy()[:int(k.item())].tobytes()) for p, k in zip(parts, ns)]
+
+    def respond_to_serialized_query(self, query: Optional[bytes]) -> Optional[bytes]:
+        q = self._bcast_bytes(query)
+        part = self._answer(q)
+        parts = self._gather_bytes(part)
+        return merge_responses(parts) if parts is not None else None

@@ -32,7 +32,15 @@ constexpr int FP = IPR_FOLD_FWD_BATCH;  // gadget-digit polynomials transformed 
 static_assert(6 % FP == 0, "forward batch must divide the 6 gadget rows");
 
 using nttr::eA;
-using nttr::eB;
+using nttr::eD;
+
+// the 8 consecutive words of layout D held by thread t (two 16-byte loads)
+__device__ __forceinline__ void load_d(uint32_t (&r)[EPT], const uint32_t* __restrict__ poly, int t) {
+    const uint4* src = reinterpret_cast<const uint4*>(poly + eD(t, 0));
+    const uint4 a = __ldg(src), b = __ldg(src + 1);
+    r[0] = a.x; r[1] = a.y; r[2] = a.z; r[3] = a.w;
+    r[4] = b.x; r[5] = b.y; r[6] = b.z; r[7] = b.w;
+}
 
 __device__ __forceinline__ uint64_t rescale_to(uint64_t v, uint64_t out_mod) {
     // rescale (src/core/arith.rs:436-452) of a canonical v in [0, q)
@@ -108,19 +116,21 @@ __global__ void __launch_bounds__(F_THREADS, 1)
             nttr::forward<FP>(v, t, xbuf, bar, fwl, fwpl, q);
 #pragma unroll
             for (int pp = 0; pp < FP; pp++) {
-                const uint32_t* bp = body + ((pb + pp) * 2 + g) * N;
+                uint32_t bv[EPT];
+                load_d(bv, body + ((pb + pp) * 2 + g) * N, t);
 #pragma unroll
                 for (int m = 0; m < EPT; m++) {
-                    acc0[m] += v[pp][m];                                   // < 6q
-                    acc1[m] += (uint64_t)__ldg(bp + eB(t, m)) * v[pp][m];  // 6 terms < 2^59
+                    acc0[m] += v[pp][m];                         // < 6q
+                    acc1[m] += (uint64_t)bv[m] * v[pp][m];       // 6 terms < 2^59
                 }
             }
         }
-        uint32_t pr[2][EPT];
+        uint32_t pr[2][EPT], r0[EPT];
+        load_d(r0, row0 + g * N, t);
 #pragma unroll
         for (int m = 0; m < EPT; m++) {
             const uint32_t a0 = mod64(acc0[m], q, br);
-            pr[0][m] = mod64((uint64_t)__ldg(row0 + g * N + eB(t, m)) * a0, q, br);
+            pr[0][m] = mod64((uint64_t)r0[m] * a0, q, br);
             pr[1][m] = mod64(acc1[m], q, br);
         }
         nttr::inverse<2>(pr, t, xbuf, bar, iwl, iwpl, q);

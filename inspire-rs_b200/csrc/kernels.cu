@@ -273,24 +273,35 @@ __global__ void __launch_bounds__(512) k_intt_crt(const uint32_t* __restrict__ S
     const int g = threadIdx.x >> 8, t = threadIdx.x & 255;
     const uint32_t q = g ? Q1 : Q0;
     uint32_t v[1][nttr::EPT];
-    const uint32_t* Sj = S + ((int64_t)j * 2 + g) * N;
+    // layout D: thread t holds the 8 consecutive slots z0 .. z0 + 7 (16-byte loads)
+    const int z0 = nttr::eD(t, 0);
+    const uint4* Sj = reinterpret_cast<const uint4*>(S + ((int64_t)j * 2 + g) * N + z0);
+    const uint4 s0 = __ldg(Sj), s1 = __ldg(Sj + 1);
+    const uint32_t sv[8] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w};
     if (z_bodies) {  // + sum_k z_c[k][z] That[j'][k][z] per limb (packing_online_kernel.cu:76-83)
         const int c = j / instances, jj = j % instances;
-        const uint64_t* zc = z_bodies + (int64_t)c * T_EXP * N;
-        const uint64_t* th = bth + (int64_t)jj * T_EXP * N;
+        const uint64_t* zc = z_bodies + (int64_t)c * T_EXP * N + z0;
+        const uint64_t* th = bth + (int64_t)jj * T_EXP * N + z0;
         const int sh = 32 * g;
+        uint64_t acc[8];
 #pragma unroll
-        for (int m = 0; m < nttr::EPT; m++) {
-            const int z = nttr::eB(t, m);
-            uint64_t acc = __ldg(Sj + z);
+        for (int m = 0; m < 8; m++) acc[m] = sv[m];
 #pragma unroll
-            for (int k = 0; k < T_EXP; k++)
-                acc += (uint64_t)(uint32_t)(__ldg(zc + k * N + z) >> sh) * (uint32_t)(__ldg(th + k * N + z) >> sh);
-            v[0][m] = mod64(acc, q, g ? BR1 : BR0);
+        for (int k = 0; k < T_EXP; k++) {
+            const ulonglong2* zp = reinterpret_cast<const ulonglong2*>(zc + k * N);
+            const ulonglong2* tp = reinterpret_cast<const ulonglong2*>(th + k * N);
+#pragma unroll
+            for (int h = 0; h < 4; h++) {
+                const ulonglong2 zv = __ldg(zp + h), tv = __ldg(tp + h);
+                acc[2 * h] += (uint64_t)(uint32_t)(zv.x >> sh) * (uint32_t)(tv.x >> sh);
+                acc[2 * h + 1] += (uint64_t)(uint32_t)(zv.y >> sh) * (uint32_t)(tv.y >> sh);
+            }
         }
+#pragma unroll
+        for (int m = 0; m < 8; m++) v[0][m] = mod64(acc[m], q, g ? BR1 : BR0);
     } else {
 #pragma unroll
-        for (int m = 0; m < nttr::EPT; m++) v[0][m] = __ldg(Sj + nttr::eB(t, m));
+        for (int m = 0; m < 8; m++) v[0][m] = sv[m];
     }
     nttr::inverse<1>(v, t, sm + g * N, 1 + g, iw + g * N, iwp + g * N, q);
 #pragma unroll

@@ -6,10 +6,17 @@
 // (rkdud007/inspire-rs src/core/ntt.rs:111-160, 731-780) with the tables of
 // build_ntt_tables (ntt.rs:74-108); outputs are canonical, so results equal
 // the reference's transforms exactly.
-//   layout A: thread t holds e = t + 256 m                  (distances 1024, 512, 256)
-//   layout B: thread t holds e = (t/32)*256 + t%32 + 32 m    (distances 128, 64, 32)
-//   distances 16 .. 1 pair lanes of one warp in layout B (warp shuffles).
-// Forward: A -> B (one shared-memory exchange).  Inverse: B -> A.
+// Thread t of the group (warp w = t / 32, lane l = t % 32) holds 8 elements
+// whose index bits are split between the thread and the register number, so
+// every butterfly pairs two registers of one thread:
+//   layout A: e = t + 256 m                          (distances 1024, 512, 256)
+//   layout B: e = 256 w + l + 32 m                   (distances 128, 64, 32)
+//   layout C: e = 256 w + 32 (l/4) + 4 k + l%4       (distances 16, 8, 4)
+//   layout D: e = 256 w + 8 l + k                    (distances 2, 1)
+// A <-> B moves data between the group's warps (shared memory + group
+// barrier); B <-> C <-> D stay inside one warp's 256 elements (shared memory,
+// XOR-swizzled so that every access is free of bank conflicts, + __syncwarp).
+// Forward: A -> D.  Inverse: D -> A.
 #pragma once
 #include <cstdint>
 
@@ -23,6 +30,12 @@ constexpr int EPT = 8;   // elements per thread
 
 __device__ __forceinline__ int eA(int t, int m) { return t + 256 * m; }
 __device__ __forceinline__ int eB(int t, int m) { return (t >> 5) * 256 + (t & 31) + 32 * m; }
+__device__ __forceinline__ int eC(int t, int k) { return (t >> 5) * 256 + ((t & 31) >> 2) * 32 + 4 * k + (t & 3); }
+__device__ __forceinline__ int eD(int t, int k) { return (t >> 5) * 256 + (t & 31) * 8 + k; }
+
+// swizzled word of local index i (< 256) inside a warp's 256-word block: the
+// row i / 32 flips bits 2..4 of the column, keeping aligned groups of 4 words
+__device__ __forceinline__ int swz(int i) { return i ^ (((i >> 5) & 7) << 2); }
 
 // named barrier 1 or 2 over one group (literal ids keep the CTA's barrier count at 3)
 __device__ __forceinline__ void group_bar(int id) {
@@ -66,115 +79,140 @@ __device__ __forceinline__ void exchange(uint32_t (&v)[P][EPT], int t, uint32_t*
     group_bar(bar);
 }
 
-// forward NTT of P polynomials of one limb: layout A in, layout B canonical out
+// intra-warp transposes; wb = the warp's 256-word block of the polynomial-0 buffer
+template <int P>
+__device__ __forceinline__ void b_to_c(uint32_t (&v)[P][EPT], int l, uint32_t* wb) {
+#pragma unroll
+    for (int p = 0; p < P; p++)
+#pragma unroll
+        for (int m = 0; m < EPT; m++) wb[p * N + swz(l + 32 * m)] = v[p][m];
+    __syncwarp();
+#pragma unroll
+    for (int p = 0; p < P; p++)
+#pragma unroll
+        for (int k = 0; k < EPT; k++) v[p][k] = wb[p * N + swz((l >> 2) * 32 + 4 * k + (l & 3))];
+    __syncwarp();
+}
+
+template <int P>
+__device__ __forceinline__ void c_to_b(uint32_t (&v)[P][EPT], int l, uint32_t* wb) {
+#pragma unroll
+    for (int p = 0; p < P; p++)
+#pragma unroll
+        for (int k = 0; k < EPT; k++) wb[p * N + swz((l >> 2) * 32 + 4 * k + (l & 3))] = v[p][k];
+    __syncwarp();
+#pragma unroll
+    for (int p = 0; p < P; p++)
+#pragma unroll
+        for (int m = 0; m < EPT; m++) v[p][m] = wb[p * N + swz(l + 32 * m)];
+    __syncwarp();
+}
+
+// layout D's 8 words of lane l sit in two aligned 4-word groups: swz(8 l + k)
+__device__ __forceinline__ int d_off(int l, int h) { return (l >> 2) * 32 + 4 * ((2 * (l & 3) + h) ^ (l >> 2)); }
+
+template <int P>
+__device__ __forceinline__ void c_to_d(uint32_t (&v)[P][EPT], int l, uint32_t* wb) {
+#pragma unroll
+    for (int p = 0; p < P; p++)
+#pragma unroll
+        for (int k = 0; k < EPT; k++) wb[p * N + swz((l >> 2) * 32 + 4 * k + (l & 3))] = v[p][k];
+    __syncwarp();
+#pragma unroll
+    for (int p = 0; p < P; p++) {
+        const uint4 a = *reinterpret_cast<const uint4*>(wb + p * N + d_off(l, 0));
+        const uint4 b = *reinterpret_cast<const uint4*>(wb + p * N + d_off(l, 1));
+        v[p][0] = a.x; v[p][1] = a.y; v[p][2] = a.z; v[p][3] = a.w;
+        v[p][4] = b.x; v[p][5] = b.y; v[p][6] = b.z; v[p][7] = b.w;
+    }
+    __syncwarp();
+}
+
+template <int P>
+__device__ __forceinline__ void d_to_c(uint32_t (&v)[P][EPT], int l, uint32_t* wb) {
+#pragma unroll
+    for (int p = 0; p < P; p++) {
+        *reinterpret_cast<uint4*>(wb + p * N + d_off(l, 0)) = make_uint4(v[p][0], v[p][1], v[p][2], v[p][3]);
+        *reinterpret_cast<uint4*>(wb + p * N + d_off(l, 1)) = make_uint4(v[p][4], v[p][5], v[p][6], v[p][7]);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int p = 0; p < P; p++)
+#pragma unroll
+        for (int k = 0; k < EPT; k++) v[p][k] = wb[p * N + swz((l >> 2) * 32 + 4 * k + (l & 3))];
+    __syncwarp();
+}
+
+// in-register stage with register distance dd and twiddle index (1 << mm) + (e(k) >> (11 - mm))
+template <int P, bool FWD, typename E>
+__device__ __forceinline__ void reg_stage(uint32_t (&v)[P][EPT], int mm, int dd, E e, const uint32_t* __restrict__ w_t,
+                                          const uint32_t* __restrict__ wp_t, uint32_t q) {
+#pragma unroll
+    for (int k = 0; k < EPT; k++) {
+        if (k & dd) continue;
+        const int idx = (1 << mm) + (e(k) >> (11 - mm));
+        const uint32_t w = __ldg(w_t + idx), wp = __ldg(wp_t + idx);
+#pragma unroll
+        for (int p = 0; p < P; p++) {
+            if (FWD) fwd_bfly(v[p][k], v[p][k + dd], w, wp, q);
+            else inv_bfly(v[p][k], v[p][k + dd], w, wp, q);
+        }
+    }
+}
+
+// forward NTT of P polynomials of one limb: layout A in, layout D canonical out.
+// xbuf holds P * 2048 words for this group.
 template <int P>
 __device__ __forceinline__ void forward(uint32_t (&v)[P][EPT], int t, uint32_t* xbuf, int bar,
                                         const uint32_t* __restrict__ fw, const uint32_t* __restrict__ fwp,
                                         uint32_t q) {
+    const int l = t & 31;
+    uint32_t* wb = xbuf + (t >> 5) * 256;
 #pragma unroll
-    for (int mm = 0; mm < 3; mm++) {  // distances 1024, 512, 256
-        const int d = 4 >> mm;
-#pragma unroll
-        for (int m = 0; m < EPT; m++) {
-            if (m & d) continue;
-            const int idx = (1 << mm) + (m >> (3 - mm));
-            const uint32_t w = __ldg(fw + idx), wp = __ldg(fwp + idx);
-#pragma unroll
-            for (int p = 0; p < P; p++) fwd_bfly(v[p][m], v[p][m + d], w, wp, q);
-        }
-    }
+    for (int mm = 0; mm < 3; mm++) reg_stage<P, true>(v, mm, 4 >> mm, [&](int k) { return eA(t, k); }, fw, fwp, q);
     exchange<P, true>(v, t, xbuf, bar);
-    const int blk = t >> 5, r = t & 31;
 #pragma unroll
-    for (int mm = 3; mm < 6; mm++) {  // distances 128, 64, 32
-        const int d = 4 >> (mm - 3);
+    for (int mm = 3; mm < 6; mm++)
+        reg_stage<P, true>(v, mm, 4 >> (mm - 3), [&](int k) { return eB(t, k); }, fw, fwp, q);
+    b_to_c<P>(v, l, wb);
 #pragma unroll
-        for (int m = 0; m < EPT; m++) {
-            if (m & d) continue;
-            const int idx = (1 << mm) + (blk << (mm - 3)) + (m >> (6 - mm));
-            const uint32_t w = __ldg(fw + idx), wp = __ldg(fwp + idx);
+    for (int mm = 6; mm < 9; mm++)
+        reg_stage<P, true>(v, mm, 4 >> (mm - 6), [&](int k) { return eC(t, k); }, fw, fwp, q);
+    c_to_d<P>(v, l, wb);
 #pragma unroll
-            for (int p = 0; p < P; p++) fwd_bfly(v[p][m], v[p][m + d], w, wp, q);
-        }
-    }
-#pragma unroll
-    for (int mm = 6; mm < 11; mm++) {  // distances 16 .. 1 across lanes
-        const int d = 1024 >> mm;
-        const bool upper = r & d;
-#pragma unroll
-        for (int m = 0; m < EPT; m++) {
-            const int idx = (1 << mm) + ((blk * 256 + r + 32 * m) >> (11 - mm));
-            const uint32_t w = __ldg(fw + idx), wp = __ldg(fwp + idx);
-#pragma unroll
-            for (int p = 0; p < P; p++) {
-                const uint32_t mine = v[p][m];
-                const uint32_t wy = shoup_lazy(mine, w, wp, q);  // used by the upper lane only
-                const uint32_t recv = __shfl_xor_sync(0xffffffffu, upper ? wy : mine, d);
-                const uint32_t x = upper ? recv : mine;
-                const uint32_t xx = x >= 2 * q ? x - 2 * q : x;
-                v[p][m] = upper ? xx + 2 * q - wy : xx + recv;
-            }
-        }
-    }
+    for (int mm = 9; mm < 11; mm++)
+        reg_stage<P, true>(v, mm, 2 >> (mm - 9), [&](int k) { return eD(t, k); }, fw, fwp, q);
 #pragma unroll
     for (int p = 0; p < P; p++)
 #pragma unroll
-        for (int m = 0; m < EPT; m++) v[p][m] = canon(v[p][m], q);
+        for (int k = 0; k < EPT; k++) v[p][k] = canon(v[p][k], q);
 }
 
-// inverse NTT of P polynomials of one limb: layout B in, layout A canonical out
+// inverse NTT of P polynomials of one limb: layout D in, layout A canonical out
 template <int P>
 __device__ __forceinline__ void inverse(uint32_t (&v)[P][EPT], int t, uint32_t* xbuf, int bar,
                                         const uint32_t* __restrict__ iw, const uint32_t* __restrict__ iwp,
                                         uint32_t q) {
-    const int blk = t >> 5, r = t & 31;
+    const int l = t & 31;
+    uint32_t* wb = xbuf + (t >> 5) * 256;
 #pragma unroll
-    for (int mm = 10; mm >= 6; mm--) {  // distances 1 .. 16 across lanes
-        const int d = 1024 >> mm;
-        const bool upper = r & d;
+    for (int mm = 10; mm >= 9; mm--)
+        reg_stage<P, false>(v, mm, 2 >> (mm - 9), [&](int k) { return eD(t, k); }, iw, iwp, q);
+    d_to_c<P>(v, l, wb);
 #pragma unroll
-        for (int m = 0; m < EPT; m++) {
-            const int idx = (1 << mm) + ((blk * 256 + r + 32 * m) >> (11 - mm));
-            const uint32_t w = __ldg(iw + idx), wp = __ldg(iwp + idx);
+    for (int mm = 8; mm >= 6; mm--)
+        reg_stage<P, false>(v, mm, 4 >> (mm - 6), [&](int k) { return eC(t, k); }, iw, iwp, q);
+    c_to_b<P>(v, l, wb);
 #pragma unroll
-            for (int p = 0; p < P; p++) {
-                const uint32_t mine = v[p][m];
-                const uint32_t other = __shfl_xor_sync(0xffffffffu, mine, d);
-                uint32_t x = upper ? other : mine, y = upper ? mine : other;
-                inv_bfly(x, y, w, wp, q);
-                v[p][m] = upper ? y : x;
-            }
-        }
-    }
-#pragma unroll
-    for (int mm = 5; mm >= 3; mm--) {  // distances 32, 64, 128
-        const int d = 4 >> (mm - 3);
-#pragma unroll
-        for (int m = 0; m < EPT; m++) {
-            if (m & d) continue;
-            const int idx = (1 << mm) + (blk << (mm - 3)) + (m >> (6 - mm));
-            const uint32_t w = __ldg(iw + idx), wp = __ldg(iwp + idx);
-#pragma unroll
-            for (int p = 0; p < P; p++) inv_bfly(v[p][m], v[p][m + d], w, wp, q);
-        }
-    }
+    for (int mm = 5; mm >= 3; mm--)
+        reg_stage<P, false>(v, mm, 4 >> (mm - 3), [&](int k) { return eB(t, k); }, iw, iwp, q);
     exchange<P, false>(v, t, xbuf, bar);
 #pragma unroll
-    for (int mm = 2; mm >= 0; mm--) {  // distances 256, 512, 1024
-        const int d = 4 >> mm;
-#pragma unroll
-        for (int m = 0; m < EPT; m++) {
-            if (m & d) continue;
-            const int idx = (1 << mm) + (m >> (3 - mm));
-            const uint32_t w = __ldg(iw + idx), wp = __ldg(iwp + idx);
-#pragma unroll
-            for (int p = 0; p < P; p++) inv_bfly(v[p][m], v[p][m + d], w, wp, q);
-        }
-    }
+    for (int mm = 2; mm >= 0; mm--) reg_stage<P, false>(v, mm, 4 >> mm, [&](int k) { return eA(t, k); }, iw, iwp, q);
 #pragma unroll
     for (int p = 0; p < P; p++)
 #pragma unroll
-        for (int m = 0; m < EPT; m++) v[p][m] = canon(v[p][m], q);
+        for (int k = 0; k < EPT; k++) v[p][k] = canon(v[p][k], q);
 }
 
 }  // namespace nttr

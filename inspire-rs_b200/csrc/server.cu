@@ -20,6 +20,7 @@
 #include "host_math.hpp"
 #include "ipr_b200.h"
 #include "kernels.cuh"
+#include "server_internal.hpp"
 
 namespace {
 
@@ -54,86 +55,6 @@ namespace ipr {
 void set_last_error(const char* msg) { g_last_error = msg; }
 }  // namespace ipr
 
-struct ipr_server {
-    int device = 0;
-    int sm_count = 148;
-    ipr::Plan plan{};
-    ipr::HostParams hp;
-    cudaStream_t stream = nullptr;
-    // resident state
-    uint16_t* d_db = nullptr;
-    uint8_t* d_db8 = nullptr;  // [2][db_cols][db_rows] byte planes for the tensor-core GEMM
-    CUtensorMap tm_db;
-    bool gemv_tc = false;      // first dimension on tcgen05 (db_rows <= 32768)
-    bool fold_regs = true;     // fold with register-resident NTTs (k_fold2) vs shared-memory NTTs
-    std::map<int, CUtensorMap> tm_qb;  // per query-byte tile height
-    uint64_t *d_ahat = nullptr, *d_bt = nullptr, *d_btb = nullptr, *d_bth = nullptr;
-    uint8_t* d_stash = nullptr;
-    uint64_t stash_count = 0, stash_entry = 0;
-    uint32_t *d_fw = nullptr, *d_fwp = nullptr, *d_iw = nullptr, *d_iwp = nullptr, *d_row0 = nullptr;
-    // per-request scratch
-    unsigned cap_q = 0;
-    uint8_t* d_query = nullptr;
-    uint64_t *d_y = nullptr, *d_z = nullptr;
-    uint32_t *d_ail = nullptr, *d_gsw = nullptr, *d_S = nullptr;
-    uint64_t *d_R = nullptr, *d_c = nullptr;
-    uint8_t* d_resp = nullptr;
-    uint8_t* d_qb = nullptr;  // query bytes [(q*2 + limb)*4 + byte][db_rows]
-    int* d_err = nullptr;     // device-side wait failures (bounded waits)
-    uint8_t *h_query = nullptr, *h_resp = nullptr;
-    int* h_err = nullptr;
-    std::map<unsigned, cudaGraphExec_t> graphs;
-    std::mutex mu;
-    // batched path: precomputation re-indexed by slot (Tpp), batch scratch
-    uint8_t* d_tpp = nullptr;
-    CUtensorMap tm_tpp;
-    int bcap = 0, y8_np = 0;
-    uint8_t* d_bq = nullptr;
-    uint64_t *d_ybs = nullptr, *d_zbs = nullptr;
-    uint8_t* d_y8 = nullptr;
-    std::map<int, CUtensorMap> tm_y8;
-    uint32_t* d_bS = nullptr;
-    uint64_t* d_bR = nullptr;
-    uint8_t* d_bresp = nullptr;
-    uint8_t *h_bq = nullptr, *h_bresp = nullptr;
-    // profiling
-    bool profiling = false;
-    std::vector<cudaEvent_t> events;  // kMaxProfileSlots * (IPR_NSTAGES + 1)
-    int slots_used = 0;
-    double stage_ms[IPR_NSTAGES] = {0};
-    uint64_t calls = 0;
-    // public parameters
-    uint64_t key_size = 0, value_size = 0, num_records = 0;
-    uint8_t cuckoo_seed[16] = {0};
-    uint64_t hbm = 0;
-    std::vector<void*> allocs;
-
-    template <typename T>
-    int alloc(T** p, size_t bytes) {
-        void* v = nullptr;
-        cudaError_t e = cudaMalloc(&v, bytes ? bytes : 16);
-        if (e != cudaSuccess)
-            return fail(IPR_E_OOM, "cudaMalloc(%zu bytes) failed on device %d: %s", bytes, device,
-                        cudaGetErrorString(e));
-        allocs.push_back(v);
-        hbm += bytes;
-        *p = static_cast<T*>(v);
-        return IPR_OK;
-    }
-    void free_ptr(void* p) {
-        for (size_t i = 0; i < allocs.size(); i++)
-            if (allocs[i] == p) {
-                cudaFree(p);
-                allocs.erase(allocs.begin() + i);
-                return;
-            }
-    }
-    uint64_t per_query_bytes() const { return plan.c * IPR_RESULT_BYTES; }
-    uint64_t response_bytes(unsigned nq) const {
-        return 4 + (uint64_t)nq * (4 + per_query_bytes()) + 4 + stash_count * (4 + stash_entry);
-    }
-};
-
 namespace {
 
 void destroy_graphs(ipr_server* s) {
@@ -165,6 +86,7 @@ int qb_map(ipr_server* s, int nt, const CUtensorMap** out) {
 int ensure_scratch(ipr_server* s, unsigned nq) {
     const unsigned want = nq < 2 ? 2 : nq;
     if (want <= s->cap_q) return IPR_OK;
+    CU(cudaStreamSynchronize(s->stream));  // work already enqueued may still use the old buffers
     destroy_graphs(s);
     for (void* p : {(void*)s->d_query, (void*)s->d_ail, (void*)s->d_gsw, (void*)s->d_c, (void*)s->d_resp,
                     (void*)s->d_qb})
@@ -261,7 +183,7 @@ int next_profile_slot(ipr_server* s) {
     return s->slots_used++;
 }
 
-constexpr int kMaxBatch = 64;  // clients per tensor-core packing launch (N = 4 bytes x clients <= 256)
+constexpr int kMaxBatch = ipr::kMaxBatchPayloads;
 
 // build the slot-indexed precomputation once (35.4 GB at 1M records)
 int ensure_tpp(ipr_server* s) {
@@ -285,6 +207,7 @@ int ensure_batch(ipr_server* s, int B) {
     if (B <= s->bcap) return IPR_OK;
     int st = ensure_tpp(s);
     if (st) return st;
+    CU(cudaStreamSynchronize(s->stream));  // work already enqueued may still use the old buffers
     if ((st = ensure_scratch(s, 2 * (unsigned)B))) return st;
     for (void* p : {(void*)s->d_bq, (void*)s->d_ybs, (void*)s->d_zbs, (void*)s->d_y8, (void*)s->d_bS, (void*)s->d_bR,
                     (void*)s->d_bresp})
@@ -491,6 +414,38 @@ int respond_locked(ipr_server* s, const uint8_t* query, size_t len, uint8_t* out
 
 }  // namespace
 
+int ipr_server::alloc_failed(size_t bytes, cudaError_t e) const {
+    return fail(IPR_E_OOM, "cudaMalloc(%zu bytes) failed on device %d: %s", bytes, device, cudaGetErrorString(e));
+}
+
+namespace ipr {
+
+int server_ensure_batch(ipr_server* s, int payloads) { return ensure_batch(s, payloads); }
+
+int server_enqueue_batch(ipr_server* s, int payloads, const uint8_t* d_queries, uint8_t* d_resps) {
+    return enqueue_batch(s, payloads, d_queries, d_resps, next_profile_slot(s));
+}
+
+int server_respond_locked(ipr_server* s, const uint8_t* query, size_t len, uint8_t* out, size_t cap,
+                          size_t* out_len) {
+    return respond_locked(s, query, len, out, cap, out_len);
+}
+
+uint64_t server_batch_bytes(const ipr_server* s, int B) {
+    const ipr::Plan& p = s->plan;
+    const uint64_t rows = p.db_rows, cols = p.db_cols, no = p.instances, nq = 2ull * B;
+    const uint64_t qb = ipr::query_bytes(rows, 2), rb = s->response_bytes(2);
+    const uint64_t tpp = s->d_tpp ? 0 : ipr::tpp_bytes((int)no);
+    // ensure_scratch(2B) + ensure_batch(B) allocations
+    const uint64_t scratch = ipr::query_bytes(rows, (unsigned)nq) + 16 + (nq + 1) / 2 * rows * 16 + nq * 12 * kN * 4 +
+                             nq * cols * 8 + s->response_bytes((unsigned)nq) + qb_rows((unsigned)nq) * rows;
+    const uint64_t batch = B * qb + 2ull * B * 3 * kN * 8 + 2ull * ipr::pack_mma_nt(B) * 3 * kN +
+                           B * no * 2 * kN * 4 + B * no * kN * 8 + B * rb;
+    return tpp + scratch + batch;
+}
+
+}  // namespace ipr
+
 extern "C" {
 
 int ipr_plan_from_shape(uint64_t record_count, uint64_t key_size, uint64_t value_size, uint64_t buckets,
@@ -514,6 +469,86 @@ int ipr_plan_from_shape(uint64_t record_count, uint64_t key_size, uint64_t value
 }
 
 uint64_t ipr_query_bytes(uint64_t db_rows, unsigned num_queries) { return ipr::query_bytes(db_rows, num_queries); }
+
+int ipr_plan_shard(const ipr_plan* full, int num_shards, int shard, ipr_plan* out, uint64_t* first_instance) {
+    if (!full || !out || num_shards < 1 || shard < 0 || shard >= num_shards)
+        return fail(IPR_E_ARGS, "bad shard arguments");
+    if ((uint64_t)num_shards > full->c)
+        return fail(IPR_E_ARGS, "%d shards for %llu fold groups: every shard needs a group", num_shards,
+                    (unsigned long long)full->c);
+    if (full->c * full->interp != full->instances || full->db_cols != full->instances * kN)
+        return fail(IPR_E_ARGS, "plan is not a whole number of fold groups");
+    const uint64_t base = full->c / num_shards, rem = full->c % num_shards, k = (uint64_t)shard;
+    const uint64_t groups = base + (k < rem ? 1 : 0);
+    const uint64_t first_group = k * base + (k < rem ? k : rem);
+    *out = *full;
+    out->c = groups;
+    out->instances = groups * full->interp;
+    out->db_cols = out->instances * kN;
+    // the reference's setup estimate for the slice (keyword.rs:105-141)
+    const uint64_t nph = 1024;
+    out->peak_bytes = out->db_rows * out->db_cols * 2 + out->db_cols * 2 * kN * 8 +
+                      2 * out->instances * nph * 2 * kN * 8 + 2 * out->instances * (nph - 1) * 3 * kN * 8;
+    if (first_instance) *first_instance = first_group * full->interp;
+    return IPR_OK;
+}
+
+int ipr_response_merge(const uint8_t* const* parts, const size_t* lens, int num_parts, uint8_t* out, size_t cap,
+                       size_t* out_len) {
+    if (!parts || !lens || num_parts < 1) return fail(IPR_E_ARGS, "no parts");
+    auto rd32 = [](const uint8_t* p) {
+        return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
+    };
+    auto wr32 = [](uint8_t* p, uint32_t v) {
+        for (int i = 0; i < 4; i++) p[i] = (uint8_t)(v >> (8 * i));
+    };
+    // parse every part: count, per query (len, bytes), then the stash block
+    std::vector<std::vector<std::pair<size_t, uint32_t>>> q(num_parts);  // (offset, length) per query
+    std::vector<size_t> stash_at(num_parts);
+    uint32_t count = 0;
+    for (int k = 0; k < num_parts; k++) {
+        const uint8_t* p = parts[k];
+        const size_t n = lens[k];
+        if (!p || n < 8) return fail(IPR_E_FORMAT, "part %d is too short", k);
+        const uint32_t c = rd32(p);
+        if (k == 0) count = c;
+        else if (c != count) return fail(IPR_E_FORMAT, "part %d has %u responses, part 0 has %u", k, c, count);
+        size_t off = 4;
+        for (uint32_t i = 0; i < c; i++) {
+            if (off + 4 > n) return fail(IPR_E_FORMAT, "part %d is truncated", k);
+            const uint32_t l = rd32(p + off);
+            if (off + 4 + l > n) return fail(IPR_E_FORMAT, "part %d is truncated", k);
+            q[k].push_back({off + 4, l});
+            off += 4 + (size_t)l;
+        }
+        if (off + 4 > n) return fail(IPR_E_FORMAT, "part %d has no stash block", k);
+        stash_at[k] = off;
+    }
+    const size_t stash_bytes = lens[0] - stash_at[0];
+    size_t total = 4 + stash_bytes;
+    for (uint32_t i = 0; i < count; i++) {
+        uint64_t l = 0;
+        for (int k = 0; k < num_parts; k++) l += q[k][i].second;
+        if (l > 0xffffffffull) return fail(IPR_E_FORMAT, "merged response %u is too long", i);
+        total += 4 + l;
+    }
+    if (out_len) *out_len = total;
+    if (!out || cap < total) return fail(IPR_E_SPACE, "merged response needs %zu bytes", total);
+    wr32(out, count);
+    size_t o = 4;
+    for (uint32_t i = 0; i < count; i++) {
+        uint32_t l = 0;
+        for (int k = 0; k < num_parts; k++) l += q[k][i].second;
+        wr32(out + o, l);
+        o += 4;
+        for (int k = 0; k < num_parts; k++) {
+            std::memcpy(out + o, parts[k] + q[k][i].first, q[k][i].second);
+            o += q[k][i].second;
+        }
+    }
+    std::memcpy(out + o, parts[0] + stash_at[0], stash_bytes);  // the stash echo of the first part
+    return IPR_OK;
+}
 
 int ipr_server_create(int device, const ipr_plan* plan, const ipr_server_data* data, ipr_server** out) {
     if (!out || !data || !data->db || !data->a_hat || !data->bold_t || !data->bold_t_bar || !data->bold_t_hat)

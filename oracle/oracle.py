@@ -238,6 +238,20 @@ class SynthDB:
         self.stash = [bytes(s) for s in stash]
         self._stash_buf = np.frombuffer(b"".join(self.stash) or b"\0", dtype=np.uint8).copy()
 
+    def shard(self, first_instance: int, instances: int, interp: int, c: int) -> "SynthDB":
+        """the state of fold groups starting at `first_instance` (views into this state)"""
+        sub = SynthDB.__new__(SynthDB)
+        sub.db_rows, sub.instances, sub.interp, sub.c, sub.seed = self.db_rows, instances, interp, c, self.seed
+        sub.db_cols = instances * N
+        f, n = first_instance, instances
+        sub.db = self.db[f * N * self.db_rows:(f + n) * N * self.db_rows]
+        sub.a_hat = self.a_hat[f * N:(f + n) * N]
+        sub.bold_t = self.bold_t[f * NINNER * N:(f + n) * NINNER * N]
+        sub.bold_t_bar = self.bold_t_bar[f * NINNER * N:(f + n) * NINNER * N]
+        sub.bold_t_hat = self.bold_t_hat[f * 3 * N:(f + n) * 3 * N]
+        sub.stash, sub._stash_buf = self.stash, self._stash_buf
+        return sub
+
     def c_struct(self) -> OracleDB:
         d = OracleDB()
         d.db_rows, d.db_cols, d.num_outputs, d.interp, d.c = (self.db_rows, self.db_cols, self.instances,

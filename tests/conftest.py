@@ -26,6 +26,11 @@ def load_package():
     return mod
 
 
+def load_oracle():
+    import oracle
+    return oracle
+
+
 def gpu_available():
     try:
         import torch

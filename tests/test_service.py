@@ -1,0 +1,138 @@
+"""Serving loop (ipr_service_*): continuous batching over one or more servers.
+
+Every response must equal the payload answered alone (ipr_server_respond) and
+the oracle, whether it ran alone, in a batch with other clients, next to
+payloads with other query counts, or next to another database's traffic.
+"""
+import threading
+import time
+
+import pytest
+
+N = 2048
+
+
+def _plan(pkg, instances, interp, db_rows=2048):
+    return pkg.Plan(num_items=max(db_rows, 32768), entry_size=1216, item_size_bits=9728, dim0=db_rows,
+                    db_rows=db_rows, db_cols=instances * N, instances=instances, interp=interp,
+                    c=instances // interp, peak_bytes=0)
+
+
+@pytest.fixture(scope="module")
+def dbs(pkg, orc):
+    """two databases of different shapes"""
+    out = []
+    for inst, interp, seed in ((8, 8, 7), (4, 2, 19)):
+        plan = _plan(pkg, inst, interp)
+        srv = pkg.KeywordServer.synthetic(plan, seed=seed)
+        sdb = orc.SynthDB(plan.db_rows, inst, interp, plan.c, seed=seed)
+        out.append((plan, srv, sdb))
+    yield out
+    for _, srv, _ in out:
+        srv.close()
+
+
+@pytest.mark.gpu
+def test_alone_equals_in_mix(pkg, orc, dbs):
+    plan, srv, sdb = dbs[0]
+    queries = [orc.synth_query(500 + i, plan.db_rows, 2) for i in range(12)]
+    queries += [orc.synth_query(600, plan.db_rows, 1), orc.synth_query(601, plan.db_rows, 3),
+                orc.synth_query(602, plan.db_rows, 0)]
+    alone = [srv.respond_to_serialized_query(q) for q in queries]
+    for q, a in zip(queries[:3] + queries[-3:], alone[:3] + alone[-3:]):
+        assert a == orc.respond(sdb, q)
+    with pkg.KeywordService([srv]) as svc:
+        # one at a time
+        for q, a in zip(queries, alone):
+            assert svc.wait(svc.submit(0, q)) == a
+        # all at once: batches form from whatever is pending
+        tickets = [svc.submit(0, q) for q in queries]
+        got = [svc.wait(t) for t in tickets]
+        assert got == alone
+        st = svc.stats()
+        assert st.completed == 2 * len(queries) and st.failed == 0 and st.in_flight == 0
+        assert st.batches >= 1 and st.batched_payloads >= 1 and st.max_batch == 64
+
+
+@pytest.mark.gpu
+def test_two_databases_concurrent_clients(pkg, orc, dbs):
+    (p0, s0, d0), (p1, s1, d1) = dbs
+    q0 = [orc.synth_query(700 + i, p0.db_rows, 2) for i in range(20)]
+    q1 = [orc.synth_query(800 + i, p1.db_rows, 2) for i in range(20)]
+    want0 = [s0.respond_to_serialized_query(q) for q in q0]
+    want1 = [s1.respond_to_serialized_query(q) for q in q1]
+    assert want1[0] == orc.respond(d1, q1[0])
+    results = {}
+    with pkg.KeywordService([s0, s1], max_batch=8) as svc:
+        def client(db, qs, key):
+            ts = []
+            for q in qs:
+                ts.append(svc.submit(db, q))
+                time.sleep(0.0005)
+            results[key] = [svc.wait(t, 60000) for t in ts]
+        th = [threading.Thread(target=client, args=(0, q0[:10], "a")),
+              threading.Thread(target=client, args=(0, q0[10:], "b")),
+              threading.Thread(target=client, args=(1, q1, "c"))]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        assert results["a"] + results["b"] == want0
+        assert results["c"] == want1
+        st = svc.stats()
+        assert st.max_batch == 8 and st.failed == 0 and st.completed == 40
+        assert st.p50_us > 0 and st.p99_us >= st.p50_us
+
+
+@pytest.mark.gpu
+def test_admission_by_hbm_budget_and_queue(pkg, orc, dbs):
+    plan, srv, _ = dbs[0]
+    srv.prepare_batch(1)  # the slot-indexed precomputation exists: footprints below are scratch only
+    with pytest.raises(pkg.IprError) as ei:
+        pkg.KeywordService([srv], hbm_budget_bytes=1 << 20)
+    assert ei.value.status == -2  # IPR_E_OOM: not even one payload fits
+    # a budget between the 3- and 4-payload footprints admits batches of 3
+    probe = [pkg.KeywordService([srv], max_batch=b, hbm_budget_bytes=1 << 40) for b in (3, 4)]
+    need3, need4 = probe[0].stats().hbm_bytes, probe[1].stats().hbm_bytes
+    for p in probe:
+        p.close()
+    assert need4 > need3
+    with pkg.KeywordService([srv], hbm_budget_bytes=(need3 + need4) // 2) as svc:
+        assert svc.stats().max_batch == 3
+        q = orc.synth_query(900, plan.db_rows, 2)
+        want = srv.respond_to_serialized_query(q)
+        ts = [svc.submit(0, q) for _ in range(7)]
+        assert all(svc.wait(t) == want for t in ts)
+        assert svc.stats().batched_payloads == 7
+    with pkg.KeywordService([srv], max_pending=2) as svc:
+        q = orc.synth_query(901, plan.db_rows, 2)
+        ts, busy = [], 0
+        for _ in range(40):
+            try:
+                ts.append(svc.submit(0, q))
+            except pkg.IprError as e:
+                assert e.status == -8  # IPR_E_BUSY
+                busy += 1
+        assert busy > 0 and svc.stats().rejected == busy
+        want = srv.respond_to_serialized_query(q)
+        assert all(svc.wait(t) == want for t in ts)
+
+
+@pytest.mark.gpu
+def test_service_errors_and_poll(pkg, orc, dbs):
+    plan, srv, _ = dbs[0]
+    with pkg.KeywordService([srv]) as svc:
+        with pytest.raises(pkg.IprError):
+            svc.submit(5, b"\x02")  # no such database
+        with pytest.raises(pkg.IprError):
+            svc.submit(0, b"\x02" + bytes(100))  # shorter than two queries need
+        t = svc.submit(0, orc.synth_query(902, plan.db_rows, 2))
+        r = None
+        for _ in range(20000):
+            r = svc.poll(t)
+            if r is not None:
+                break
+            time.sleep(0.001)
+        assert r == srv.respond_to_serialized_query(orc.synth_query(902, plan.db_rows, 2))
+        with pytest.raises(pkg.IprError):
+            svc.poll(t)  # collected tickets are released
