@@ -10,7 +10,9 @@
 // group transforms the 6 gadget-digit polynomials of its limb together (one
 // twiddle load per 6 butterflies, one exchange barrier pair for all six),
 // accumulates both rows of the 2x6 product in registers, and runs the 2
-// inverse NTTs together; the two limbs meet only at the CRT compose.
+// inverse NTTs together; the two limbs meet only at the CRT compose.  The
+// query's RGSW bodies sit in shared memory for the whole chain, and each
+// step's packed operands are copied in asynchronously while its transforms run.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -30,6 +32,15 @@ constexpr int EPT = nttr::EPT;
 #endif
 constexpr int FP = IPR_FOLD_FWD_BATCH;  // gadget-digit polynomials transformed together
 static_assert(6 % FP == 0, "forward batch must divide the 6 gadget rows");
+constexpr int XB = 3;  // polynomials per exchange buffer (the 6 forward transforms pass in two halves)
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 using nttr::eA;
 using nttr::eD;
@@ -64,39 +75,55 @@ __global__ void __launch_bounds__(F_THREADS, 1)
             const uint32_t* __restrict__ iwp, int interp, int64_t db_cols, int qpp, uint8_t* __restrict__ resp,
             int64_t resp_payload_stride, int64_t resp_query_stride) {
     extern __shared__ uint64_t fold_smem[];
-    uint64_t(*sum)[N] = reinterpret_cast<uint64_t(*)[N]>(fold_smem);                  // [2 rows][N]
-    uint32_t* xbase = reinterpret_cast<uint32_t*>(fold_smem + 2 * N);                 // [2 limbs][FP][N]
+    uint64_t(*sum)[N] = reinterpret_cast<uint64_t(*)[N]>(fold_smem);             // [2 rows][N]
+    uint64_t(*pk)[N] = reinterpret_cast<uint64_t(*)[N]>(fold_smem + 2 * N);      // a_hat, c, R rows of step j
+    uint32_t* sbody = reinterpret_cast<uint32_t*>(fold_smem + 5 * N);            // [6][2][N] RGSW bodies
+    uint32_t* xbase = reinterpret_cast<uint32_t*>(fold_smem + 11 * N);           // [2 limbs][XB][N]
     const int wp = blockIdx.x, qg = blockIdx.y;
     const int payload = qg / qpp, qin = qg % qpp;
     const uint64_t* Rp = R + (int64_t)payload * r_payload_stride;
-    const uint32_t* body = gsw + (int64_t)qg * 12 * N;  // [6][2][N]
     const uint64_t* cq = cvec + (int64_t)qg * db_cols;
     const int g = threadIdx.x >> 8, t = threadIdx.x & 255;
     const int bar = 1 + g;
     const uint32_t q = g ? Q1 : Q0;
     const uint64_t br = g ? BR1 : BR0;
-    uint32_t* xbuf = xbase + g * FP * N;
+    uint32_t* xbuf = xbase + g * XB * N;
     // after the inverse transforms a group's exchange buffer holds its limb of both rows
     const uint32_t* lb0 = xbase;
-    const uint32_t* lb1 = xbase + FP * N;
+    const uint32_t* lb1 = xbase + XB * N;
     const uint32_t* fwl = fw + g * N;
     const uint32_t* fwpl = fwp + g * N;
     const uint32_t* iwl = iw + g * N;
     const uint32_t* iwpl = iwp + g * N;
     const uint64_t mask = (1ull << GADGET_BITS) - 1;
 
-    // first step: s = 0, the product vanishes -> s = packed[interp-1] mod q
-    {
-        const int j = wp * interp + interp - 1;
-        for (int i = threadIdx.x; i < 2 * N; i += F_THREADS) {
-            const int rr = i >> 11, e = i & (N - 1);
-            const uint64_t pk = rr == 0 ? a_hat[(int64_t)j * N + e] : cq[(int64_t)j * N + e] + Rp[(int64_t)j * N + e];
-            sum[rr][e] = pk % QQ;
+    // the rows of packed[j] (a_hat[j]; c[j], R[j] of this query / payload) land in pk while the
+    // step's transforms run: 3 x 16 KB in 16-byte asynchronous copies
+    auto fetch_packed = [&](int j) {
+        for (int i = threadIdx.x; i < 3 * N / 2; i += F_THREADS) {
+            const int r = i / (N / 2), o = (i % (N / 2)) * 2;
+            const uint64_t* src = r == 0 ? a_hat : (r == 1 ? cq : Rp);
+            cp_async16(&pk[r][o], src + (int64_t)j * N + o);
         }
-        __syncthreads();
+        cp_async_commit();
+    };
+
+    // the query's six RGSW bodies stay in shared memory for the whole chain
+    {
+        const uint32_t* gb = gsw + (int64_t)qg * 12 * N;
+        for (int i = threadIdx.x; i < 12 * N / 4; i += F_THREADS) cp_async16(sbody + 4 * i, gb + 4 * i);
     }
+    // first step: s = 0, the product vanishes -> s = packed[interp-1] mod q
+    fetch_packed(wp * interp + interp - 1);
+    cp_async_wait_all();
+    __syncthreads();
+    for (int i = threadIdx.x; i < 2 * N; i += F_THREADS) {
+        const int rr = i >> 11, e = i & (N - 1);
+        sum[rr][e] = (rr == 0 ? pk[0][e] : pk[1][e] + pk[2][e]) % QQ;
+    }
+    __syncthreads();
     for (int step = interp - 2; step >= 0; step--) {
-        const int j = wp * interp + step;
+        fetch_packed(wp * interp + step);
         uint32_t acc0[EPT];
         uint64_t acc1[EPT];
 #pragma unroll
@@ -113,11 +140,12 @@ __global__ void __launch_bounds__(F_THREADS, 1)
 #pragma unroll
                 for (int m = 0; m < EPT; m++) v[pp][m] = (uint32_t)((sum[rr][eA(t, m)] >> (k * GADGET_BITS)) & mask);
             }
-            nttr::forward<FP>(v, t, xbuf, bar, fwl, fwpl, q);
+            nttr::forward<FP, XB>(v, t, xbuf, bar, fwl, fwpl, q);
 #pragma unroll
             for (int pp = 0; pp < FP; pp++) {
-                uint32_t bv[EPT];
-                load_d(bv, body + ((pb + pp) * 2 + g) * N, t);
+                const uint4* bp = reinterpret_cast<const uint4*>(sbody + ((pb + pp) * 2 + g) * N + eD(t, 0));
+                const uint4 b0 = bp[0], b1 = bp[1];
+                const uint32_t bv[EPT] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
 #pragma unroll
                 for (int m = 0; m < EPT; m++) {
                     acc0[m] += v[pp][m];                         // < 6q
@@ -133,17 +161,18 @@ __global__ void __launch_bounds__(F_THREADS, 1)
             pr[0][m] = mod64((uint64_t)r0[m] * a0, q, br);
             pr[1][m] = mod64(acc1[m], q, br);
         }
-        nttr::inverse<2>(pr, t, xbuf, bar, iwl, iwpl, q);
+        nttr::inverse<2, XB>(pr, t, xbuf, bar, iwl, iwpl, q);
 #pragma unroll
         for (int m = 0; m < EPT; m++) {
             xbuf[eA(t, m)] = pr[0][m];
             xbuf[N + eA(t, m)] = pr[1][m];
         }
+        cp_async_wait_all();
         __syncthreads();
         for (int i = threadIdx.x; i < 2 * N; i += F_THREADS) {
             const int rr = i >> 11, e = i & (N - 1);
             uint64_t v = crt2(lb0[rr * N + e], lb1[rr * N + e], Q0INV, BR1);
-            v += rr == 0 ? a_hat[(int64_t)j * N + e] : cq[(int64_t)j * N + e] + Rp[(int64_t)j * N + e];  // < 3q
+            v += rr == 0 ? pk[0][e] : pk[1][e] + pk[2][e];  // < 3q
             v = v >= QQ ? v - QQ : v;
             v = v >= QQ ? v - QQ : v;
             sum[rr][e] = v;
@@ -163,7 +192,8 @@ __global__ void __launch_bounds__(F_THREADS, 1)
     }
 }
 
-constexpr int FOLD2_SMEM = 2 * N * 8 + 2 * FP * N * 4;  // 128 KB at FP = 6
+// sum 32 KB + packed rows 48 KB + RGSW bodies 96 KB + exchange buffers 2 x 3 x 8 KB = 224 KB
+constexpr int FOLD2_SMEM = (2 + 3 + 6 + 3) * N * 8;
 
 cudaError_t init_fold2_kernel() {
     return cudaFuncSetAttribute(k_fold2, cudaFuncAttributeMaxDynamicSharedMemorySize, FOLD2_SMEM);

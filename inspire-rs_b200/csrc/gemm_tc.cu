@@ -10,9 +10,10 @@
 // P_pb < 255^2 * db_rows < 2^31 for db_rows <= 32768, so accumulation is exact,
 // and the recombination sum_{p,b} 256^(p+b) P_pb < 2^63 fits a u64.
 //
-// Kernel shape: persistent CTAs of 6 warps.  Warp 0 issues TMA loads of
-// [128 rows x 128 bytes] DB tiles and [NT x 128 bytes] query-byte tiles into a
-// multi-stage shared-memory ring (128-byte swizzle); warp 1 issues the MMAs
+// Kernel shape: persistent CTAs of 6 warps.  Warp 0 issues TMA loads into a
+// multi-stage shared-memory ring (128-byte swizzle); one stage holds the same
+// [128 rows x 128 bytes] K-slice of both DB planes and one [NT x 128 bytes]
+// query-byte tile, so each query tile feeds two MMAs; warp 1 issues the MMAs
 // (M = 128 DB columns, N = NT query-byte columns, K = 32 bytes each) into
 // TMEM accumulators, one per plane, double buffered when they fit; warps 2-5
 // read the accumulators, recombine, reduce mod q0 / q1 and CRT-compose.
@@ -54,8 +55,8 @@ __global__ void __launch_bounds__(G1_THREADS, 1)
     volatile int* err = &sh->err;
     uint8_t* tiles = base + 1024;
     const int b_stage_bytes = nt * TILE_K;
-    uint8_t* a_tiles = tiles;
-    uint8_t* b_tiles = tiles + stages * A_STAGE_BYTES;
+    uint8_t* a_tiles = tiles;  // [stage][plane][128 x 128]
+    uint8_t* b_tiles = tiles + stages * 2 * A_STAGE_BYTES;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nbuf = (4 * nt <= 512) ? 2 : 1;
@@ -80,8 +81,7 @@ __global__ void __launch_bounds__(G1_THREADS, 1)
     umma::fence_after();
     const uint32_t tmem = sh->tmem_base;
 
-    const int kpp = db_rows / TILE_K;  // stages per plane
-    const int ks_total = 2 * kpp;
+    const int ks_total = db_rows / TILE_K;  // stages per tile (both planes in each)
     const int64_t m_tiles = db_cols / TILE_M;
     const int64_t total = m_tiles * n_tiles;
 
@@ -99,11 +99,12 @@ __global__ void __launch_bounds__(G1_THREADS, 1)
                         *err = 1;
                         break;
                     }
-                    umma::mbar_expect_tx(&sh->full[stage], A_STAGE_BYTES + b_stage_bytes);
-                    const int p = ks / kpp, kk = ks % kpp;
-                    umma::tma_load_2d(a_tiles + stage * A_STAGE_BYTES, &tm_db, kk * TILE_K,
-                                      (int)(p * db_cols + m * TILE_M), &sh->full[stage]);
-                    umma::tma_load_2d(b_tiles + stage * b_stage_bytes, &tm_qb, kk * TILE_K, n * nt, &sh->full[stage]);
+                    umma::mbar_expect_tx(&sh->full[stage], 2 * A_STAGE_BYTES + b_stage_bytes);
+                    uint8_t* at = a_tiles + stage * 2 * A_STAGE_BYTES;
+                    umma::tma_load_2d(at, &tm_db, ks * TILE_K, (int)(m * TILE_M), &sh->full[stage]);
+                    umma::tma_load_2d(at + A_STAGE_BYTES, &tm_db, ks * TILE_K, (int)(db_cols + m * TILE_M),
+                                      &sh->full[stage]);
+                    umma::tma_load_2d(b_tiles + stage * b_stage_bytes, &tm_qb, ks * TILE_K, n * nt, &sh->full[stage]);
                     last_phase[stage] = (int)phase;
                     if (++stage == stages) {
                         stage = 0;
@@ -134,15 +135,16 @@ __global__ void __launch_bounds__(G1_THREADS, 1)
                         break;
                     }
                     umma::fence_after();
-                    const int p = ks / kpp;
-                    const bool first = (ks % kpp) == 0;
-                    const uint32_t d = tmem + (uint32_t)((buf * 2 + p) * nt);
-                    const uint32_t sa = umma::smem_addr(a_tiles + stage * A_STAGE_BYTES);
+                    const uint32_t d0 = tmem + (uint32_t)(buf * 2 * nt), d1 = d0 + (uint32_t)nt;
+                    const uint32_t sa = umma::smem_addr(a_tiles + stage * 2 * A_STAGE_BYTES);
                     const uint32_t sb = umma::smem_addr(b_tiles + stage * b_stage_bytes);
 #pragma unroll
-                    for (int k4 = 0; k4 < TILE_K / 32; k4++)
-                        umma::mma_u8(d, umma::desc_sw128(sa + 32 * k4), umma::desc_sw128(sb + 32 * k4), idesc,
-                                     (first && k4 == 0) ? 0u : 1u);
+                    for (int k4 = 0; k4 < TILE_K / 32; k4++) {
+                        const uint64_t db = umma::desc_sw128(sb + 32 * k4);
+                        const uint32_t acc = (ks == 0 && k4 == 0) ? 0u : 1u;
+                        umma::mma_u8(d0, umma::desc_sw128(sa + 32 * k4), db, idesc, acc);
+                        umma::mma_u8(d1, umma::desc_sw128(sa + A_STAGE_BYTES + 32 * k4), db, idesc, acc);
+                    }
                     umma::commit(&sh->empty[stage]);  // frees the smem stage when these MMAs finish
                     last_stage = stage;
                     last_parity = phase;
@@ -264,12 +266,12 @@ cudaError_t make_u8_tile_map(CUtensorMap* map, const void* base, uint64_t row_by
 }
 
 int gemm1_stages(int nt) {
-    const int per = A_STAGE_BYTES + nt * TILE_K;
-    int s = (200 * 1024) / per;
+    const int per = 2 * A_STAGE_BYTES + nt * TILE_K;
+    int s = (210 * 1024) / per;
     return s > 8 ? 8 : (s < 2 ? 2 : s);
 }
 
-size_t gemm1_smem_bytes(int nt) { return 2048 + (size_t)gemm1_stages(nt) * (A_STAGE_BYTES + nt * TILE_K); }
+size_t gemm1_smem_bytes(int nt) { return 2048 + (size_t)gemm1_stages(nt) * (2 * A_STAGE_BYTES + nt * TILE_K); }
 
 cudaError_t init_gemm1_kernel() {
     size_t mx = 0;  // the largest footprint over every tile height the launcher can pick

@@ -64,83 +64,102 @@ __device__ __forceinline__ uint32_t canon(uint32_t v, uint32_t q) {
     return v >= q ? v - q : v;
 }
 
-// A <-> B exchange of P polynomials through xbuf (P * 2048 words), group barrier id bar
-template <int P, bool A_TO_B>
+// A <-> B exchange of P polynomials through xbuf (XP * 2048 words, XP <= P polynomials at a
+// time), group barrier id bar
+template <int P, bool A_TO_B, int XP = P>
 __device__ __forceinline__ void exchange(uint32_t (&v)[P][EPT], int t, uint32_t* xbuf, int bar) {
 #pragma unroll
-    for (int p = 0; p < P; p++)
+    for (int c0 = 0; c0 < P; c0 += XP) {
 #pragma unroll
-        for (int m = 0; m < EPT; m++) xbuf[p * N + (A_TO_B ? eA(t, m) : eB(t, m))] = v[p][m];
-    group_bar(bar);
+        for (int p = c0; p < c0 + XP && p < P; p++)
 #pragma unroll
-    for (int p = 0; p < P; p++)
+            for (int m = 0; m < EPT; m++) xbuf[(p - c0) * N + (A_TO_B ? eA(t, m) : eB(t, m))] = v[p][m];
+        group_bar(bar);
 #pragma unroll
-        for (int m = 0; m < EPT; m++) v[p][m] = xbuf[p * N + (A_TO_B ? eB(t, m) : eA(t, m))];
-    group_bar(bar);
+        for (int p = c0; p < c0 + XP && p < P; p++)
+#pragma unroll
+            for (int m = 0; m < EPT; m++) v[p][m] = xbuf[(p - c0) * N + (A_TO_B ? eB(t, m) : eA(t, m))];
+        group_bar(bar);
+    }
 }
 
-// intra-warp transposes; wb = the warp's 256-word block of the polynomial-0 buffer
-template <int P>
-__device__ __forceinline__ void b_to_c(uint32_t (&v)[P][EPT], int l, uint32_t* wb) {
-#pragma unroll
-    for (int p = 0; p < P; p++)
-#pragma unroll
-        for (int m = 0; m < EPT; m++) wb[p * N + swz(l + 32 * m)] = v[p][m];
-    __syncwarp();
-#pragma unroll
-    for (int p = 0; p < P; p++)
-#pragma unroll
-        for (int k = 0; k < EPT; k++) v[p][k] = wb[p * N + swz((l >> 2) * 32 + 4 * k + (l & 3))];
-    __syncwarp();
-}
-
-template <int P>
-__device__ __forceinline__ void c_to_b(uint32_t (&v)[P][EPT], int l, uint32_t* wb) {
-#pragma unroll
-    for (int p = 0; p < P; p++)
-#pragma unroll
-        for (int k = 0; k < EPT; k++) wb[p * N + swz((l >> 2) * 32 + 4 * k + (l & 3))] = v[p][k];
-    __syncwarp();
-#pragma unroll
-    for (int p = 0; p < P; p++)
-#pragma unroll
-        for (int m = 0; m < EPT; m++) v[p][m] = wb[p * N + swz(l + 32 * m)];
-    __syncwarp();
-}
-
+// intra-warp transposes; wb = the warp's 256-word block of the buffer's polynomial 0, the
+// buffer holding XP polynomials (P are moved, XP at a time)
+__device__ __forceinline__ int c_word(int l, int k) { return swz((l >> 2) * 32 + 4 * k + (l & 3)); }
+__device__ __forceinline__ int b_word(int l, int m) { return swz(l + 32 * m); }
 // layout D's 8 words of lane l sit in two aligned 4-word groups: swz(8 l + k)
 __device__ __forceinline__ int d_off(int l, int h) { return (l >> 2) * 32 + 4 * ((2 * (l & 3) + h) ^ (l >> 2)); }
 
-template <int P>
-__device__ __forceinline__ void c_to_d(uint32_t (&v)[P][EPT], int l, uint32_t* wb) {
+template <int P, int XP = P>
+__device__ __forceinline__ void b_to_c(uint32_t (&v)[P][EPT], int l, uint32_t* wb) {
 #pragma unroll
-    for (int p = 0; p < P; p++)
+    for (int c0 = 0; c0 < P; c0 += XP) {
 #pragma unroll
-        for (int k = 0; k < EPT; k++) wb[p * N + swz((l >> 2) * 32 + 4 * k + (l & 3))] = v[p][k];
-    __syncwarp();
+        for (int p = c0; p < c0 + XP && p < P; p++)
 #pragma unroll
-    for (int p = 0; p < P; p++) {
-        const uint4 a = *reinterpret_cast<const uint4*>(wb + p * N + d_off(l, 0));
-        const uint4 b = *reinterpret_cast<const uint4*>(wb + p * N + d_off(l, 1));
-        v[p][0] = a.x; v[p][1] = a.y; v[p][2] = a.z; v[p][3] = a.w;
-        v[p][4] = b.x; v[p][5] = b.y; v[p][6] = b.z; v[p][7] = b.w;
+            for (int m = 0; m < EPT; m++) wb[(p - c0) * N + b_word(l, m)] = v[p][m];
+        __syncwarp();
+#pragma unroll
+        for (int p = c0; p < c0 + XP && p < P; p++)
+#pragma unroll
+            for (int k = 0; k < EPT; k++) v[p][k] = wb[(p - c0) * N + c_word(l, k)];
+        __syncwarp();
     }
-    __syncwarp();
 }
 
-template <int P>
+template <int P, int XP = P>
+__device__ __forceinline__ void c_to_b(uint32_t (&v)[P][EPT], int l, uint32_t* wb) {
+#pragma unroll
+    for (int c0 = 0; c0 < P; c0 += XP) {
+#pragma unroll
+        for (int p = c0; p < c0 + XP && p < P; p++)
+#pragma unroll
+            for (int k = 0; k < EPT; k++) wb[(p - c0) * N + c_word(l, k)] = v[p][k];
+        __syncwarp();
+#pragma unroll
+        for (int p = c0; p < c0 + XP && p < P; p++)
+#pragma unroll
+            for (int m = 0; m < EPT; m++) v[p][m] = wb[(p - c0) * N + b_word(l, m)];
+        __syncwarp();
+    }
+}
+
+template <int P, int XP = P>
+__device__ __forceinline__ void c_to_d(uint32_t (&v)[P][EPT], int l, uint32_t* wb) {
+#pragma unroll
+    for (int c0 = 0; c0 < P; c0 += XP) {
+#pragma unroll
+        for (int p = c0; p < c0 + XP && p < P; p++)
+#pragma unroll
+            for (int k = 0; k < EPT; k++) wb[(p - c0) * N + c_word(l, k)] = v[p][k];
+        __syncwarp();
+#pragma unroll
+        for (int p = c0; p < c0 + XP && p < P; p++) {
+            const uint4 a = *reinterpret_cast<const uint4*>(wb + (p - c0) * N + d_off(l, 0));
+            const uint4 b = *reinterpret_cast<const uint4*>(wb + (p - c0) * N + d_off(l, 1));
+            v[p][0] = a.x; v[p][1] = a.y; v[p][2] = a.z; v[p][3] = a.w;
+            v[p][4] = b.x; v[p][5] = b.y; v[p][6] = b.z; v[p][7] = b.w;
+        }
+        __syncwarp();
+    }
+}
+
+template <int P, int XP = P>
 __device__ __forceinline__ void d_to_c(uint32_t (&v)[P][EPT], int l, uint32_t* wb) {
 #pragma unroll
-    for (int p = 0; p < P; p++) {
-        *reinterpret_cast<uint4*>(wb + p * N + d_off(l, 0)) = make_uint4(v[p][0], v[p][1], v[p][2], v[p][3]);
-        *reinterpret_cast<uint4*>(wb + p * N + d_off(l, 1)) = make_uint4(v[p][4], v[p][5], v[p][6], v[p][7]);
+    for (int c0 = 0; c0 < P; c0 += XP) {
+#pragma unroll
+        for (int p = c0; p < c0 + XP && p < P; p++) {
+            *reinterpret_cast<uint4*>(wb + (p - c0) * N + d_off(l, 0)) = make_uint4(v[p][0], v[p][1], v[p][2], v[p][3]);
+            *reinterpret_cast<uint4*>(wb + (p - c0) * N + d_off(l, 1)) = make_uint4(v[p][4], v[p][5], v[p][6], v[p][7]);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int p = c0; p < c0 + XP && p < P; p++)
+#pragma unroll
+            for (int k = 0; k < EPT; k++) v[p][k] = wb[(p - c0) * N + c_word(l, k)];
+        __syncwarp();
     }
-    __syncwarp();
-#pragma unroll
-    for (int p = 0; p < P; p++)
-#pragma unroll
-        for (int k = 0; k < EPT; k++) v[p][k] = wb[p * N + swz((l >> 2) * 32 + 4 * k + (l & 3))];
-    __syncwarp();
 }
 
 // in-register stage with register distance dd and twiddle index (1 << mm) + (e(k) >> (11 - mm))
@@ -161,8 +180,8 @@ __device__ __forceinline__ void reg_stage(uint32_t (&v)[P][EPT], int mm, int dd,
 }
 
 // forward NTT of P polynomials of one limb: layout A in, layout D canonical out.
-// xbuf holds P * 2048 words for this group.
-template <int P>
+// xbuf holds XP * 2048 words for this group.
+template <int P, int XP = P>
 __device__ __forceinline__ void forward(uint32_t (&v)[P][EPT], int t, uint32_t* xbuf, int bar,
                                         const uint32_t* __restrict__ fw, const uint32_t* __restrict__ fwp,
                                         uint32_t q) {
@@ -170,15 +189,15 @@ __device__ __forceinline__ void forward(uint32_t (&v)[P][EPT], int t, uint32_t* 
     uint32_t* wb = xbuf + (t >> 5) * 256;
 #pragma unroll
     for (int mm = 0; mm < 3; mm++) reg_stage<P, true>(v, mm, 4 >> mm, [&](int k) { return eA(t, k); }, fw, fwp, q);
-    exchange<P, true>(v, t, xbuf, bar);
+    exchange<P, true, XP>(v, t, xbuf, bar);
 #pragma unroll
     for (int mm = 3; mm < 6; mm++)
         reg_stage<P, true>(v, mm, 4 >> (mm - 3), [&](int k) { return eB(t, k); }, fw, fwp, q);
-    b_to_c<P>(v, l, wb);
+    b_to_c<P, XP>(v, l, wb);
 #pragma unroll
     for (int mm = 6; mm < 9; mm++)
         reg_stage<P, true>(v, mm, 4 >> (mm - 6), [&](int k) { return eC(t, k); }, fw, fwp, q);
-    c_to_d<P>(v, l, wb);
+    c_to_d<P, XP>(v, l, wb);
 #pragma unroll
     for (int mm = 9; mm < 11; mm++)
         reg_stage<P, true>(v, mm, 2 >> (mm - 9), [&](int k) { return eD(t, k); }, fw, fwp, q);
@@ -189,7 +208,7 @@ __device__ __forceinline__ void forward(uint32_t (&v)[P][EPT], int t, uint32_t* 
 }
 
 // inverse NTT of P polynomials of one limb: layout D in, layout A canonical out
-template <int P>
+template <int P, int XP = P>
 __device__ __forceinline__ void inverse(uint32_t (&v)[P][EPT], int t, uint32_t* xbuf, int bar,
                                         const uint32_t* __restrict__ iw, const uint32_t* __restrict__ iwp,
                                         uint32_t q) {
@@ -198,15 +217,15 @@ __device__ __forceinline__ void inverse(uint32_t (&v)[P][EPT], int t, uint32_t* 
 #pragma unroll
     for (int mm = 10; mm >= 9; mm--)
         reg_stage<P, false>(v, mm, 2 >> (mm - 9), [&](int k) { return eD(t, k); }, iw, iwp, q);
-    d_to_c<P>(v, l, wb);
+    d_to_c<P, XP>(v, l, wb);
 #pragma unroll
     for (int mm = 8; mm >= 6; mm--)
         reg_stage<P, false>(v, mm, 4 >> (mm - 6), [&](int k) { return eC(t, k); }, iw, iwp, q);
-    c_to_b<P>(v, l, wb);
+    c_to_b<P, XP>(v, l, wb);
 #pragma unroll
     for (int mm = 5; mm >= 3; mm--)
         reg_stage<P, false>(v, mm, 4 >> (mm - 3), [&](int k) { return eB(t, k); }, iw, iwp, q);
-    exchange<P, false>(v, t, xbuf, bar);
+    exchange<P, false, XP>(v, t, xbuf, bar);
 #pragma unroll
     for (int mm = 2; mm >= 0; mm--) reg_stage<P, false>(v, mm, 4 >> mm, [&](int k) { return eA(t, k); }, iw, iwp, q);
 #pragma unroll
