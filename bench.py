@@ -197,7 +197,68 @@ def poisson_load(svc, payloads, rate, seconds):
     return {"offered_payloads_per_s": rate, "arrived_payloads_per_s": n / offered_s, "payloads": n,
             "completed_payloads_per_s": n / (done[-1] - t_start), "p50_ms": st.p50_us / 1e3,
             "p99_ms": st.p99_us / 1e3, "mean_ms": st.mean_us / 1e3, "max_ms": st.max_us / 1e3,
-            "mean_batch": st.batched_payloads / max(st.batches, 1), "failed": st.failed}
+            "mean_batch": st.batched_payloads / max(st.batches, 1), "failed": st.failed,
+            "batch_ms_mean": st.batch_ms_mean, "batch_ms_max": st.batch_ms_max,
+            "queue_ms_mean": st.queue_ms_mean, "queue_ms_max": st.queue_ms_max}
+
+
+def micro_bench(pkg, steps, warmup):
+    """Kernel microbenchmarks on seeded data: batched limb NTT / INTT of 4096 polynomials
+    (64 MB of u64 coefficients in and out per prime) and NTT-domain automorphisms of the
+    same batch under all 2048 odd t < 4096 (137 GB of writes per prime, produced 64 t at a
+    time into a 4 GB rotating output).  One JSON line per measurement."""
+    import numpy as np
+    import torch
+    torch.cuda.set_device(0)
+    peak, peak_kind = read_peaks()
+    count = 4096
+    lines = []
+
+    def roofline(nbytes, ms):
+        gbs = nbytes / (ms / 1000.0) / 1e9
+        return {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                "peak_source": peak_kind}
+
+    for limb, q in ((0, 268369921), (1, 249561089)):
+        rng = np.random.default_rng(limb)
+        polys = torch.from_numpy(rng.integers(0, q, (count, N), dtype=np.uint64).view(np.int64)).cuda()
+        for inverse in (False, True):
+            for _ in range(warmup):
+                pkg.ntt_batch(polys.data_ptr(), count, limb, inverse=inverse)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(steps):
+                pkg.ntt_batch(polys.data_ptr(), count, limb, inverse=inverse)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            lines.append({"metric": f"{'intt' if inverse else 'ntt'} limb {limb}: 4096 x 2048 u64 coefficients",
+                          "value": count / (ms / 1000.0), "unit": "polys/s", "ms_per_launch": ms,
+                          "roofline": roofline(2 * count * N * 8, ms)})
+        nk = 64
+        ks_all = np.arange(1, 4096, 2, dtype=np.uint32)
+        d_ks = torch.from_numpy(ks_all.view(np.int32)).cuda()
+        out = torch.empty((nk, count, N), dtype=torch.int64, device="cuda")
+        launches = len(ks_all) // nk
+        for w in range(min(warmup, launches)):
+            pkg.automorph_batch(polys.data_ptr(), count, d_ks.data_ptr() + 4 * nk * w, nk, out.data_ptr())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for i in range(launches):
+            pkg.automorph_batch(polys.data_ptr(), count, d_ks.data_ptr() + 4 * nk * i, nk, out.data_ptr())
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        written = len(ks_all) * count * N * 8
+        lines.append({"metric": f"galois limb {limb}: 4096 polys x all 2048 odd t",
+                      "value": written / (ms / 1000.0) / 1e9, "unit": "GB/s written", "ms_total": ms,
+                      "roofline": roofline(written, ms)})
+        del out
+    for ln in lines:
+        print(json.dumps(ln))
+    return 0
 
 
 def main():
@@ -216,8 +277,12 @@ def main():
     ap.add_argument("--serve-rates", type=float, nargs="*", default=[1000.0, 2500.0],
                     help="offered Poisson loads (payloads/s) for the serving measurement")
     ap.add_argument("--serve-seconds", type=float, default=3.0)
+    ap.add_argument("--micro", action="store_true",
+                    help="kernel microbenchmarks (batched NTT / INTT, Galois automorphisms) instead of the step")
     args = ap.parse_args()
     small = args.records != RECORDS
+    if args.micro:
+        return micro_bench(load_package(), max(args.steps, 3), max(args.warmup, 1))
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

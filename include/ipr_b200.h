@@ -192,6 +192,19 @@ const char *ipr_version(void);
  * Returns IPR_OK or a negative status (message in ipr_last_error()). */
 int ipr_gemv_query_noalloc(uint64_t *h_c, const uint64_t *h_a, const uint16_t *d_db, int db_rows, int b_cols);
 
+/* Kernel-level building blocks over device buffers (no reference counterpart as
+ * entry points: the reference runs them inside respond()).  Polynomials are
+ * 2048 u64 coefficients of one CRT limb (canonical residues mod q_limb).
+ * ipr_ntt_batch: in place, the negacyclic NTT of ntt_forward / ntt_inverse
+ * (src/core/ntt.rs:111-160, 731-780) for `count` polynomials of limb 0 or 1.
+ * ipr_automorph_batch: out[j][p] = the NTT-domain image of in[p] under
+ * x -> x^ks[j] (ks odd, < 4096; the rotation gather of
+ * native/cuda/rotation_kernel.cu:21-59), out holding nk * count polynomials.
+ * Both are enqueued on `stream` (a cudaStream_t, NULL = legacy default). */
+int ipr_ntt_batch(int device, uint64_t *d_polys, uint64_t count, int limb, int inverse, void *stream);
+int ipr_automorph_batch(int device, const uint64_t *d_in, uint64_t count, const uint32_t *d_ks, int nk,
+                        uint64_t *d_out, void *stream);
+
 /* ---------------------------------------------------------------------------
  * Serving loop with continuous batching (no reference counterpart: the
  * reference answers one payload at a time, keyword.rs:534-640).  One
@@ -225,6 +238,8 @@ typedef struct ipr_service_stats {
     uint64_t hbm_bytes;                 /* device bytes the batch path and the I/O slots hold */
     double p50_us, p99_us, mean_us, max_us; /* submit -> completion, completed requests since the last reset */
     uint64_t latency_samples;
+    double batch_ms_mean, batch_ms_max;     /* device time per batch (its start to its responses on the host) */
+    double queue_ms_mean, queue_ms_max;     /* submit -> launch of the request's batch */
 } ipr_service_stats;
 
 int ipr_service_create(ipr_server *const *servers, int num_servers, const ipr_service_config *cfg,

@@ -20,7 +20,7 @@ __all__ = [
     "IprError", "Plan", "KeywordServer", "plan_from_shape", "query_bytes", "lib",
     "KeywordQueryPayload", "KeywordResponsePayload", "serialize_keyword_query",
     "deserialize_keyword_response", "POLY_LEN", "RESULT_BYTES", "KeywordService", "ServiceStats",
-    "shard_plan", "merge_responses", "ShardedKeywordServer",
+    "shard_plan", "merge_responses", "ShardedKeywordServer", "ntt_batch", "automorph_batch",
 ]
 
 POLY_LEN = 2048
@@ -93,13 +93,16 @@ class _ServiceStats(ctypes.Structure):
                 ("batches", _u64), ("batched_payloads", _u64), ("pending", _u64), ("in_flight", _u64),
                 ("max_batch", _i32), ("hbm_bytes", _u64), ("p50_us", ctypes.c_double),
                 ("p99_us", ctypes.c_double), ("mean_us", ctypes.c_double), ("max_us", ctypes.c_double),
-                ("latency_samples", _u64)]
+                ("latency_samples", _u64), ("batch_ms_mean", ctypes.c_double), ("batch_ms_max", ctypes.c_double),
+                ("queue_ms_mean", ctypes.c_double), ("queue_ms_max", ctypes.c_double)]
 
 
 _plan_shard = _sig("ipr_plan_shard", _i32, ctypes.POINTER(_Plan), _i32, _i32, ctypes.POINTER(_Plan),
                    ctypes.POINTER(_u64))
 _merge = _sig("ipr_response_merge", _i32, ctypes.POINTER(_u8p), ctypes.POINTER(_sz), _i32, _u8p, _sz,
               ctypes.POINTER(_sz))
+_ntt_batch = _sig("ipr_ntt_batch", _i32, _i32, _vp, _u64, _i32, _i32, _vp)
+_automorph_batch = _sig("ipr_automorph_batch", _i32, _i32, _vp, _u64, _vp, _i32, _vp, _vp)
 _svc_create = _sig("ipr_service_create", _i32, ctypes.POINTER(_vp), _i32, ctypes.POINTER(_ServiceConfig),
                    ctypes.POINTER(_vp))
 _svc_submit = _sig("ipr_service_submit", _i32, _vp, _i32, _u8p, _sz, ctypes.POINTER(_u64))
@@ -421,6 +424,10 @@ class ServiceStats:
     mean_us: float
     max_us: float
     latency_samples: int
+    batch_ms_mean: float
+    batch_ms_max: float
+    queue_ms_mean: float
+    queue_ms_max: float
 
 
 class KeywordService:
@@ -583,3 +590,16 @@ class ShardedKeywordServer:
         part = self._answer(q)
         parts = self._gather_bytes(part)
         return merge_responses(parts) if parts is not None else None
+
+
+# ---------------------------------------------------------------------------
+# kernel-level building blocks on device buffers (pointers to device memory)
+# ---------------------------------------------------------------------------
+def ntt_batch(d_polys: int, count: int, limb: int, inverse: bool = False, device: int = 0, stream: int = 0):
+    """in place: `count` polynomials of 2048 u64 coefficients of CRT limb `limb`"""
+    _check(_ntt_batch(device, _vp(d_polys), count, limb, 1 if inverse else 0, _vp(stream)), "ntt_batch")
+
+
+def automorph_batch(d_in: int, count: int, d_ks: int, nk: int, d_out: int, device: int = 0, stream: int = 0):
+    """out[j][p] = NTT-domain automorphism x -> x^ks[j] of in[p] (ks: device u32 array)"""
+    _check(_automorph_batch(device, _vp(d_in), count, _vp(d_ks), nk, _vp(d_out), _vp(stream)), "automorph_batch")

@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
 #pragma unroll
                         for (int a = 0; a < 4; a++) v += (uint64_t)d[ci * 4 + a] << (8 * a);
                         const uint32_t r = mod64(v, q, br);
-                        xch[(((g - ch * 4) * 4 + ci) * 4 + b) * 32 + lane] = mod64((uint64_t)r << (8 * b), q, br);
+                        xch[(((g - ch * 4) * 4 + ci) * 4 + b) * 32 + lane] = r;  // r < q: shifted by byte b below
                     }
                 }
                 if (ch == chunks - 1) {  // every TMEM read of this unit is done: free the buffer
@@ -285,8 +285,11 @@ __global__ void __launch_bounds__(P_THREADS, 1)
                     for (int cl = b; cl < 16; cl += 4) {
                         const int c = ch * 16 + cl;
                         if (c >= clients) break;
-                        const uint64_t tot = (uint64_t)xch[(cl * 4 + 0) * 32 + lane] + xch[(cl * 4 + 1) * 32 + lane] +
-                                             xch[(cl * 4 + 2) * 32 + lane] + xch[(cl * 4 + 3) * 32 + lane];
+                        // sum_b 256^b r_b < 2^28 * (1 + 2^8 + 2^16 + 2^24) < 2^53: one reduction
+                        const uint64_t tot = (uint64_t)xch[(cl * 4 + 0) * 32 + lane] +
+                                             ((uint64_t)xch[(cl * 4 + 1) * 32 + lane] << 8) +
+                                             ((uint64_t)xch[(cl * 4 + 2) * 32 + lane] << 16) +
+                                             ((uint64_t)xch[(cl * 4 + 3) * 32 + lane] << 24);
                         S[(((int64_t)c * instances + j) * 2 + l) * N + z] = mod64(tot, q, br);
                     }
                 }

@@ -107,6 +107,8 @@ struct ipr_service {
     uint64_t submitted = 0, completed = 0, rejected = 0, failed = 0, batches = 0, batched_payloads = 0;
     uint64_t npending = 0, in_flight = 0;
     std::vector<double> lat_us;
+    double batch_ms_sum = 0, batch_ms_max = 0, queue_ms_sum = 0, queue_ms_max = 0;
+    uint64_t timed_batches = 0, queued_requests = 0;
     uint64_t hbm = 0;
     int admitted_batch = 0;
 };
@@ -211,6 +213,16 @@ void harvest(ipr_service* v, Lane& ln, Slot& sl) {
         double& e = ln.est_ms[sl.batch.size()];
         e = e > 0 ? 0.8 * e + 0.2 * ms : ms;
         ln.last_ready = sl.t_ready;
+        std::lock_guard<std::mutex> lk(v->mu);
+        v->timed_batches++;
+        v->batch_ms_sum += ms;
+        v->batch_ms_max = std::max(v->batch_ms_max, ms);
+        for (Request* r : sl.batch) {  // time from submission to the launch of the request's batch
+            const double qms = std::chrono::duration<double, std::milli>(sl.t_launch - r->t_submit).count();
+            v->queued_requests++;
+            v->queue_ms_sum += qms;
+            v->queue_ms_max = std::max(v->queue_ms_max, qms);
+        }
     }
     for (size_t b = 0; b < sl.batch.size(); b++) {
         Request* r = sl.batch[b];
@@ -531,6 +543,13 @@ int ipr_service_get_stats(ipr_service* v, ipr_service_stats* out) {
         out->max_us = lat.back();
     }
     out->latency_samples = lat.size();
+    {
+        std::lock_guard<std::mutex> lk(v->mu);
+        out->batch_ms_mean = v->timed_batches ? v->batch_ms_sum / (double)v->timed_batches : 0;
+        out->batch_ms_max = v->batch_ms_max;
+        out->queue_ms_mean = v->queued_requests ? v->queue_ms_sum / (double)v->queued_requests : 0;
+        out->queue_ms_max = v->queue_ms_max;
+    }
     return IPR_OK;
 }
 
@@ -538,6 +557,8 @@ int ipr_service_reset_stats(ipr_service* v) {
     if (!v) return svc_fail(IPR_E_ARGS, "null service");
     std::lock_guard<std::mutex> lk(v->mu);
     v->lat_us.clear();
+    v->batch_ms_sum = v->batch_ms_max = v->queue_ms_sum = v->queue_ms_max = 0;
+    v->timed_batches = v->queued_requests = 0;
     v->batches = v->batched_payloads = 0;
     v->submitted = v->completed = v->rejected = v->failed = 0;
     return IPR_OK;

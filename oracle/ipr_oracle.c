@@ -824,6 +824,27 @@ void ipr_synth_precomp(uint64_t seed, uint64_t no, uint64_t *a_hat, uint64_t *bt
     for (uint64_t i = 0; i < no * IPR_T * IPR_N; i++) bth[i] = synth_condensed(seed, 5, i);
 }
 
+/* the slice of ipr_synth_db + ipr_synth_precomp belonging to instances
+ * [first, first + count) of a server with `db_rows` rows: the same global element
+ * indices, so a fold-group shard of a large synthetic server is generated alone */
+void ipr_synth_shard(uint64_t seed, uint64_t db_rows, uint64_t first, uint64_t count, uint16_t *db,
+                     uint64_t *a_hat, uint64_t *bt, uint64_t *btb, uint64_t *bth) {
+    const uint64_t q = IPR_Q0 * IPR_Q1;
+    const int64_t ndb = (int64_t)(count * IPR_N * db_rows);
+    const uint64_t db0 = first * IPR_N * db_rows;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < ndb; i++) db[i] = (uint16_t)(ipr_synth(seed, 1, db0 + (uint64_t)i) % IPR_PT);
+    for (uint64_t i = 0; i < count * IPR_N; i++) a_hat[i] = ipr_synth(seed, 2, first * IPR_N + i) % q;
+    const int64_t n = (int64_t)(count * IPR_NINNER * IPR_N);
+    const uint64_t b0 = first * IPR_NINNER * IPR_N;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; i++) {
+        bt[i] = synth_condensed(seed, 3, b0 + (uint64_t)i);
+        btb[i] = synth_condensed(seed, 4, b0 + (uint64_t)i);
+    }
+    for (uint64_t i = 0; i < count * IPR_T * IPR_N; i++) bth[i] = synth_condensed(seed, 5, first * IPR_T * IPR_N + i);
+}
+
 /* a well-formed query payload with canonical limbs (serialize_keyword_query layout) */
 int ipr_synth_query(uint64_t seed, uint64_t db_rows, unsigned nq, uint8_t *out, size_t cap,
                     size_t *out_len) {

@@ -151,6 +151,8 @@ uint64_t ipr_synth(uint64_t seed, uint64_t stream, uint64_t idx);
 void ipr_synth_db(uint64_t seed, uint64_t db_rows, uint64_t db_cols, uint16_t *db);
 void ipr_synth_precomp(uint64_t seed, uint64_t num_outputs, uint64_t *a_hat, uint64_t *bold_t,
                        uint64_t *bold_t_bar, uint64_t *bold_t_hat);
+void ipr_synth_shard(uint64_t seed, uint64_t db_rows, uint64_t first, uint64_t count, uint16_t *db,
+                     uint64_t *a_hat, uint64_t *bt, uint64_t *btb, uint64_t *bth);
 int ipr_synth_query(uint64_t seed, uint64_t db_rows, unsigned num_queries, uint8_t *out,
                     size_t cap, size_t *out_len);
 

@@ -97,6 +97,7 @@ _respond = _sig("ipr_oracle_respond", ctypes.c_int, ctypes.POINTER(Params), ctyp
 synth = _sig("ipr_synth", _u64, _u64, _u64, _u64)
 _synth_db = _sig("ipr_synth_db", None, _u64, _u64, _u64, _p)
 _synth_pre = _sig("ipr_synth_precomp", None, _u64, _u64, _p, _p, _p, _p)
+_synth_shard = _sig("ipr_synth_shard", None, _u64, _u64, _u64, _u64, _p, _p, _p, _p, _p)
 _synth_q = _sig("ipr_synth_query", ctypes.c_int, _u64, _u64, ctypes.c_uint, _p, _sz, ctypes.POINTER(_sz))
 threads = _sig("ipr_oracle_threads", ctypes.c_int)
 
@@ -237,6 +238,24 @@ class SynthDB:
                    _ptr(self.bold_t_hat))
         self.stash = [bytes(s) for s in stash]
         self._stash_buf = np.frombuffer(b"".join(self.stash) or b"\0", dtype=np.uint8).copy()
+
+    @classmethod
+    def shard_of(cls, db_rows, first_instance, instances, interp, c, seed, stash=()):
+        """the state of instances [first_instance, first_instance + instances) of a synthetic
+        server with `seed`, generated alone (same element indices as the whole server)"""
+        sub = cls.__new__(cls)
+        sub.db_rows, sub.instances, sub.interp, sub.c, sub.seed = db_rows, instances, interp, c, seed
+        sub.db_cols = instances * N
+        sub.db = np.zeros(sub.db_cols * db_rows, dtype=np.uint16)
+        sub.a_hat = np.zeros(instances * N, dtype=np.uint64)
+        sub.bold_t = np.zeros(instances * NINNER * N, dtype=np.uint64)
+        sub.bold_t_bar = np.zeros(instances * NINNER * N, dtype=np.uint64)
+        sub.bold_t_hat = np.zeros(instances * 3 * N, dtype=np.uint64)
+        _synth_shard(seed, db_rows, first_instance, instances, _ptr(sub.db), _ptr(sub.a_hat), _ptr(sub.bold_t),
+                     _ptr(sub.bold_t_bar), _ptr(sub.bold_t_hat))
+        sub.stash = [bytes(s) for s in stash]
+        sub._stash_buf = np.frombuffer(b"".join(sub.stash) or b"\0", dtype=np.uint8).copy()
+        return sub
 
     def shard(self, first_instance: int, instances: int, interp: int, c: int) -> "SynthDB":
         """the state of fold groups starting at `first_instance` (views into this state)"""

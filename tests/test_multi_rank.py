@@ -145,3 +145,15 @@ def test_shards_on_one_gpu_merge_to_full(pkg, orc):
     finally:
         for s in shards + [whole]:
             s.close()
+
+
+def test_synth_shard_of_equals_slice(orc):
+    """a fold-group slice generated alone equals the same slice of the whole synthetic state"""
+    import numpy as np
+    full = orc.SynthDB(2048, 6, 2, 3, seed=31)
+    alone = orc.SynthDB.shard_of(2048, 2, 2, 2, 1, seed=31)
+    view = full.shard(2, 2, 2, 1)
+    for a in ("db", "a_hat", "bold_t", "bold_t_bar", "bold_t_hat"):
+        assert np.array_equal(getattr(alone, a), getattr(view, a)), a
+    q = orc.synth_query(3, 2048, 2)
+    assert orc.respond(alone, q) == orc.respond(view, q)
