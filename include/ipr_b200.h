@@ -253,6 +253,14 @@ int ipr_service_poll(ipr_service *svc, uint64_t ticket, uint8_t *out, size_t cap
 /* As poll, blocking up to timeout_ms (< 0: no limit); IPR_PENDING on timeout. */
 int ipr_service_wait(ipr_service *svc, uint64_t ticket, int timeout_ms, uint8_t *out, size_t cap, size_t *out_len);
 int ipr_service_get_stats(ipr_service *svc, ipr_service_stats *out);
+/* The most recent batches (up to 4096 kept), oldest first: times in ms since the
+ * service was created — launch (enqueued), start (device free for it), ready
+ * (responses on the host) — and the longest submit -> launch wait in it. */
+typedef struct ipr_service_batch {
+    int db, payloads;
+    double launch_ms, start_ms, ready_ms, queue_ms_max;
+} ipr_service_batch;
+int ipr_service_batch_log(ipr_service *svc, ipr_service_batch *out, int cap, int *n);
 int ipr_service_reset_stats(ipr_service *svc);
 /* Finishes the batches in flight, drops queued and uncollected requests. */
 void ipr_service_destroy(ipr_service *svc);

@@ -110,6 +110,14 @@ _svc_poll = _sig("ipr_service_poll", _i32, _vp, _u64, _u8p, _sz, ctypes.POINTER(
 _svc_wait = _sig("ipr_service_wait", _i32, _vp, _u64, _i32, _u8p, _sz, ctypes.POINTER(_sz))
 _svc_stats = _sig("ipr_service_get_stats", _i32, _vp, ctypes.POINTER(_ServiceStats))
 _svc_reset = _sig("ipr_service_reset_stats", _i32, _vp)
+
+
+class _ServiceBatch(ctypes.Structure):
+    _fields_ = [("db", _i32), ("payloads", _i32), ("launch_ms", ctypes.c_double), ("start_ms", ctypes.c_double),
+                ("ready_ms", ctypes.c_double), ("queue_ms_max", ctypes.c_double)]
+
+
+_svc_log = _sig("ipr_service_batch_log", _i32, _vp, ctypes.POINTER(_ServiceBatch), _i32, ctypes.POINTER(_i32))
 _svc_destroy = _sig("ipr_service_destroy", None, _vp)
 _version = _sig("ipr_version", ctypes.c_char_p)
 
@@ -482,6 +490,13 @@ class KeywordService:
 
     def reset_stats(self):
         _check(_svc_reset(self._h), "service_reset_stats")
+
+    def batch_log(self, cap: int = 4096):
+        """the most recent batches, oldest first: dicts of db, payloads, launch/start/ready ms, queue_ms_max"""
+        arr = (_ServiceBatch * cap)()
+        n = _i32()
+        _check(_svc_log(self._h, arr, cap, ctypes.byref(n)), "service_batch_log")
+        return [{f: getattr(arr[i], f) for f, _ in _ServiceBatch._fields_} for i in range(n.value)]
 
     def close(self):
         if self._h and self._h.value:

@@ -35,6 +35,7 @@
 namespace {
 
 using Clock = std::chrono::steady_clock;
+constexpr size_t kBatchLog = 4096;
 
 int svc_fail(int code, const std::string& msg) {
     ipr::set_last_error(msg.c_str());
@@ -108,6 +109,9 @@ struct ipr_service {
     uint64_t npending = 0, in_flight = 0;
     std::vector<double> lat_us;
     double batch_ms_sum = 0, batch_ms_max = 0, queue_ms_sum = 0, queue_ms_max = 0;
+    Clock::time_point t0 = Clock::now();
+    std::vector<ipr_service_batch> log;  // ring of the most recent batches
+    uint64_t log_next = 0;
     uint64_t timed_batches = 0, queued_requests = 0;
     uint64_t hbm = 0;
     int admitted_batch = 0;
@@ -217,12 +221,24 @@ void harvest(ipr_service* v, Lane& ln, Slot& sl) {
         v->timed_batches++;
         v->batch_ms_sum += ms;
         v->batch_ms_max = std::max(v->batch_ms_max, ms);
+        double qmax = 0;
         for (Request* r : sl.batch) {  // time from submission to the launch of the request's batch
             const double qms = std::chrono::duration<double, std::milli>(sl.t_launch - r->t_submit).count();
             v->queued_requests++;
             v->queue_ms_sum += qms;
             v->queue_ms_max = std::max(v->queue_ms_max, qms);
+            qmax = std::max(qmax, qms);
         }
+        ipr_service_batch rec;
+        rec.db = (int)(&ln - v->lanes.data());
+        rec.payloads = (int)sl.batch.size();
+        rec.launch_ms = std::chrono::duration<double, std::milli>(sl.t_launch - v->t0).count();
+        rec.start_ms = std::chrono::duration<double, std::milli>(start - v->t0).count();
+        rec.ready_ms = std::chrono::duration<double, std::milli>(sl.t_ready - v->t0).count();
+        rec.queue_ms_max = qmax;
+        if (v->log.size() < kBatchLog) v->log.push_back(rec);
+        else v->log[v->log_next % kBatchLog] = rec;
+        v->log_next++;
     }
     for (size_t b = 0; b < sl.batch.size(); b++) {
         Request* r = sl.batch[b];
@@ -553,12 +569,28 @@ int ipr_service_get_stats(ipr_service* v, ipr_service_stats* out) {
     return IPR_OK;
 }
 
+int ipr_service_batch_log(ipr_service* v, ipr_service_batch* out, int cap, int* n) {
+    if (!v || !n || cap < 0 || (cap && !out)) return svc_fail(IPR_E_ARGS, "null argument");
+    std::lock_guard<std::mutex> lk(v->mu);
+    const size_t have = v->log.size();
+    const size_t k = std::min(have, (size_t)cap);
+    // oldest first among the last k recorded
+    for (size_t i = 0; i < k; i++) {
+        const uint64_t idx = v->log_next - k + i;
+        out[i] = v->log[have < kBatchLog ? idx : idx % kBatchLog];
+    }
+    *n = (int)k;
+    return IPR_OK;
+}
+
 int ipr_service_reset_stats(ipr_service* v) {
     if (!v) return svc_fail(IPR_E_ARGS, "null service");
     std::lock_guard<std::mutex> lk(v->mu);
     v->lat_us.clear();
     v->batch_ms_sum = v->batch_ms_max = v->queue_ms_sum = v->queue_ms_max = 0;
     v->timed_batches = v->queued_requests = 0;
+    v->log.clear();
+    v->log_next = 0;
     v->batches = v->batched_payloads = 0;
     v->submitted = v->completed = v->rejected = v->failed = 0;
     return IPR_OK;

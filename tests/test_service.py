@@ -52,6 +52,10 @@ def test_alone_equals_in_mix(pkg, orc, dbs):
         st = svc.stats()
         assert st.completed == 2 * len(queries) and st.failed == 0 and st.in_flight == 0
         assert st.batches >= 1 and st.batched_payloads >= 1 and st.max_batch == 64
+        log = svc.batch_log()
+        assert len(log) == st.batches and sum(b["payloads"] for b in log) == st.batched_payloads
+        assert all(b["launch_ms"] <= b["ready_ms"] and b["start_ms"] <= b["ready_ms"] for b in log)
+        assert all(log[i]["ready_ms"] <= log[i + 1]["ready_ms"] for i in range(len(log) - 1))
 
 
 @pytest.mark.gpu
