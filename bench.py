@@ -161,13 +161,15 @@ def cpu_sample(orc, reps=3):
     return s.describe(t, reps)
 
 
-def poisson_load(svc, payloads, rate, seconds):
+def poisson_load(svc, payloads, rate, seconds, per_db=None):
     """Poisson arrivals at `rate` payloads/s for `seconds`; latency = submit -> response ready
-    inside the service (p50/p99 over all requests), throughput = completions / elapsed."""
+    inside the service (p50/p99 over all requests), throughput = completions / elapsed.
+    With `per_db` (one payload list per database) each arrival picks a database uniformly."""
     import queue
     import random
     svc.reset_stats()
     rng = random.Random(int(rate))
+    pick = random.Random(int(rate) + 1)
     n = max(1, int(rate * seconds))
     q = queue.Queue()
     done = []
@@ -189,7 +191,11 @@ def poisson_load(svc, payloads, rate, seconds):
         d = t_next - time.perf_counter()
         if d > 0:
             time.sleep(d)
-        q.put(svc.submit(0, payloads[i % len(payloads)]))
+        if per_db:
+            db = pick.randrange(len(per_db))
+            q.put(svc.submit(db, per_db[db][i % len(per_db[db])]))
+        else:
+            q.put(svc.submit(0, payloads[i % len(payloads)]))
     offered_s = time.perf_counter() - t_start
     q.put(None)
     th.join()
@@ -200,6 +206,66 @@ def poisson_load(svc, payloads, rate, seconds):
             "mean_batch": st.batched_payloads / max(st.batches, 1), "failed": st.failed,
             "batch_ms_mean": st.batch_ms_mean, "batch_ms_max": st.batch_ms_max,
             "queue_ms_mean": st.queue_ms_mean, "queue_ms_max": st.queue_ms_max}
+
+
+CONFIG4 = (  # (name, records, key bytes, value bytes, buckets, seed): three databases at dim0 = 8192
+    ("ML-KEM-512 x 4M", 4_000_000, 32, 800, 1 << 23, 7),
+    ("ML-KEM-768 x 1M", 1_000_000, 32, 1184, 1 << 21, 8),
+    ("ML-KEM-1024 x 2M", 2_000_000, 32, 1568, 1 << 22, 9),
+)
+
+
+def serve_config4(pkg, rates, seconds):
+    """Serving three databases from one GPU (ML-KEM-512 x 4M, -768 x 1M, -1024 x 2M records,
+    dim0 8192, seeds 7/8/9): saturation throughput of the serving loop and p50/p99 latency
+    under Poisson arrivals spread uniformly over the databases.  One JSON line."""
+    import numpy as np
+    import torch
+    torch.cuda.set_device(0)
+    servers, plans, per_db = [], [], []
+    t0 = time.perf_counter()
+    for name, rec, key, val, buckets, seed in CONFIG4:
+        plan = pkg.plan_from_shape(rec, key, val, buckets, 8192)
+        srv = pkg.KeywordServer.synthetic(plan, seed=seed)
+        servers.append(srv)
+        plans.append(plan)
+        rng = np.random.default_rng(seed)
+        pays = []
+        for _ in range(32):
+            nvals = 3 * N * 2 + 2 * (plan.db_rows + 6 * N)
+            lo = rng.integers(0, 268369921, nvals, dtype=np.uint64)
+            hi = rng.integers(0, 249561089, nvals, dtype=np.uint64)
+            v = (lo | (hi << np.uint64(28))).astype("<u8")
+            pays.append(bytes([2]) + v.view(np.uint8).reshape(-1, 8)[:, :7].tobytes())
+        per_db.append(pays)
+    svc = pkg.KeywordService(servers, max_batch=64)
+    setup_s = time.perf_counter() - t0
+    for db in range(3):
+        for t in [svc.submit(db, per_db[db][i % 32]) for i in range(64)]:
+            svc.wait(t)
+    # saturation: every database kept full
+    n_each = 6 * 64
+    t1 = time.perf_counter()
+    tickets = [svc.submit(i % 3, per_db[i % 3][(i // 3) % 32]) for i in range(3 * n_each)]
+    for t in tickets:
+        svc.wait(t)
+    sat = 3 * n_each / (time.perf_counter() - t1)
+    serving = [poisson_load(svc, None, r, seconds, per_db=per_db) for r in rates]
+    st = svc.stats()
+    hbm = sum(s.hbm_bytes() for s in servers) + st.hbm_bytes
+    svc.close()
+    for s in servers:
+        s.close()
+    line = {"metric": "serving three keyword databases on one GPU (Poisson arrivals, uniform over databases)",
+            "value": sat, "unit": "payloads/s at saturation", "n_gpus": 1, "higher_is_better": True,
+            "data": "synthetic",
+            "config": {"workload": "config 4: " + ", ".join(c[0] for c in CONFIG4) + ", dim0 8192",
+                       "databases": [{"name": c[0], "db_rows": p.db_rows, "db_cols": p.db_cols,
+                                      "instances": p.instances, "c": p.c} for c, p in zip(CONFIG4, plans)],
+                       "max_batch": st.max_batch, "device_bytes": hbm, "setup_s": setup_s},
+            "serving": serving}
+    print(json.dumps(line))
+    return 0
 
 
 def micro_bench(pkg, steps, warmup):
@@ -277,12 +343,17 @@ def main():
     ap.add_argument("--serve-rates", type=float, nargs="*", default=[1000.0, 2500.0],
                     help="offered Poisson loads (payloads/s) for the serving measurement")
     ap.add_argument("--serve-seconds", type=float, default=3.0)
+    ap.add_argument("--serve-config4", action="store_true",
+                    help="serve three databases (ML-KEM-512 x4M, -768 x1M, -1024 x2M at dim0 8192) under Poisson load")
     ap.add_argument("--micro", action="store_true",
                     help="kernel microbenchmarks (batched NTT / INTT, Galois automorphisms) instead of the step")
     args = ap.parse_args()
     small = args.records != RECORDS
     if args.micro:
         return micro_bench(load_package(), max(args.steps, 3), max(args.warmup, 1))
+    if args.serve_config4:
+        rates = args.serve_rates if args.serve_rates != [1000.0, 2500.0] else [300.0, 600.0, 1200.0]
+        return serve_config4(load_package(), rates, args.serve_seconds)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

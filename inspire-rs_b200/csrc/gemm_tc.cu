@@ -10,13 +10,15 @@
 // P_pb < 255^2 * db_rows < 2^31 for db_rows <= 32768, so accumulation is exact,
 // and the recombination sum_{p,b} 256^(p+b) P_pb < 2^63 fits a u64.
 //
-// Kernel shape: persistent CTAs of 6 warps.  Warp 0 issues TMA loads into a
+// Kernel shape: persistent CTAs of 10 warps.  Warp 0 issues TMA loads into a
 // multi-stage shared-memory ring (128-byte swizzle); one stage holds the same
 // [128 rows x 128 bytes] K-slice of both DB planes and one [NT x 128 bytes]
 // query-byte tile, so each query tile feeds two MMAs; warp 1 issues the MMAs
 // (M = 128 DB columns, N = NT query-byte columns, K = 32 bytes each) into
 // TMEM accumulators, one per plane, double buffered when they fit; warps 2-5
 // read the accumulators, recombine, reduce mod q0 / q1 and CRT-compose.
+// Eight epilogue warps (two per TMEM lane quarter) keep the drain short while
+// both accumulators of a tile occupy all of TMEM.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -30,7 +32,7 @@ namespace ipr {
 
 namespace {
 
-constexpr int G1_THREADS = 192;
+constexpr int G1_THREADS = 320;  // producer, MMA, 8 epilogue warps
 constexpr int TILE_M = 128;
 constexpr int TILE_K = 128;  // bytes per stage along K (one 128-byte swizzle row)
 constexpr int A_STAGE_BYTES = TILE_M * TILE_K;
@@ -70,7 +72,7 @@ __global__ void __launch_bounds__(G1_THREADS, 1)
         }
         for (int b = 0; b < 2; b++) {
             umma::mbar_init(&sh->acc_full[b], 1);
-            umma::mbar_init(&sh->acc_empty[b], 4);
+            umma::mbar_init(&sh->acc_empty[b], 8);
         }
         *err = 0;
         umma::fence_mbar_init();
@@ -166,8 +168,10 @@ __global__ void __launch_bounds__(G1_THREADS, 1)
             if (last_stage >= 0) umma::mbar_wait(&sh->empty[last_stage], last_parity, 1u << 22);
         }
     } else {
-        // epilogue: warps 2..5 -> TMEM lane quarters 2,3,0,1
+        // epilogue: warps 2..9 -> TMEM lane quarters 2,3,0,1 (twice); the two warps of a quarter
+        // split the accumulator's column groups between them
         const int quarter = warp & 3;
+        const int half = (warp - 2) >> 2;
         const int row = quarter * 32 + lane;
         int buf = 0;
         uint32_t acc_phase = 0;
@@ -181,7 +185,7 @@ __global__ void __launch_bounds__(G1_THREADS, 1)
             const int n_tile = (int)(t % n_tiles);
             const int64_t j = m * TILE_M + row;
             const uint32_t lane_off = (uint32_t)(quarter * 32) << 16;
-            for (int g = 0; g < nt / 16; g++) {
+            for (int g = half; g < nt / 16; g += 2) {
                 uint32_t p0[16], p1[16];
                 umma::tmem_ld16(tmem + lane_off + (uint32_t)((buf * 2 + 0) * nt + g * 16), p0);
                 umma::tmem_ld16(tmem + lane_off + (uint32_t)((buf * 2 + 1) * nt + g * 16), p1);

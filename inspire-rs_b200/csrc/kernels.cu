@@ -260,55 +260,68 @@ __global__ void __launch_bounds__(PACK_THREADS) k_pack(const uint64_t* __restric
 // ---------------------------------------------------------------------------
 // R[j] = from_ntt(S[j]) : inverse NTT per limb + CRT compose (one CTA per output)
 // ---------------------------------------------------------------------------
-// One CTA of 512 threads per output j: group g (256 threads) runs the inverse
-// NTT of limb g in registers (ntt_regs.cuh), the limbs meet at the CRT compose.
+// One CTA of 512 threads per pair of outputs (j0, j0 + 1): group g (256 threads) runs the
+// inverse NTTs of limb g of both in registers (ntt_regs.cuh, one twiddle load per two
+// butterflies); the limbs meet at the CRT compose.
+constexpr int INTT_P = 2;
+
 __global__ void __launch_bounds__(512) k_intt_crt(const uint32_t* __restrict__ S,
                                                   const uint32_t* __restrict__ iw,
                                                   const uint32_t* __restrict__ iwp,
-                                                  uint64_t* __restrict__ R,
+                                                  uint64_t* __restrict__ R, int num_outputs,
                                                   const uint64_t* __restrict__ z_bodies,
                                                   const uint64_t* __restrict__ bth, int instances) {
-    __shared__ uint32_t sm[2 * N];
-    const int j = blockIdx.x;
+    __shared__ uint32_t sm[2][INTT_P][N];  // [limb][output][slot]
+    const int j0 = blockIdx.x * INTT_P;
     const int g = threadIdx.x >> 8, t = threadIdx.x & 255;
     const uint32_t q = g ? Q1 : Q0;
-    uint32_t v[1][nttr::EPT];
+    uint32_t v[INTT_P][nttr::EPT];
     // layout D: thread t holds the 8 consecutive slots z0 .. z0 + 7 (16-byte loads)
     const int z0 = nttr::eD(t, 0);
-    const uint4* Sj = reinterpret_cast<const uint4*>(S + ((int64_t)j * 2 + g) * N + z0);
-    const uint4 s0 = __ldg(Sj), s1 = __ldg(Sj + 1);
-    const uint32_t sv[8] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w};
-    if (z_bodies) {  // + sum_k z_c[k][z] That[j'][k][z] per limb (packing_online_kernel.cu:76-83)
-        const int c = j / instances, jj = j % instances;
-        const uint64_t* zc = z_bodies + (int64_t)c * T_EXP * N + z0;
-        const uint64_t* th = bth + (int64_t)jj * T_EXP * N + z0;
-        const int sh = 32 * g;
-        uint64_t acc[8];
 #pragma unroll
-        for (int m = 0; m < 8; m++) acc[m] = sv[m];
+    for (int p = 0; p < INTT_P; p++) {
+        const int j = j0 + p < num_outputs ? j0 + p : num_outputs - 1;  // an odd count repeats the last
+        const uint4* Sj = reinterpret_cast<const uint4*>(S + ((int64_t)j * 2 + g) * N + z0);
+        const uint4 s0 = __ldg(Sj), s1 = __ldg(Sj + 1);
+        const uint32_t sv[8] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w};
+        if (z_bodies) {  // + sum_k z_c[k][z] That[j'][k][z] per limb (packing_online_kernel.cu:76-83)
+            const int c = j / instances, jj = j % instances;
+            const uint64_t* zc = z_bodies + (int64_t)c * T_EXP * N + z0;
+            const uint64_t* th = bth + (int64_t)jj * T_EXP * N + z0;
+            const int sh = 32 * g;
+            uint64_t acc[8];
 #pragma unroll
-        for (int k = 0; k < T_EXP; k++) {
-            const ulonglong2* zp = reinterpret_cast<const ulonglong2*>(zc + k * N);
-            const ulonglong2* tp = reinterpret_cast<const ulonglong2*>(th + k * N);
+            for (int m = 0; m < 8; m++) acc[m] = sv[m];
 #pragma unroll
-            for (int h = 0; h < 4; h++) {
-                const ulonglong2 zv = __ldg(zp + h), tv = __ldg(tp + h);
-                acc[2 * h] += (uint64_t)(uint32_t)(zv.x >> sh) * (uint32_t)(tv.x >> sh);
-                acc[2 * h + 1] += (uint64_t)(uint32_t)(zv.y >> sh) * (uint32_t)(tv.y >> sh);
+            for (int k = 0; k < T_EXP; k++) {
+                const ulonglong2* zp = reinterpret_cast<const ulonglong2*>(zc + k * N);
+                const ulonglong2* tp = reinterpret_cast<const ulonglong2*>(th + k * N);
+#pragma unroll
+                for (int h = 0; h < 4; h++) {
+                    const ulonglong2 zv = __ldg(zp + h), tv = __ldg(tp + h);
+                    acc[2 * h] += (uint64_t)(uint32_t)(zv.x >> sh) * (uint32_t)(tv.x >> sh);
+                    acc[2 * h + 1] += (uint64_t)(uint32_t)(zv.y >> sh) * (uint32_t)(tv.y >> sh);
+                }
             }
+#pragma unroll
+            for (int m = 0; m < 8; m++) v[p][m] = mod64(acc[m], q, g ? BR1 : BR0);
+        } else {
+#pragma unroll
+            for (int m = 0; m < 8; m++) v[p][m] = sv[m];
         }
-#pragma unroll
-        for (int m = 0; m < 8; m++) v[0][m] = mod64(acc[m], q, g ? BR1 : BR0);
-    } else {
-#pragma unroll
-        for (int m = 0; m < 8; m++) v[0][m] = sv[m];
     }
-    nttr::inverse<1>(v, t, sm + g * N, 1 + g, iw + g * N, iwp + g * N, q);
+    nttr::inverse<INTT_P>(v, t, &sm[g][0][0], 1 + g, iw + g * N, iwp + g * N, q);
 #pragma unroll
-    for (int m = 0; m < nttr::EPT; m++) sm[g * N + nttr::eA(t, m)] = v[0][m];
+    for (int p = 0; p < INTT_P; p++)
+#pragma unroll
+        for (int m = 0; m < nttr::EPT; m++) sm[g][p][nttr::eA(t, m)] = v[p][m];
     __syncthreads();
-    for (int z = threadIdx.x; z < N; z += blockDim.x)
-        R[(int64_t)j * N + z] = crt2(sm[z], sm[N + z], Q0INV, BR1);
+#pragma unroll
+    for (int p = 0; p < INTT_P; p++) {
+        if (j0 + p >= num_outputs) break;
+        for (int z = threadIdx.x; z < N; z += blockDim.x)
+            R[(int64_t)(j0 + p) * N + z] = crt2(sm[0][p][z], sm[1][p][z], Q0INV, BR1);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -594,7 +607,8 @@ cudaError_t launch_pack(const uint64_t* bt, const uint64_t* btb, const uint64_t*
 cudaError_t launch_intt_crt(const uint32_t* S, const uint32_t* iw, const uint32_t* iwp, uint64_t* R,
                             int num_outputs, cudaStream_t st, const uint64_t* z_bodies, const uint64_t* bth,
                             int instances) {
-    k_intt_crt<<<num_outputs, 512, 0, st>>>(S, iw, iwp, R, z_bodies, bth, instances);
+    k_intt_crt<<<(num_outputs + INTT_P - 1) / INTT_P, 512, 0, st>>>(S, iw, iwp, R, num_outputs, z_bodies, bth,
+                                                                    instances);
     return cudaGetLastError();
 }
 
