@@ -252,7 +252,8 @@ def serve_config4(pkg, rates, seconds):
     sat = 3 * n_each / (time.perf_counter() - t1)
     serving = [poisson_load(svc, None, r, seconds, per_db=per_db) for r in rates]
     st = svc.stats()
-    hbm = sum(s.hbm_bytes() for s in servers) + st.hbm_bytes
+    free_b, total_b = torch.cuda.mem_get_info()
+    hbm = total_b - free_b  # the whole device in use while serving
     svc.close()
     for s in servers:
         s.close()
@@ -262,7 +263,7 @@ def serve_config4(pkg, rates, seconds):
             "config": {"workload": "config 4: " + ", ".join(c[0] for c in CONFIG4) + ", dim0 8192",
                        "databases": [{"name": c[0], "db_rows": p.db_rows, "db_cols": p.db_cols,
                                       "instances": p.instances, "c": p.c} for c, p in zip(CONFIG4, plans)],
-                       "max_batch": st.max_batch, "device_bytes": hbm, "setup_s": setup_s},
+                       "max_batch": st.max_batch, "device_bytes_in_use": hbm, "setup_s": setup_s},
             "serving": serving}
     print(json.dumps(line))
     return 0
@@ -523,9 +524,9 @@ def main():
 
     peak, peak_kind = read_peaks()
     pack_ms = stage_ms["pack"] / max(calls, 1)
-    if B > 1:  # k_pack_mma streams the slot-indexed precomputation once per batch
+    if B > 1:  # the packing GEMM streams the slot-indexed precomputation once per batch
         pack_bytes = N * 2 * ((plan.instances + 31) // 32) * 128 * 3 * N  # [slot][limb][tile][128 rows][6144]
-        kname = "k_pack_mma"
+        kname = "k_pack_mma_pair" if B >= 48 else "k_pack_mma"  # the server's default choice of form
     else:
         pack_bytes = plan.instances * (2 * 3069 + 3) * N * 8  # bold_t + bold_t_bar + bold_t_hat per launch
         kname = "k_pack"

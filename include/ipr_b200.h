@@ -167,9 +167,14 @@ int ipr_server_set_profiling(ipr_server *srv, int on);
  * tensor cores over DB byte planes (default where db_rows <= 32768), 0 = the
  * CUDA-core kernel on the u16 DB.  Both give identical results. */
 #define IPR_OPT_TENSOR_GEMV 1
-/* IPR_OPT_FOLD_REGISTER_NTT: 1 = RGSW fold with register-resident NTTs and
- * warp-shuffle butterflies (default), 0 = shared-memory NTTs.  Identical results. */
+/* IPR_OPT_FOLD_REGISTER_NTT: 1 = RGSW fold with register-resident NTTs
+ * (default), 0 = shared-memory NTTs.  Identical results. */
 #define IPR_OPT_FOLD_REGISTER_NTT 2
+/* IPR_OPT_PACK_CTA_PAIR: 1 = the batch path's packing GEMM runs on CTA pairs
+ * (tcgen05 cta_group::2, M = 256 across two SMs); 0 = one CTA per unit;
+ * 2 (default) = pairs from 48 payloads per batch up, where they are faster.
+ * Identical results. */
+#define IPR_OPT_PACK_CTA_PAIR 3
 int ipr_server_set_option(ipr_server *srv, int option, int64_t value);
 int ipr_server_stage_times(ipr_server *srv, double *ms_sum, uint64_t *calls);
 

@@ -43,6 +43,10 @@ cudaError_t launch_relayout_tpp(const uint64_t* bt, const uint64_t* btb, uint8_t
                                 cudaStream_t st);
 cudaError_t launch_build_y8(const uint64_t* y_bodies, uint8_t* y8, int clients, int np, cudaStream_t st);
 // S[c][j][l][z] without the z_body x That term (added by launch_intt_crt when given z_bodies)
+// the CTA-pair form: tm_y_half has boxes of pack_mma_nt(clients)/2 rows
+cudaError_t init_pack_pair_kernel();
+cudaError_t launch_pack_mma_pair(const CUtensorMap* tm_t, const CUtensorMap* tm_y_half, int instances, int clients,
+                                 int np, uint32_t* S, int* err_flag, int sm_count, cudaStream_t st);
 cudaError_t launch_pack_mma(const CUtensorMap* tm_t, const CUtensorMap* tm_y, int instances, int clients, int np,
                             uint32_t* S, int* err_flag, int sm_count, cudaStream_t st);
 cudaError_t launch_rotations(const uint64_t* y_body, uint64_t* y_all, uint64_t* y_bar_all, int num_rotations,

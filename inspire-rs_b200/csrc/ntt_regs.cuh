@@ -43,9 +43,13 @@ __device__ __forceinline__ void group_bar(int id) {
     else asm volatile("bar.sync 2, 256;" ::: "memory");
 }
 
+// conditional subtractions as unsigned minima: for v < 4q, min(v, v - 2q) is v - 2q when
+// v >= 2q and v otherwise (the difference wraps above v)
+__device__ __forceinline__ uint32_t csub(uint32_t v, uint32_t m) { return min(v, v - m); }
+
 __device__ __forceinline__ void fwd_bfly(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wp, uint32_t q) {
     const uint32_t two_q = 2 * q;
-    const uint32_t xx = x >= two_q ? x - two_q : x;
+    const uint32_t xx = csub(x, two_q);
     const uint32_t qn = shoup_lazy(y, w, wp, q);
     x = xx + qn;
     y = xx + two_q - qn;
@@ -54,15 +58,12 @@ __device__ __forceinline__ void fwd_bfly(uint32_t& x, uint32_t& y, uint32_t w, u
 __device__ __forceinline__ void inv_bfly(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wp, uint32_t q) {
     const uint32_t two_q = 2 * q;
     const uint32_t tt = two_q - y + x;
-    const uint32_t cx = x + y - ((2 * x >= tt) ? two_q : 0);
-    x = (cx + ((tt & 1) ? q : 0)) >> 1;
+    const uint32_t cx = csub(x + y, two_q);  // x + y >= 2q exactly when 2x >= tt
+    x = (cx + (q & (0u - (tt & 1)))) >> 1;
     y = w * tt - __umulhi(tt, wp) * q;
 }
 
-__device__ __forceinline__ uint32_t canon(uint32_t v, uint32_t q) {
-    v = v >= 2 * q ? v - 2 * q : v;
-    return v >= q ? v - q : v;
-}
+__device__ __forceinline__ uint32_t canon(uint32_t v, uint32_t q) { return csub(csub(v, 2 * q), q); }
 
 // A <-> B exchange of P polynomials through xbuf (XP * 2048 words, XP <= P polynomials at a
 // time), group barrier id bar

@@ -36,6 +36,7 @@ namespace ipr {
 namespace {
 
 constexpr int P_THREADS = 320;
+constexpr int Q_THREADS = 192;  // CTA-pair form: producer, MMA, 4 epilogue warps
 constexpr int P_TILE_M = 128;
 constexpr int P_TILE_K = 128;
 constexpr int P_K = 3 * N;  // 6144
@@ -310,6 +311,207 @@ __global__ void __launch_bounds__(P_THREADS, 1)
 }
 
 // ---------------------------------------------------------------------------
+// CTA-pair form: a cluster of 2 CTAs issues M = 256 MMAs (tcgen05 cta_group::2).
+// CTA r of the pair holds slot z0 + r of the unit (its 128 precomputation rows)
+// and client rows r*nt/2 .. of Y, so each SM stages 16 KB + nt*64 bytes per
+// k-step (half of the single-CTA form), and each CTA's TMEM holds only its own
+// nt-column accumulator: double buffered, so the epilogue of one unit overlaps
+// the MMAs of the next.
+// Warps: 0 TMA producer (both CTAs), 1 MMA issuer (CTA 0), 2..5 epilogue (both).
+// Barriers: full[] used in CTA 0 (both CTAs' loads complete on it), empty[] and
+// acc_full[] in both (CTA 0's MMA commits to each), acc_empty[] in CTA 0
+// (8 arrivals: the epilogue warps of both CTAs).
+// ---------------------------------------------------------------------------
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Q_THREADS, 1)
+    k_pack_mma_pair(const __grid_constant__ CUtensorMap tm_t, const __grid_constant__ CUtensorMap tm_y, int instances,
+                    int mt_count, int clients, int np, int nt, int stages, uint32_t* __restrict__ S,
+                    int* __restrict__ err_flag) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* base = smem_raw + ((1024 - (umma::smem_addr(smem_raw) & 1023)) & 1023);
+    PSmem* sh = reinterpret_cast<PSmem*>(base);
+    volatile int* err = &sh->err;
+    const int half = nt / 2;
+    const int b_stage = half * P_TILE_K;
+    uint8_t* a_tiles = base + 1024;                                           // [stage][128 x 128]
+    uint8_t* b_tiles = a_tiles + stages * P_A_STAGE;                          // [stage][nt/2 x 128]
+    uint32_t* xch = reinterpret_cast<uint32_t*>(b_tiles + stages * b_stage);  // [16 clients][4][32]
+
+    const uint32_t rank = umma::cluster_rank();
+    const bool leader = rank == 0;
+    const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t ncols = 32;
+    while (ncols < (uint32_t)(2 * nt)) ncols <<= 1;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < stages; s++) {
+            umma::mbar_init(&sh->full[s], 1);
+            umma::mbar_init(&sh->empty[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            umma::mbar_init(&sh->acc_full[b], 1);
+            umma::mbar_init(&sh->acc_empty[b], 8);
+        }
+        *err = 0;
+        sh->ep_fail[0] = sh->ep_fail[1] = 0;
+        umma::fence_mbar_init();
+    }
+    if (warp == 1) umma::tmem_alloc_pair(&sh->tmem_base, ncols);
+    umma::fence_before();
+    umma::cluster_sync();  // barriers of both CTAs initialised before any cross-CTA arrive
+    umma::fence_after();
+    const uint32_t tmem = sh->tmem_base;
+
+    const int ks_total = P_K / P_TILE_K;                    // 48
+    const int64_t total = (int64_t)2 * mt_count * (N / 2);  // units (l, mt, zp), zp fastest
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            int last_phase[P_MAX_STAGES];
+            for (int s = 0; s < P_MAX_STAGES; s++) last_phase[s] = -1;
+            const uint32_t tx = 2u * (uint32_t)(P_A_STAGE + b_stage);  // both CTAs' bytes land on CTA 0's barrier
+            for (int64_t u = pair; u < total && !*err; u += npairs) {
+                const int z = (int)(u & (N / 2 - 1)) * 2 + (int)rank;
+                const int lm = (int)(u >> (LOGN - 1));
+                const int l = lm / mt_count, mt = lm % mt_count;
+                const int arow = (int)(((int64_t)(z * 2 + l) * mt_count + mt) * P_TILE_M);
+                const int brow = l * np + (int)rank * half;
+                for (int ks = 0; ks < ks_total; ks++) {
+                    if (!umma::mbar_wait(&sh->empty[stage], phase ^ 1)) {
+                        *err = 21;
+                        break;
+                    }
+                    if (leader) umma::mbar_expect_tx(&sh->full[stage], tx);
+                    const uint32_t fb = umma::map_to_rank(&sh->full[stage], 0);
+                    umma::tma_load_2d_pair(a_tiles + stage * P_A_STAGE, &tm_t, ks * P_TILE_K, arow, fb);
+                    umma::tma_load_2d_pair(b_tiles + stage * b_stage, &tm_y, ks * P_TILE_K, brow, fb);
+                    last_phase[stage] = (int)phase;
+                    if (++stage == stages) {
+                        stage = 0;
+                        phase ^= 1;
+                    }
+                }
+            }
+            if (leader)  // every load of either CTA has landed before the pair may exit
+                for (int s = 0; s < stages; s++)
+                    if (last_phase[s] >= 0) umma::mbar_wait(&sh->full[s], (uint32_t)last_phase[s], 1u << 22);
+        }
+    } else if (warp == 1) {
+        if (leader && lane == 0) {
+            const uint32_t idesc = umma::idesc_u8(2 * P_TILE_M, nt);
+            int stage = 0, buf = 0, last_stage = -1;
+            uint32_t phase = 0, acc_phase = 0, last_parity = 0;
+            for (int64_t u = pair; u < total && !*err; u += npairs) {
+                if (!umma::mbar_wait(&sh->acc_empty[buf], acc_phase ^ 1)) {
+                    *err = 22;
+                    break;
+                }
+                umma::fence_after();
+                bool ok = true;
+                const uint32_t d = tmem + (uint32_t)(buf * nt);
+                for (int ks = 0; ks < ks_total; ks++) {
+                    if (!umma::mbar_wait(&sh->full[stage], phase)) {
+                        *err = 23;
+                        ok = false;
+                        break;
+                    }
+                    umma::fence_after();
+                    const uint32_t sa = umma::smem_addr(a_tiles + stage * P_A_STAGE);
+                    const uint32_t sb = umma::smem_addr(b_tiles + stage * b_stage);
+#pragma unroll
+                    for (int k4 = 0; k4 < P_TILE_K / 32; k4++)
+                        umma::mma_u8_pair(d, umma::desc_sw128(sa + 32 * k4), umma::desc_sw128(sb + 32 * k4), idesc,
+                                          (ks == 0 && k4 == 0) ? 0u : 1u);
+                    umma::commit_pair(umma::map_to_rank(&sh->empty[stage], 0));
+                    umma::commit_pair(umma::map_to_rank(&sh->empty[stage], 1));
+                    last_stage = stage;
+                    last_parity = phase;
+                    if (++stage == stages) {
+                        stage = 0;
+                        phase ^= 1;
+                    }
+                }
+                if (!ok) break;
+                umma::commit_pair(umma::map_to_rank(&sh->acc_full[buf], 0));
+                umma::commit_pair(umma::map_to_rank(&sh->acc_full[buf], 1));
+                buf ^= 1;
+                if (buf == 0) acc_phase ^= 1;
+            }
+            if (last_stage >= 0) umma::mbar_wait(&sh->empty[last_stage], last_parity, 1u << 22);
+        }
+    } else {
+        // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 = byte b of outputs mt*32 + lane, slot z0 + rank
+        const int b = warp & 3;
+        volatile int* ep_fail = &sh->ep_fail[0];
+        const uint32_t acc_empty0 = umma::map_to_rank(&sh->acc_empty[0], 0);
+        const uint32_t acc_empty1 = umma::map_to_rank(&sh->acc_empty[1], 0);
+        int buf = 0;
+        uint32_t acc_phase = 0;
+        const int chunks = (clients + 15) / 16;
+        for (int64_t u = pair; u < total; u += npairs) {
+            // the four warps leave together: the decision uses a flag only they write
+            if (!umma::mbar_wait(&sh->acc_full[buf], acc_phase) && lane == 0) *ep_fail = 1;
+            umma::named_bar(1, 128);
+            if (*ep_fail) {
+                if (b == 0 && lane == 0) *err = 24;
+                break;
+            }
+            umma::fence_after();
+            const int z = (int)(u & (N / 2 - 1)) * 2 + (int)rank;
+            const int lm = (int)(u >> (LOGN - 1));
+            const int l = lm / mt_count, mt = lm % mt_count;
+            const uint32_t q = l ? Q1 : Q0;
+            const uint64_t br = l ? BR1 : BR0;
+            const uint32_t lane_off = (uint32_t)(b * 32) << 16;
+            const uint32_t col0 = (uint32_t)(buf * nt);
+            const int j = mt * 32 + lane;
+            for (int ch = 0; ch < chunks; ch++) {
+                for (int g = ch * 4; g < ch * 4 + 4 && g < nt / 16; g++) {
+                    uint32_t d[16];
+                    umma::tmem_ld16(tmem + lane_off + col0 + (uint32_t)(g * 16), d);
+                    umma::tmem_wait_ld();
+#pragma unroll
+                    for (int ci = 0; ci < 4; ci++) {
+                        uint64_t v = 0;
+#pragma unroll
+                        for (int a = 0; a < 4; a++) v += (uint64_t)d[ci * 4 + a] << (8 * a);
+                        xch[(((g - ch * 4) * 4 + ci) * 4 + b) * 32 + lane] = mod64(v, q, br);
+                    }
+                }
+                if (ch == chunks - 1) {  // every TMEM read of this unit is done: free the buffer
+                    umma::fence_before();
+                    __syncwarp();
+                    if (lane == 0) umma::mbar_arrive_remote(buf ? acc_empty1 : acc_empty0);
+                }
+                umma::named_bar(1, 128);
+                if (j < instances) {
+                    for (int cl = b; cl < 16; cl += 4) {
+                        const int c = ch * 16 + cl;
+                        if (c >= clients) break;
+                        // sum_b 256^b r_b < 2^28 * (1 + 2^8 + 2^16 + 2^24) < 2^53: one reduction
+                        const uint64_t tot = (uint64_t)xch[(cl * 4 + 0) * 32 + lane] +
+                                             ((uint64_t)xch[(cl * 4 + 1) * 32 + lane] << 8) +
+                                             ((uint64_t)xch[(cl * 4 + 2) * 32 + lane] << 16) +
+                                             ((uint64_t)xch[(cl * 4 + 3) * 32 + lane] << 24);
+                        S[(((int64_t)c * instances + j) * 2 + l) * N + z] = mod64(tot, q, br);
+                    }
+                }
+                umma::named_bar(1, 128);
+            }
+            buf ^= 1;
+            if (buf == 0) acc_phase ^= 1;
+        }
+    }
+    umma::fence_before();
+    __syncthreads();
+    umma::cluster_sync();  // the pair's MMAs and cross-CTA arrivals are complete in both CTAs
+    if (warp == 1) umma::tmem_dealloc_pair(tmem, ncols);
+    if (threadIdx.x == 0 && *err) atomicExch(err_flag, *err);
+}
+
+// ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
 int pack_mma_nt(int clients) {
@@ -333,6 +535,62 @@ cudaError_t init_pack_mma_kernel() {
     size_t mx = 0;  // the largest footprint over every client count the launcher can pick
     for (int nt = 16; nt <= 256; nt += 16) mx = pack_mma_smem(nt) > mx ? pack_mma_smem(nt) : mx;
     return cudaFuncSetAttribute(k_pack_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
+}
+
+constexpr int Q_XCH_BYTES = 16 * 4 * 32 * 4;
+
+int pack_pair_stages(int nt) {
+    const int per = P_A_STAGE + (nt / 2) * P_TILE_K;
+    int s = (210 * 1024 - Q_XCH_BYTES) / per;
+    return s > P_MAX_STAGES ? P_MAX_STAGES : (s < 2 ? 2 : s);
+}
+
+size_t pack_pair_smem(int nt) {
+    return 2048 + (size_t)pack_pair_stages(nt) * (P_A_STAGE + (nt / 2) * P_TILE_K) + Q_XCH_BYTES;
+}
+
+cudaError_t init_pack_pair_kernel() {
+    size_t mx = 0;
+    for (int nt = 16; nt <= 256; nt += 16) mx = pack_pair_smem(nt) > mx ? pack_pair_smem(nt) : mx;
+    return cudaFuncSetAttribute(k_pack_mma_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
+}
+
+// CTA pairs that can be resident at once (a pair needs two SMs of one GPC).  The kernel is
+// persistent, so the grid is exactly that many pairs.
+int pack_pair_resident(int nt, int sm_count) {
+    static int cached[17] = {0};
+    const int key = nt / 16;
+    if (!cached[key]) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(sm_count & ~1));
+        cfg.blockDim = dim3(Q_THREADS);
+        cfg.dynamicSmemBytes = pack_pair_smem(nt);
+        cudaLaunchAttribute attr;
+        attr.id = cudaLaunchAttributeClusterDimension;
+        attr.val.clusterDim.x = 2;
+        attr.val.clusterDim.y = 1;
+        attr.val.clusterDim.z = 1;
+        cfg.attrs = &attr;
+        cfg.numAttrs = 1;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, (void*)k_pack_mma_pair, &cfg) != cudaSuccess || n < 1) {
+            cudaGetLastError();
+            n = sm_count / 2;
+        }
+        cached[key] = n < sm_count / 2 ? n : sm_count / 2;
+    }
+    return cached[key];
+}
+
+cudaError_t launch_pack_mma_pair(const CUtensorMap* tm_t, const CUtensorMap* tm_y_half, int instances, int clients,
+                                 int np, uint32_t* S, int* err_flag, int sm_count, cudaStream_t st) {
+    const int nt = pack_mma_nt(clients);
+    if (clients < 1 || clients > 64 || np < nt) return cudaErrorInvalidValue;
+    const int mt_count = (instances + 31) / 32;
+    const int grid = 2 * pack_pair_resident(nt, sm_count);
+    k_pack_mma_pair<<<grid, Q_THREADS, pack_pair_smem(nt), st>>>(*tm_t, *tm_y_half, instances, mt_count, clients, np,
+                                                                 nt, pack_pair_stages(nt), S, err_flag);
+    return cudaGetLastError();
 }
 
 uint64_t tpp_bytes(int instances) {

@@ -264,11 +264,17 @@ int enqueue_batch(ipr_server* s, int B, const uint8_t* d_queries, uint8_t* d_res
     rec(2);
     {
         const int nt = ipr::pack_mma_nt(B);
+        const bool pair = s->pack_pair == 1 || (s->pack_pair == 2 && B >= 48);
         const CUtensorMap* ty;
-        int e = y8_map(s, nt, &ty);
+        int e = y8_map(s, pair ? nt / 2 : nt, &ty);  // the pair form loads half the client rows per CTA
         if (e) return e;
         CU(ipr::launch_build_y8(s->d_ybs, s->d_y8, B, s->y8_np, st));
-        CU(ipr::launch_pack_mma(&s->tm_tpp, ty, (int)p.instances, B, s->y8_np, s->d_bS, s->d_err, s->sm_count, st));
+        if (pair)
+            CU(ipr::launch_pack_mma_pair(&s->tm_tpp, ty, (int)p.instances, B, s->y8_np, s->d_bS, s->d_err, s->sm_count,
+                                         st));
+        else
+            CU(ipr::launch_pack_mma(&s->tm_tpp, ty, (int)p.instances, B, s->y8_np, s->d_bS, s->d_err, s->sm_count,
+                                    st));
     }
     rec(3);
     CU(ipr::launch_intt_crt(s->d_bS, s->d_iw, s->d_iwp, s->d_bR, (int)(B * p.instances), st, s->d_zbs, s->d_bth,
@@ -345,6 +351,7 @@ int init_common(ipr_server* s, int device, const ipr_plan* plan) {
     CU(ipr::init_gemm1_kernel());
     CU(ipr::init_fold2_kernel());
     CU(ipr::init_pack_mma_kernel());
+    CU(ipr::init_pack_pair_kernel());
     ipr::host_params_init(s->hp);
     CU(ipr::set_constants(s->hp.barrett, s->hp.q0_inv_mod_q1));
     int st;
@@ -807,6 +814,10 @@ int ipr_server_set_option(ipr_server* s, int option, int64_t value) {
         case IPR_OPT_FOLD_REGISTER_NTT:
             s->fold_regs = value != 0;
             destroy_graphs(s);
+            return IPR_OK;
+        case IPR_OPT_PACK_CTA_PAIR:
+            if (value < 0 || value > 2) return fail(IPR_E_ARGS, "IPR_OPT_PACK_CTA_PAIR takes 0, 1 or 2");
+            s->pack_pair = (int)value;
             return IPR_OK;
         default:
             return fail(IPR_E_ARGS, "unknown option %d", option);

@@ -293,3 +293,29 @@ def test_respond_batch_device_entry(cfg0, orc):
     host = bytes(dout.cpu().numpy())
     for i, q in enumerate(qs):
         assert host[i * rb:(i + 1) * rb] == orc.respond(sdb, q)
+
+
+@pytest.mark.parametrize("pair", [0, 1])
+@pytest.mark.parametrize("B", [1, 5, 32, 64])
+def test_packing_gemm_forms(cfg0, pkg, orc, pair, B):
+    """the CTA-pair (M = 256 over two SMs) and one-CTA packing GEMMs give the oracle's bytes
+    for client counts across the tile widths (N = 16 .. 256)"""
+    import torch
+    plan, srv, sdb = cfg0
+    qs = [orc.synth_query(6000 + 97 * B + i, plan.db_rows, 2) for i in range(B)]
+    srv.set_option(pkg.KeywordServer.OPT_PACK_CTA_PAIR, pair)
+    try:
+        if B > 1:
+            got = srv.respond_batch(qs)
+        else:  # a one-payload batch through the device entry
+            dq = torch.frombuffer(bytearray(qs[0]), dtype=torch.uint8).cuda()
+            dout = torch.zeros(srv.response_bytes(2), dtype=torch.uint8, device="cuda")
+            srv.respond_batch_device(1, dq.data_ptr(), dout.data_ptr())
+            srv.sync()
+            got = [bytes(dout.cpu().numpy())]
+    finally:
+        srv.set_option(pkg.KeywordServer.OPT_PACK_CTA_PAIR, 2)
+    for i in sorted({0, B // 2, B - 1}):
+        assert got[i] == orc.respond(sdb, qs[i])
+    if B > 1:
+        assert got == [srv.respond_to_serialized_query(q) for q in qs]
