@@ -250,6 +250,7 @@ def serve_config4(pkg, rates, seconds):
     for t in tickets:
         svc.wait(t)
     sat = 3 * n_each / (time.perf_counter() - t1)
+    poisson_load(svc, None, rates[0], 0.5, per_db=per_db)  # warm-up at the first load, not reported
     serving = [poisson_load(svc, None, r, seconds, per_db=per_db) for r in rates]
     st = svc.stats()
     free_b, total_b = torch.cuda.mem_get_info()
@@ -489,6 +490,7 @@ def main():
     # ---- serving at stated Poisson loads (1-GPU runs) -----------------------------------
     serving = []
     if svc is not None and world == 1 and not args.no_serving:
+        poisson_load(svc, payloads, args.serve_rates[0], 0.5)  # warm-up at the first load, not reported
         for rate in args.serve_rates:
             serving.append(poisson_load(svc, payloads, rate, args.serve_seconds))
     if svc is not None:

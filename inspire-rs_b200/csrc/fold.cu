@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(F_THREADS, 1)
 #pragma unroll
                 for (int m = 0; m < EPT; m++) v[pp][m] = (uint32_t)((sum[rr][eA(t, m)] >> (k * GADGET_BITS)) & mask);
             }
-            nttr::forward<FP, XB>(v, t, xbuf, bar, fwl, fwpl, q);
+            nttr::forward<FP, XB, true>(v, t, xbuf, bar, fwl, fwpl, q);  // outputs in [0, 2q)
 #pragma unroll
             for (int pp = 0; pp < FP; pp++) {
                 const uint4* bp = reinterpret_cast<const uint4*>(sbody + ((pb + pp) * 2 + g) * N + eD(t, 0));
@@ -148,8 +148,8 @@ __global__ void __launch_bounds__(F_THREADS, 1)
                 const uint32_t bv[EPT] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
 #pragma unroll
                 for (int m = 0; m < EPT; m++) {
-                    acc0[m] += v[pp][m];                         // < 6q
-                    acc1[m] += (uint64_t)bv[m] * v[pp][m];       // 6 terms < 2^59
+                    acc0[m] += v[pp][m];                         // 6 terms < 12q < 2^32
+                    acc1[m] += (uint64_t)bv[m] * v[pp][m];       // 6 terms < 2q * q < 2^61
                 }
             }
         }

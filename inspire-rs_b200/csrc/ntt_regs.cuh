@@ -180,9 +180,10 @@ __device__ __forceinline__ void reg_stage(uint32_t (&v)[P][EPT], int mm, int dd,
     }
 }
 
-// forward NTT of P polynomials of one limb: layout A in, layout D canonical out.
+// forward NTT of P polynomials of one limb: layout A in, layout D canonical out (in [0, 2q)
+// instead with HALF_REDUCED, for callers that only accumulate the outputs).
 // xbuf holds XP * 2048 words for this group.
-template <int P, int XP = P>
+template <int P, int XP = P, bool HALF_REDUCED = false>
 __device__ __forceinline__ void forward(uint32_t (&v)[P][EPT], int t, uint32_t* xbuf, int bar,
                                         const uint32_t* __restrict__ fw, const uint32_t* __restrict__ fwp,
                                         uint32_t q) {
@@ -205,7 +206,7 @@ __device__ __forceinline__ void forward(uint32_t (&v)[P][EPT], int t, uint32_t* 
 #pragma unroll
     for (int p = 0; p < P; p++)
 #pragma unroll
-        for (int k = 0; k < EPT; k++) v[p][k] = canon(v[p][k], q);
+        for (int k = 0; k < EPT; k++) v[p][k] = HALF_REDUCED ? csub(v[p][k], 2 * q) : canon(v[p][k], q);
 }
 
 // inverse NTT of P polynomials of one limb: layout D in, layout A canonical out
