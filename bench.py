@@ -324,6 +324,22 @@ def micro_bench(pkg, steps, warmup):
                       "value": written / (ms / 1000.0) / 1e9, "unit": "GB/s written", "ms_total": ms,
                       "roofline": roofline(written, ms)})
         del out
+    # setup-time DB encode at the 1M shape: 2048 x 720,896 u16, interpolation degree 32
+    rows, cols, interp = 2048, 720896, 32
+    raw = torch.randint(0, 65535, (rows * cols,), dtype=torch.int32, device="cuda").to(torch.int16)
+    enc = torch.empty_like(raw)
+    for _ in range(warmup):
+        pkg.encode_db(raw.data_ptr(), enc.data_ptr(), rows, cols, interp)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        pkg.encode_db(raw.data_ptr(), enc.data_ptr(), rows, cols, interp)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    lines.append({"metric": "DB encode (1M ML-KEM-768 shape: 2048 x 720896 u16, interp 32)", "value": ms,
+                  "unit": "ms", "higher_is_better": False, "roofline": roofline(2 * rows * cols * 2, ms)})
     for ln in lines:
         print(json.dumps(ln))
     return 0

@@ -104,6 +104,11 @@ typedef struct ipr_server_data {
  * rotation_kernel.cu:71-94).  Fails with IPR_E_OOM if it does not fit. */
 int ipr_server_create(int device, const ipr_plan *plan, const ipr_server_data *data, ipr_server **out);
 
+/* Same, with data->db the RAW database (KeywordCuckooTable::to_raw_db layout,
+ * src/pir/keyword/cuckoo.rs:314-353): the server encodes it on the device
+ * (ipr_encode_db) instead of the caller running gpu_encode_db first. */
+int ipr_server_create_from_raw(int device, const ipr_plan *plan, const ipr_server_data *data, ipr_server **out);
+
 /* Same, with seeded synthetic DB / precomputation generated on the device
  * (uniform u16 < 65535, uniform residues), the timing mode the reference
  * itself uses (online_only, src/pir/server/engine.rs:693-729). */
@@ -209,6 +214,21 @@ int ipr_gemv_query_noalloc(uint64_t *h_c, const uint64_t *h_a, const uint16_t *d
 int ipr_ntt_batch(int device, uint64_t *d_polys, uint64_t count, int limb, int inverse, void *stream);
 int ipr_automorph_batch(int device, const uint64_t *d_in, uint64_t count, const uint32_t *d_ks, int nk,
                         uint64_t *d_out, void *stream);
+
+/* Setup-time database layout and encode on device buffers.
+ * ipr_cuckoo_to_raw_db: KeywordCuckooTable::to_raw_db (cuckoo.rs:314-353) — bucket
+ * entries (num_buckets x entry_size bytes, row-major) and occupancy flags (one byte
+ * per bucket) -> the column-major u16 raw DB [db_cols][db_rows], per = buckets per
+ * DB row, entry bytes (2j, 2j+1) big-endian into column item * entry_size/2 + j.
+ * ipr_encode_db: gpu_encode_db (native/cuda/encode_kernel.cu:264-386) — the
+ * interpolation of each fold group's interp polynomials over Z_65535[X]/(X^2048+1),
+ * raw -> encoded ([db_cols][db_rows] u16 both; interp a power of two <= 32,
+ * db_rows a multiple of 16; input and output distinct). */
+int ipr_cuckoo_to_raw_db(int device, const uint8_t *d_entries, const uint8_t *d_occupied, uint64_t num_buckets,
+                         uint64_t entry_size, uint64_t db_rows, uint64_t db_cols, uint64_t per, uint16_t *d_raw,
+                         void *stream);
+int ipr_encode_db(int device, const uint16_t *d_raw, uint16_t *d_encoded, uint64_t db_rows, uint64_t db_cols,
+                  uint64_t interp, void *stream);
 
 /* ---------------------------------------------------------------------------
  * Serving loop with continuous batching (no reference counterpart: the

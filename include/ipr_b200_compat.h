@@ -25,6 +25,16 @@ void gpu_init_memory_pool(void);
 void gpu_trim_memory_pool(void);
 uint64_t gpu_available_memory_bytes(void);
 
+/* src/pir/gpu/encode.rs:7-20 (native/cuda/encode_kernel.cu:264-480): encode the host raw
+ * DB and keep the encoded DB on the device (h_db_out is not written, as in the
+ * reference); modulus must be 65535 and num_inv interp^-1 mod 65535. */
+void gpu_encode_db(uint16_t *d_db_in, uint16_t *d_db_out, int db_rows, int db_cols, int interp_degree, int gamma,
+                   int c, uint32_t modulus, uint32_t num_inv);
+void gpu_encode_db_from_host(const uint16_t *h_db_in, uint16_t *h_db_out, int db_rows, int db_cols,
+                             int interp_degree, int gamma, int c, uint32_t modulus, uint32_t num_inv);
+const uint16_t *gpu_encode_get_device_db(void);
+void gpu_encode_free_device_db(void);
+
 /* src/pir/gpu/gemv.rs:5-25 (native/cuda/gemv_kernel.cu:106-194) */
 void gpu_gemv_upload_db(const uint16_t *h_db, uint16_t **d_db_out, size_t db_size_bytes);
 void gpu_gemv_set_device_db(uint16_t **d_db_out, const uint16_t *d_db_in, size_t db_size_bytes);

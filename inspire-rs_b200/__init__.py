@@ -20,7 +20,8 @@ __all__ = [
     "IprError", "Plan", "KeywordServer", "plan_from_shape", "query_bytes", "lib",
     "KeywordQueryPayload", "KeywordResponsePayload", "serialize_keyword_query",
     "deserialize_keyword_response", "POLY_LEN", "RESULT_BYTES", "KeywordService", "ServiceStats",
-    "shard_plan", "merge_responses", "ShardedKeywordServer", "ntt_batch", "automorph_batch",
+    "shard_plan", "merge_responses", "ShardedKeywordServer", "ntt_batch", "automorph_batch", "encode_db",
+    "cuckoo_to_raw_db",
 ]
 
 POLY_LEN = 2048
@@ -103,6 +104,10 @@ _merge = _sig("ipr_response_merge", _i32, ctypes.POINTER(_u8p), ctypes.POINTER(_
               ctypes.POINTER(_sz))
 _ntt_batch = _sig("ipr_ntt_batch", _i32, _i32, _vp, _u64, _i32, _i32, _vp)
 _automorph_batch = _sig("ipr_automorph_batch", _i32, _i32, _vp, _u64, _vp, _i32, _vp, _vp)
+_create_raw = _sig("ipr_server_create_from_raw", _i32, _i32, ctypes.POINTER(_Plan), ctypes.POINTER(_ServerData),
+                   ctypes.POINTER(_vp))
+_encode = _sig("ipr_encode_db", _i32, _i32, _vp, _vp, _u64, _u64, _u64, _vp)
+_raw_db = _sig("ipr_cuckoo_to_raw_db", _i32, _i32, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _vp, _vp)
 _svc_create = _sig("ipr_service_create", _i32, ctypes.POINTER(_vp), _i32, ctypes.POINTER(_ServiceConfig),
                    ctypes.POINTER(_vp))
 _svc_submit = _sig("ipr_service_submit", _i32, _vp, _i32, _u8p, _sz, ctypes.POINTER(_u64))
@@ -254,9 +259,14 @@ class KeywordServer:
         self.device = device
 
     @classmethod
+    def from_raw(cls, plan: Plan, raw_db, a_hat, bold_t, bold_t_bar, bold_t_hat, **kw) -> "KeywordServer":
+        """as from_encoded, with the RAW database (to_raw_db layout), encoded on the device"""
+        return cls.from_encoded(plan, raw_db, a_hat, bold_t, bold_t_bar, bold_t_hat, _raw=True, **kw)
+
+    @classmethod
     def from_encoded(cls, plan: Plan, db, a_hat, bold_t, bold_t_bar, bold_t_hat, stash=(),
                      key_size: int = 32, value_size: Optional[int] = None, num_records: int = 0,
-                     cuckoo_seed: bytes = bytes(16), device: int = 0) -> "KeywordServer":
+                     cuckoo_seed: bytes = bytes(16), device: int = 0, _raw: bool = False) -> "KeywordServer":
         import numpy as np
         arrs = {
             "db": np.ascontiguousarray(db, dtype=np.uint16),
@@ -287,7 +297,8 @@ class KeywordServer:
         d.cuckoo_seed[:] = list(cuckoo_seed[:16].ljust(16, b"\0"))
         h = _vp()
         pc = plan._c()
-        _check(_create(device, ctypes.byref(pc), ctypes.byref(d), ctypes.byref(h)), "ipr_server_create")
+        fn, name = (_create_raw, "ipr_server_create_from_raw") if _raw else (_create, "ipr_server_create")
+        _check(fn(device, ctypes.byref(pc), ctypes.byref(d), ctypes.byref(h)), name)
         return cls(h.value, plan, device)
 
     @classmethod
@@ -619,3 +630,15 @@ def ntt_batch(d_polys: int, count: int, limb: int, inverse: bool = False, device
 def automorph_batch(d_in: int, count: int, d_ks: int, nk: int, d_out: int, device: int = 0, stream: int = 0):
     """out[j][p] = NTT-domain automorphism x -> x^ks[j] of in[p] (ks: device u32 array)"""
     _check(_automorph_batch(device, _vp(d_in), count, _vp(d_ks), nk, _vp(d_out), _vp(stream)), "automorph_batch")
+
+
+def encode_db(d_raw: int, d_encoded: int, db_rows: int, db_cols: int, interp: int, device: int = 0, stream: int = 0):
+    """ipr_encode_db on device buffers: raw -> encoded u16 DB ([db_cols][db_rows])"""
+    _check(_encode(device, _vp(d_raw), _vp(d_encoded), db_rows, db_cols, interp, _vp(stream)), "encode_db")
+
+
+def cuckoo_to_raw_db(d_entries: int, d_occupied: int, num_buckets: int, entry_size: int, db_rows: int, db_cols: int,
+                     per: int, d_raw: int, device: int = 0, stream: int = 0):
+    """ipr_cuckoo_to_raw_db on device buffers"""
+    _check(_raw_db(device, _vp(d_entries), _vp(d_occupied), num_buckets, entry_size, db_rows, db_cols, per,
+                   _vp(d_raw), _vp(stream)), "cuckoo_to_raw_db")

@@ -15,6 +15,12 @@
 #include "ipr_device.cuh"
 #include "kernels.cuh"
 
+namespace ipr {
+uint32_t encode_num_inv(uint64_t interp);
+int encode_db_device(const uint16_t* d_raw, uint16_t* d_out, uint64_t db_rows, uint64_t db_cols, uint64_t interp,
+                     cudaStream_t st);
+}  // namespace ipr
+
 namespace {
 
 std::mutex g_mu;
@@ -29,6 +35,7 @@ uint64_t *d_bold_t = nullptr, *d_bold_t_bar = nullptr, *d_bold_t_hat = nullptr, 
 uint64_t *d_y_all = nullptr, *d_y_bar_all = nullptr, *d_z_body = nullptr;
 bool g_adopted = false;
 int g_n_inner = 0, g_poly_len = 0;
+uint16_t* g_encoded_db = nullptr;  // gpu_encode_db_from_host's result, kept on the device
 
 bool report(const char* tag, cudaError_t e, int line) {
     if (e == cudaSuccess) return false;
@@ -97,6 +104,47 @@ void gpu_init_memory_pool(void) {
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
     }
     CHK("GPU", ensure_stream_and_constants());
+}
+
+void gpu_encode_db(uint16_t* d_db_in, uint16_t* d_db_out, int db_rows, int db_cols, int interp_degree, int gamma,
+                   int c, uint32_t modulus, uint32_t num_inv) {
+    if (gamma != ipr::N || modulus != 65535u || interp_degree < 1 || db_rows < 1 || db_cols < 1 ||
+        (int64_t)interp_degree * gamma * c != db_cols || num_inv != ipr::encode_num_inv((uint64_t)interp_degree)) {
+        fprintf(stderr, "[GPU Encode] unsupported arguments (gamma %d, modulus %u, interp %d, c %d)\n", gamma,
+                modulus, interp_degree, c);
+        return;
+    }
+    int st = ipr::encode_db_device(d_db_in, d_db_out, (uint64_t)db_rows, (uint64_t)db_cols, (uint64_t)interp_degree,
+                                   cudaStreamPerThread);
+    if (st) fprintf(stderr, "[GPU Encode] %s\n", ipr_last_error());
+    cudaStreamSynchronize(cudaStreamPerThread);
+}
+
+void gpu_encode_db_from_host(const uint16_t* h_db_in, uint16_t* h_db_out, int db_rows, int db_cols,
+                             int interp_degree, int gamma, int c, uint32_t modulus, uint32_t num_inv) {
+    (void)h_db_out;  // the encoded DB stays on the device (gpu_encode_get_device_db)
+    std::lock_guard<std::mutex> lk(g_mu);
+    const size_t bytes = (size_t)db_rows * (size_t)db_cols * sizeof(uint16_t);
+    uint16_t *d_in = nullptr, *d_out = nullptr;
+    if (report("GPU Encode", cudaMalloc(&d_in, bytes), __LINE__) ||
+        report("GPU Encode", cudaMalloc(&d_out, bytes), __LINE__) ||
+        report("GPU Encode", cudaMemcpy(d_in, h_db_in, bytes, cudaMemcpyHostToDevice), __LINE__)) {
+        if (d_in) cudaFree(d_in);
+        if (d_out) cudaFree(d_out);
+        return;
+    }
+    gpu_encode_db(d_in, d_out, db_rows, db_cols, interp_degree, gamma, c, modulus, num_inv);
+    cudaFree(d_in);
+    if (g_encoded_db) cudaFree(g_encoded_db);
+    g_encoded_db = d_out;
+}
+
+const uint16_t* gpu_encode_get_device_db(void) { return g_encoded_db; }
+
+void gpu_encode_free_device_db(void) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_encoded_db) cudaFree(g_encoded_db);
+    g_encoded_db = nullptr;
 }
 
 void gpu_trim_memory_pool(void) {

@@ -51,6 +51,8 @@ constexpr int kMaxProfileSlots = 8192;
 }  // namespace
 
 namespace ipr {
+int encode_db_device(const uint16_t* d_raw, uint16_t* d_out, uint64_t db_rows, uint64_t db_cols, uint64_t interp,
+                     cudaStream_t st);
 // lets other translation units of the library report through ipr_last_error()
 void set_last_error(const char* msg) { g_last_error = msg; }
 }  // namespace ipr
@@ -557,7 +559,19 @@ int ipr_response_merge(const uint8_t* const* parts, const size_t* lens, int num_
     return IPR_OK;
 }
 
+static int create_server(int device, const ipr_plan* plan, const ipr_server_data* data, bool raw_db,
+                         ipr_server** out);
+
 int ipr_server_create(int device, const ipr_plan* plan, const ipr_server_data* data, ipr_server** out) {
+    return create_server(device, plan, data, false, out);
+}
+
+int ipr_server_create_from_raw(int device, const ipr_plan* plan, const ipr_server_data* data, ipr_server** out) {
+    return create_server(device, plan, data, true, out);
+}
+
+static int create_server(int device, const ipr_plan* plan, const ipr_server_data* data, bool raw_db,
+                         ipr_server** out) {
     if (!out || !data || !data->db || !data->a_hat || !data->bold_t || !data->bold_t_bar || !data->bold_t_hat)
         return fail(IPR_E_ARGS, "null argument");
     if (data->stash_count && (!data->stash || !data->stash_entry_bytes)) return fail(IPR_E_ARGS, "bad stash");
@@ -576,8 +590,22 @@ int ipr_server_create(int device, const ipr_plan* plan, const ipr_server_data* d
     if ((st = up(s->d_db, data->db, plan->db_rows * plan->db_cols * 2)) || (st = up(s->d_ahat, data->a_hat, no * kN * 8)) ||
         (st = up(s->d_bt, data->bold_t, no * (uint64_t)kNInner * kN * 8)) ||
         (st = up(s->d_btb, data->bold_t_bar, no * (uint64_t)kNInner * kN * 8)) ||
-        (st = up(s->d_bth, data->bold_t_hat, no * 3 * kN * 8)) ||
-        (st = (ipr::launch_db_to_planes(s->d_db, s->d_db8, (int64_t)(plan->db_rows * plan->db_cols), s->stream) ==
+        (st = up(s->d_bth, data->bold_t_hat, no * 3 * kN * 8))) {
+        ipr_server_destroy(s);
+        return st;
+    }
+    if (raw_db) {  // encode on the device: the byte-plane buffer has the DB's size and is free until below
+        uint16_t* tmp = reinterpret_cast<uint16_t*>(s->d_db8);
+        if ((st = ipr::encode_db_device(s->d_db, tmp, plan->db_rows, plan->db_cols, plan->interp, s->stream)) ||
+            (st = (cudaMemcpyAsync(s->d_db, tmp, plan->db_rows * plan->db_cols * 2, cudaMemcpyDeviceToDevice,
+                                   s->stream) == cudaSuccess
+                       ? IPR_OK
+                       : fail(IPR_E_CUDA, "encoded DB copy: %s", cudaGetErrorString(cudaGetLastError()))))) {
+            ipr_server_destroy(s);
+            return st;
+        }
+    }
+    if ((st = (ipr::launch_db_to_planes(s->d_db, s->d_db8, (int64_t)(plan->db_rows * plan->db_cols), s->stream) ==
                        cudaSuccess && cudaStreamSynchronize(s->stream) == cudaSuccess
                    ? IPR_OK
                    : fail(IPR_E_CUDA, "DB byte planes: %s", cudaGetErrorString(cudaGetLastError()))))) {

@@ -876,3 +876,94 @@ int ipr_synth_query(uint64_t seed, uint64_t db_rows, unsigned nq, uint8_t *out, 
     }
     return IPR_OK;
 }
+
+/* ---- setup-time DB layout and encode -------------------------------------- */
+
+/* KeywordCuckooTable::to_raw_db (src/pir/keyword/cuckoo.rs:314-353): raw[(item*ise + j) *
+ * db_rows + row] = big-endian u16 of entry bytes (2j, 2j+1) of bucket row*per + item, zero
+ * for empty buckets and buckets past the table; ise = entry_size / 2 u16 elements. */
+void ipr_oracle_raw_db(const uint8_t *entries, const uint8_t *occupied, uint64_t num_buckets,
+                       uint64_t entry_size, uint64_t db_rows, uint64_t db_cols, uint64_t per,
+                       uint16_t *raw) {
+    const uint64_t ise = entry_size / 2;
+    memset(raw, 0, db_rows * db_cols * sizeof(uint16_t));
+    for (uint64_t item = 0; item < per; item++)
+        for (uint64_t row = 0; row < db_rows; row++) {
+            const uint64_t b = row * per + item;
+            if (b >= num_buckets || !occupied[b]) continue;
+            const uint8_t *e = entries + b * entry_size;
+            for (uint64_t j = 0; j < ise; j++)
+                raw[(item * ise + j) * db_rows + row] = (uint16_t)(((uint16_t)e[2 * j] << 8) | e[2 * j + 1]);
+        }
+}
+
+/* sums mod p = 65535 (the plaintext modulus, 2^16 - 1): fold the carry back in */
+static uint32_t fold65535(uint32_t x) {
+    uint32_t r = (x & 0xFFFFu) + (x >> 16);
+    r = (r & 0xFFFFu) + (r >> 16);
+    return r >= 65535u ? r - 65535u : r;
+}
+
+/* The DB encode of gpu_encode_db (native/cuda/encode_kernel.cu:18-228, 264-386):
+ * per DB row and fold group wp, the interp polynomials of columns wp*interp*N + j*N + k are
+ * interpolated by a radix-2 Cooley-Tukey pass over Z_65535[X]/(X^N + 1) whose twiddles are
+ * monomials: inputs in bit-reversed order, level L pairs (even, odd) at distance 2^L and
+ * adds / subtracts odd * X^e with e = (2N - 2N*i/2^(L+1)) mod 2N for the i-th pair of a
+ * group; the results are scaled by interp^-1 mod 65535 and stored in natural order. */
+int ipr_oracle_encode_db(const uint16_t *raw, uint16_t *out, uint64_t db_rows, uint64_t db_cols,
+                         uint64_t interp) {
+    const uint64_t n = IPR_N, two_n = 2 * IPR_N;
+    if (!interp || (interp & (interp - 1)) || db_cols % (interp * n)) return IPR_E_ARGS;
+    const uint64_t c = db_cols / (interp * n);
+    unsigned logi = 0;
+    while ((1ull << logi) < interp) logi++;
+    uint32_t inv = 1; /* interp^-1 mod 65535 (interp is a power of two, 2^16 = 1 mod 65535) */
+    for (unsigned b = 0; b < (16 - logi) % 16; b++) inv = fold65535(inv * 2);
+    const uint64_t unit = interp * n;
+    int err = 0;
+#pragma omp parallel
+    {
+        uint32_t *a = (uint32_t *)malloc(unit * sizeof(uint32_t));
+        uint32_t *b = (uint32_t *)malloc(unit * sizeof(uint32_t));
+        if (!a || !b) {
+#pragma omp atomic write
+            err = 1;
+        } else {
+#pragma omp for schedule(static) collapse(2)
+            for (int64_t row = 0; row < (int64_t)db_rows; row++)
+                for (int64_t wp = 0; wp < (int64_t)c; wp++) {
+                    for (uint64_t j = 0; j < interp; j++) {
+                        uint64_t r = 0;
+                        for (unsigned t = 0; t < logi; t++) r |= ((j >> t) & 1) << (logi - 1 - t);
+                        for (uint64_t k = 0; k < n; k++)
+                            a[r * n + k] = raw[((uint64_t)wp * unit + j * n + k) * db_rows + (uint64_t)row];
+                    }
+                    for (unsigned lv = 0; lv < logi; lv++) {
+                        const uint64_t gs = 2ull << lv, half = 1ull << lv;
+                        for (uint64_t g = 0; g < interp / gs; g++)
+                            for (uint64_t i = 0; i < half; i++) {
+                                const uint64_t ev = g * gs + i, od = ev + half;
+                                const uint64_t e = (two_n - two_n * i / gs) % two_n;
+                                for (uint64_t k = 0; k < n; k++) {
+                                    const uint64_t src = (k + two_n - e) % two_n;
+                                    const uint32_t o = a[od * n + (src % n)];
+                                    const uint32_t tw = src < n ? o : 65535u - o;  /* X^N = -1 */
+                                    b[ev * n + k] = fold65535(a[ev * n + k] + tw);
+                                    b[od * n + k] = fold65535(a[ev * n + k] + 65535u - tw);
+                                }
+                            }
+                        uint32_t *tmp = a;
+                        a = b;
+                        b = tmp;
+                    }
+                    for (uint64_t j = 0; j < interp; j++)
+                        for (uint64_t k = 0; k < n; k++)
+                            out[((uint64_t)wp * unit + j * n + k) * db_rows + (uint64_t)row] =
+                                (uint16_t)fold65535(a[j * n + k] * inv);
+                }
+        }
+        free(a);
+        free(b);
+    }
+    return err ? IPR_E_SPACE : IPR_OK;
+}

@@ -153,6 +153,11 @@ void ipr_synth_precomp(uint64_t seed, uint64_t num_outputs, uint64_t *a_hat, uin
                        uint64_t *bold_t_bar, uint64_t *bold_t_hat);
 void ipr_synth_shard(uint64_t seed, uint64_t db_rows, uint64_t first, uint64_t count, uint16_t *db,
                      uint64_t *a_hat, uint64_t *bt, uint64_t *btb, uint64_t *bth);
+void ipr_oracle_raw_db(const uint8_t *entries, const uint8_t *occupied, uint64_t num_buckets,
+                       uint64_t entry_size, uint64_t db_rows, uint64_t db_cols, uint64_t per,
+                       uint16_t *raw);
+int ipr_oracle_encode_db(const uint16_t *raw, uint16_t *out, uint64_t db_rows, uint64_t db_cols,
+                         uint64_t interp);
 int ipr_synth_query(uint64_t seed, uint64_t db_rows, unsigned num_queries, uint8_t *out,
                     size_t cap, size_t *out_len);
 

@@ -98,6 +98,8 @@ synth = _sig("ipr_synth", _u64, _u64, _u64, _u64)
 _synth_db = _sig("ipr_synth_db", None, _u64, _u64, _u64, _p)
 _synth_pre = _sig("ipr_synth_precomp", None, _u64, _u64, _p, _p, _p, _p)
 _synth_shard = _sig("ipr_synth_shard", None, _u64, _u64, _u64, _u64, _p, _p, _p, _p, _p)
+_raw_db = _sig("ipr_oracle_raw_db", None, _p, _p, _u64, _u64, _u64, _u64, _u64, _p)
+_encode_db = _sig("ipr_oracle_encode_db", ctypes.c_int, _p, _p, _u64, _u64, _u64)
 _synth_q = _sig("ipr_synth_query", ctypes.c_int, _u64, _u64, ctypes.c_uint, _p, _sz, ctypes.POINTER(_sz))
 threads = _sig("ipr_oracle_threads", ctypes.c_int)
 
@@ -367,3 +369,23 @@ def switch(result) -> bytes:
     out = np.zeros(RESULT_BYTES, dtype=np.uint8)
     _switch(ctypes.byref(params()), _ptr(r), _ptr(out))
     return out.tobytes()
+
+
+def raw_db(entries: np.ndarray, occupied: np.ndarray, entry_size: int, db_rows: int, db_cols: int,
+           per: int) -> np.ndarray:
+    """KeywordCuckooTable::to_raw_db: column-major u16 [db_cols][db_rows]"""
+    e = np.ascontiguousarray(entries, dtype=np.uint8)
+    o = np.ascontiguousarray(occupied, dtype=np.uint8)
+    out = np.zeros(db_rows * db_cols, dtype=np.uint16)
+    _raw_db(_ptr(e), _ptr(o), o.size, entry_size, db_rows, db_cols, per, _ptr(out))
+    return out
+
+
+def encode_db(raw: np.ndarray, db_rows: int, db_cols: int, interp: int) -> np.ndarray:
+    """gpu_encode_db: the interpolation encode of a column-major raw DB"""
+    r = np.ascontiguousarray(raw, dtype=np.uint16)
+    out = np.zeros(db_rows * db_cols, dtype=np.uint16)
+    st = _encode_db(_ptr(r), _ptr(out), db_rows, db_cols, interp)
+    if st:
+        raise ValueError(f"oracle encode status {st}")
+    return out

@@ -114,3 +114,13 @@ def test_error_string_reports_status(pkg):
     with pytest.raises(pkg.IprError) as e:
         pkg.plan_from_shape(1_000_000, 32, 1184, 262_144, 2048)
     assert "IPR_E_ARGS" in str(e.value) and "buckets" in str(e.value)
+
+
+def test_library_has_no_unresolved_symbols():
+    """every symbol the library needs comes from a versioned system library (a missing
+    definition would only show when the library is loaded on the GPU box)"""
+    import subprocess
+    lib = os.path.join(ROOT, "inspire-rs_b200", "libipr_b200.so")
+    out = subprocess.run(["nm", "-D", "--undefined-only", lib], capture_output=True, text=True, check=True).stdout
+    missing = [ln.split()[-1] for ln in out.splitlines() if ln.split() and ln.split()[0] == "U" and "@" not in ln]
+    assert missing == []
