@@ -223,7 +223,7 @@ int ipr_automorph_batch(int device, const uint64_t *d_in, uint64_t count, const 
  * ipr_encode_db: gpu_encode_db (native/cuda/encode_kernel.cu:264-386) — the
  * interpolation of each fold group's interp polynomials over Z_65535[X]/(X^2048+1),
  * raw -> encoded ([db_cols][db_rows] u16 both; interp a power of two <= 32,
- * db_rows a multiple of 16; input and output distinct). */
+ * db_rows a multiple of 32; input and output distinct, 16-byte aligned). */
 int ipr_cuckoo_to_raw_db(int device, const uint8_t *d_entries, const uint8_t *d_occupied, uint64_t num_buckets,
                          uint64_t entry_size, uint64_t db_rows, uint64_t db_cols, uint64_t per, uint16_t *d_raw,
                          void *stream);

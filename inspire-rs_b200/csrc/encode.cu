@@ -12,9 +12,9 @@
 // B200 design.  Every twiddle X^e of the pass has e a multiple of S = 2N/I, so a shift
 // moves whole chunks of S coefficients and keeps the offset o = k mod S: the pass
 // splits into S independent sub-problems of I polynomials x I/2 chunks.  One CTA takes
-// 16 DB rows x one (fold group, offset): it reads its 16 x I x I/2 values once (16 rows
-// = one 32-byte sector per column), runs all log2(I) levels in shared memory (ping-pong
-// buffers, rows fastest, conflict-free), scales, and writes them back once — one HBM
+// 32 DB rows x one (fold group, offset): it reads its 32 x I x I/2 values once (16-byte
+// accesses of 8 rows, 64 bytes per column), runs all log2(I) levels in shared memory
+// (ping-pong buffers, 8 rows per thread and step), scales, and writes them back once — one HBM
 // round trip for the whole encode where the reference makes one per level plus a
 // gather and a scatter.
 #include <cuda_runtime.h>
@@ -29,7 +29,7 @@ void set_last_error(const char* msg);
 
 namespace {
 
-constexpr int E_ROWS = 16;  // DB rows per CTA
+constexpr int E_ROWS = 32;  // DB rows per CTA (four 16-byte groups per column)
 constexpr uint32_t PMOD = 65535;
 
 __device__ __forceinline__ uint32_t fold65535(uint32_t x) {
@@ -70,53 +70,75 @@ __global__ void k_encode_scale1(const uint16_t* __restrict__ in, uint16_t* __res
         out[i] = (uint16_t)fold65535(in[i]);
 }
 
+// one 16-byte group = 8 consecutive DB rows of one column
+__device__ __forceinline__ void unpack8(const uint4& v, uint32_t (&x)[8]) {
+    x[0] = v.x & 0xFFFFu; x[1] = v.x >> 16; x[2] = v.y & 0xFFFFu; x[3] = v.y >> 16;
+    x[4] = v.z & 0xFFFFu; x[5] = v.z >> 16; x[6] = v.w & 0xFFFFu; x[7] = v.w >> 16;
+}
+__device__ __forceinline__ uint4 pack8(const uint32_t (&x)[8]) {
+    return make_uint4(x[0] | (x[1] << 16), x[2] | (x[3] << 16), x[4] | (x[5] << 16), x[6] | (x[7] << 16));
+}
+
 template <int I>
 __global__ void __launch_bounds__(256) k_encode(const uint16_t* __restrict__ in, uint16_t* __restrict__ out,
                                                 int64_t db_rows, uint32_t inv) {
-    constexpr int H = I / 2;             // chunks of S coefficients in [0, N)
-    constexpr int S = 2 * N / I;         // coefficient stride between chunks
-    constexpr int VALS = I * H * E_ROWS;
+    constexpr int H = I / 2;        // chunks of S coefficients in [0, N)
+    constexpr int S = 2 * N / I;    // coefficient stride between chunks
+    constexpr int RG = E_ROWS / 8;  // 8-row groups per column
+    constexpr int GROUPS = I * H * RG;
     constexpr int LOGI = I == 2 ? 1 : I == 4 ? 2 : I == 8 ? 3 : I == 16 ? 4 : 5;
-    __shared__ uint16_t buf[2][I][H][E_ROWS];  // [ping-pong][poly][chunk][row]
-    const int o = blockIdx.x;          // offset within a chunk, < S
-    const int64_t g_wp = blockIdx.y;   // fold group
-    const int64_t row0 = (int64_t)blockIdx.z * E_ROWS;
-    const int64_t col0 = g_wp * I * N + o;
+    extern __shared__ __align__(16) uint16_t ebuf[];  // [ping-pong][poly][chunk][row]
+    auto buf = reinterpret_cast<uint16_t(*)[I][H][E_ROWS]>(ebuf);
+    // row tiles vary fastest: the CTAs resident together read whole 4 KB columns between them
+    const int64_t row0 = (int64_t)blockIdx.x * E_ROWS;
+    const int o = blockIdx.y;         // offset within a chunk, < S
+    const int64_t wp = blockIdx.z;    // fold group
+    const int64_t col0 = wp * I * N + o;
 
-    // gather in bit-reversed polynomial order
-    for (int i = threadIdx.x; i < VALS; i += blockDim.x) {
-        const int r = i % E_ROWS, q = i / E_ROWS;
+    // gather in bit-reversed polynomial order, 16 bytes (8 rows) per access
+    for (int i = threadIdx.x; i < GROUPS; i += blockDim.x) {
+        const int rg = i % RG, q = i / RG;
         const int j = q / H, kc = q % H;
         const int jr = (int)(__brev((unsigned)j) >> (32 - LOGI));
-        buf[0][jr][kc][r] = in[(col0 + (int64_t)j * N + (int64_t)kc * S) * db_rows + row0 + r];
+        *reinterpret_cast<uint4*>(&buf[0][jr][kc][rg * 8]) = __ldg(reinterpret_cast<const uint4*>(
+            in + (col0 + (int64_t)j * N + (int64_t)kc * S) * db_rows + row0 + rg * 8));
     }
     __syncthreads();
     int cur = 0;
 #pragma unroll
     for (int lv = 0; lv < LOGI; lv++) {
         const int gs = 2 << lv, half = 1 << lv;
-        for (int i = threadIdx.x; i < E_ROWS * (I / 2) * H; i += blockDim.x) {
-            const int r = i % E_ROWS, rest2 = i / E_ROWS;
-            const int kc = rest2 % H, pr = rest2 / H;
+        for (int i = threadIdx.x; i < (I / 2) * H * RG; i += blockDim.x) {
+            const int rg = i % RG, rest = i / RG;
+            const int kc = rest % H, pr = rest / H;
             const int g = pr / half, t = pr % half;
             const int ev = g * gs + t, od = ev + half;
             const int e = (2 * N - 2 * N * t / gs) % (2 * N);  // twiddle X^e, e a multiple of S
             const int src = (kc + I - e / S) % I;                // chunk of coefficient k - e (mod 2N)
-            const uint32_t ov = buf[cur][od][src < H ? src : src - H][r];
-            const uint32_t tw = src < H ? ov : PMOD - ov;       // X^N = -1
-            const uint32_t evv = buf[cur][ev][kc][r];
-            buf[cur ^ 1][ev][kc][r] = (uint16_t)fold65535(evv + tw);
-            buf[cur ^ 1][od][kc][r] = (uint16_t)fold65535(evv + PMOD - tw);
+            uint32_t xo[8], xe[8], ye[8], yo[8];
+            unpack8(*reinterpret_cast<const uint4*>(&buf[cur][od][src < H ? src : src - H][rg * 8]), xo);
+            unpack8(*reinterpret_cast<const uint4*>(&buf[cur][ev][kc][rg * 8]), xe);
+#pragma unroll
+            for (int r = 0; r < 8; r++) {
+                const uint32_t tw = src < H ? xo[r] : PMOD - xo[r];  // X^N = -1
+                ye[r] = fold65535(xe[r] + tw);
+                yo[r] = fold65535(xe[r] + PMOD - tw);
+            }
+            *reinterpret_cast<uint4*>(&buf[cur ^ 1][ev][kc][rg * 8]) = pack8(ye);
+            *reinterpret_cast<uint4*>(&buf[cur ^ 1][od][kc][rg * 8]) = pack8(yo);
         }
         __syncthreads();
         cur ^= 1;
     }
     // scale and store in natural polynomial order
-    for (int i = threadIdx.x; i < VALS; i += blockDim.x) {
-        const int r = i % E_ROWS, q = i / E_ROWS;
+    for (int i = threadIdx.x; i < GROUPS; i += blockDim.x) {
+        const int rg = i % RG, q = i / RG;
         const int j = q / H, kc = q % H;
-        out[(col0 + (int64_t)j * N + (int64_t)kc * S) * db_rows + row0 + r] =
-            (uint16_t)fold65535((uint32_t)buf[cur][j][kc][r] * inv);
+        uint32_t x[8];
+        unpack8(*reinterpret_cast<const uint4*>(&buf[cur][j][kc][rg * 8]), x);
+#pragma unroll
+        for (int r = 0; r < 8; r++) x[r] = fold65535(x[r] * inv);
+        *reinterpret_cast<uint4*>(out + (col0 + (int64_t)j * N + (int64_t)kc * S) * db_rows + row0 + rg * 8) = pack8(x);
     }
 }
 
@@ -140,8 +162,9 @@ uint32_t encode_num_inv(uint64_t interp) {
 int encode_db_device(const uint16_t* d_raw, uint16_t* d_out, uint64_t db_rows, uint64_t db_cols, uint64_t interp,
                      cudaStream_t st) {
     if (!d_raw || !d_out || !interp || (interp & (interp - 1)) || interp > 32 || db_rows % E_ROWS ||
-        db_cols % (interp * N)) {
-        set_last_error("encode: interp must be a power of two <= 32, db_rows a multiple of 16 and db_cols of interp*2048");
+        db_cols % (interp * N) || (reinterpret_cast<uintptr_t>(d_raw) | reinterpret_cast<uintptr_t>(d_out)) % 16) {
+        set_last_error("encode: interp must be a power of two <= 32, db_rows a multiple of 32, db_cols of "
+                       "interp*2048, buffers 16-byte aligned");
         return IPR_E_ARGS;
     }
     if (d_raw == d_out) {
@@ -149,7 +172,7 @@ int encode_db_device(const uint16_t* d_raw, uint16_t* d_out, uint64_t db_rows, u
         return IPR_E_ARGS;
     }
     const uint64_t c = db_cols / (interp * N);
-    if (c > 65535 || db_rows / E_ROWS > 65535) {
+    if (c > 65535 || 2 * N / interp > 65535) {
         set_last_error("encode: shape too large for one launch");
         return IPR_E_ARGS;
     }
@@ -157,13 +180,19 @@ int encode_db_device(const uint16_t* d_raw, uint16_t* d_out, uint64_t db_rows, u
     if (interp == 1) {
         k_encode_scale1<<<148 * 8, 256, 0, st>>>(d_raw, d_out, (int64_t)(db_rows * db_cols));
     } else {
-        const dim3 grid((unsigned)(2 * N / interp), (unsigned)c, (unsigned)(db_rows / E_ROWS));
+        const dim3 grid((unsigned)(db_rows / E_ROWS), (unsigned)(2 * N / interp), (unsigned)c);
+        const int smem = (int)(2 * interp * (interp / 2) * E_ROWS * sizeof(uint16_t));  // 64 KB at interp 32
+        cudaError_t e = cudaSuccess;
         switch (interp) {
-            case 2: k_encode<2><<<grid, 256, 0, st>>>(d_raw, d_out, (int64_t)db_rows, inv); break;
-            case 4: k_encode<4><<<grid, 256, 0, st>>>(d_raw, d_out, (int64_t)db_rows, inv); break;
-            case 8: k_encode<8><<<grid, 256, 0, st>>>(d_raw, d_out, (int64_t)db_rows, inv); break;
-            case 16: k_encode<16><<<grid, 256, 0, st>>>(d_raw, d_out, (int64_t)db_rows, inv); break;
-            default: k_encode<32><<<grid, 256, 0, st>>>(d_raw, d_out, (int64_t)db_rows, inv); break;
+            case 2: k_encode<2><<<grid, 256, smem, st>>>(d_raw, d_out, (int64_t)db_rows, inv); break;
+            case 4: k_encode<4><<<grid, 256, smem, st>>>(d_raw, d_out, (int64_t)db_rows, inv); break;
+            case 8: k_encode<8><<<grid, 256, smem, st>>>(d_raw, d_out, (int64_t)db_rows, inv); break;
+            case 16: k_encode<16><<<grid, 256, smem, st>>>(d_raw, d_out, (int64_t)db_rows, inv); break;
+            default:
+                e = cudaFuncSetAttribute(k_encode<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+                if (e != cudaSuccess) return cuda_status(e);
+                k_encode<32><<<grid, 256, smem, st>>>(d_raw, d_out, (int64_t)db_rows, inv);
+                break;
         }
     }
     return cuda_status(cudaGetLastError());

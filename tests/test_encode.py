@@ -78,8 +78,8 @@ def _dev(a):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("interp,c,db_rows", [(1, 2, 32), (2, 1, 16), (4, 2, 48), (8, 1, 256), (16, 1, 32),
-                                              (32, 1, 16), (32, 2, 64)])
+@pytest.mark.parametrize("interp,c,db_rows", [(1, 2, 32), (2, 1, 32), (4, 2, 64), (8, 1, 256), (16, 1, 32),
+                                              (32, 1, 32), (32, 2, 96)])
 def test_device_encode_matches_oracle(pkg, orc, interp, c, db_rows):
     import torch
     rng = np.random.default_rng(100 + interp + c)
