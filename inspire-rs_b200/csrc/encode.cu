@@ -70,6 +70,13 @@ __global__ void k_encode_scale1(const uint16_t* __restrict__ in, uint16_t* __res
         out[i] = (uint16_t)fold65535(in[i]);
 }
 
+// a + b mod 65535 on both 16-bit halves (ones'-complement sum: the carry out of a half is
+// added back into it; operands and result in [0, 65535] with 65535 = 0)
+__device__ __forceinline__ uint32_t oadd2(uint32_t a, uint32_t b) {
+    const uint32_t r = __vadd2(a, b);
+    return __vsub2(r, __vcmpltu2(r, a));  // a carry leaves r < a: add 1 to that half
+}
+
 // one 16-byte group = 8 consecutive DB rows of one column
 __device__ __forceinline__ void unpack8(const uint4& v, uint32_t (&x)[8]) {
     x[0] = v.x & 0xFFFFu; x[1] = v.x >> 16; x[2] = v.y & 0xFFFFu; x[3] = v.y >> 16;
@@ -115,17 +122,16 @@ __global__ void __launch_bounds__(256) k_encode(const uint16_t* __restrict__ in,
             const int ev = g * gs + t, od = ev + half;
             const int e = (2 * N - 2 * N * t / gs) % (2 * N);  // twiddle X^e, e a multiple of S
             const int src = (kc + I - e / S) % I;                // chunk of coefficient k - e (mod 2N)
-            uint32_t xo[8], xe[8], ye[8], yo[8];
-            unpack8(*reinterpret_cast<const uint4*>(&buf[cur][od][src < H ? src : src - H][rg * 8]), xo);
-            unpack8(*reinterpret_cast<const uint4*>(&buf[cur][ev][kc][rg * 8]), xe);
-#pragma unroll
-            for (int r = 0; r < 8; r++) {
-                const uint32_t tw = src < H ? xo[r] : PMOD - xo[r];  // X^N = -1
-                ye[r] = fold65535(xe[r] + tw);
-                yo[r] = fold65535(xe[r] + PMOD - tw);
-            }
-            *reinterpret_cast<uint4*>(&buf[cur ^ 1][ev][kc][rg * 8]) = pack8(ye);
-            *reinterpret_cast<uint4*>(&buf[cur ^ 1][od][kc][rg * 8]) = pack8(yo);
+            // two values per 32-bit word in ones'-complement form (65535 stands for 0):
+            // -x is ~x and a sum folds its carry back in, so the butterfly runs on packed halves
+            const uint4 ov = *reinterpret_cast<const uint4*>(&buf[cur][od][src < H ? src : src - H][rg * 8]);
+            const uint4 evv = *reinterpret_cast<const uint4*>(&buf[cur][ev][kc][rg * 8]);
+            const bool neg = src >= H;  // X^N = -1
+            const uint4 tw = neg ? make_uint4(~ov.x, ~ov.y, ~ov.z, ~ov.w) : ov;
+            *reinterpret_cast<uint4*>(&buf[cur ^ 1][ev][kc][rg * 8]) =
+                make_uint4(oadd2(evv.x, tw.x), oadd2(evv.y, tw.y), oadd2(evv.z, tw.z), oadd2(evv.w, tw.w));
+            *reinterpret_cast<uint4*>(&buf[cur ^ 1][od][kc][rg * 8]) =
+                make_uint4(oadd2(evv.x, ~tw.x), oadd2(evv.y, ~tw.y), oadd2(evv.z, ~tw.z), oadd2(evv.w, ~tw.w));
         }
         __syncthreads();
         cur ^= 1;
