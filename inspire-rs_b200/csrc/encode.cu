@@ -14,7 +14,8 @@
 // splits into S independent sub-problems of I polynomials x I/2 chunks.  One CTA takes
 // 32 DB rows x one (fold group, offset): it reads its 32 x I x I/2 values once (16-byte
 // accesses of 8 rows, 64 bytes per column), runs all log2(I) levels in shared memory
-// (ping-pong buffers, 8 rows per thread and step), scales, and writes them back once — one HBM
+// (in place: each step reads its inputs into registers before a barrier, 8 rows
+// per thread and step), scales, and writes them back once — one HBM
 // round trip for the whole encode where the reference makes one per level plus a
 // gather and a scatter.
 #include <cuda_runtime.h>
@@ -86,62 +87,99 @@ __device__ __forceinline__ uint4 pack8(const uint32_t (&x)[8]) {
     return make_uint4(x[0] | (x[1] << 16), x[2] | (x[3] << 16), x[4] | (x[5] << 16), x[6] | (x[7] << 16));
 }
 
+constexpr int E_THREADS = 256;
+
 template <int I>
-__global__ void __launch_bounds__(256) k_encode(const uint16_t* __restrict__ in, uint16_t* __restrict__ out,
-                                                int64_t db_rows, uint32_t inv) {
+__global__ void __launch_bounds__(E_THREADS) k_encode(const uint16_t* __restrict__ in, uint16_t* __restrict__ out,
+                                                      int64_t db_rows, uint32_t inv) {
     constexpr int H = I / 2;        // chunks of S coefficients in [0, N)
     constexpr int S = 2 * N / I;    // coefficient stride between chunks
     constexpr int RG = E_ROWS / 8;  // 8-row groups per column
     constexpr int GROUPS = I * H * RG;
+    constexpr int BFLY = (I / 2) * H * RG;  // butterflies (of 8 rows) per level
+    constexpr int BPT = (BFLY + E_THREADS - 1) / E_THREADS;
     constexpr int LOGI = I == 2 ? 1 : I == 4 ? 2 : I == 8 ? 3 : I == 16 ? 4 : 5;
-    extern __shared__ __align__(16) uint16_t ebuf[];  // [ping-pong][poly][chunk][row]
-    auto buf = reinterpret_cast<uint16_t(*)[I][H][E_ROWS]>(ebuf);
+    __shared__ __align__(16) uint16_t buf[I][H][E_ROWS];  // [poly][chunk][row], 32 KB at interp 32
     // row tiles vary fastest: the CTAs resident together read whole 4 KB columns between them
     const int64_t row0 = (int64_t)blockIdx.x * E_ROWS;
     const int o = blockIdx.y;         // offset within a chunk, < S
     const int64_t wp = blockIdx.z;    // fold group
     const int64_t col0 = wp * I * N + o;
 
-    // gather in bit-reversed polynomial order, 16 bytes (8 rows) per access
-    for (int i = threadIdx.x; i < GROUPS; i += blockDim.x) {
-        const int rg = i % RG, q = i / RG;
-        const int j = q / H, kc = q % H;
-        const int jr = (int)(__brev((unsigned)j) >> (32 - LOGI));
-        *reinterpret_cast<uint4*>(&buf[0][jr][kc][rg * 8]) = __ldg(reinterpret_cast<const uint4*>(
-            in + (col0 + (int64_t)j * N + (int64_t)kc * S) * db_rows + row0 + rg * 8));
+    // gather in bit-reversed polynomial order, 16 bytes (8 rows) per access; the loads of
+    // a thread are all issued before the first store
+    {
+        constexpr int LPT = (GROUPS + E_THREADS - 1) / E_THREADS;
+        uint4 v[LPT];
+#pragma unroll
+        for (int u = 0; u < LPT; u++) {
+            const int i = threadIdx.x + u * E_THREADS;
+            if (GROUPS % E_THREADS == 0 || i < GROUPS) {
+                const int rg = i % RG, q = i / RG;
+                const int j = q / H, kc = q % H;
+                v[u] = __ldg(reinterpret_cast<const uint4*>(in + (col0 + (int64_t)j * N + (int64_t)kc * S) * db_rows +
+                                                            row0 + rg * 8));
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < LPT; u++) {
+            const int i = threadIdx.x + u * E_THREADS;
+            if (GROUPS % E_THREADS == 0 || i < GROUPS) {
+                const int rg = i % RG, q = i / RG;
+                const int j = q / H, kc = q % H;
+                const int jr = (int)(__brev((unsigned)j) >> (32 - LOGI));
+                *reinterpret_cast<uint4*>(&buf[jr][kc][rg * 8]) = v[u];
+            }
+        }
     }
     __syncthreads();
-    int cur = 0;
 #pragma unroll
     for (int lv = 0; lv < LOGI; lv++) {
         const int gs = 2 << lv, half = 1 << lv;
-        for (int i = threadIdx.x; i < (I / 2) * H * RG; i += blockDim.x) {
-            const int rg = i % RG, rest = i / RG;
-            const int kc = rest % H, pr = rest / H;
-            const int g = pr / half, t = pr % half;
-            const int ev = g * gs + t, od = ev + half;
-            const int e = (2 * N - 2 * N * t / gs) % (2 * N);  // twiddle X^e, e a multiple of S
-            const int src = (kc + I - e / S) % I;                // chunk of coefficient k - e (mod 2N)
-            // two values per 32-bit word in ones'-complement form (65535 stands for 0):
-            // -x is ~x and a sum folds its carry back in, so the butterfly runs on packed halves
-            const uint4 ov = *reinterpret_cast<const uint4*>(&buf[cur][od][src < H ? src : src - H][rg * 8]);
-            const uint4 evv = *reinterpret_cast<const uint4*>(&buf[cur][ev][kc][rg * 8]);
-            const bool neg = src >= H;  // X^N = -1
-            const uint4 tw = neg ? make_uint4(~ov.x, ~ov.y, ~ov.z, ~ov.w) : ov;
-            *reinterpret_cast<uint4*>(&buf[cur ^ 1][ev][kc][rg * 8]) =
-                make_uint4(oadd2(evv.x, tw.x), oadd2(evv.y, tw.y), oadd2(evv.z, tw.z), oadd2(evv.w, tw.w));
-            *reinterpret_cast<uint4*>(&buf[cur ^ 1][od][kc][rg * 8]) =
-                make_uint4(oadd2(evv.x, ~tw.x), oadd2(evv.y, ~tw.y), oadd2(evv.z, ~tw.z), oadd2(evv.w, ~tw.w));
+        // each butterfly reads its two inputs into registers; after a barrier all outputs
+        // overwrite them in place
+        uint4 ra[BPT], rb[BPT];
+#pragma unroll
+        for (int u = 0; u < BPT; u++) {
+            const int i = threadIdx.x + u * E_THREADS;
+            if (BFLY % E_THREADS == 0 || i < BFLY) {
+                const int rg = i % RG, rest = i / RG;
+                const int kc = rest % H, pr = rest / H;
+                const int g = pr / half, t = pr % half;
+                const int ev = g * gs + t, od = ev + half;
+                const int e = (2 * N - 2 * N * t / gs) % (2 * N);  // twiddle X^e, e a multiple of S
+                const int src = (kc + I - e / S) % I;                // chunk of coefficient k - e (mod 2N)
+                // two values per 32-bit word in ones'-complement form (65535 stands for 0):
+                // -x is ~x and a sum folds its carry back in, so the butterfly runs on packed halves
+                const uint4 ov = *reinterpret_cast<const uint4*>(&buf[od][src < H ? src : src - H][rg * 8]);
+                const uint4 evv = *reinterpret_cast<const uint4*>(&buf[ev][kc][rg * 8]);
+                const bool neg = src >= H;  // X^N = -1
+                const uint4 tw = neg ? make_uint4(~ov.x, ~ov.y, ~ov.z, ~ov.w) : ov;
+                ra[u] = make_uint4(oadd2(evv.x, tw.x), oadd2(evv.y, tw.y), oadd2(evv.z, tw.z), oadd2(evv.w, tw.w));
+                rb[u] = make_uint4(oadd2(evv.x, ~tw.x), oadd2(evv.y, ~tw.y), oadd2(evv.z, ~tw.z), oadd2(evv.w, ~tw.w));
+            }
         }
         __syncthreads();
-        cur ^= 1;
+#pragma unroll
+        for (int u = 0; u < BPT; u++) {
+            const int i = threadIdx.x + u * E_THREADS;
+            if (BFLY % E_THREADS == 0 || i < BFLY) {
+                const int rg = i % RG, rest = i / RG;
+                const int kc = rest % H, pr = rest / H;
+                const int ev = pr / half * gs + pr % half;
+                *reinterpret_cast<uint4*>(&buf[ev][kc][rg * 8]) = ra[u];
+                *reinterpret_cast<uint4*>(&buf[ev + half][kc][rg * 8]) = rb[u];
+            }
+        }
+        __syncthreads();
     }
     // scale and store in natural polynomial order
-    for (int i = threadIdx.x; i < GROUPS; i += blockDim.x) {
+#pragma unroll 4
+    for (int i = threadIdx.x; i < GROUPS; i += E_THREADS) {
         const int rg = i % RG, q = i / RG;
         const int j = q / H, kc = q % H;
         uint32_t x[8];
-        unpack8(*reinterpret_cast<const uint4*>(&buf[cur][j][kc][rg * 8]), x);
+        unpack8(*reinterpret_cast<const uint4*>(&buf[j][kc][rg * 8]), x);
 #pragma unroll
         for (int r = 0; r < 8; r++) x[r] = fold65535(x[r] * inv);
         *reinterpret_cast<uint4*>(out + (col0 + (int64_t)j * N + (int64_t)kc * S) * db_rows + row0 + rg * 8) = pack8(x);
@@ -187,18 +225,12 @@ int encode_db_device(const uint16_t* d_raw, uint16_t* d_out, uint64_t db_rows, u
         k_encode_scale1<<<148 * 8, 256, 0, st>>>(d_raw, d_out, (int64_t)(db_rows * db_cols));
     } else {
         const dim3 grid((unsigned)(db_rows / E_ROWS), (unsigned)(2 * N / interp), (unsigned)c);
-        const int smem = (int)(2 * interp * (interp / 2) * E_ROWS * sizeof(uint16_t));  // 64 KB at interp 32
-        cudaError_t e = cudaSuccess;
         switch (interp) {
-            case 2: k_encode<2><<<grid, 256, smem, st>>>(d_raw, d_out, (int64_t)db_rows, inv); break;
-            case 4: k_encode<4><<<grid, 256, smem, st>>>(d_raw, d_out, (int64_t)db_rows, inv); break;
-            case 8: k_encode<8><<<grid, 256, smem, st>>>(d_raw, d_out, (int64_t)db_rows, inv); break;
-            case 16: k_encode<16><<<grid, 256, smem, st>>>(d_raw, d_out, (int64_t)db_rows, inv); break;
-            default:
-                e = cudaFuncSetAttribute(k_encode<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-                if (e != cudaSuccess) return cuda_status(e);
-                k_encode<32><<<grid, 256, smem, st>>>(d_raw, d_out, (int64_t)db_rows, inv);
-                break;
+            case 2: k_encode<2><<<grid, E_THREADS, 0, st>>>(d_raw, d_out, (int64_t)db_rows, inv); break;
+            case 4: k_encode<4><<<grid, E_THREADS, 0, st>>>(d_raw, d_out, (int64_t)db_rows, inv); break;
+            case 8: k_encode<8><<<grid, E_THREADS, 0, st>>>(d_raw, d_out, (int64_t)db_rows, inv); break;
+            case 16: k_encode<16><<<grid, E_THREADS, 0, st>>>(d_raw, d_out, (int64_t)db_rows, inv); break;
+            default: k_encode<32><<<grid, E_THREADS, 0, st>>>(d_raw, d_out, (int64_t)db_rows, inv); break;
         }
     }
     return cuda_status(cudaGetLastError());
