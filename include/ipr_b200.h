@@ -27,10 +27,11 @@ extern "C" {
 #define IPR_E_OOM -2      /* device or host allocation failed, or HBM budget exceeded */
 #define IPR_E_CUDA -3     /* CUDA runtime error (message in ipr_last_error) */
 #define IPR_E_TIMEOUT -4  /* a bounded wait ran out */
-#define IPR_E_FORMAT -5   /* malformed query bytes */
+#define IPR_E_FORMAT -5   /* malformed query bytes or state file */
 #define IPR_E_SPACE -6    /* output buffer too small (required size reported) */
 #define IPR_E_STATE -7    /* call made in the wrong state */
 #define IPR_E_BUSY -8     /* request queue full (serving loop admission) */
+#define IPR_E_IO -9       /* file read/write failed (state files) */
 #define IPR_PENDING 1     /* request accepted, result not ready yet */
 
 #define IPR_POLY_LEN 2048
@@ -214,6 +215,24 @@ int ipr_gemv_query_noalloc(uint64_t *h_c, const uint64_t *h_a, const uint16_t *d
 int ipr_ntt_batch(int device, uint64_t *d_polys, uint64_t count, int limb, int inverse, void *stream);
 int ipr_automorph_batch(int device, const uint64_t *d_in, uint64_t count, const uint32_t *d_ks, int nk,
                         uint64_t *d_out, void *stream);
+
+/* Server state file (no reference counterpart: the reference reruns encode and the
+ * offline precomputation on every start, keyword.rs:366-457).  ipr_server_save writes
+ * the setup outputs the server was built from (the arrays of ipr_server_data: encoded
+ * DB, a_hat, bold_t, bold_t_bar, bold_t_hat, stash) with the plan and public
+ * parameters; ipr_server_load rebuilds a server from such a file on `device`, answering
+ * byte for byte like the saved one, without the caller holding the arrays in host memory.
+ * Format: a 4096-byte header (magic "IPRSTATE", version 1, the ipr_plan fields, key /
+ * value sizes, record count, cuckoo seed, stash shape, one {offset, bytes, checksum}
+ * entry per section, a header checksum), then the six sections in that order, each
+ * starting on a 4096-byte boundary, the file ending on one.  Checksums are
+ * sum_i mix64(w_i + i * 0x9E3779B97F4A7C15) mod 2^64 over the section's little-endian
+ * 64-bit words w_i (last word zero-padded), mix64 the splitmix64 finaliser.  A file
+ * whose header, section table, size or checksums disagree is refused with IPR_E_FORMAT;
+ * I/O failures return IPR_E_IO.  ipr_state_file_plan reads only the header (no GPU). */
+int ipr_server_save(ipr_server *srv, const char *path);
+int ipr_server_load(int device, const char *path, ipr_server **out);
+int ipr_state_file_plan(const char *path, ipr_plan *out);
 
 /* Setup-time database layout and encode on device buffers.
  * ipr_cuckoo_to_raw_db: KeywordCuckooTable::to_raw_db (cuckoo.rs:314-353) — bucket

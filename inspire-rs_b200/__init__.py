@@ -21,7 +21,7 @@ __all__ = [
     "KeywordQueryPayload", "KeywordResponsePayload", "serialize_keyword_query",
     "deserialize_keyword_response", "POLY_LEN", "RESULT_BYTES", "KeywordService", "ServiceStats",
     "shard_plan", "merge_responses", "ShardedKeywordServer", "ntt_batch", "automorph_batch", "encode_db",
-    "cuckoo_to_raw_db",
+    "cuckoo_to_raw_db", "state_file_plan",
 ]
 
 POLY_LEN = 2048
@@ -108,6 +108,9 @@ _create_raw = _sig("ipr_server_create_from_raw", _i32, _i32, ctypes.POINTER(_Pla
                    ctypes.POINTER(_vp))
 _encode = _sig("ipr_encode_db", _i32, _i32, _vp, _vp, _u64, _u64, _u64, _vp)
 _raw_db = _sig("ipr_cuckoo_to_raw_db", _i32, _i32, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _vp, _vp)
+_save = _sig("ipr_server_save", _i32, _vp, ctypes.c_char_p)
+_load = _sig("ipr_server_load", _i32, _i32, ctypes.c_char_p, ctypes.POINTER(_vp))
+_state_plan = _sig("ipr_state_file_plan", _i32, ctypes.c_char_p, ctypes.POINTER(_Plan))
 _svc_create = _sig("ipr_service_create", _i32, ctypes.POINTER(_vp), _i32, ctypes.POINTER(_ServiceConfig),
                    ctypes.POINTER(_vp))
 _svc_submit = _sig("ipr_service_submit", _i32, _vp, _i32, _u8p, _sz, ctypes.POINTER(_u64))
@@ -127,7 +130,8 @@ _svc_destroy = _sig("ipr_service_destroy", None, _vp)
 _version = _sig("ipr_version", ctypes.c_char_p)
 
 STATUS = {0: "IPR_OK", 1: "IPR_PENDING", -1: "IPR_E_ARGS", -2: "IPR_E_OOM", -3: "IPR_E_CUDA",
-          -4: "IPR_E_TIMEOUT", -5: "IPR_E_FORMAT", -6: "IPR_E_SPACE", -7: "IPR_E_STATE", -8: "IPR_E_BUSY"}
+          -4: "IPR_E_TIMEOUT", -5: "IPR_E_FORMAT", -6: "IPR_E_SPACE", -7: "IPR_E_STATE", -8: "IPR_E_BUSY",
+          -9: "IPR_E_IO"}
 IPR_PENDING = 1
 IPR_E_BUSY = -8
 
@@ -164,6 +168,13 @@ class Plan:
     @property
     def query_bytes(self) -> int:
         return query_bytes(self.db_rows, 2)
+
+
+def state_file_plan(path: str) -> Plan:
+    """the plan recorded in a server state file's header (reads the header only)"""
+    p = _Plan()
+    _check(_state_plan(os.fsencode(path), ctypes.byref(p)), "ipr_state_file_plan")
+    return Plan(*[getattr(p, f) for f, _ in _Plan._fields_])
 
 
 def plan_from_shape(record_count: int, key_size: int, value_size: int,
@@ -307,6 +318,19 @@ class KeywordServer:
         pc = plan._c()
         _check(_create_synth(device, ctypes.byref(pc), seed, ctypes.byref(h)), "ipr_server_create_synthetic")
         return cls(h.value, plan, device)
+
+    @classmethod
+    def load(cls, path: str, device: int = 0) -> "KeywordServer":
+        """rebuild a server from a state file written by ``save`` (no setup rerun)"""
+        plan = state_file_plan(path)
+        h = _vp()
+        _check(_load(device, os.fsencode(path), ctypes.byref(h)), "ipr_server_load")
+        return cls(h.value, plan, device)
+
+    def save(self, path: str):
+        """write the setup outputs this server was built from to a state file
+        (format: ipr_server_save in include/ipr_b200.h)"""
+        _check(_save(self._h, os.fsencode(path)), "ipr_server_save")
 
     def close(self):
         if self._h and self._h.value:

@@ -72,26 +72,36 @@ __global__ void k_encode_scale1(const uint16_t* __restrict__ in, uint16_t* __res
 }
 
 // a + b mod 65535 on both 16-bit halves (ones'-complement sum: the carry out of a half is
-// added back into it; operands and result in [0, 65535] with 65535 = 0)
+// added back into it; operands and result in [0, 65535] with 65535 = 0).  One 64-bit add
+// gives the high half's carry c1 and the carry c0 out of the low half (bit 16 of
+// s ^ a ^ b); c0 moves from the high half back into the low one, c1 re-enters the high
+// half, and neither re-addition can carry again.
 __device__ __forceinline__ uint32_t oadd2(uint32_t a, uint32_t b) {
-    const uint32_t r = __vadd2(a, b);
-    return __vsub2(r, __vcmpltu2(r, a));  // a carry leaves r < a: add 1 to that half
+    const uint64_t s64 = (uint64_t)a + b;
+    const uint32_t s = (uint32_t)s64;
+    const uint32_t c1 = (uint32_t)(s64 >> 32);
+    const uint32_t c0 = ((s ^ a ^ b) >> 16) & 1u;
+    return s + c0 * 0xFFFF0001u + (c1 << 16);
 }
 
-// one 16-byte group = 8 consecutive DB rows of one column
-__device__ __forceinline__ void unpack8(const uint4& v, uint32_t (&x)[8]) {
-    x[0] = v.x & 0xFFFFu; x[1] = v.x >> 16; x[2] = v.y & 0xFFFFu; x[3] = v.y >> 16;
-    x[4] = v.z & 0xFFFFu; x[5] = v.z >> 16; x[6] = v.w & 0xFFFFu; x[7] = v.w >> 16;
-}
-__device__ __forceinline__ uint4 pack8(const uint32_t (&x)[8]) {
-    return make_uint4(x[0] | (x[1] << 16), x[2] | (x[3] << 16), x[4] | (x[5] << 16), x[6] | (x[7] << 16));
+// x * 2^K mod 65535 on both halves, canonical (65535 -> 0): multiplying by 2^K modulo
+// 2^16 - 1 rotates the 16 bits left by K; afterwards a half that is all ones (a zero
+// in ones'-complement form) is cleared
+template <int K>
+__device__ __forceinline__ uint32_t rotl_canon2(uint32_t w) {
+    constexpr uint32_t HI = ((0xFFFFu << K) & 0xFFFFu) * 0x10001u, LO = ((1u << K) - 1) * 0x10001u;
+    w = ((w << K) & HI) | ((w >> (16 - K)) & LO);
+    const uint32_t nw = ~w;
+    const uint32_t nz = ((nw & 0x7FFF7FFFu) + 0x7FFF7FFFu) | nw;  // bit 15 of a half: that half of nw != 0
+    const uint32_t ones = ~nz & 0x80008000u;
+    return w & ~((ones >> 15) * 0xFFFFu);
 }
 
 constexpr int E_THREADS = 256;
 
 template <int I>
 __global__ void __launch_bounds__(E_THREADS) k_encode(const uint16_t* __restrict__ in, uint16_t* __restrict__ out,
-                                                      int64_t db_rows, uint32_t inv) {
+                                                      int64_t db_rows) {
     constexpr int H = I / 2;        // chunks of S coefficients in [0, N)
     constexpr int S = 2 * N / I;    // coefficient stride between chunks
     constexpr int RG = E_ROWS / 8;  // 8-row groups per column
@@ -173,16 +183,15 @@ __global__ void __launch_bounds__(E_THREADS) k_encode(const uint16_t* __restrict
         }
         __syncthreads();
     }
-    // scale and store in natural polynomial order
+    // scale by I^-1 = 2^(16 - log2 I) mod 65535 and store in natural polynomial order
 #pragma unroll 4
     for (int i = threadIdx.x; i < GROUPS; i += E_THREADS) {
         const int rg = i % RG, q = i / RG;
         const int j = q / H, kc = q % H;
-        uint32_t x[8];
-        unpack8(*reinterpret_cast<const uint4*>(&buf[j][kc][rg * 8]), x);
-#pragma unroll
-        for (int r = 0; r < 8; r++) x[r] = fold65535(x[r] * inv);
-        *reinterpret_cast<uint4*>(out + (col0 + (int64_t)j * N + (int64_t)kc * S) * db_rows + row0 + rg * 8) = pack8(x);
+        uint4 w = *reinterpret_cast<const uint4*>(&buf[j][kc][rg * 8]);
+        w = make_uint4(rotl_canon2<16 - LOGI>(w.x), rotl_canon2<16 - LOGI>(w.y), rotl_canon2<16 - LOGI>(w.z),
+                       rotl_canon2<16 - LOGI>(w.w));
+        *reinterpret_cast<uint4*>(out + (col0 + (int64_t)j * N + (int64_t)kc * S) * db_rows + row0 + rg * 8) = w;
     }
 }
 
@@ -220,17 +229,16 @@ int encode_db_device(const uint16_t* d_raw, uint16_t* d_out, uint64_t db_rows, u
         set_last_error("encode: shape too large for one launch");
         return IPR_E_ARGS;
     }
-    const uint32_t inv = encode_num_inv(interp);
     if (interp == 1) {
         k_encode_scale1<<<148 * 8, 256, 0, st>>>(d_raw, d_out, (int64_t)(db_rows * db_cols));
     } else {
         const dim3 grid((unsigned)(db_rows / E_ROWS), (unsigned)(2 * N / interp), (unsigned)c);
         switch (interp) {
-            case 2: k_encode<2><<<grid, E_THREADS, 0, st>>>(d_raw, d_out, (int64_t)db_rows, inv); break;
-            case 4: k_encode<4><<<grid, E_THREADS, 0, st>>>(d_raw, d_out, (int64_t)db_rows, inv); break;
-            case 8: k_encode<8><<<grid, E_THREADS, 0, st>>>(d_raw, d_out, (int64_t)db_rows, inv); break;
-            case 16: k_encode<16><<<grid, E_THREADS, 0, st>>>(d_raw, d_out, (int64_t)db_rows, inv); break;
-            default: k_encode<32><<<grid, E_THREADS, 0, st>>>(d_raw, d_out, (int64_t)db_rows, inv); break;
+            case 2: k_encode<2><<<grid, E_THREADS, 0, st>>>(d_raw, d_out, (int64_t)db_rows); break;
+            case 4: k_encode<4><<<grid, E_THREADS, 0, st>>>(d_raw, d_out, (int64_t)db_rows); break;
+            case 8: k_encode<8><<<grid, E_THREADS, 0, st>>>(d_raw, d_out, (int64_t)db_rows); break;
+            case 16: k_encode<16><<<grid, E_THREADS, 0, st>>>(d_raw, d_out, (int64_t)db_rows); break;
+            default: k_encode<32><<<grid, E_THREADS, 0, st>>>(d_raw, d_out, (int64_t)db_rows); break;
         }
     }
     return cuda_status(cudaGetLastError());

@@ -453,6 +453,33 @@ uint64_t server_batch_bytes(const ipr_server* s, int B) {
     return tpp + scratch + batch;
 }
 
+int server_init(ipr_server* s, int device, const ipr_plan* plan) { return init_common(s, device, plan); }
+
+int server_finish(ipr_server* s, bool raw_db, const ipr_server_data* data) {
+    const ipr::Plan& plan = s->plan;
+    int st;
+    if (raw_db) {  // encode on the device: the byte-plane buffer has the DB's size and is free until below
+        uint16_t* tmp = reinterpret_cast<uint16_t*>(s->d_db8);
+        if ((st = ipr::encode_db_device(s->d_db, tmp, plan.db_rows, plan.db_cols, plan.interp, s->stream))) return st;
+        CU(cudaMemcpyAsync(s->d_db, tmp, plan.db_rows * plan.db_cols * 2, cudaMemcpyDeviceToDevice, s->stream));
+    }
+    CU(ipr::launch_db_to_planes(s->d_db, s->d_db8, (int64_t)(plan.db_rows * plan.db_cols), s->stream));
+    CU(cudaStreamSynchronize(s->stream));
+    s->stash_count = data->stash_count;
+    s->stash_entry = data->stash_entry_bytes;
+    if (s->stash_count) {
+        if ((st = s->alloc(&s->d_stash, s->stash_count * s->stash_entry))) return st;
+        CU(cudaMemcpy(s->d_stash, data->stash, s->stash_count * s->stash_entry, cudaMemcpyHostToDevice));
+    }
+    s->key_size = data->key_size;
+    s->value_size = data->value_size;
+    s->num_records = data->num_records;
+    std::memcpy(s->cuckoo_seed, data->cuckoo_seed, 16);
+    // response buffers depend on the stash size: rebuild scratch
+    s->cap_q = 0;
+    return ensure_scratch(s, 2);
+}
+
 }  // namespace ipr
 
 extern "C" {
@@ -590,44 +617,7 @@ static int create_server(int device, const ipr_plan* plan, const ipr_server_data
     if ((st = up(s->d_db, data->db, plan->db_rows * plan->db_cols * 2)) || (st = up(s->d_ahat, data->a_hat, no * kN * 8)) ||
         (st = up(s->d_bt, data->bold_t, no * (uint64_t)kNInner * kN * 8)) ||
         (st = up(s->d_btb, data->bold_t_bar, no * (uint64_t)kNInner * kN * 8)) ||
-        (st = up(s->d_bth, data->bold_t_hat, no * 3 * kN * 8))) {
-        ipr_server_destroy(s);
-        return st;
-    }
-    if (raw_db) {  // encode on the device: the byte-plane buffer has the DB's size and is free until below
-        uint16_t* tmp = reinterpret_cast<uint16_t*>(s->d_db8);
-        if ((st = ipr::encode_db_device(s->d_db, tmp, plan->db_rows, plan->db_cols, plan->interp, s->stream)) ||
-            (st = (cudaMemcpyAsync(s->d_db, tmp, plan->db_rows * plan->db_cols * 2, cudaMemcpyDeviceToDevice,
-                                   s->stream) == cudaSuccess
-                       ? IPR_OK
-                       : fail(IPR_E_CUDA, "encoded DB copy: %s", cudaGetErrorString(cudaGetLastError()))))) {
-            ipr_server_destroy(s);
-            return st;
-        }
-    }
-    if ((st = (ipr::launch_db_to_planes(s->d_db, s->d_db8, (int64_t)(plan->db_rows * plan->db_cols), s->stream) ==
-                       cudaSuccess && cudaStreamSynchronize(s->stream) == cudaSuccess
-                   ? IPR_OK
-                   : fail(IPR_E_CUDA, "DB byte planes: %s", cudaGetErrorString(cudaGetLastError()))))) {
-        ipr_server_destroy(s);
-        return st;
-    }
-    s->stash_count = data->stash_count;
-    s->stash_entry = data->stash_entry_bytes;
-    if (s->stash_count) {
-        if ((st = s->alloc(&s->d_stash, s->stash_count * s->stash_entry)) ||
-            (st = up(s->d_stash, data->stash, s->stash_count * s->stash_entry))) {
-            ipr_server_destroy(s);
-            return st;
-        }
-    }
-    s->key_size = data->key_size;
-    s->value_size = data->value_size;
-    s->num_records = data->num_records;
-    std::memcpy(s->cuckoo_seed, data->cuckoo_seed, 16);
-    // response buffers depend on the stash size: rebuild scratch
-    s->cap_q = 0;
-    if ((st = ensure_scratch(s, 2))) {
+        (st = up(s->d_bth, data->bold_t_hat, no * 3 * kN * 8)) || (st = ipr::server_finish(s, raw_db, data))) {
         ipr_server_destroy(s);
         return st;
     }

@@ -104,6 +104,12 @@ constexpr int kMaxBatchPayloads = 64;
 int server_ensure_batch(ipr_server* s, int payloads);
 int server_enqueue_batch(ipr_server* s, int payloads, const uint8_t* d_queries, uint8_t* d_resps);
 int server_respond_locked(ipr_server* s, const uint8_t* query, size_t len, uint8_t* out, size_t cap, size_t* out_len);
+// setup steps shared with the state-file loader: validate the plan, allocate the resident
+// state and tables (server_init); after the resident arrays hold the setup outputs, encode
+// a raw DB if asked, build the byte planes, upload the stash, set the public parameters
+// and the request scratch (server_finish)
+int server_init(ipr_server* s, int device, const ipr_plan* plan);
+int server_finish(ipr_server* s, bool raw_db, const ipr_server_data* data);
 // device bytes the batch path holds for `payloads` (slot-indexed precomputation + scratch)
 uint64_t server_batch_bytes(const ipr_server* s, int payloads);
 }  // namespace ipr
