@@ -161,6 +161,27 @@ int ipr_oracle_encode_db(const uint16_t *raw, uint16_t *out, uint64_t db_rows, u
 int ipr_synth_query(uint64_t seed, uint64_t db_rows, unsigned num_queries, uint8_t *out,
                     size_t cap, size_t *out_len);
 
+/* ---- offline precomputation (ipr_offline.c; engine.rs:677-1042, packing.rs) ---- */
+/* generate_pseudorandom_query(SEED_0) engine.rs:500-534: `polys` = db_rows/2048 NTT polys [polys][2N] */
+void ipr_oracle_hint_query(const ipr_params *p, unsigned polys, uint64_t *out);
+/* a_ct_tilde of instance `inst` (hint columns inst*2048 .. +2048): [2048][2N] NTT */
+void ipr_oracle_prep_pack(const ipr_params *p, const uint16_t *db, uint64_t db_rows, uint64_t inst,
+                          const uint64_t *query, uint64_t *a_ct);
+/* OfflinePackingKeys::init_full: w_mask, v_mask [3][2N]; w_all, w_bar_all [1023][3][2N] */
+void ipr_oracle_offline_keys(const ipr_params *p, uint64_t *w_mask, uint64_t *v_mask, uint64_t *w_all,
+                             uint64_t *w_bar_all);
+/* packing sums (brute force, CPU branch packing.rs:2627-2679): r_all, r_bar_all [1024][2N] */
+void ipr_oracle_pack_r(const ipr_params *p, const uint64_t *a_ct, uint64_t *r_all, uint64_t *r_bar_all);
+/* collapse (packing.rs:2683-2734); r_all / r_bar_all are updated in place.  a_hat [N] raw,
+ * bold_t / bold_t_bar [1023*3][N] condensed, bold_t_hat [3][N] condensed */
+void ipr_oracle_collapse(const ipr_params *p, uint64_t *r_all, uint64_t *r_bar_all, const uint64_t *w_all,
+                         const uint64_t *w_bar_all, const uint64_t *v_mask, uint64_t *a_hat, uint64_t *bold_t,
+                         uint64_t *bold_t_bar, uint64_t *bold_t_hat);
+int ipr_oracle_offline_instance(const ipr_params *p, const uint16_t *db, uint64_t db_rows, uint64_t inst,
+                                const uint64_t *query, const uint64_t *w_all, const uint64_t *w_bar_all,
+                                const uint64_t *v_mask, uint64_t *a_hat, uint64_t *bold_t, uint64_t *bold_t_bar,
+                                uint64_t *bold_t_hat);
+
 int ipr_oracle_threads(void);
 
 #ifdef __cplusplus

@@ -389,3 +389,77 @@ def encode_db(raw: np.ndarray, db_rows: int, db_cols: int, interp: int) -> np.nd
     if st:
         raise ValueError(f"oracle encode status {st}")
     return out
+
+
+# --- offline precomputation (ipr_offline.c) ---------------------------------
+_hint_query = _sig("ipr_oracle_hint_query", None, ctypes.POINTER(Params), ctypes.c_uint, _p)
+_prep_pack = _sig("ipr_oracle_prep_pack", None, ctypes.POINTER(Params), _p, _u64, _u64, _p, _p)
+_offline_keys = _sig("ipr_oracle_offline_keys", None, ctypes.POINTER(Params), _p, _p, _p, _p)
+_pack_r = _sig("ipr_oracle_pack_r", None, ctypes.POINTER(Params), _p, _p, _p)
+_collapse = _sig("ipr_oracle_collapse", None, ctypes.POINTER(Params), _p, _p, _p, _p, _p, _p, _p, _p, _p)
+
+
+def hint_query(polys: int) -> np.ndarray:
+    """generate_pseudorandom_query(SEED_0): [polys][2][N] NTT"""
+    out = np.zeros(polys * 2 * N, dtype=np.uint64)
+    _hint_query(ctypes.byref(params()), polys, _ptr(out))
+    return out.reshape(polys, 2, N)
+
+
+def prep_pack(db: np.ndarray, db_rows: int, inst: int, query: np.ndarray) -> np.ndarray:
+    """a_ct_tilde of instance `inst`: [2048][2][N] NTT"""
+    d = np.ascontiguousarray(db, dtype=np.uint16)
+    q = np.ascontiguousarray(query, dtype=np.uint64)
+    out = np.zeros(N * 2 * N, dtype=np.uint64)
+    _prep_pack(ctypes.byref(params()), _ptr(d), db_rows, inst, _ptr(q), _ptr(out))
+    return out.reshape(N, 2, N)
+
+
+def offline_keys():
+    """OfflinePackingKeys::init_full(W_SEED, V_SEED): w_mask, v_mask [3][2][N];
+    w_all, w_bar_all [1023][3][2][N]"""
+    wm = np.zeros(3 * 2 * N, dtype=np.uint64)
+    vm = np.zeros(3 * 2 * N, dtype=np.uint64)
+    wa = np.zeros(1023 * 3 * 2 * N, dtype=np.uint64)
+    wb = np.zeros(1023 * 3 * 2 * N, dtype=np.uint64)
+    _offline_keys(ctypes.byref(params()), _ptr(wm), _ptr(vm), _ptr(wa), _ptr(wb))
+    return wm.reshape(3, 2, N), vm.reshape(3, 2, N), wa.reshape(1023, 3, 2, N), wb.reshape(1023, 3, 2, N)
+
+
+def pack_r(a_ct: np.ndarray):
+    """brute-force packing sums of one instance: r_all, r_bar_all [1024][2][N]"""
+    a = np.ascontiguousarray(a_ct, dtype=np.uint64)
+    r = np.zeros(1024 * 2 * N, dtype=np.uint64)
+    rb = np.zeros(1024 * 2 * N, dtype=np.uint64)
+    _pack_r(ctypes.byref(params()), _ptr(a), _ptr(r), _ptr(rb))
+    return r.reshape(1024, 2, N), rb.reshape(1024, 2, N)
+
+
+def collapse(r_all: np.ndarray, r_bar_all: np.ndarray, w_all, w_bar_all, v_mask):
+    """1023-step collapse of one instance: a_hat [N], bold_t / bold_t_bar [3069][N] condensed,
+    bold_t_hat [3][N] condensed (r_all, r_bar_all are copied, not modified)"""
+    r = np.ascontiguousarray(r_all, dtype=np.uint64).copy()
+    rb = np.ascontiguousarray(r_bar_all, dtype=np.uint64).copy()
+    wa, wb, vm = (np.ascontiguousarray(x, dtype=np.uint64) for x in (w_all, w_bar_all, v_mask))
+    a_hat = np.zeros(N, dtype=np.uint64)
+    bt = np.zeros(NINNER * N, dtype=np.uint64)
+    btb = np.zeros(NINNER * N, dtype=np.uint64)
+    bth = np.zeros(3 * N, dtype=np.uint64)
+    _collapse(ctypes.byref(params()), _ptr(r), _ptr(rb), _ptr(wa), _ptr(wb), _ptr(vm), _ptr(a_hat), _ptr(bt),
+              _ptr(btb), _ptr(bth))
+    return a_hat, bt.reshape(NINNER, N), btb.reshape(NINNER, N), bth.reshape(3, N)
+
+
+def offline_precompute(db: np.ndarray, db_rows: int, instances: int):
+    """the whole offline precomputation for `instances` packing outputs:
+    a_hat [inst][N], bold_t / bold_t_bar [inst][3069][N], bold_t_hat [inst][3][N]"""
+    q = hint_query(db_rows // N)
+    _, vm, wa, wb = offline_keys()
+    a_hat = np.zeros((instances, N), dtype=np.uint64)
+    bt = np.zeros((instances, NINNER, N), dtype=np.uint64)
+    btb = np.zeros((instances, NINNER, N), dtype=np.uint64)
+    bth = np.zeros((instances, 3, N), dtype=np.uint64)
+    for i in range(instances):
+        r, rb = pack_r(prep_pack(db, db_rows, i, q))
+        a_hat[i], bt[i], btb[i], bth[i] = collapse(r, rb, wa, wb, vm)
+    return a_hat, bt, btb, bth
