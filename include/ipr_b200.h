@@ -110,6 +110,14 @@ int ipr_server_create(int device, const ipr_plan *plan, const ipr_server_data *d
  * (ipr_encode_db) instead of the caller running gpu_encode_db first. */
 int ipr_server_create_from_raw(int device, const ipr_plan *plan, const ipr_server_data *data, ipr_server **out);
 
+/* KeywordServer::setup on the device (keyword.rs:366-468 with the GPU branches of
+ * perform_offline_precomputation_simplepir): data->db is the DB (the RAW to_raw_db layout
+ * when db_is_raw, else already encoded); the encode and the whole offline precomputation
+ * run on `device` (ipr_encode_db, ipr_offline_precompute), so data->a_hat, bold_t,
+ * bold_t_bar and bold_t_hat are ignored (may be NULL).  Stash and public parameters as
+ * in ipr_server_create. */
+int ipr_server_setup(int device, const ipr_plan *plan, const ipr_server_data *data, int db_is_raw, ipr_server **out);
+
 /* Same, with seeded synthetic DB / precomputation generated on the device
  * (uniform u16 < 65535, uniform residues), the timing mode the reference
  * itself uses (online_only, src/pir/server/engine.rs:693-729). */
@@ -215,6 +223,20 @@ int ipr_gemv_query_noalloc(uint64_t *h_c, const uint64_t *h_a, const uint16_t *d
 int ipr_ntt_batch(int device, uint64_t *d_polys, uint64_t count, int limb, int inverse, void *stream);
 int ipr_automorph_batch(int device, const uint64_t *d_in, uint64_t count, const uint32_t *d_ks, int nk,
                         uint64_t *d_out, void *stream);
+
+/* Offline precomputation on the GPU: PirServer::perform_offline_precomputation_simplepir
+ * (src/pir/server/engine.rs:677-1042; hint, prep_pack, packing sums, automorphisms and
+ * the 1023-step collapse of full_packing_with_preprocessing_offline, packing.rs:2440-2734)
+ * for the encoded column-major DB d_db ([instances * 2048][db_rows] u16, db_rows a
+ * multiple of 2048).  Writes the arrays of ipr_server_data on the device:
+ * d_a_hat [instances][2048] u64 mod q, d_bold_t / d_bold_t_bar [instances][3069][2048]
+ * condensed, d_bold_t_hat [instances][3][2048] condensed.  Replaces the reference's
+ * gpu_hint_*, gpu_prep_pack_*, gpu_packing_* and gpu_collapse_* sequence.  Scratch is
+ * allocated inside, at most scratch_bytes (0 = 4 GiB; 64 MiB per instance processed
+ * together); the call returns when the outputs are complete. */
+int ipr_offline_precompute(int device, const uint16_t *d_db, uint64_t db_rows, uint64_t instances,
+                           uint64_t *d_a_hat, uint64_t *d_bold_t, uint64_t *d_bold_t_bar, uint64_t *d_bold_t_hat,
+                           uint64_t scratch_bytes, void *stream);
 
 /* Server state file (no reference counterpart: the reference reruns encode and the
  * offline precomputation on every start, keyword.rs:366-457).  ipr_server_save writes

@@ -21,7 +21,7 @@ __all__ = [
     "KeywordQueryPayload", "KeywordResponsePayload", "serialize_keyword_query",
     "deserialize_keyword_response", "POLY_LEN", "RESULT_BYTES", "KeywordService", "ServiceStats",
     "shard_plan", "merge_responses", "ShardedKeywordServer", "ntt_batch", "automorph_batch", "encode_db",
-    "cuckoo_to_raw_db", "state_file_plan",
+    "cuckoo_to_raw_db", "state_file_plan", "offline_precompute",
 ]
 
 POLY_LEN = 2048
@@ -104,10 +104,13 @@ _merge = _sig("ipr_response_merge", _i32, ctypes.POINTER(_u8p), ctypes.POINTER(_
               ctypes.POINTER(_sz))
 _ntt_batch = _sig("ipr_ntt_batch", _i32, _i32, _vp, _u64, _i32, _i32, _vp)
 _automorph_batch = _sig("ipr_automorph_batch", _i32, _i32, _vp, _u64, _vp, _i32, _vp, _vp)
+_setup = _sig("ipr_server_setup", _i32, _i32, ctypes.POINTER(_Plan), ctypes.POINTER(_ServerData), _i32,
+              ctypes.POINTER(_vp))
 _create_raw = _sig("ipr_server_create_from_raw", _i32, _i32, ctypes.POINTER(_Plan), ctypes.POINTER(_ServerData),
                    ctypes.POINTER(_vp))
 _encode = _sig("ipr_encode_db", _i32, _i32, _vp, _vp, _u64, _u64, _u64, _vp)
 _raw_db = _sig("ipr_cuckoo_to_raw_db", _i32, _i32, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _vp, _vp)
+_offline = _sig("ipr_offline_precompute", _i32, _i32, _vp, _u64, _u64, _vp, _vp, _vp, _vp, _u64, _vp)
 _save = _sig("ipr_server_save", _i32, _vp, ctypes.c_char_p)
 _load = _sig("ipr_server_load", _i32, _i32, ctypes.c_char_p, ctypes.POINTER(_vp))
 _state_plan = _sig("ipr_state_file_plan", _i32, ctypes.c_char_p, ctypes.POINTER(_Plan))
@@ -168,6 +171,15 @@ class Plan:
     @property
     def query_bytes(self) -> int:
         return query_bytes(self.db_rows, 2)
+
+
+def offline_precompute(d_db: int, db_rows: int, instances: int, d_a_hat: int, d_bold_t: int, d_bold_t_bar: int,
+                       d_bold_t_hat: int, scratch_bytes: int = 0, device: int = 0, stream: int = 0):
+    """ipr_offline_precompute on device pointers: the encoded DB [instances*2048][db_rows] u16
+    -> a_hat [inst][2048], bold_t / bold_t_bar [inst][3069][2048], bold_t_hat [inst][3][2048]
+    (u64; the setup outputs of perform_offline_precomputation_simplepir)"""
+    _check(_offline(device, d_db, db_rows, instances, d_a_hat, d_bold_t, d_bold_t_bar, d_bold_t_hat, scratch_bytes,
+                    stream or None), "ipr_offline_precompute")
 
 
 def state_file_plan(path: str) -> Plan:
@@ -310,6 +322,34 @@ class KeywordServer:
         pc = plan._c()
         fn, name = (_create_raw, "ipr_server_create_from_raw") if _raw else (_create, "ipr_server_create")
         _check(fn(device, ctypes.byref(pc), ctypes.byref(d), ctypes.byref(h)), name)
+        return cls(h.value, plan, device)
+
+    @classmethod
+    def setup(cls, plan: Plan, db, raw: bool = False, stash=(), key_size: int = 32,
+              value_size: Optional[int] = None, num_records: int = 0, cuckoo_seed: bytes = bytes(16),
+              device: int = 0) -> "KeywordServer":
+        """KeywordServer::setup on the GPU: from the DB alone (raw to_raw_db layout when `raw`,
+        else encoded), running the encode and the offline precomputation on the device"""
+        import numpy as np
+        d8 = np.ascontiguousarray(db, dtype=np.uint16)
+        if d8.size != plan.db_rows * plan.db_cols:
+            raise ValueError(f"db has {d8.size} elements, plan needs {plan.db_rows * plan.db_cols}")
+        stash = [bytes(s) for s in stash]
+        entry = len(stash[0]) if stash else 0
+        if any(len(s) != entry for s in stash):
+            raise ValueError("stash entries must have equal length")
+        stash_buf = np.frombuffer(b"".join(stash), dtype=np.uint8) if stash else None
+        d = _ServerData()
+        d.db = d8.ctypes.data
+        d.stash = stash_buf.ctypes.data if stash_buf is not None else None
+        d.stash_count, d.stash_entry_bytes = len(stash), entry
+        d.key_size = key_size
+        d.value_size = plan.entry_size - key_size if value_size is None else value_size
+        d.num_records = num_records
+        d.cuckoo_seed[:] = list(cuckoo_seed[:16].ljust(16, b"\0"))
+        h = _vp()
+        pc = plan._c()
+        _check(_setup(device, ctypes.byref(pc), ctypes.byref(d), 1 if raw else 0, ctypes.byref(h)), "ipr_server_setup")
         return cls(h.value, plan, device)
 
     @classmethod

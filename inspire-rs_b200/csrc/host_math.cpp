@@ -224,6 +224,57 @@ void host_params_init(HostParams& p) {
     for (int i = 0; i < 2 * kN; i++) p.row0[i] = (uint32_t)a[i];
 }
 
+namespace {
+ChaCha chacha_from_seed(const uint8_t seed[32]) {
+    ChaCha rng;
+    for (int i = 0; i < 8; i++)
+        rng.key[i] = (uint32_t)seed[4 * i] | ((uint32_t)seed[4 * i + 1] << 8) | ((uint32_t)seed[4 * i + 2] << 16) |
+                     ((uint32_t)seed[4 * i + 3] << 24);
+    return rng;
+}
+
+// PolyMatrixNTT::random_rng(params, 1, 3, ChaCha20Rng::from_seed(seed)) (poly.rs:418-440):
+// column c, limb l, coefficient j <- next_u64 % q_l
+void random_ntt_3(const HostParams& p, const uint8_t seed[32], std::vector<uint32_t>& out) {
+    ChaCha rng = chacha_from_seed(seed);
+    out.assign(3 * 2 * kN, 0);
+    for (int c = 0; c < 3; c++)
+        for (int l = 0; l < 2; l++)
+            for (int j = 0; j < kN; j++) out[(c * 2 + l) * kN + j] = (uint32_t)(rng.next_u64() % p.q[l]);
+}
+}  // namespace
+
+void offline_host_inputs(const HostParams& p, unsigned polys, std::vector<uint32_t>& query,
+                         std::vector<uint32_t>& w_mask, std::vector<uint32_t>& v_mask) {
+    // generate_pseudorandom_query(SEED_0) (engine.rs:500-534): ChaCha20Rng from get_seed(0), the
+    // all-zero seed (client/online.rs:164-168); poly r is a_r = random_rng mod q, the query keeps
+    // ct.raw() row 0 = -a_r mod q (client/base.rs:438-457), negacyclic_perm(., 0, q)
+    // (utils.rs:5-21) maps c(X) to c(X^-1): coefficient 0 stays, coefficient i >= 1 is
+    // -c[N - i] = a_r[N - i]; then to_ntt
+    uint8_t zero[32];
+    std::memset(zero, 0, sizeof(zero));
+    ChaCha rng = chacha_from_seed(zero);
+    query.assign((size_t)polys * 2 * kN, 0);
+    std::vector<uint64_t> a(kN), t(2 * kN);
+    for (unsigned r = 0; r < polys; r++) {
+        for (int i = 0; i < kN; i++) a[i] = rng.next_u64() % p.modulus;
+        for (int i = 0; i < kN; i++) {
+            const uint64_t c = i == 0 ? (a[0] ? p.modulus - a[0] : 0) : a[kN - i];
+            t[i] = c % p.q[0];
+            t[kN + i] = c % p.q[1];
+        }
+        forward_ntt_u64(p, t.data());
+        for (int i = 0; i < 2 * kN; i++) query[(size_t)r * 2 * kN + i] = (uint32_t)t[i];
+    }
+    // OfflinePackingKeys::init_full (packing.rs:1843-1870) with W_SEED / V_SEED (scheme.rs:46-51)
+    uint8_t ws[32], vs[32];
+    std::memset(ws, 7, 32);
+    std::memset(vs, 7, 32);
+    vs[0] = vs[1] = 8;
+    random_ntt_3(p, ws, w_mask);
+    random_ntt_3(p, vs, v_mask);
+}
+
 void host_moduli_constants(uint64_t barrett[2], uint32_t* q0_inv_mod_q1) {
     const uint64_t q0 = 268369921ull, q1 = 249561089ull;
     barrett[0] = (uint64_t)((((u128)1) << 64) / q0);

@@ -26,6 +26,12 @@ struct HostParams {
 
 void host_params_init(HostParams& p);
 
+// Inputs of the offline precomputation derived from fixed seeds: the hint query of
+// generate_pseudorandom_query(SEED_0) ([polys][2][N] NTT) and the W / V masks of
+// OfflinePackingKeys::init_full ([3][2][N] NTT each).
+void offline_host_inputs(const HostParams& p, unsigned polys, std::vector<uint32_t>& query,
+                         std::vector<uint32_t>& w_mask, std::vector<uint32_t>& v_mask);
+
 // Only the two reduction constants the kernels keep in constant memory
 // (floor(2^64 / q_l) and q0^-1 mod q1); computes them without touching the heap.
 void host_moduli_constants(uint64_t barrett[2], uint32_t* q0_inv_mod_q1);

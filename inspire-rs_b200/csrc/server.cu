@@ -53,6 +53,9 @@ constexpr int kMaxProfileSlots = 8192;
 namespace ipr {
 int encode_db_device(const uint16_t* d_raw, uint16_t* d_out, uint64_t db_rows, uint64_t db_cols, uint64_t interp,
                      cudaStream_t st);
+int offline_precompute_device(const uint16_t* d_db, uint64_t db_rows, uint64_t instances, uint64_t* d_a_hat,
+                              uint64_t* d_bt, uint64_t* d_btb, uint64_t* d_bth, uint64_t scratch_budget,
+                              cudaStream_t st);
 // lets other translation units of the library report through ipr_last_error()
 void set_last_error(const char* msg) { g_last_error = msg; }
 }  // namespace ipr
@@ -621,6 +624,36 @@ static int create_server(int device, const ipr_plan* plan, const ipr_server_data
         ipr_server_destroy(s);
         return st;
     }
+    *out = s;
+    return IPR_OK;
+}
+
+int ipr_server_setup(int device, const ipr_plan* plan, const ipr_server_data* data, int db_is_raw,
+                     ipr_server** out) {
+    if (!out || !data || !data->db) return fail(IPR_E_ARGS, "null argument");
+    if (data->stash_count && (!data->stash || !data->stash_entry_bytes)) return fail(IPR_E_ARGS, "bad stash");
+    *out = nullptr;
+    auto* s = new ipr_server();
+    int st = init_common(s, device, plan);
+    auto bail = [&](int code) {
+        ipr_server_destroy(s);
+        return code;
+    };
+    if (st) return bail(st);
+    const uint64_t db_bytes = plan->db_rows * plan->db_cols * 2;
+    if (cudaMemcpy(s->d_db, data->db, db_bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+        return bail(fail(IPR_E_CUDA, "DB upload: %s", cudaGetErrorString(cudaGetLastError())));
+    if (db_is_raw) {  // encode first: the precomputation reads the encoded DB
+        uint16_t* tmp = reinterpret_cast<uint16_t*>(s->d_db8);
+        if ((st = ipr::encode_db_device(s->d_db, tmp, plan->db_rows, plan->db_cols, plan->interp, s->stream)))
+            return bail(st);
+        if (cudaMemcpyAsync(s->d_db, tmp, db_bytes, cudaMemcpyDeviceToDevice, s->stream) != cudaSuccess)
+            return bail(fail(IPR_E_CUDA, "encoded DB copy: %s", cudaGetErrorString(cudaGetLastError())));
+    }
+    if ((st = ipr::offline_precompute_device(s->d_db, plan->db_rows, plan->instances, s->d_ahat, s->d_bt, s->d_btb,
+                                             s->d_bth, 0, s->stream)) ||
+        (st = ipr::server_finish(s, false, data)))
+        return bail(st);
     *out = s;
     return IPR_OK;
 }
