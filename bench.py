@@ -340,6 +340,40 @@ def micro_bench(pkg, steps, warmup):
     ms = e0.elapsed_time(e1) / steps
     lines.append({"metric": "DB encode (1M ML-KEM-768 shape: 2048 x 720896 u16, interp 32)", "value": ms,
                   "unit": "ms", "higher_is_better": False, "roofline": roofline(2 * rows * cols * 2, ms)})
+    del raw
+    # offline precomputation at the 1M shape: 352 packing instances from the encoded DB above
+    inst = cols // N
+    a_hat = torch.empty(inst * N, dtype=torch.int64, device="cuda")
+    bt = torch.empty(inst * 3069 * N, dtype=torch.int64, device="cuda")
+    btb = torch.empty_like(bt)
+    bth = torch.empty(inst * 3 * N, dtype=torch.int64, device="cuda")
+    args = (enc.data_ptr(), rows, inst, a_hat.data_ptr(), bt.data_ptr(), btb.data_ptr(), bth.data_ptr())
+    pkg.offline_precompute(*args)  # warm-up
+    reps = 3
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        pkg.offline_precompute(*args)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    # bytes that must cross HBM once: the DB read, bold_t + bold_t_bar + bold_t_hat + a_hat written
+    algo = rows * cols * 2 + (2 * 3069 + 3 + 1) * N * 8 * inst
+    line = {"metric": "offline precomputation (1M ML-KEM-768 shape: 352 instances, db_rows 2048)", "value": ms,
+            "unit": "ms", "higher_is_better": False, "roofline": roofline(algo, ms)}
+    try:  # the oracle on one instance of the same DB, scaled to 352 (reference CPU loops)
+        sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "oracle"))
+        import oracle as orc
+        db0 = enc[: N * rows].cpu().numpy().view(np.uint16).copy()
+        t0 = time.perf_counter()
+        orc.offline_precompute(db0, rows, 1)
+        cpu_s = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": cpu_s * inst * 1000.0, "unit": "ms", "cores": orc.threads(),
+                                "kind": "port", "sample": f"1 of {inst} instances ({cpu_s:.1f} s), scaled"}
+    except Exception as exc:  # the timing line stands without it
+        line["cpu_baseline"] = {"unavailable": str(exc)[:120]}
+    lines.append(line)
     for ln in lines:
         print(json.dumps(ln))
     return 0
