@@ -374,6 +374,44 @@ def micro_bench(pkg, steps, warmup):
     except Exception as exc:  # the timing line stands without it
         line["cpu_baseline"] = {"unavailable": str(exc)[:120]}
     lines.append(line)
+    del a_hat, bt, btb, bth, enc
+    # InspiRING: pack 2048 LWEs (uniform mod q, seeded) into one RLWE, packing_fully_online;
+    # one set alone (latency) and 16 sets per call (throughput)
+    rng = np.random.default_rng(2048)
+    qq = 268369921 * 249561089
+    max_sets = 16
+    lwe = torch.from_numpy(rng.integers(0, qq, (max_sets, N + 1, N), dtype=np.uint64).view(np.int64)).cuda()
+    keys = (rng.integers(0, 268369921, (2, 3, N), dtype=np.uint64)
+            | (rng.integers(0, 249561089, (2, 3, N), dtype=np.uint64) << np.uint64(32)))
+    d_y = torch.from_numpy(keys[0].view(np.int64)).cuda()
+    d_z = torch.from_numpy(keys[1].view(np.int64)).cuda()
+    out = torch.empty((max_sets, 2, N), dtype=torch.int64, device="cuda")
+    with pkg.InspiringPacker(max_sets=max_sets) as pk:
+        for sets in (1, max_sets):
+            for _ in range(max(warmup, 1)):
+                pk.pack(sets, lwe.data_ptr(), d_y.data_ptr(), d_z.data_ptr(), out.data_ptr())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(steps):
+                pk.pack(sets, lwe.data_ptr(), d_y.data_ptr(), d_z.data_ptr(), out.data_ptr())
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            line = {"metric": f"InspiRING pack: {sets} x 2048 LWEs -> {sets} RLWE (packing_fully_online)",
+                    "value": sets * 2048 / (ms / 1000.0), "unit": "LWEs packed/s", "ms_per_call": ms}
+            if sets == 1:
+                try:
+                    import oracle as orc
+                    l0 = lwe[0].cpu().numpy().view(np.uint64).copy()
+                    t0 = time.perf_counter()
+                    orc.inspiring_pack(l0, keys[0], keys[1])
+                    cpu_s = time.perf_counter() - t0
+                    line["cpu_baseline"] = {"value": 2048 / cpu_s, "unit": "LWEs packed/s", "cores": orc.threads(),
+                                            "kind": "port", "sample": f"1 set ({cpu_s:.1f} s)"}
+                except Exception as exc:
+                    line["cpu_baseline"] = {"unavailable": str(exc)[:120]}
+            lines.append(line)
     for ln in lines:
         print(json.dumps(ln))
     return 0

@@ -238,6 +238,24 @@ int ipr_offline_precompute(int device, const uint16_t *d_db, uint64_t db_rows, u
                            uint64_t *d_a_hat, uint64_t *d_bold_t, uint64_t *d_bold_t_bar, uint64_t *d_bold_t_hat,
                            uint64_t scratch_bytes, void *stream);
 
+/* InspiRING packing of LWE ciphertexts into RLWE ciphertexts on the GPU:
+ * packing_fully_online (src/pir/packing.rs:3122-3162) for sets of 2048 LWEs each —
+ * the offline precomputation of full_packing_with_preprocessing_offline on the
+ * sets' a-vectors (as in ipr_offline_precompute) followed by
+ * full_packing_with_preprocessing_online (packing.rs:2941-3021) with the packing
+ * keys.  d_lwe [sets][2049][2048] u64: row j < 2048 holds coefficient j of the
+ * 2048 a-vectors (LWE i in column i), row 2048 the b values; d_y_body / d_z_body:
+ * the packing keys' y_body / z_body, condensed [3][2048] (lo32 = mod q0, hi32 =
+ * mod q1).  d_out [sets][2][2048] u64: row 0 = a_hat mod q, row 1 = b + the packed
+ * sum mod q (not reduced, < 2q, as add_raw leaves it).  The context holds the
+ * tables, the W / V masks and scratch for up to max_sets sets (about 150 MB each);
+ * calls on one context must not overlap on the GPU. */
+typedef struct ipr_inspiring ipr_inspiring;
+int ipr_inspiring_create(int device, int max_sets, ipr_inspiring **out);
+int ipr_inspiring_pack(ipr_inspiring *ctx, int sets, const uint64_t *d_lwe, const uint64_t *d_y_body,
+                       const uint64_t *d_z_body, uint64_t *d_out, void *stream);
+void ipr_inspiring_destroy(ipr_inspiring *ctx);
+
 /* Server state file (no reference counterpart: the reference reruns encode and the
  * offline precomputation on every start, keyword.rs:366-457).  ipr_server_save writes
  * the setup outputs the server was built from (the arrays of ipr_server_data: encoded

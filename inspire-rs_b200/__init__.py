@@ -21,7 +21,7 @@ __all__ = [
     "KeywordQueryPayload", "KeywordResponsePayload", "serialize_keyword_query",
     "deserialize_keyword_response", "POLY_LEN", "RESULT_BYTES", "KeywordService", "ServiceStats",
     "shard_plan", "merge_responses", "ShardedKeywordServer", "ntt_batch", "automorph_batch", "encode_db",
-    "cuckoo_to_raw_db", "state_file_plan", "offline_precompute",
+    "cuckoo_to_raw_db", "state_file_plan", "offline_precompute", "InspiringPacker",
 ]
 
 POLY_LEN = 2048
@@ -111,6 +111,9 @@ _create_raw = _sig("ipr_server_create_from_raw", _i32, _i32, ctypes.POINTER(_Pla
 _encode = _sig("ipr_encode_db", _i32, _i32, _vp, _vp, _u64, _u64, _u64, _vp)
 _raw_db = _sig("ipr_cuckoo_to_raw_db", _i32, _i32, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _vp, _vp)
 _offline = _sig("ipr_offline_precompute", _i32, _i32, _vp, _u64, _u64, _vp, _vp, _vp, _vp, _u64, _vp)
+_insp_create = _sig("ipr_inspiring_create", _i32, _i32, _i32, ctypes.POINTER(_vp))
+_insp_pack = _sig("ipr_inspiring_pack", _i32, _vp, _i32, _vp, _vp, _vp, _vp, _vp)
+_insp_destroy = _sig("ipr_inspiring_destroy", None, _vp)
 _save = _sig("ipr_server_save", _i32, _vp, ctypes.c_char_p)
 _load = _sig("ipr_server_load", _i32, _i32, ctypes.c_char_p, ctypes.POINTER(_vp))
 _state_plan = _sig("ipr_state_file_plan", _i32, ctypes.c_char_p, ctypes.POINTER(_Plan))
@@ -180,6 +183,36 @@ def offline_precompute(d_db: int, db_rows: int, instances: int, d_a_hat: int, d_
     (u64; the setup outputs of perform_offline_precomputation_simplepir)"""
     _check(_offline(device, d_db, db_rows, instances, d_a_hat, d_bold_t, d_bold_t_bar, d_bold_t_hat, scratch_bytes,
                     stream or None), "ipr_offline_precompute")
+
+
+class InspiringPacker:
+    """packing_fully_online on the GPU (ipr_inspiring_*): packs sets of 2048 LWE ciphertexts
+    (device arrays [sets][2049][2048] u64) into RLWE ciphertexts [sets][2][2048]"""
+
+    def __init__(self, max_sets: int = 1, device: int = 0):
+        h = _vp()
+        _check(_insp_create(device, max_sets, ctypes.byref(h)), "ipr_inspiring_create")
+        self._h, self.max_sets, self.device = h, max_sets, device
+
+    def pack(self, sets: int, d_lwe: int, d_y_body: int, d_z_body: int, d_out: int, stream: int = 0):
+        _check(_insp_pack(self._h, sets, d_lwe, d_y_body, d_z_body, d_out, stream or None), "ipr_inspiring_pack")
+
+    def close(self):
+        if self._h and self._h.value:
+            _insp_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def state_file_plan(path: str) -> Plan:

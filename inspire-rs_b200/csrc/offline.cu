@@ -34,6 +34,7 @@
 #include "host_math.hpp"
 #include "ipr_b200.h"
 #include "ipr_device.cuh"
+#include "kernels.cuh"
 #include "ntt_regs.cuh"
 
 namespace ipr {
@@ -301,6 +302,51 @@ __global__ void __launch_bounds__(512, 1)
     for (int e = threadIdx.x; e < N; e += 512) a_hat[(inst0 + I) * N + e] = sm.x[e];
 }
 
+// act[l][c][i][s] = NTT_l(negacyclic_perm(a-vector of LWE i of set c)) (prep_pack_lwes,
+// packing.rs:1032-1062) for LWE matrices lwe[c][N + 1][N] (row j = coefficient j of the 2048
+// a-vectors, row N = the b values).  negacyclic_perm keeps coefficient 0 and puts
+// q - a[N - k] at k >= 1; modulo q_l (q = 0 mod q_l) that is -a[N - k].
+__global__ void __launch_bounds__(512, 1)
+    k_lwe_prep(const uint64_t* __restrict__ lwe, int64_t sets, const uint32_t* __restrict__ fw,
+               const uint32_t* __restrict__ fwp, uint32_t* __restrict__ act) {
+    extern __shared__ uint32_t lsm[];  // [2 groups][HCOLS][N]
+    const int g = threadIdx.x >> 8, t = threadIdx.x & 255;
+    const uint32_t q = limb_q(g);
+    const uint64_t br = limb_br(g);
+    const int i0 = blockIdx.x * HCOLS;
+    const int64_t c = blockIdx.y;
+    const uint64_t* L = lwe + c * (int64_t)(N + 1) * N;
+    uint32_t v[HCOLS][EPT];
+#pragma unroll
+    for (int m = 0; m < EPT; m++) {
+        const int k = eA(t, m);
+        const uint64_t* row = L + (int64_t)(k ? N - k : 0) * N + i0;
+#pragma unroll
+        for (int p = 0; p < HCOLS; p++) {
+            const uint32_t x = mod64(__ldg(row + p), q, br);
+            v[p][m] = (k == 0 || x == 0) ? x : q - x;
+        }
+    }
+    nttr::forward<HCOLS>(v, t, lsm + g * HCOLS * N, 1 + g, fw + g * N, fwp + g * N, q);  // layout D, canonical
+#pragma unroll
+    for (int p = 0; p < HCOLS; p++) {
+        uint4* dst = reinterpret_cast<uint4*>(act + (((int64_t)g * sets + c) * N + i0 + p) * N + eD(t, 0));
+        dst[0] = make_uint4(v[p][0], v[p][1], v[p][2], v[p][3]);
+        dst[1] = make_uint4(v[p][4], v[p][5], v[p][6], v[p][7]);
+    }
+}
+
+// packed RLWE of set c: row 0 = a_hat, row 1 = b + raw(sum), the sum not reduced (add_raw,
+// packing.rs:3011-3016)
+__global__ void k_inspiring_out(const uint64_t* __restrict__ a_hat, const uint64_t* __restrict__ R,
+                                const uint64_t* __restrict__ lwe, int64_t sets, uint64_t* __restrict__ out) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < sets * N; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = e / N, k = e % N;
+        out[c * 2 * N + k] = a_hat[e];
+        out[c * 2 * N + N + k] = lwe[(c * (N + 1) + N) * N + k] + R[e];
+    }
+}
+
 int cuda_fail(cudaError_t e, const char* what) {
     static thread_local char buf[256];
     snprintf(buf, sizeof(buf), "offline precomputation: %s: %s", what, cudaGetErrorString(e));
@@ -400,3 +446,106 @@ extern "C" int ipr_offline_precompute(int device, const uint16_t* d_db, uint64_t
     return ipr::offline_precompute_device(d_db, db_rows, instances, d_a_hat, d_bold_t, d_bold_t_bar, d_bold_t_hat,
                                           scratch_bytes, static_cast<cudaStream_t>(stream));
 }
+
+// ---------------------------------------------------------------------------
+// InspiRING packing of LWE sets (packing_fully_online, packing.rs:3122-3162): the offline
+// kernels above on the sets' own a-vectors, then the online packing sum and INTT of the
+// respond() path (k_pack, k_intt_crt) with the caller's packing keys.
+// ---------------------------------------------------------------------------
+struct ipr_inspiring {
+    int device = 0;
+    int max_sets = 0;
+    std::vector<void*> allocs;
+    uint32_t *fw = nullptr, *fwp = nullptr, *iw = nullptr, *iwp = nullptr, *wm = nullptr, *vm = nullptr;
+    uint32_t *act = nullptr, *E = nullptr, *r0 = nullptr, *S = nullptr;
+    uint64_t *xb = nullptr, *a_hat = nullptr, *bt = nullptr, *btb = nullptr, *bth = nullptr, *R = nullptr;
+    template <typename T>
+    cudaError_t alloc(T** p, size_t bytes) {
+        void* v = nullptr;
+        cudaError_t e = cudaMalloc(&v, bytes);
+        if (e == cudaSuccess) allocs.push_back(v), *p = static_cast<T*>(v);
+        return e;
+    }
+};
+
+extern "C" {
+
+void ipr_inspiring_destroy(ipr_inspiring* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    for (void* p : ctx->allocs) cudaFree(p);
+    delete ctx;
+}
+
+int ipr_inspiring_create(int device, int max_sets, ipr_inspiring** out) {
+    if (!out || max_sets < 1 || max_sets > 1024) {
+        ipr::set_last_error("ipr_inspiring_create: max_sets must be in [1, 1024]");
+        return IPR_E_ARGS;
+    }
+    *out = nullptr;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return ipr::cuda_fail(e, "set device");
+    auto* c = new ipr_inspiring();
+    c->device = device;
+    c->max_sets = max_sets;
+    ipr::HostParams hp;
+    ipr::host_params_init(hp);
+    std::vector<uint32_t> query, wmask, vmask;
+    ipr::offline_host_inputs(hp, 1, query, wmask, vmask);
+    const size_t tb = 2 * ipr::N * 4, ms = (size_t)max_sets, NN = (size_t)ipr::N * ipr::N;
+    if ((e = c->alloc(&c->fw, tb)) || (e = c->alloc(&c->fwp, tb)) || (e = c->alloc(&c->iw, tb)) ||
+        (e = c->alloc(&c->iwp, tb)) || (e = c->alloc(&c->wm, wmask.size() * 4)) ||
+        (e = c->alloc(&c->vm, vmask.size() * 4)) || (e = c->alloc(&c->act, ms * 2 * NN * 4)) ||
+        (e = c->alloc(&c->E, ms * 2 * NN * 4)) || (e = c->alloc(&c->r0, ms * 2 * ipr::N * 4)) ||
+        (e = c->alloc(&c->xb, ms * ipr::N * 8)) || (e = c->alloc(&c->a_hat, ms * ipr::N * 8)) ||
+        (e = c->alloc(&c->bt, ms * ipr::NINNER * ipr::N * 8)) || (e = c->alloc(&c->btb, ms * ipr::NINNER * ipr::N * 8)) ||
+        (e = c->alloc(&c->bth, ms * 3 * ipr::N * 8)) || (e = c->alloc(&c->S, ms * 2 * ipr::N * 4)) ||
+        (e = c->alloc(&c->R, ms * ipr::N * 8)) ||
+        (e = cudaMemcpy(c->fw, hp.fw.data(), tb, cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(c->fwp, hp.fwp.data(), tb, cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(c->iw, hp.iw.data(), tb, cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(c->iwp, hp.iwp.data(), tb, cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(c->wm, wmask.data(), wmask.size() * 4, cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(c->vm, vmask.data(), vmask.size() * 4, cudaMemcpyHostToDevice)) ||
+        (e = ipr::init_device_kernels()) || (e = ipr::set_constants(hp.barrett, hp.q0_inv_mod_q1)) ||
+        (e = cudaFuncSetAttribute(ipr::k_lwe_prep, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * ipr::HCOLS * ipr::N * 4)) ||
+        (e = cudaFuncSetAttribute(ipr::k_off_gather, cudaFuncAttributeMaxDynamicSharedMemorySize, ipr::N * ipr::GZ * 4)) ||
+        (e = cudaFuncSetAttribute(ipr::k_off_collapse, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sizeof(ipr::CollapseSmem))) ||
+        (e = cudaFuncSetAttribute(ipr::k_off_finish, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sizeof(ipr::CollapseSmem)))) {
+        ipr_inspiring_destroy(c);
+        return ipr::cuda_fail(e, "ipr_inspiring_create");
+    }
+    *out = c;
+    return IPR_OK;
+}
+
+int ipr_inspiring_pack(ipr_inspiring* c, int sets, const uint64_t* d_lwe, const uint64_t* d_y_body,
+                       const uint64_t* d_z_body, uint64_t* d_out, void* stream) {
+    if (!c || !d_lwe || !d_y_body || !d_z_body || !d_out || sets < 1 || sets > c->max_sets) {
+        ipr::set_last_error("ipr_inspiring_pack: null argument or sets outside [1, max_sets]");
+        return IPR_E_ARGS;
+    }
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return ipr::cuda_fail(e, "set device");
+    using namespace ipr;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int coll_smem = (int)sizeof(CollapseSmem);
+    k_lwe_prep<<<dim3(N / HCOLS, (unsigned)sets), 512, 2 * HCOLS * N * 4, st>>>(d_lwe, sets, c->fw, c->fwp, c->act);
+    k_off_jntt<<<dim3(N / JS, (unsigned)sets, 2), 256, 0, st>>>(c->act, sets, c->fw, c->fwp, c->E);
+    k_off_gather<<<dim3(N / GZ, (unsigned)sets, 2), 256, N * GZ * 4, st>>>(c->E, sets, c->act);
+    k_off_collapse<<<dim3((unsigned)sets, 2), 512, coll_smem, st>>>(c->act, 0, c->wm, c->fw, c->fwp, c->iw, c->iwp,
+                                                                   c->bt, c->btb, c->r0, c->xb);
+    k_off_finish<<<(unsigned)sets, 512, coll_smem, st>>>(c->r0, c->xb, 0, c->vm, c->fw, c->fwp, c->iw, c->iwp, c->bth,
+                                                         c->a_hat);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "offline kernels");
+    if ((e = launch_pack(c->bt, c->btb, c->bth, d_y_body, d_z_body, c->S, sets, st)) != cudaSuccess ||
+        (e = launch_intt_crt(c->S, c->iw, c->iwp, c->R, sets, st)) != cudaSuccess)
+        return cuda_fail(e, "online kernels");
+    k_inspiring_out<<<148, 256, 0, st>>>(c->a_hat, c->R, d_lwe, sets, d_out);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "output");
+    return IPR_OK;
+}
+
+}  // extern "C"

@@ -62,31 +62,59 @@ __device__ __forceinline__ uint32_t pow5(uint32_t i) {  // 5^i mod 2N
 
 }  // namespace
 
-// Tpp rows ((z*2 + l)*mt_count + mt)*128 + b*32 + jl, columns k*N + s (zeroed beforehand)
-__global__ void k_relayout_tpp(const uint64_t* __restrict__ bt, const uint64_t* __restrict__ btb, uint8_t* __restrict__ tpp,
-                               int instances, int mt_count) {
-    const int64_t total = (int64_t)instances * 2 * NINNER * N;
-    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-         idx += (int64_t)gridDim.x * blockDim.x) {
-        const int z = (int)(idx & (N - 1));
-        int64_t rest = idx >> LOGN;
-        const int rr = (int)(rest % NINNER);
-        rest /= NINNER;
-        const int kind = (int)(rest & 1);
-        const int j = (int)(rest >> 1);
-        const int i = rr / T_EXP, k = rr % T_EXP;
-        const uint32_t g = pow5((uint32_t)i);
-        const uint32_t s = auto_src(kind ? 2 * N - g : g, (uint32_t)z);
-        const uint64_t v = (kind ? btb : bt)[((int64_t)j * NINNER + rr) * N + z];
-        const int mt = j >> 5, jl = j & 31;
+// discrete logarithm base 5 of the odd residues mod 2N: entry (t - 1) / 2 = i for t = 5^i,
+// i | 0x400 for t = 2N - 5^i (i < N / 2; the two cosets cover every odd t)
+__device__ uint16_t g_dlog5[N];
+
+__global__ void k_init_dlog5() {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N / 2) return;
+    const uint32_t g = pow5((uint32_t)i);
+    g_dlog5[(g - 1) / 2] = (uint16_t)i;
+    g_dlog5[(2 * N - g - 1) / 2] = (uint16_t)(i | 0x400);
+}
+
+// Tpp rows ((z*2 + l)*mt_count + mt)*128 + b*32 + jl, columns k*N + s.  Entry (row, k*N + s)
+// is byte b of limb l of (kind ? bold_t_bar : bold_t)[j = mt*32 + jl][i*3 + k][z] where
+// x -> x^t with t = 5^i (kind 0) or 2N - 5^i (kind 1) carries slot z to slot s, i.e.
+// t = exponent(s) / exponent(z) mod 2N; i = 1023 (no such row) and j >= instances give 0.
+// One CTA assembles a 256-row x 256-column byte tile (rows (l, b, jl), slots s0 .. s0 + 255)
+// of one (z, mt, k) in shared memory and writes it as contiguous row segments; its reads
+// are single 8-byte words of the precomputation.  grid (N / 256, N, mt_count * 3)
+__global__ void __launch_bounds__(256)
+    k_relayout_tpp(const uint64_t* __restrict__ bt, const uint64_t* __restrict__ btb, uint8_t* __restrict__ tpp,
+                   int instances, int mt_count) {
+    extern __shared__ __align__(16) uint8_t rtile[];  // [256 rows][256 bytes]
+    const int s0 = blockIdx.x * 256, z = blockIdx.y, mt = blockIdx.z / T_EXP, k = blockIdx.z % T_EXP;
+    const int t = threadIdx.x, s = s0 + t;
+    // exponent(z)^-1 mod 2N by Newton's iteration (x * x = 1 mod 8 for odd x)
+    const uint32_t ez = exponent_of_slot((uint32_t)z);
+    uint32_t iz = ez;
+#pragma unroll
+    for (int it = 0; it < 3; it++) iz = (iz * (2u - ez * iz)) & (2 * N - 1);
+    const uint32_t tt = (exponent_of_slot((uint32_t)s) * iz) & (2 * N - 1);
+    const uint32_t dl = g_dlog5[(tt - 1) / 2];
+    const int i = (int)(dl & 0x3FF);
+    const uint64_t* src = (dl & 0x400) ? btb : bt;
+    const bool row_ok = i < NROT;
+#pragma unroll 8
+    for (int jl = 0; jl < 32; jl++) {
+        const int j = mt * 32 + jl;
+        const uint64_t v = (row_ok && j < instances) ? __ldg(src + ((int64_t)j * NINNER + i * T_EXP + k) * N + z) : 0;
 #pragma unroll
         for (int l = 0; l < 2; l++) {
             const uint32_t limb = (uint32_t)(l ? (v >> 32) : v);
-            const int64_t row0 = (((int64_t)z * 2 + l) * mt_count + mt) * P_TILE_M + jl;
 #pragma unroll
-            for (int b = 0; b < 4; b++)
-                tpp[(row0 + b * 32) * P_K + k * N + s] = (uint8_t)(limb >> (8 * b));
+            for (int b = 0; b < 4; b++) rtile[(l * P_TILE_M + b * 32 + jl) * 256 + t] = (uint8_t)(limb >> (8 * b));
         }
+    }
+    __syncthreads();
+    for (int c = t; c < 256 * 16; c += 256) {
+        const int r = c >> 4, seg = c & 15;
+        const int l = r / P_TILE_M, rb = r % P_TILE_M;  // rb = b*32 + jl
+        const int64_t row = (((int64_t)z * 2 + l) * mt_count + mt) * P_TILE_M + rb;
+        *reinterpret_cast<uint4*>(tpp + row * P_K + k * N + s0 + seg * 16) =
+            *reinterpret_cast<const uint4*>(rtile + r * 256 + seg * 16);
     }
 }
 
@@ -600,9 +628,11 @@ uint64_t tpp_bytes(int instances) {
 
 cudaError_t launch_relayout_tpp(const uint64_t* bt, const uint64_t* btb, uint8_t* tpp, int instances,
                                 cudaStream_t st) {
-    cudaError_t e = cudaMemsetAsync(tpp, 0, tpp_bytes(instances), st);
+    const int mt_count = (instances + 31) / 32;
+    cudaError_t e = cudaFuncSetAttribute(k_relayout_tpp, cudaFuncAttributeMaxDynamicSharedMemorySize, 256 * 256);
     if (e != cudaSuccess) return e;
-    k_relayout_tpp<<<148 * 16, 256, 0, st>>>(bt, btb, tpp, instances, (instances + 31) / 32);
+    k_init_dlog5<<<N / 2 / 256, 256, 0, st>>>();
+    k_relayout_tpp<<<dim3(N / 256, N, mt_count * T_EXP), 256, 256 * 256, st>>>(bt, btb, tpp, instances, mt_count);
     return cudaGetLastError();
 }
 

@@ -100,6 +100,18 @@ void ipr_oracle_prep_pack(const ipr_params *p, const uint16_t *db, uint64_t db_r
     }
 }
 
+void ipr_oracle_prep_pack_lwes(const ipr_params *p, const uint64_t *lwe, uint64_t *a_ct) {
+    /* prep_pack_lwes (packing.rs:1032-1062): LWE i's a-vector is column i of rows 0..N-1
+     * (row N holds the b values, skipped); to negacyclic order, then to NTT */
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < IPR_N; i++) {
+        uint64_t poly[IPR_N], perm[IPR_N];
+        for (int j = 0; j < IPR_N; j++) poly[j] = lwe[(size_t)j * IPR_N + (size_t)i];
+        negacyclic_perm0(poly, p->modulus, perm);
+        ipr_to_ntt(p, perm, a_ct + (size_t)i * 2 * IPR_N);
+    }
+}
+
 /* PolyMatrixNTT::random_rng(params, 1, 3, ChaCha20Rng::from_seed(seed)) (poly.rs:418-440):
  * column c, limb l, coefficient j <- next_u64 % q_l */
 static void random_ntt_3(const ipr_params *p, const uint8_t seed[32], uint64_t *out) {

@@ -167,6 +167,9 @@ void ipr_oracle_hint_query(const ipr_params *p, unsigned polys, uint64_t *out);
 /* a_ct_tilde of instance `inst` (hint columns inst*2048 .. +2048): [2048][2N] NTT */
 void ipr_oracle_prep_pack(const ipr_params *p, const uint16_t *db, uint64_t db_rows, uint64_t inst,
                           const uint64_t *query, uint64_t *a_ct);
+/* prep_pack_lwes (packing.rs:1032-1062): lwe [N+1][N] (row j = coefficient j of the 2048
+ * LWE a-vectors, row N = the b values) -> a_ct [N][2N] NTT */
+void ipr_oracle_prep_pack_lwes(const ipr_params *p, const uint64_t *lwe, uint64_t *a_ct);
 /* OfflinePackingKeys::init_full: w_mask, v_mask [3][2N]; w_all, w_bar_all [1023][3][2N] */
 void ipr_oracle_offline_keys(const ipr_params *p, uint64_t *w_mask, uint64_t *v_mask, uint64_t *w_all,
                              uint64_t *w_bar_all);

@@ -463,3 +463,35 @@ def offline_precompute(db: np.ndarray, db_rows: int, instances: int):
         r, rb = pack_r(prep_pack(db, db_rows, i, q))
         a_hat[i], bt[i], btb[i], bth[i] = collapse(r, rb, wa, wb, vm)
     return a_hat, bt, btb, bth
+
+
+_prep_pack_lwes = _sig("ipr_oracle_prep_pack_lwes", None, ctypes.POINTER(Params), _p, _p)
+
+
+def prep_pack_lwes(lwe: np.ndarray) -> np.ndarray:
+    """prep_pack_lwes: lwe [N+1][N] (rows = a-vector coefficients, last row = b) -> a_ct [N][2][N]"""
+    l = np.ascontiguousarray(lwe, dtype=np.uint64)
+    assert l.size == (N + 1) * N
+    out = np.zeros(N * 2 * N, dtype=np.uint64)
+    _prep_pack_lwes(ctypes.byref(params()), _ptr(l), _ptr(out))
+    return out.reshape(N, 2, N)
+
+
+def inspiring_pack(lwe: np.ndarray, y_body: np.ndarray, z_body: np.ndarray) -> np.ndarray:
+    """packing_fully_online (packing.rs:3122-3162) for 2048 LWEs: the offline precomputation of
+    full_packing_with_preprocessing_offline (r / r_bar sums, 1023-step collapse) on their
+    a-vectors, then full_packing_with_preprocessing_online (packing.rs:2941-3021) with the
+    packing keys (y_body, z_body condensed [3][N]) and the b row -> RLWE [2][N] raw
+    (row 1 = b + sum, not reduced)"""
+    lwe = np.ascontiguousarray(lwe, dtype=np.uint64).reshape(N + 1, N)
+    r, rb = pack_r(prep_pack_lwes(lwe))
+    _, vm, wa, wb = offline_keys()
+    a_hat, bt, btb, bth = collapse(r, rb, wa, wb, vm)
+    sdb = SynthDB.__new__(SynthDB)
+    sdb.db_rows, sdb.instances, sdb.interp, sdb.c, sdb.seed, sdb.db_cols = N, 1, 1, 1, 0, N
+    sdb.db = np.zeros(N * N, dtype=np.uint16)
+    sdb.a_hat, sdb.bold_t, sdb.bold_t_bar, sdb.bold_t_hat = (np.ascontiguousarray(x).reshape(-1)
+                                                               for x in (a_hat, bt, btb, bth))
+    sdb.stash, sdb._stash_buf = [], np.zeros(1, dtype=np.uint8)
+    S = packing_sum(sdb, y_body, z_body)
+    return postprocess(sdb, S, lwe[N])[0]

@@ -224,3 +224,37 @@ def test_reference_offline_kernels_match_oracle(orc):
     for name, w, g in zip(("a_hat", "bold_t", "bold_t_bar", "bold_t_hat"), want,
                           (a_hat, bt.reshape(3069, N), btb.reshape(3069, N), bth.reshape(3, N))):
         assert np.array_equal(w, g), name
+
+
+def _random_condensed(rng, rows):
+    lo = rng.integers(0, orc_q()[0], (rows, N), dtype=np.uint64)
+    hi = rng.integers(0, orc_q()[1], (rows, N), dtype=np.uint64)
+    return lo | (hi << np.uint64(32))
+
+
+def orc_q():
+    return 268369921, 249561089
+
+
+@pytest.mark.gpu
+def test_inspiring_pack_matches_oracle(pkg, orc):
+    """packing_fully_online for two sets of 2048 LWEs (uniform mod q, seeded) with random keys"""
+    import torch
+    rng = np.random.default_rng(31)
+    sets = 2
+    lwe = rng.integers(0, orc.Q, (sets, N + 1, N), dtype=np.uint64)
+    y = _random_condensed(rng, 3)
+    z = _random_condensed(rng, 3)
+    want = [orc.inspiring_pack(lwe[c], y, z) for c in range(sets)]
+    d_lwe = torch.from_numpy(lwe.view(np.int64)).cuda()
+    d_y = torch.from_numpy(y.view(np.int64)).cuda()
+    d_z = torch.from_numpy(z.view(np.int64)).cuda()
+    d_out = torch.zeros((sets, 2, N), dtype=torch.int64, device="cuda")
+    with pkg.InspiringPacker(max_sets=sets) as pk:
+        for n in (sets, 1):  # both sets together, then the first alone
+            d_out.zero_()
+            pk.pack(n, d_lwe.data_ptr(), d_y.data_ptr(), d_z.data_ptr(), d_out.data_ptr())
+            torch.cuda.synchronize()
+            got = d_out.cpu().numpy().view(np.uint64)
+            for c in range(n):
+                assert np.array_equal(got[c], want[c]), (n, c)
