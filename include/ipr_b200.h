@@ -189,6 +189,10 @@ int ipr_server_set_profiling(ipr_server *srv, int on);
  * 2 (default) = pairs from 48 payloads per batch up, where they are faster.
  * Identical results. */
 #define IPR_OPT_PACK_CTA_PAIR 3
+/* IPR_OPT_GEMV_TILE: cap on the first-dimension GEMM's query-byte tile height
+ * (N of each MMA: 16, 32, 64, 128 or 256; 0 = 256, the default).  Up to 128 the
+ * two accumulators of a tile are double-buffered in TMEM. */
+#define IPR_OPT_GEMV_TILE 4
 int ipr_server_set_option(ipr_server *srv, int option, int64_t value);
 int ipr_server_stage_times(ipr_server *srv, double *ms_sum, uint64_t *calls);
 

@@ -77,6 +77,13 @@ unsigned qb_rows(unsigned nq) {
     return (8 * nq + nt - 1) / nt * nt;
 }
 
+// the GEMM's tile height: the query-byte tile, capped by the server option where the cap
+// divides it (then it also divides qb_rows)
+int g1_nt(const ipr_server* s, unsigned nq) {
+    const int nt = qb_tile(nq);
+    return s->g1_tile && s->g1_tile < nt && nt % s->g1_tile == 0 ? s->g1_tile : nt;
+}
+
 int qb_map(ipr_server* s, int nt, const CUtensorMap** out) {
     auto it = s->tm_qb.find(nt);
     if (it == s->tm_qb.end()) {
@@ -128,7 +135,7 @@ int enqueue(ipr_server* s, unsigned nq, const uint8_t* d_query, uint8_t* d_resp,
                                    s->gemv_tc ? s->d_qb : nullptr, 0, st));
         rec(1);
         if (s->gemv_tc) {
-            const int nt = qb_tile(nq);
+            const int nt = g1_nt(s, nq);
             const CUtensorMap* tq;
             int e = qb_map(s, nt, &tq);
             if (e) return e;
@@ -259,7 +266,7 @@ int enqueue_batch(ipr_server* s, int B, const uint8_t* d_queries, uint8_t* d_res
     CU(ipr::launch_parse_batch(d_queries, B, qb, 2, (int)p.db_rows, s->d_ybs, s->d_zbs, s->d_gsw, s->d_qb, st));
     rec(1);
     {
-        const int nt = qb_tile((unsigned)nqt);
+        const int nt = g1_nt(s, (unsigned)nqt);
         const CUtensorMap* tq;
         int e = qb_map(s, nt, &tq);
         if (e) return e;
@@ -869,6 +876,12 @@ int ipr_server_set_option(ipr_server* s, int option, int64_t value) {
         case IPR_OPT_PACK_CTA_PAIR:
             if (value < 0 || value > 2) return fail(IPR_E_ARGS, "IPR_OPT_PACK_CTA_PAIR takes 0, 1 or 2");
             s->pack_pair = (int)value;
+            return IPR_OK;
+        case IPR_OPT_GEMV_TILE:
+            if (value && (value < 16 || value > 256 || (256 % value)))
+                return fail(IPR_E_ARGS, "IPR_OPT_GEMV_TILE takes 0 or a divisor of 256 from 16 up");
+            s->g1_tile = (int)value;
+            destroy_graphs(s);
             return IPR_OK;
         default:
             return fail(IPR_E_ARGS, "unknown option %d", option);

@@ -29,6 +29,7 @@ struct ipr_server {
     bool gemv_tc = false;      // first dimension on tcgen05 (db_rows <= 32768)
     bool fold_regs = true;     // fold with register-resident NTTs (k_fold2) vs shared-memory NTTs
     int pack_pair = 2;         // batch packing GEMM on CTA pairs: 0 never, 1 always, 2 from 48 payloads up
+    int g1_tile = 0;           // first-dimension GEMM query-byte tile height cap (0 = 256)
     std::map<int, CUtensorMap> tm_qb;  // per query-byte tile height
     uint64_t *d_ahat = nullptr, *d_bt = nullptr, *d_btb = nullptr, *d_bth = nullptr;
     uint8_t* d_stash = nullptr;
