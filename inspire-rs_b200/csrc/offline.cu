@@ -203,11 +203,13 @@ __device__ __forceinline__ void to_raw(CollapseSmem& sm, uint32_t (&y)[1][EPT], 
 // one CTA per (instance, chain); chain 0 folds r_all with W rotated by 5^i into bold_t,
 // chain 1 folds r_bar_all with W rotated by -5^i into bold_t_bar.  Leaves the final
 // NTT-domain r_all[0] (chain 0) or raw(r_bar_all[0]) (chain 1) for k_off_finish.
+// With wrows non-null the W row of step i is read from wrows[chain][i][k][l][z] instead of
+// being rotated out of the mask (the reference's collapse takes w_all / w_bar_all as arrays).
 __global__ void __launch_bounds__(512, 1)
     k_off_collapse(const uint32_t* __restrict__ F, int64_t inst0, const uint32_t* __restrict__ wmask,
                    const uint32_t* __restrict__ fw, const uint32_t* __restrict__ fwp, const uint32_t* __restrict__ iw,
                    const uint32_t* __restrict__ iwp, uint64_t* __restrict__ bt, uint64_t* __restrict__ btb,
-                   uint32_t* __restrict__ r0, uint64_t* __restrict__ xbar0) {
+                   uint32_t* __restrict__ r0, uint64_t* __restrict__ xbar0, const uint32_t* __restrict__ wrows) {
     extern __shared__ __align__(16) uint8_t csm_raw[];
     CollapseSmem& sm = *reinterpret_cast<CollapseSmem*>(csm_raw);
     const int g = threadIdx.x >> 8, t = threadIdx.x & 255;
@@ -217,7 +219,9 @@ __global__ void __launch_bounds__(512, 1)
     const uint64_t br = limb_br(g);
     const uint32_t* Fc = F + (I * 2 + chain) * (int64_t)HALF * 2 * N;  // [i][l][z]
     uint32_t* out = reinterpret_cast<uint32_t*>((chain ? btb : bt) + (inst0 + I) * (int64_t)NINNER * N);
-    for (int e = threadIdx.x; e < 3 * 2 * N; e += 512) (&sm.wm[0][0][0])[e] = __ldg(wmask + e);
+    if (!wrows)
+        for (int e = threadIdx.x; e < 3 * 2 * N; e += 512) (&sm.wm[0][0][0])[e] = __ldg(wmask + e);
+    const uint32_t* wr = wrows ? wrows + (int64_t)chain * NROT * 3 * 2 * N : nullptr;
     // x = raw(r_all[1023]): r_all[1023] is never updated (packing.rs:2691)
     uint32_t y[1][EPT];
     {
@@ -246,10 +250,14 @@ __global__ void __launch_bounds__(512, 1)
         const uint32_t gi = gen_pow((uint32_t)i), ti = chain ? 2 * N - gi : gi;
 #pragma unroll
         for (int m = 0; m < EPT; m++) {
-            const uint32_t src = auto_src(ti, (uint32_t)eD(t, m));  // W rotated by t_i (apply_automorph_ntt)
+            const uint32_t z = (uint32_t)eD(t, m);
+            const uint32_t src = auto_src(ti, z);  // W rotated by t_i (apply_automorph_ntt)
             uint64_t acc = (uint64_t)f[m];
 #pragma unroll
-            for (int k = 0; k < 3; k++) acc += (uint64_t)sm.wm[k][g][src] * v[k][m];  // < 2^31 + 3 q^2
+            for (int k = 0; k < 3; k++) {
+                const uint32_t w = wr ? __ldg(wr + (((int64_t)i * 3 + k) * 2 + g) * N + z) : sm.wm[k][g][src];
+                acc += (uint64_t)w * v[k][m];  // < 2^31 + 3 q^2
+            }
             y[0][m] = mod64(acc, q, br);
         }
         if (i == 0 && chain == 0) {  // r_all[0] stays in the NTT domain for k_off_finish
@@ -347,6 +355,23 @@ __global__ void k_inspiring_out(const uint64_t* __restrict__ a_hat, const uint64
     }
 }
 
+// F[c][chain][i][l][z] (u32) from the reference's r_all / r_bar_all ([c][i][l*N + z] u64, canonical)
+__global__ void k_off_to_f(const uint64_t* __restrict__ r_all, const uint64_t* __restrict__ r_bar_all, int64_t cols,
+                           uint32_t* __restrict__ F) {
+    const int64_t n = cols * HALF * 2 * N;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = e / ((int64_t)HALF * 2 * N), rest = e % ((int64_t)HALF * 2 * N);
+        F[(c * 2 + 0) * (int64_t)HALF * 2 * N + rest] = (uint32_t)r_all[e];
+        F[(c * 2 + 1) * (int64_t)HALF * 2 * N + rest] = (uint32_t)r_bar_all[e];
+    }
+}
+
+// u64 [n] -> u32 [n] (canonical residues)
+__global__ void k_narrow(const uint64_t* __restrict__ in, int64_t n, uint32_t* __restrict__ out) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+        out[e] = (uint32_t)in[e];
+}
+
 int cuda_fail(cudaError_t e, const char* what) {
     static thread_local char buf[256];
     snprintf(buf, sizeof(buf), "offline precomputation: %s: %s", what, cudaGetErrorString(e));
@@ -355,6 +380,39 @@ int cuda_fail(cudaError_t e, const char* what) {
 }
 
 }  // namespace
+
+// The collapse of `cols` columns from the reference's r_all / r_bar_all arrays with explicit W
+// rows (wrows = [2][1023][3][2][N] u32: w_all then w_bar_all) and the V mask ([3][2][N] u32):
+// bold_t / bold_t_bar [cols][3069][N], bold_t_hat [cols][3][N] condensed, a_hat [cols][N].
+// Scratch: F (cols * 32 MB), r0 (cols * 16 KB), xb (cols * 16 KB).
+cudaError_t offline_collapse_arrays(const uint64_t* r_all, const uint64_t* r_bar_all, int64_t cols,
+                                    const uint32_t* wrows, const uint32_t* vmask, const uint32_t* tab /*fw fwp iw iwp*/,
+                                    uint32_t* F, uint32_t* r0, uint64_t* xb, uint64_t* bt, uint64_t* btb, uint64_t* bth,
+                                    uint64_t* a_hat, cudaStream_t st) {
+    const int coll_smem = (int)sizeof(CollapseSmem);
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k_off_collapse, cudaFuncAttributeMaxDynamicSharedMemorySize, coll_smem)) ||
+        (e = cudaFuncSetAttribute(k_off_finish, cudaFuncAttributeMaxDynamicSharedMemorySize, coll_smem)))
+        return e;
+    const uint32_t *fw = tab, *fwp = tab + 2 * N, *iw = tab + 4 * N, *iwp = tab + 6 * N;
+    k_off_to_f<<<148 * 8, 256, 0, st>>>(r_all, r_bar_all, cols, F);
+    k_off_collapse<<<dim3((unsigned)cols, 2), 512, coll_smem, st>>>(F, 0, nullptr, fw, fwp, iw, iwp, bt, btb, r0, xb,
+                                                                   wrows);
+    k_off_finish<<<(unsigned)cols, 512, coll_smem, st>>>(r0, xb, 0, vmask, fw, fwp, iw, iwp, bth, a_hat);
+    return cudaGetLastError();
+}
+
+// E[l][I][s][z] = N^-1 * NTT over j of act[l][I][j][s] for `inst` instances
+cudaError_t offline_jntt(const uint32_t* act, int64_t inst, const uint32_t* fw, const uint32_t* fwp, uint32_t* E,
+                         cudaStream_t st) {
+    k_off_jntt<<<dim3(N / JS, (unsigned)inst, 2), 256, 0, st>>>(act, inst, fw, fwp, E);
+    return cudaGetLastError();
+}
+
+cudaError_t narrow_u64(const uint64_t* in, int64_t n, uint32_t* out, cudaStream_t st) {
+    k_narrow<<<148 * 4, 256, 0, st>>>(in, n, out);
+    return cudaGetLastError();
+}
 
 // scratch bytes per instance: act / F (32 MB) + E (32 MB) + the chain ends (32 KB)
 constexpr uint64_t kOfflineScratchPerInstance = 2ull * 2 * N * N * 4 + 2ull * N * 4 + (uint64_t)N * 8;
@@ -421,7 +479,7 @@ int offline_precompute_device(const uint16_t* d_db, uint64_t db_rows, uint64_t i
             k_off_jntt<<<dim3(N / JS, (unsigned)c, 2), 256, 0, st>>>(d_act, c, d_fw, d_fwp, d_E);
             k_off_gather<<<dim3(N / GZ, (unsigned)c, 2), 256, gather_smem, st>>>(d_E, c, d_act);  // F reuses act
             k_off_collapse<<<dim3((unsigned)c, 2), 512, coll_smem, st>>>(d_act, (int64_t)i0, d_wm, d_fw, d_fwp, d_iw,
-                                                                       d_iwp, d_bt, d_btb, d_r0, d_xb);
+                                                                       d_iwp, d_bt, d_btb, d_r0, d_xb, nullptr);
             k_off_finish<<<(unsigned)c, 512, coll_smem, st>>>(d_r0, d_xb, (int64_t)i0, d_vm, d_fw, d_fwp, d_iw, d_iwp,
                                                               d_bth, d_a_hat);
             if ((e = cudaGetLastError()) != cudaSuccess) status = cuda_fail(e, "launch");
@@ -536,7 +594,7 @@ int ipr_inspiring_pack(ipr_inspiring* c, int sets, const uint64_t* d_lwe, const 
     k_off_jntt<<<dim3(N / JS, (unsigned)sets, 2), 256, 0, st>>>(c->act, sets, c->fw, c->fwp, c->E);
     k_off_gather<<<dim3(N / GZ, (unsigned)sets, 2), 256, N * GZ * 4, st>>>(c->E, sets, c->act);
     k_off_collapse<<<dim3((unsigned)sets, 2), 512, coll_smem, st>>>(c->act, 0, c->wm, c->fw, c->fwp, c->iw, c->iwp,
-                                                                   c->bt, c->btb, c->r0, c->xb);
+                                                                   c->bt, c->btb, c->r0, c->xb, nullptr);
     k_off_finish<<<(unsigned)sets, 512, coll_smem, st>>>(c->r0, c->xb, 0, c->vm, c->fw, c->fwp, c->iw, c->iwp, c->bth,
                                                          c->a_hat);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "offline kernels");
