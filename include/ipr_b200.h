@@ -278,6 +278,12 @@ int ipr_server_save(ipr_server *srv, const char *path);
 int ipr_server_load(int device, const char *path, ipr_server **out);
 int ipr_state_file_plan(const char *path, ipr_plan *out);
 
+/* Failure detection self-test: launches one CTA that waits, with the bounded wait every
+ * tensor-core kernel of this library uses on its mbarriers, on a barrier nothing arrives
+ * on.  The wait gives up after `budget` polls; the call returns IPR_E_TIMEOUT (the status a
+ * server call returns when one of its kernels' waits runs out) and the device stays usable. */
+int ipr_selftest_bounded_wait(int device, uint32_t budget);
+
 /* Setup-time database layout and encode on device buffers.
  * ipr_cuckoo_to_raw_db: KeywordCuckooTable::to_raw_db (cuckoo.rs:314-353) — bucket
  * entries (num_buckets x entry_size bytes, row-major) and occupancy flags (one byte

@@ -110,6 +110,7 @@ _create_raw = _sig("ipr_server_create_from_raw", _i32, _i32, ctypes.POINTER(_Pla
                    ctypes.POINTER(_vp))
 _encode = _sig("ipr_encode_db", _i32, _i32, _vp, _vp, _u64, _u64, _u64, _vp)
 _raw_db = _sig("ipr_cuckoo_to_raw_db", _i32, _i32, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _vp, _vp)
+_wait_selftest = _sig("ipr_selftest_bounded_wait", _i32, _i32, ctypes.c_uint32)
 _offline = _sig("ipr_offline_precompute", _i32, _i32, _vp, _u64, _u64, _vp, _vp, _vp, _vp, _u64, _vp)
 _insp_create = _sig("ipr_inspiring_create", _i32, _i32, _i32, ctypes.POINTER(_vp))
 _insp_pack = _sig("ipr_inspiring_pack", _i32, _vp, _i32, _vp, _vp, _vp, _vp, _vp)
@@ -174,6 +175,12 @@ class Plan:
     @property
     def query_bytes(self) -> int:
         return query_bytes(self.db_rows, 2)
+
+
+def selftest_bounded_wait(budget: int = 1 << 16, device: int = 0) -> int:
+    """ipr_selftest_bounded_wait: the status of a bounded mbarrier wait that nobody
+    satisfies (IPR_E_TIMEOUT = -4 when the failure is detected)"""
+    return int(_wait_selftest(device, budget))
 
 
 def offline_precompute(d_db: int, db_rows: int, instances: int, d_a_hat: int, d_bold_t: int, d_bold_t_bar: int,

@@ -19,6 +19,7 @@
 #include "ipr_b200.h"
 #include "ipr_device.cuh"
 #include "ntt_regs.cuh"
+#include "umma.cuh"
 
 namespace ipr {
 void set_last_error(const char* msg);
@@ -94,6 +95,20 @@ __global__ void __launch_bounds__(256) k_automorph(const uint64_t* __restrict__ 
             for (int s = threadIdx.x; s < N; s += blockDim.x) o[s] = poly[auto_src(k, (uint32_t)s)];
         }
     }
+}
+
+// The bounded wait the tensor-core kernels use on their mbarriers (umma::mbar_wait), on a
+// barrier nothing arrives on: the wait gives up after `budget` polls and the kernel reports it
+// instead of hanging, as the GEMM kernels do through their error flags.
+__global__ void k_wait_selftest(uint32_t budget, int* out) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        umma::mbar_init(&bar, 1);
+        umma::fence_mbar_init();
+    }
+    __syncthreads();
+    const bool done = umma::mbar_wait(&bar, 0, budget);  // phase 0 never completes
+    if (threadIdx.x == 0) *out = done ? 1 : 0;
 }
 
 // per-device NTT tables (fw, fwp, iw, iwp: [4][2 limbs][N] u32), built on first use
@@ -172,6 +187,27 @@ int ipr_automorph_batch(int device, const uint64_t* d_in, uint64_t count, const 
     ipr::k_automorph<<<(unsigned)grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(d_in, (int64_t)count, d_ks, nk,
                                                                                    d_out);
     return ipr::cuda_status(cudaGetLastError());
+}
+
+int ipr_selftest_bounded_wait(int device, uint32_t budget) {
+    int st = ipr::cuda_status(cudaSetDevice(device));
+    if (st) return st;
+    int* d = nullptr;
+    int h = -1;
+    cudaError_t e = cudaMalloc(&d, sizeof(int));
+    if (e == cudaSuccess) {
+        ipr::k_wait_selftest<<<1, 32>>>(budget, d);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(int), cudaMemcpyDeviceToHost);
+        cudaFree(d);
+    }
+    if (e != cudaSuccess) return ipr::cuda_status(e);
+    if (h == 0) {
+        ipr::set_last_error("bounded wait ran out (self-test: nothing arrives on the barrier)");
+        return IPR_E_TIMEOUT;
+    }
+    ipr::set_last_error("bounded wait self-test: the barrier completed unexpectedly");
+    return IPR_E_STATE;
 }
 
 }  // extern "C"

@@ -140,3 +140,17 @@ def test_service_errors_and_poll(pkg, orc, dbs):
         assert r == srv.respond_to_serialized_query(orc.synth_query(902, plan.db_rows, 2))
         with pytest.raises(pkg.IprError):
             svc.poll(t)  # collected tickets are released
+
+
+@pytest.mark.gpu
+def test_bounded_wait_reports_timeout_and_device_stays_usable(pkg, orc):
+    """failure detection without a GPU fault: a kernel's bounded mbarrier wait on a barrier
+    nothing arrives on gives up and is reported as IPR_E_TIMEOUT; afterwards the same
+    process answers a query bit-exactly"""
+    assert pkg.selftest_bounded_wait(1 << 12) == -4
+    assert "bounded wait ran out" in (pkg.lib.ipr_last_error() or b"").decode()
+    plan = pkg.plan_from_shape(10_000, 32, 1184)
+    with pkg.KeywordServer.synthetic(plan, seed=3) as srv:
+        sdb = orc.SynthDB(plan.db_rows, plan.instances, plan.interp, plan.c, seed=3)
+        q = orc.synth_query(9, plan.db_rows, 2)
+        assert srv.respond_to_serialized_query(q) == orc.respond(sdb, q)
