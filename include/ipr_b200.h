@@ -340,6 +340,11 @@ int ipr_service_create(ipr_server *const *servers, int num_servers, const ipr_se
                        ipr_service **out);
 /* Queue one serialized KeywordQueryPayload for database `db`; *ticket names it. */
 int ipr_service_submit(ipr_service *svc, int db, const uint8_t *query, size_t len, uint64_t *ticket);
+/* n payloads queued atomically (all or none: IPR_E_BUSY if the queue cannot take all,
+ * IPR_E_FORMAT if any is malformed), so the dispatcher sees them together and fills whole
+ * batches at once, e.g. for a frontend forwarding a burst.  tickets[i] for queries[i]. */
+int ipr_service_submit_batch(ipr_service *svc, int db, int n, const uint8_t *const *queries, const size_t *lens,
+                             uint64_t *tickets);
 /* IPR_PENDING while running; otherwise the request's status, with the serialized
  * response copied to out (IPR_E_SPACE and *out_len = size if cap is short; the
  * result is kept for a retry).  A collected ticket is released. */

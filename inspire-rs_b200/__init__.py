@@ -121,6 +121,8 @@ _state_plan = _sig("ipr_state_file_plan", _i32, ctypes.c_char_p, ctypes.POINTER(
 _svc_create = _sig("ipr_service_create", _i32, ctypes.POINTER(_vp), _i32, ctypes.POINTER(_ServiceConfig),
                    ctypes.POINTER(_vp))
 _svc_submit = _sig("ipr_service_submit", _i32, _vp, _i32, _u8p, _sz, ctypes.POINTER(_u64))
+_svc_submit_batch = _sig("ipr_service_submit_batch", _i32, _vp, _i32, _i32, ctypes.POINTER(_u8p),
+                         ctypes.POINTER(_sz), ctypes.POINTER(_u64))
 _svc_poll = _sig("ipr_service_poll", _i32, _vp, _u64, _u8p, _sz, ctypes.POINTER(_sz))
 _svc_wait = _sig("ipr_service_wait", _i32, _vp, _u64, _i32, _u8p, _sz, ctypes.POINTER(_sz))
 _svc_stats = _sig("ipr_service_get_stats", _i32, _vp, ctypes.POINTER(_ServiceStats))
@@ -577,6 +579,16 @@ class KeywordService:
         ptr = ctypes.cast(ctypes.c_char_p(query), _u8p)  # no copy: the service copies on submit
         _check(_svc_submit(self._h, db, ptr, len(query), ctypes.byref(t)), "service_submit")
         return t.value
+
+    def submit_many(self, db: int, queries: Sequence[bytes]) -> List[int]:
+        """ipr_service_submit_batch: all payloads queued at once (all or none)"""
+        n = len(queries)
+        qs = [bytes(q) for q in queries]
+        ptrs = (_u8p * n)(*[ctypes.cast(ctypes.c_char_p(q), _u8p) for q in qs])
+        lens = (_sz * n)(*[len(q) for q in qs])
+        out = (_u64 * n)()
+        _check(_svc_submit_batch(self._h, db, n, ptrs, lens, out), "service_submit_batch")
+        return list(out)
 
     def _collect(self, fn, ticket, *extra):
         cap = self._cap

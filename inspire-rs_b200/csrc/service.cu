@@ -490,6 +490,59 @@ int ipr_service_submit(ipr_service* v, int db, const uint8_t* query, size_t len,
     return IPR_OK;
 }
 
+int ipr_service_submit_batch(ipr_service* v, int db, int n, const uint8_t* const* queries, const size_t* lens,
+                             uint64_t* tickets) {
+    if (!v || n < 0 || (n && (!queries || !lens || !tickets))) return svc_fail(IPR_E_ARGS, "null argument");
+    if (db < 0 || db >= (int)v->lanes.size()) return svc_fail(IPR_E_ARGS, "no such database");
+    Lane& ln = v->lanes[db];
+    std::vector<Request*> rs;
+    rs.reserve((size_t)n);
+    auto drop = [&]() {
+        for (Request* r : rs) delete r;
+    };
+    for (int i = 0; i < n; i++) {  // every query is checked before any is queued
+        if (!queries[i] || lens[i] < 1) {
+            drop();
+            return svc_fail(IPR_E_FORMAT, "empty query");
+        }
+        const uint64_t want = ipr_server_query_bytes(ln.s, queries[i][0]);
+        if (lens[i] < want) {
+            drop();
+            return svc_fail(IPR_E_FORMAT, "query shorter than its query count needs");
+        }
+        auto* r = new Request();
+        r->db = db;
+        r->query.assign(queries[i], queries[i] + want);
+        rs.push_back(r);
+    }
+    {
+        std::lock_guard<std::mutex> lk(v->mu);
+        if (v->stop) {
+            drop();
+            return svc_fail(IPR_E_STATE, "service is shutting down");
+        }
+        if (v->npending + (uint64_t)n > (uint64_t)v->cfg.max_pending) {
+            v->rejected += (uint64_t)n;
+            drop();
+            return svc_fail(IPR_E_BUSY, "request queue cannot take all of them");
+        }
+        const auto now = Clock::now();
+        for (int i = 0; i < n; i++) {
+            Request* r = rs[(size_t)i];
+            r->t_submit = now;
+            r->ticket = v->next_ticket++;
+            v->reqs[r->ticket] = r;
+            ln.pending.push_back(r);
+            tickets[i] = r->ticket;
+        }
+        v->npending += (uint64_t)n;
+        v->in_flight += (uint64_t)n;
+        v->submitted += (uint64_t)n;
+    }
+    v->cv_work.notify_one();
+    return IPR_OK;
+}
+
 static int collect_locked(ipr_service* v, Request* r, uint8_t* out, size_t cap, size_t* out_len) {
     if (out_len) *out_len = r->resp.size();
     const int st = r->status;

@@ -154,3 +154,22 @@ def test_bounded_wait_reports_timeout_and_device_stays_usable(pkg, orc):
         sdb = orc.SynthDB(plan.db_rows, plan.instances, plan.interp, plan.c, seed=3)
         q = orc.synth_query(9, plan.db_rows, 2)
         assert srv.respond_to_serialized_query(q) == orc.respond(sdb, q)
+
+
+@pytest.mark.gpu
+def test_submit_many_answers_each_payload_like_alone(pkg, orc):
+    """ipr_service_submit_batch: a burst queued atomically, every response bit-exact"""
+    plan = pkg.plan_from_shape(10_000, 32, 1184)
+    sdb = orc.SynthDB(plan.db_rows, plan.instances, plan.interp, plan.c, seed=5)
+    qs = [orc.synth_query(40 + i, plan.db_rows, 2) for i in range(70)] + [orc.synth_query(9, plan.db_rows, 1)]
+    with pkg.KeywordServer.synthetic(plan, seed=5) as srv:
+        svc = pkg.KeywordService([srv], max_batch=64)
+        try:
+            tickets = svc.submit_many(0, qs)
+            got = [svc.wait(t) for t in tickets]
+            with pytest.raises(pkg.IprError):
+                svc.submit_many(0, [qs[0], b""])  # one malformed payload: none queued
+        finally:
+            svc.close()
+    for q, g in zip(qs, got):
+        assert g == orc.respond(sdb, q)
