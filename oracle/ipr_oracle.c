@@ -440,6 +440,21 @@ void ipr_rgsw_row0(const ipr_params *p, uint64_t out[2 * IPR_N]) {
     ipr_to_ntt(p, a, out);
 }
 
+/* PolyMatrixRaw::random_rng (poly.rs:211-231): `count` coefficients, each one ChaCha20Rng u64
+ * reduced mod q, from a generator seeded with `seed`.  The test client draws with it the public
+ * `a` polynomials of its query ciphertexts (get_seed(SEED_0), client/online.rs:164-168, 216-250)
+ * and of its RGSW ciphertexts (RGSW_SEEDS, client/keyword.rs:168-181). */
+void ipr_oracle_random_raw(const ipr_params *p, const uint8_t seed[32], uint64_t count, uint64_t *out) {
+    ipr_chacha_rng r;
+    ipr_chacha_seed(&r, seed);
+    for (uint64_t i = 0; i < count; i++) out[i] = ipr_chacha_next_u64(&r) % p->modulus;
+}
+
+/* rescale (arith.rs:436-452) over an array */
+void ipr_oracle_rescale_many(const uint64_t *in, uint64_t n, uint64_t inp_mod, uint64_t out_mod, uint64_t *out) {
+    for (uint64_t i = 0; i < n; i++) out[i] = ipr_rescale(in[i], inp_mod, out_mod);
+}
+
 /* ------------------------------------------------------------------ */
 /* shape plan                                                           */
 /* ------------------------------------------------------------------ */

@@ -102,6 +102,9 @@ _raw_db = _sig("ipr_oracle_raw_db", None, _p, _p, _u64, _u64, _u64, _u64, _u64, 
 _encode_db = _sig("ipr_oracle_encode_db", ctypes.c_int, _p, _p, _u64, _u64, _u64)
 _synth_q = _sig("ipr_synth_query", ctypes.c_int, _u64, _u64, ctypes.c_uint, _p, _sz, ctypes.POINTER(_sz))
 threads = _sig("ipr_oracle_threads", ctypes.c_int)
+_random_raw = _sig("ipr_oracle_random_raw", None, ctypes.POINTER(Params), _p, _u64, _p)
+_rescale_many = _sig("ipr_oracle_rescale_many", None, _p, _u64, _u64, _u64, _p)
+
 
 _PARAMS = None
 
@@ -207,6 +210,23 @@ def chacha20_rfc8439_block(key: bytes, counter: int, nonce: bytes) -> bytes:
     out = np.zeros(16, dtype=np.uint32)
     _chacha_rfc(_ptr(k), counter, _ptr(n), _ptr(out))
     return out.astype("<u4").tobytes()
+
+
+def random_raw(seed: bytes, count: int) -> np.ndarray:
+    """PolyMatrixRaw::random_rng (poly.rs:211-231): `count` ChaCha20Rng u64 draws mod q"""
+    sd = np.frombuffer(bytes(seed), dtype=np.uint8).copy()
+    assert sd.size == 32
+    out = np.zeros(count, dtype=np.uint64)
+    _random_raw(ctypes.byref(params()), _ptr(sd), count, _ptr(out))
+    return out
+
+
+def rescale_many(vals: np.ndarray, inp_mod: int, out_mod: int) -> np.ndarray:
+    """rescale (arith.rs:436-452) of every element"""
+    v = np.ascontiguousarray(vals, dtype=np.uint64)
+    out = np.zeros(v.size, dtype=np.uint64)
+    _rescale_many(_ptr(v), v.size, inp_mod, out_mod, _ptr(out))
+    return out.reshape(v.shape)
 
 
 def rgsw_row0() -> np.ndarray:

@@ -1,0 +1,166 @@
+"""End to end through a real client: a query encrypted under a secret key
+decrypts, after respond(), to the database values it asked for.
+
+The reference pins respond() only this way (tests/e2e_mlkem.rs:8-39: the
+client decrypts the right key); it has no golden response.  The client here
+(oracle/pir_client.py) restates the reference client: ternary secret key,
+scaled-Regev first-dimension query under the public seed, RGSW bodies under
+RGSW_SEEDS, InspiRING packing keys, the wire format and the decryption after
+the modulus switch.  A server whose packing keys, precomputation, fold or
+switch were wrong in any step would not decrypt to the DB.
+
+CPU tests run the oracle's respond() on a small server built from a raw DB
+(encode and the offline precomputation included); GPU tests build the device
+server from records (encode and offline precomputation on the device) at the
+10k ML-KEM-768 shape and at the 1M benchmark shape, and decrypt single and
+batch-64 answers.
+"""
+import numpy as np
+import pytest
+
+import pir_client as pc
+
+N = 2048
+
+
+def _entries(rng, buckets, entry_size, fill=0.9):
+    """random entries with no aligned 0xFFFF pair (the plaintext modulus is 65535, so the
+    DB value 0xFFFF reads back as 0), and the occupancy bitmap"""
+    e = rng.integers(0, 256, (buckets, entry_size), dtype=np.uint8)
+    pairs = e[:, :entry_size // 2 * 2].reshape(buckets, -1, 2)
+    pairs[(pairs[..., 0] == 255) & (pairs[..., 1] == 255), 1] = 254
+    occ = (rng.random(buckets) < fill).astype(np.uint8)
+    return e, occ
+
+
+def _check_plaintexts(cl, raw_cm, db_rows, db_cols, buckets, results):
+    """every result of every sub-query equals the raw DB row it selects"""
+    R = raw_cm.reshape(db_cols, db_rows)
+    for b, r in zip(buckets, results):
+        row, _, sub = cl.target(b)
+        assert r.shape == (cl.c, N)
+        for wp in range(cl.c):
+            col0 = (wp * cl.interp + sub) * N
+            np.testing.assert_array_equal(r[wp], R[col0:col0 + N, row].astype(np.uint64) % 65535,
+                                          err_msg=f"bucket {b} group {wp}")
+
+
+# --- CPU: the oracle server ----------------------------------------------------
+SMALL = dict(db_rows=2048, instances=2, interp=2, c=1, per=6, item_elems=608, entry_size=1216)
+
+
+@pytest.fixture(scope="module")
+def small_server(orc):
+    s = SMALL
+    db_cols = s["instances"] * N
+    rng = np.random.default_rng(2026)
+    entries, occ = _entries(rng, s["db_rows"] * s["per"], s["entry_size"])
+    raw = orc.raw_db(entries, occ, s["entry_size"], s["db_rows"], db_cols, s["per"])
+    enc = orc.encode_db(raw, s["db_rows"], db_cols, s["interp"])
+    a_hat, bt, btb, bth = orc.offline_precompute(enc, s["db_rows"], s["instances"])
+    sdb = orc.SynthDB.__new__(orc.SynthDB)
+    sdb.db_rows, sdb.instances, sdb.interp, sdb.c, sdb.seed = s["db_rows"], s["instances"], s["interp"], s["c"], 0
+    sdb.db_cols, sdb.db = db_cols, enc
+    sdb.a_hat, sdb.bold_t, sdb.bold_t_bar, sdb.bold_t_hat = (np.ascontiguousarray(x).reshape(-1)
+                                                               for x in (a_hat, bt, btb, bth))
+    sdb.stash, sdb._stash_buf = [], np.zeros(1, dtype=np.uint8)
+    return sdb, raw, entries, occ
+
+
+def _client(seed, s=SMALL):
+    return pc.TestClient(s["db_rows"], s["interp"], s["c"], s["per"], s["item_elems"], seed=seed)
+
+
+def test_oracle_response_decrypts_to_the_db(orc, small_server):
+    sdb, raw, entries, occ = small_server
+    cl = _client(11)
+    per = SMALL["per"]
+    # item 0 / 2 lie in DB polynomial 0 (sub-column 0), items 4 / 5 in polynomial 1
+    buckets = [7 * per + 0, 1500 * per + 4, 2047 * per + 5, 3 * per + 2]
+    q, _ = cl.query(buckets)
+    assert len(q) == orc.query_bytes(SMALL["db_rows"], len(buckets))
+    results, stash = cl.decrypt(orc.respond(sdb, q))
+    assert stash == []
+    _check_plaintexts(cl, raw, SMALL["db_rows"], sdb.db_cols, buckets, results)
+    for b, r in zip(buckets, results):
+        got = cl.extract(b, r)
+        assert got == (entries[b].tobytes() if occ[b] else bytes(SMALL["entry_size"]))
+
+
+def test_another_key_does_not_decrypt(orc, small_server):
+    """control: the same response under a different secret key is noise"""
+    sdb, raw, _, _ = small_server
+    cl, other = _client(12), _client(13)
+    b = 100 * SMALL["per"] + 1
+    q, _ = cl.query([b])
+    resp = orc.respond(sdb, q)
+    row, _, sub = cl.target(b)
+    want = raw.reshape(sdb.db_cols, SMALL["db_rows"])[sub * N:(sub + 1) * N, row].astype(np.uint64) % 65535
+    assert np.array_equal(cl.decrypt(resp)[0][0][0], want)
+    assert np.count_nonzero(other.decrypt(resp)[0][0][0] == want) < 16
+
+
+def test_client_bytes_match_the_package_serializer(pkg):
+    cl = _client(14)
+    q, f = cl.query([5, 6000])
+    p = pkg.KeywordQueryPayload(f["y_body"], f["z_body"], [(r, g) for r, g in f["queries"]])
+    assert pkg.serialize_keyword_query(p) == q
+
+
+# --- GPU: the device server built from records ----------------------------------
+@pytest.fixture(scope="module")
+def config0(pkg, orc):
+    plan = pkg.plan_from_shape(10_000, 32, 1184)
+    assert (plan.db_rows, plan.db_cols, plan.instances, plan.interp, plan.c) == (2048, 16384, 8, 8, 1)
+    per = plan.num_items // plan.db_rows
+    rng = np.random.default_rng(7)
+    entries, occ = _entries(rng, plan.num_items, plan.entry_size, fill=10_000 / plan.num_items)
+    raw = orc.raw_db(entries, occ, plan.entry_size, plan.db_rows, plan.db_cols, per)
+    srv = pkg.KeywordServer.setup(plan, raw, raw=True, key_size=32, value_size=1184, num_records=int(occ.sum()))
+    yield plan, per, raw, entries, occ, srv
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_device_response_decrypts_to_the_entry(config0):
+    plan, per, raw, entries, occ, srv = config0
+    cl = pc.TestClient(plan.db_rows, plan.interp, plan.c, per, plan.item_size_bits // 16, seed=21)
+    occupied = np.flatnonzero(occ)
+    # two positions as the keyword client sends them; entries inside one DB polynomial
+    buckets = [int(b) for b in occupied if (b % per) * 608 % N + 608 <= N][:2]
+    q, _ = cl.query(buckets)
+    results, stash = cl.decrypt(srv.respond_to_serialized_query(q))
+    _check_plaintexts(cl, raw, plan.db_rows, plan.db_cols, buckets, results)
+    for b, r in zip(buckets, results):
+        entry = cl.extract(b, r)
+        assert entry == entries[b].tobytes()
+        assert entry[32:32 + 1184] == entries[b, 32:1216].tobytes()  # the value after the 32-byte key
+
+
+@pytest.mark.gpu
+def test_device_batch_of_distinct_clients_decrypts(config0):
+    plan, per, raw, entries, occ, srv = config0
+    rng = np.random.default_rng(5)
+    clients = [pc.TestClient(plan.db_rows, plan.interp, plan.c, per, 608, seed=100 + i) for i in range(16)]
+    asks = [[int(x) for x in rng.integers(0, plan.num_items, 2)] for _ in clients]
+    qs = [cl.query(b)[0] for cl, b in zip(clients, asks)]
+    for cl, b, resp in zip(clients, asks, srv.respond_batch(qs)):
+        _check_plaintexts(cl, raw, plan.db_rows, plan.db_cols, b, cl.decrypt(resp)[0])
+
+
+@pytest.mark.gpu
+def test_batch_of_64_decrypts_at_1m(pkg):
+    """the benchmark configuration: 1M ML-KEM-768 records (buckets 2^21, dim0 2048), the
+    server set up on the device from a raw DB, 64 distinct clients in one batched pass"""
+    plan = pkg.plan_from_shape(1_000_000, 32, 1184, 2_097_152, 2048)
+    assert (plan.db_rows, plan.db_cols, plan.instances, plan.interp, plan.c) == (2048, 720896, 352, 32, 11)
+    per = plan.num_items // plan.db_rows
+    raw = np.random.default_rng(1).integers(0, 65535, plan.db_rows * plan.db_cols, dtype=np.uint16)
+    with pkg.KeywordServer.setup(plan, raw, raw=True, num_records=1_000_000) as srv:
+        rng = np.random.default_rng(64)
+        clients = [pc.TestClient(plan.db_rows, plan.interp, plan.c, per, 608, seed=500 + i) for i in range(64)]
+        asks = [[int(x) for x in rng.integers(0, plan.num_items, 2)] for _ in clients]
+        qs = [cl.query(b)[0] for cl, b in zip(clients, asks)]
+        batch = srv.respond_batch(qs)
+    for cl, b, resp in zip(clients, asks, batch):
+        _check_plaintexts(cl, raw, plan.db_rows, plan.db_cols, b, cl.decrypt(resp)[0])
