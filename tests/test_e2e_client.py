@@ -164,3 +164,38 @@ def test_batch_of_64_decrypts_at_1m(pkg):
         batch = srv.respond_batch(qs)
     for cl, b, resp in zip(clients, asks, batch):
         _check_plaintexts(cl, raw, plan.db_rows, plan.db_cols, b, cl.decrypt(resp)[0])
+
+
+@pytest.mark.gpu
+def test_service_state_file_and_shards_decrypt(pkg, orc, tmp_path):
+    """the other public entry points answer decryptably too: the serving API, a server
+    reloaded from its state file, and two fold-group shards whose parts are merged"""
+    plan = pkg.Plan(num_items=8 * 2048, entry_size=1216, item_size_bits=9728, dim0=2048, db_rows=2048,
+                    db_cols=4 * N, instances=4, interp=2, c=2, peak_bytes=0)
+    per = 8
+    rng = np.random.default_rng(77)
+    entries, occ = _entries(rng, plan.num_items, plan.entry_size)
+    raw = orc.raw_db(entries, occ, plan.entry_size, plan.db_rows, plan.db_cols, per)
+    clients = [pc.TestClient(plan.db_rows, plan.interp, plan.c, per, 608, seed=900 + i) for i in range(3)]
+    asks = [[1 * per + 0, 2047 * per + 7], [600 * per + 4], [9 * per + 3, 10 * per + 5, 11 * per + 1]]
+    qs = [cl.query(b)[0] for cl, b in zip(clients, asks)]
+
+    def check(answers):
+        for cl, b, resp in zip(clients, asks, answers):
+            _check_plaintexts(cl, raw, plan.db_rows, plan.db_cols, b, cl.decrypt(resp)[0])
+
+    path = str(tmp_path / "real.state")
+    with pkg.KeywordServer.setup(plan, raw, raw=True) as srv:
+        check([srv.respond_to_serialized_query(q) for q in qs])
+        with pkg.KeywordService([srv], max_batch=4) as svc:
+            check([svc.wait(t) for t in svc.submit_many(0, qs)])
+        srv.save(path)
+    with pkg.KeywordServer.load(path) as loaded:
+        check(loaded.respond_batch(qs))
+    parts = []
+    for k in range(2):
+        sub, sl = pkg.shard_slices(plan, 2, k)
+        lo, hi = sl["db"]
+        with pkg.KeywordServer.setup(sub, raw[lo:hi], raw=True) as shard:
+            parts.append([shard.respond_to_serialized_query(q) for q in qs])
+    check([pkg.merge_responses([parts[0][i], parts[1][i]]) for i in range(len(qs))])
