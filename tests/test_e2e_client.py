@@ -199,3 +199,66 @@ def test_service_state_file_and_shards_decrypt(pkg, orc, tmp_path):
         with pkg.KeywordServer.setup(sub, raw[lo:hi], raw=True) as shard:
             parts.append([shard.respond_to_serialized_query(q) for q in qs])
     check([pkg.merge_responses([parts[0][i], parts[1][i]]) for i in range(len(qs))])
+
+
+# --- InspiRING packing: packed LWEs decrypt to their messages ------------------------
+def _lwes_of_rlwe(cl, msgs):
+    """2048 LWE ciphertexts from one RLWE encryption of sum_j scale_k m_j X^j, the public
+    polynomial from ChaCha20Rng([2; 32]) as in test_packing_inspir (packing.rs:3428-3526):
+    rlwe_to_lwe (client/online.rs:18-24) -> [N + 1][N], column j = the LWE of coefficient j
+    (rows: the negacyclic matrix of row 0 = -a, then the b row)"""
+    Q = pc.Q
+    a = pc._o.random_raw(bytes([2] * 32), N)
+    msg = (np.asarray(msgs, dtype=np.uint64) * np.uint64(pc.SCALE_K)) % np.uint64(Q)
+    b = pc.from_ntt(pc.ntt_add(pc.to_ntt(cl.noise_raw()), pc.ntt_mul(cl.s_ntt, pc.to_ntt(a)), pc.to_ntt(msg)))
+    row0 = (np.uint64(Q) - a) % np.uint64(Q)
+    r, j = np.arange(N)[:, None], np.arange(N)[None, :]
+    m = row0[(j - r) % N]
+    wrap = j < r
+    m[wrap] = (np.uint64(Q) - m[wrap]) % np.uint64(Q)
+    return np.ascontiguousarray(np.vstack([m, b[None, :]]))
+
+
+def _decrypt_rlwe(cl, packed):
+    """decrypt_matrix_reg + rescale to 65535 of an RLWE [2][N] raw (row 1 may be < 2q)"""
+    p0, p1 = (np.asarray(packed[k], dtype=np.uint64) % np.uint64(pc.Q) for k in (0, 1))
+    dec = pc.from_ntt(pc.ntt_add(pc.ntt_mul(cl.s_ntt, pc.to_ntt(p0)), pc.to_ntt(p1)))
+    return pc._o.rescale_many(dec, pc.Q, pc.P)
+
+
+def _packing_keys_condensed(cl):
+    y, z = cl.packing_keys()
+    return (np.stack([pc.condense(y[k]) for k in range(3)]), np.stack([pc.condense(z[k]) for k in range(3)]))
+
+
+def test_oracle_inspiring_pack_decrypts(orc):
+    """test_packing_inspir (packing.rs:3428-3526) with all 2048 LWEs packed (packing_fully_online,
+    full keys): the packed RLWE decrypts to every message"""
+    cl = _client(31)
+    msgs = (np.arange(N, dtype=np.uint64) * 7919) % 65535
+    y, z = _packing_keys_condensed(cl)
+    packed = orc.inspiring_pack(_lwes_of_rlwe(cl, msgs), y, z)
+    np.testing.assert_array_equal(_decrypt_rlwe(cl, packed), msgs)
+
+
+@pytest.mark.gpu
+def test_device_inspiring_pack_decrypts(pkg):
+    """ipr_inspiring_pack of two sets of 2048 LWEs under one client's keys (a call takes one
+    key pair): each packed RLWE decrypts to its set's messages"""
+    import torch
+    sets = 2
+    cl = _client(40)
+    rng = np.random.default_rng(8)
+    msgs = [rng.integers(0, 65535, N, dtype=np.uint64) for _ in range(sets)]
+    y, z = _packing_keys_condensed(cl)
+    lwe = np.stack([_lwes_of_rlwe(cl, m) for m in msgs])
+    d_lwe = torch.from_numpy(lwe.view(np.int64)).cuda()
+    d_y = torch.from_numpy(y.view(np.int64)).cuda()
+    d_z = torch.from_numpy(z.view(np.int64)).cuda()
+    d_out = torch.zeros((sets, 2, N), dtype=torch.int64, device="cuda")
+    with pkg.InspiringPacker(max_sets=sets) as pk:
+        pk.pack(sets, d_lwe.data_ptr(), d_y.data_ptr(), d_z.data_ptr(), d_out.data_ptr())
+        torch.cuda.synchronize()
+    got = d_out.cpu().numpy().view(np.uint64)
+    for c in range(sets):
+        np.testing.assert_array_equal(_decrypt_rlwe(cl, got[c]), msgs[c])
