@@ -119,6 +119,15 @@ def read_peaks():
         return 6650.0, "fallback"
 
 
+def read_bf16_peak():
+    """dense bf16 TFLOP/s of a cuBLAS GEMM timed alone (burst), measured or the fallback"""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
+
+
 def read_traffic(kernel="k_pack"):
     """dram bytes per launch of `kernel` from its committed ncu summary (scaled to the full launch), or None"""
     path = os.path.join(ROOT, "profiles", f"{kernel}_1M_dram.md")
@@ -502,6 +511,10 @@ def main():
         return bytes([2]) + v.view(np.uint8).reshape(-1, 8)[:, :7].tobytes()
 
     B = max(1, args.batch)
+    # one batched pass answers up to 64 payloads (the packing GEMM's N = 64 clients x 4 byte
+    # limbs = 256 columns); larger batches run as consecutive passes of 64
+    PASS = 64
+    passes = (B + PASS - 1) // PASS if B > 1 else 1
     npay = max(2 * B, 4)
     payloads = [synth_payload(1000 * rank + i) for i in range(npay)]
     assert len(payloads[0]) == qbytes
@@ -511,12 +524,13 @@ def main():
                  for k in range(2)]
     d_out = torch.empty(B * rbytes, dtype=torch.uint8, device=dev)
     if B > 1:
-        srv.prepare_batch(B)
+        srv.prepare_batch(min(B, PASS))
 
     def run_device(i):
         d = d_batches[i % 2]
         if B > 1:
-            srv.respond_batch_device(B, d.data_ptr(), d_out.data_ptr())
+            for c0 in range(0, B, PASS):
+                srv.respond_batch_device(min(PASS, B - c0), d.data_ptr() + c0 * qbytes, d_out.data_ptr() + c0 * rbytes)
         else:
             srv.respond_device(d.data_ptr(), qbytes, d_out.data_ptr(), rbytes)
 
@@ -556,7 +570,7 @@ def main():
 
     # ---- end-to-end through the serving API: host buffers, H2D + D2H of every batch ---------
     # (KeywordService: continuous batching, pinned staging, copies overlapped with compute)
-    svc = pkg.KeywordService([srv], max_batch=B) if B > 1 else None
+    svc = pkg.KeywordService([srv], max_batch=min(B, PASS)) if B > 1 else None
     barrier()
     # the blocking call (ipr_server_respond_batch / ipr_server_respond), for comparison
     t0 = time.perf_counter()
@@ -620,11 +634,27 @@ def main():
     pack_ms = stage_ms["pack"] / max(calls, 1)
     if B > 1:  # the packing GEMM streams the slot-indexed precomputation once per batch
         pack_bytes = N * 2 * ((plan.instances + 31) // 32) * 128 * 3 * N  # [slot][limb][tile][128 rows][6144]
-        kname = "k_pack_mma_pair" if B >= 48 else "k_pack_mma"  # the server's default choice of form
+        kname = "k_pack_mma_pair" if min(B, PASS) >= 48 else "k_pack_mma"  # the server's default choice of form
     else:
         pack_bytes = plan.instances * (2 * 3069 + 3) * N * 8  # bold_t + bold_t_bar + bold_t_hat per launch
         kname = "k_pack"
     achieved = pack_bytes / (pack_ms / 1000.0) / 1e9
+    tensor = None
+    if B > 1:
+        # the packing GEMM multiplies every precomputation byte with every client byte column:
+        # 2 ops x bytes streamed x N, N = 4 byte limbs x clients of a pass, rounded to 16
+        nt = max(16, (4 * min(B, PASS) + 15) // 16 * 16)
+        ops = 2.0 * pack_bytes * nt
+        bf16, bf16_kind = read_bf16_peak()
+        i8_peak = 2 * bf16  # dense int8 issues at twice the bf16 rate on B200 (4.5 vs 2.25 P nominal)
+        hbm_floor_ms, tensor_floor_ms = pack_bytes / (peak * 1e9) * 1e3, ops / (i8_peak * 1e12) * 1e3
+        tensor = {"bound": "tensor", "kernel": kname, "ops_per_launch": ops,
+                  "achieved_tops": ops / (pack_ms / 1000.0) / 1e12, "peak_tops": i8_peak,
+                  "peak_source": f"2 x {bf16_kind} bf16 TFLOP/s" + ("" if bf16_kind == "measured"
+                                                                     else " (MEASURED_PEAKS.json absent)"),
+                  "frac": tensor_floor_ms / pack_ms, "hbm_floor_ms": hbm_floor_ms,
+                  "tensor_floor_ms": tensor_floor_ms,
+                  "binding": "tensor" if tensor_floor_ms > hbm_floor_ms else "hbm"}
 
     out = None
     if rank == 0:
@@ -649,7 +679,7 @@ def main():
                        "l2": "inputs larger than L2 (packing stream of %.1f GB + DB of %.2f GB per step)" % (
                            pack_bytes / 1e9, plan.db_rows * plan.db_cols * 2 / 1e9)},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": B * qbytes, "d2h_bytes_per_step": B * rbytes,
-                    "api": ("KeywordService (ipr_service_submit_batch per 64 payloads / ipr_service_wait)" if B > 1
+                    "api": (f"KeywordService (ipr_service_submit_batch per {B} payloads / ipr_service_wait)" if B > 1
                             else "ipr_server_respond"),
                     "blocking_batch_call_payloads_per_s": args.steps * B / (blocking_ms / 1000.0)},
             "serving": serving or None,
@@ -659,8 +689,9 @@ def main():
                          "frac": achieved / peak, "peak_source": ("measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                                          else "fallback 6.65 TB/s (MEASURED_PEAKS.json absent)"),
                          "traffic": read_traffic(kname), "algorithmic_bytes": pack_bytes, "avg_launch_ms": pack_ms},
+            "tensor_roofline": tensor,
             "stage_ms": stage_avg,
-            "gpu_launches": (7 if B > 1 else 6) * args.steps,
+            "gpu_launches": (7 * passes if B > 1 else 6) * args.steps,
             "clocks": clk,
             "cpu_baseline": cpu,
         }
