@@ -278,6 +278,30 @@ int ipr_server_save(ipr_server *srv, const char *path);
 int ipr_server_load(int device, const char *path, ipr_server **out);
 int ipr_state_file_plan(const char *path, ipr_plan *out);
 
+/* ---- keyword-PIR client on the GPU (KeywordClient, src/pir/client/keyword.rs) ----------
+ * Query generation and response decryption for a server plan.  The secret key (ternary,
+ * 256 coefficients +1 and 256 -1, gen_ternary_mat, client/base.rs:126-139) and all noise are
+ * drawn deterministically from `seed` with ChaCha20: key placement from stream 1, the noise
+ * of a query from stream 2 + nonce (centered binomial, eta = 82: sigma 6.40, the width of the
+ * reference's discrete Gaussian).  A nonce must not be reused under one seed. */
+typedef struct ipr_client ipr_client;
+
+/* KeywordClient::setup_from_public_params (keyword.rs:60-115) for `plan` */
+int ipr_client_create(int device, const ipr_plan *plan, const uint8_t seed[32], ipr_client **out);
+/* build_query_payload + serialize_query (keyword.rs:193-214, wire.rs:542-615): one payload
+ * whose n sub-queries ask for the given buckets (cuckoo positions); writes
+ * ipr_query_bytes(db_rows, n) bytes (IPR_E_SPACE when `cap` is smaller; *out_len is set). */
+int ipr_client_query(ipr_client *c, uint64_t nonce, unsigned n, const uint64_t *buckets, uint8_t *out,
+                     size_t cap, size_t *out_len);
+/* decrypt_response_values (keyword.rs:216-245) of every response of a serialized
+ * KeywordResponsePayload: values[q][w][z] (u16 plaintexts mod 65535, fold group w, slot z),
+ * *count = responses x c x 2048.  The stash block is not read. */
+int ipr_client_decrypt(ipr_client *c, const uint8_t *response, size_t len, uint16_t *values, size_t cap,
+                       size_t *count);
+/* the client's secret key, 2048 coefficients in {-1, 0, 1} (for tests) */
+int ipr_client_secret_key(const ipr_client *c, int8_t *out);
+void ipr_client_destroy(ipr_client *c);
+
 /* Failure detection self-test: launches one CTA that waits, with the bounded wait every
  * tensor-core kernel of this library uses on its mbarriers, on a barrier nothing arrives
  * on.  The wait gives up after `budget` polls; the call returns IPR_E_TIMEOUT (the status a

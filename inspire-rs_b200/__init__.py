@@ -646,6 +646,94 @@ class KeywordService:
 
 
 # ---------------------------------------------------------------------------
+# the keyword-PIR client on the GPU (ipr_client_*, KeywordClient of src/pir/client/keyword.rs)
+# ---------------------------------------------------------------------------
+_cl_create = _sig("ipr_client_create", _i32, _i32, ctypes.POINTER(_Plan), ctypes.c_char_p, ctypes.POINTER(_vp))
+_cl_query = _sig("ipr_client_query", _i32, _vp, _u64, ctypes.c_uint, ctypes.POINTER(_u64), _u8p, _sz,
+                 ctypes.POINTER(_sz))
+_cl_decrypt = _sig("ipr_client_decrypt", _i32, _vp, _u8p, _sz, ctypes.POINTER(ctypes.c_uint16), _sz,
+                   ctypes.POINTER(_sz))
+_cl_key = _sig("ipr_client_secret_key", _i32, _vp, ctypes.POINTER(ctypes.c_int8))
+_cl_destroy = _sig("ipr_client_destroy", None, _vp)
+
+
+class KeywordClient:
+    """KeywordClient on the GPU for a server plan: query payloads for buckets (cuckoo
+    positions) and decryption of the server's response.  Key and noise are deterministic in
+    the 32-byte `seed`; every query takes a fresh nonce (counted up from 0 unless given)."""
+
+    def __init__(self, plan: Plan, seed: bytes, device: int = 0):
+        if len(seed) != 32:
+            raise ValueError("seed must be 32 bytes")
+        self.plan, self.device, self._nonce = plan, device, 0
+        self.per = plan.num_items // plan.db_rows
+        self.item_elems = plan.item_size_bits // 16
+        h = _vp()
+        pc = plan._c()
+        _check(_cl_create(device, ctypes.byref(pc), bytes(seed), ctypes.byref(h)), "ipr_client_create")
+        self._h = h.value
+
+    def query(self, buckets: Sequence[int], nonce: Optional[int] = None) -> bytes:
+        """build_query_payload + serialize_query (keyword.rs:193-214) for these buckets"""
+        if nonce is None:
+            nonce, self._nonce = self._nonce, self._nonce + 1
+        b = (_u64 * max(len(buckets), 1))(*buckets)
+        need = query_bytes(self.plan.db_rows, len(buckets))
+        out = (ctypes.c_uint8 * need)()
+        n = _sz()
+        _check(_cl_query(self._h, nonce, len(buckets), b, out, need, ctypes.byref(n)), "ipr_client_query")
+        return bytes(out)
+
+    def decrypt(self, response: bytes):
+        """plaintexts [responses][c][2048] (u16 mod 65535) of a serialized response"""
+        import numpy as np
+        buf = (ctypes.c_uint8 * max(len(response), 1)).from_buffer_copy(response or b"\0")
+        n = _sz()
+        st = _cl_decrypt(self._h, buf, len(response), None, 0, ctypes.byref(n))
+        if st not in (0, -6):
+            _check(st, "ipr_client_decrypt")
+        vals = np.zeros(n.value, dtype=np.uint16)
+        _check(_cl_decrypt(self._h, buf, len(response), vals.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)),
+                           vals.size, ctypes.byref(n)), "ipr_client_decrypt")
+        return vals.reshape(-1, self.plan.c, POLY_LEN)
+
+    def extract(self, bucket: int, plaintext) -> Optional[bytes]:
+        """the entry bytes of `bucket` from its sub-query's plaintexts (keyword.rs:246-257);
+        None when the entry crosses a polynomial boundary and is not all in the returned one"""
+        import numpy as np
+        col = (bucket % self.per) * self.item_elems
+        poly, coeff = col // POLY_LEN, col % POLY_LEN
+        if coeff + self.item_elems > POLY_LEN:
+            return None
+        flat = np.asarray(plaintext, dtype=np.uint16).reshape(-1)
+        off = (poly // self.plan.interp) * POLY_LEN + coeff
+        return flat[off:off + self.item_elems].astype(">u2").tobytes()
+
+    def secret_key(self):
+        import numpy as np
+        out = np.zeros(POLY_LEN, dtype=np.int8)
+        _check(_cl_key(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int8))), "ipr_client_secret_key")
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _cl_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+# ---------------------------------------------------------------------------
 # fold-group sharding across GPUs (one process per GPU)
 # ---------------------------------------------------------------------------
 def shard_plan(plan: Plan, num_shards: int, shard: int):

@@ -74,44 +74,52 @@ void root_powers(uint64_t root, uint64_t m, uint64_t* out) {
 
 uint64_t half_mod(uint64_t x, uint64_t m) { return (x & 1) ? (uint64_t)(((u128)x + m) >> 1) : x >> 1; }
 
-// ChaCha20 keystream in rand_chacha's layout: 64-bit block counter in words
-// 12-13, 64-bit stream id (0) in words 14-15; u64 = two consecutive words, low first
-struct ChaCha {
-    uint32_t key[8];
-    uint64_t counter = 0;
-    uint32_t buf[16];
-    int idx = 16;
-    static uint32_t rotl(uint32_t x, int n) { return (x << n) | (x >> (32 - n)); }
-    void block() {
-        static const uint32_t sigma[4] = {0x61707865, 0x3320646e, 0x79622d32, 0x6b206574};
-        uint32_t s[16], x[16];
-        std::memcpy(s, sigma, 16);
-        std::memcpy(s + 4, key, 32);
-        s[12] = (uint32_t)counter;
-        s[13] = (uint32_t)(counter >> 32);
-        s[14] = s[15] = 0;
-        std::memcpy(x, s, sizeof(x));
-        auto qr = [&](int a, int b, int c, int d) {
-            x[a] += x[b]; x[d] ^= x[a]; x[d] = rotl(x[d], 16);
-            x[c] += x[d]; x[b] ^= x[c]; x[b] = rotl(x[b], 12);
-            x[a] += x[b]; x[d] ^= x[a]; x[d] = rotl(x[d], 8);
-            x[c] += x[d]; x[b] ^= x[c]; x[b] = rotl(x[b], 7);
-        };
-        for (int r = 0; r < 10; r++) {
-            qr(0, 4, 8, 12); qr(1, 5, 9, 13); qr(2, 6, 10, 14); qr(3, 7, 11, 15);
-            qr(0, 5, 10, 15); qr(1, 6, 11, 12); qr(2, 7, 8, 13); qr(3, 4, 9, 14);
-        }
-        for (int i = 0; i < 16; i++) buf[i] = x[i] + s[i];
-        counter++;
-        idx = 0;
+}  // namespace
+
+// ChaCha20 keystream in rand_chacha's layout: 64-bit block counter in words 12-13,
+// 64-bit stream id in words 14-15; a u64 is two consecutive words, low first
+uint32_t ChaCha::rotl(uint32_t x, int n) { return (x << n) | (x >> (32 - n)); }
+
+void ChaCha::block() {
+    static const uint32_t sigma[4] = {0x61707865, 0x3320646e, 0x79622d32, 0x6b206574};
+    uint32_t s[16], x[16];
+    std::memcpy(s, sigma, 16);
+    std::memcpy(s + 4, key, 32);
+    s[12] = (uint32_t)counter;
+    s[13] = (uint32_t)(counter >> 32);
+    s[14] = (uint32_t)stream;
+    s[15] = (uint32_t)(stream >> 32);
+    std::memcpy(x, s, sizeof(x));
+    auto qr = [&](int a, int b, int c, int d) {
+        x[a] += x[b]; x[d] ^= x[a]; x[d] = rotl(x[d], 16);
+        x[c] += x[d]; x[b] ^= x[c]; x[b] = rotl(x[b], 12);
+        x[a] += x[b]; x[d] ^= x[a]; x[d] = rotl(x[d], 8);
+        x[c] += x[d]; x[b] ^= x[c]; x[b] = rotl(x[b], 7);
+    };
+    for (int r = 0; r < 10; r++) {
+        qr(0, 4, 8, 12); qr(1, 5, 9, 13); qr(2, 6, 10, 14); qr(3, 7, 11, 15);
+        qr(0, 5, 10, 15); qr(1, 6, 11, 12); qr(2, 7, 8, 13); qr(3, 4, 9, 14);
     }
-    uint64_t next_u64() {
-        if (idx + 2 > 16) block();
-        uint64_t lo = buf[idx], hi = buf[idx + 1];
-        idx += 2;
-        return lo | (hi << 32);
-    }
-};
+    for (int i = 0; i < 16; i++) buf[i] = x[i] + s[i];
+    counter++;
+    idx = 0;
+}
+
+uint64_t ChaCha::next_u64() {
+    if (idx + 2 > 16) block();
+    uint64_t lo = buf[idx], hi = buf[idx + 1];
+    idx += 2;
+    return lo | (hi << 32);
+}
+
+ChaCha chacha_from_seed(const uint8_t seed[32], uint64_t stream) {
+    ChaCha rng;
+    for (int i = 0; i < 8; i++)
+        rng.key[i] = (uint32_t)seed[4 * i] | ((uint32_t)seed[4 * i + 1] << 8) | ((uint32_t)seed[4 * i + 2] << 16) |
+                     ((uint32_t)seed[4 * i + 3] << 24);
+    rng.stream = stream;
+    return rng;
+}
 
 void forward_ntt_u64(const HostParams& p, uint64_t* a) {  // exact reference-order forward NTT
     for (int l = 0; l < 2; l++) {
@@ -130,6 +138,8 @@ void forward_ntt_u64(const HostParams& p, uint64_t* a) {  // exact reference-ord
         }
     }
 }
+
+namespace {
 
 // params_rgswpir_given_input_size_and_dim0 -> (instances, interp, db_rows)
 int rgswpir(uint64_t num_items, uint64_t item_bits, uint64_t dim0, uint64_t& inst, uint64_t& interp,
@@ -225,13 +235,6 @@ void host_params_init(HostParams& p) {
 }
 
 namespace {
-ChaCha chacha_from_seed(const uint8_t seed[32]) {
-    ChaCha rng;
-    for (int i = 0; i < 8; i++)
-        rng.key[i] = (uint32_t)seed[4 * i] | ((uint32_t)seed[4 * i + 1] << 8) | ((uint32_t)seed[4 * i + 2] << 16) |
-                     ((uint32_t)seed[4 * i + 3] << 24);
-    return rng;
-}
 
 // PolyMatrixNTT::random_rng(params, 1, 3, ChaCha20Rng::from_seed(seed)) (poly.rs:418-440):
 // column c, limb l, coefficient j <- next_u64 % q_l

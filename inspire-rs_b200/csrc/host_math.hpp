@@ -26,6 +26,24 @@ struct HostParams {
 
 void host_params_init(HostParams& p);
 
+// ChaCha20Rng keystream (rand_chacha 0.10 layout): 64-bit block counter in words 12-13,
+// 64-bit stream id in words 14-15, u64 = two consecutive words, low first
+struct ChaCha {
+    uint32_t key[8];
+    uint64_t counter = 0;
+    uint64_t stream = 0;
+    uint32_t buf[16];
+    int idx = 16;
+    static uint32_t rotl(uint32_t x, int n);
+    void block();
+    uint64_t next_u64();
+};
+ChaCha chacha_from_seed(const uint8_t seed[32], uint64_t stream = 0);
+
+// ntt_forward (src/core/ntt.rs:111-160) of a [2][N] array of limb residues, in place,
+// reference evaluation order
+void forward_ntt_u64(const HostParams& p, uint64_t* a);
+
 // Inputs of the offline precomputation derived from fixed seeds: the hint query of
 // generate_pseudorandom_query(SEED_0) ([polys][2][N] NTT) and the W / V masks of
 // OfflinePackingKeys::init_full ([3][2][N] NTT each).

@@ -450,6 +450,19 @@ void ipr_oracle_random_raw(const ipr_params *p, const uint8_t seed[32], uint64_t
     for (uint64_t i = 0; i < count; i++) out[i] = ipr_chacha_next_u64(&r) % p->modulus;
 }
 
+/* `count` ChaCha20 blocks of stream `stream` from block counter `first`, key = the 32-byte
+ * seed read as little-endian words (rand_chacha's layout): the test model of the device
+ * client draws its key shuffle and its centered binomial noise from these */
+void ipr_oracle_chacha_blocks(const uint8_t seed[32], uint64_t stream, uint64_t first, uint64_t count,
+                              uint32_t *out) {
+    uint32_t key[8];
+    for (int i = 0; i < 8; i++)
+        key[i] = (uint32_t)seed[4 * i] | ((uint32_t)seed[4 * i + 1] << 8) | ((uint32_t)seed[4 * i + 2] << 16) |
+                 ((uint32_t)seed[4 * i + 3] << 24);
+#pragma omp parallel for schedule(static)
+    for (int64_t b = 0; b < (int64_t)count; b++) ipr_chacha20_block(key, first + (uint64_t)b, stream, out + 16 * b);
+}
+
 /* rescale (arith.rs:436-452) over an array */
 void ipr_oracle_rescale_many(const uint64_t *in, uint64_t n, uint64_t inp_mod, uint64_t out_mod, uint64_t *out) {
     for (uint64_t i = 0; i < n; i++) out[i] = ipr_rescale(in[i], inp_mod, out_mod);

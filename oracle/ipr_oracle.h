@@ -105,6 +105,8 @@ uint64_t ipr_chacha_next_u64(ipr_chacha_rng *r);
 /* NTT(-a) with a = PolyMatrixRaw::random_rng(ChaCha20(RGSW_SEEDS[i])) (keyword.rs:546-555) */
 void ipr_rgsw_row0(const ipr_params *p, uint64_t out[2 * IPR_N]);
 void ipr_oracle_random_raw(const ipr_params *p, const uint8_t seed[32], uint64_t count, uint64_t *out);
+void ipr_oracle_chacha_blocks(const uint8_t seed[32], uint64_t stream, uint64_t first, uint64_t count,
+                              uint32_t *out);
 void ipr_oracle_rescale_many(const uint64_t *in, uint64_t n, uint64_t inp_mod, uint64_t out_mod, uint64_t *out);
 
 /* ---- shape plan (keyword.rs:29-31,145-233; wire.rs:386-477) ---- */

@@ -104,6 +104,7 @@ _synth_q = _sig("ipr_synth_query", ctypes.c_int, _u64, _u64, ctypes.c_uint, _p, 
 threads = _sig("ipr_oracle_threads", ctypes.c_int)
 _random_raw = _sig("ipr_oracle_random_raw", None, ctypes.POINTER(Params), _p, _u64, _p)
 _rescale_many = _sig("ipr_oracle_rescale_many", None, _p, _u64, _u64, _u64, _p)
+_chacha_blocks = _sig("ipr_oracle_chacha_blocks", None, _p, _u64, _u64, _u64, _p)
 
 
 _PARAMS = None
@@ -219,6 +220,15 @@ def random_raw(seed: bytes, count: int) -> np.ndarray:
     out = np.zeros(count, dtype=np.uint64)
     _random_raw(ctypes.byref(params()), _ptr(sd), count, _ptr(out))
     return out
+
+
+def chacha_blocks(seed: bytes, stream: int, first: int, count: int) -> np.ndarray:
+    """ChaCha20 blocks [count][16] u32 of (seed, stream) from block counter `first`"""
+    sd = np.frombuffer(bytes(seed), dtype=np.uint8).copy()
+    assert sd.size == 32
+    out = np.zeros(count * 16, dtype=np.uint32)
+    _chacha_blocks(_ptr(sd), stream, first, count, _ptr(out))
+    return out.reshape(count, 16)
 
 
 def rescale_many(vals: np.ndarray, inp_mod: int, out_mod: int) -> np.ndarray:

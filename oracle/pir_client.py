@@ -248,3 +248,44 @@ def serialize_query(fields) -> bytes:
         parts.append((g[:, 0, :] | (g[:, 1, :] << np.uint64(28))).reshape(-1))
     words = np.concatenate(parts).astype("<u8")
     return bytes([len(fields["queries"])]) + words.view(np.uint8).reshape(-1, 8)[:, :7].tobytes()
+
+
+class SeededClient(TestClient):
+    """The device client's deterministic randomness (ipr_client_*), restated for parity:
+    the ternary key is placed by a Fisher-Yates shuffle of [+1 x 256, -1 x 256, 0 ...] whose
+    step i (from N-1 down to 1) swaps with j = (u * (i + 1)) >> 64, u the next u64 of
+    ChaCha20(seed, stream 1); the noise of a query with nonce n is, for its global coefficient
+    index g, a centered binomial sample with eta = 82 from ChaCha20 block g of stream 2 + n
+    (popcount of words 0, 1 and the low 18 bits of word 2 minus that of words 3, 4, 5).  The
+    noise polynomials follow the order in which TestClient.query draws them."""
+
+    def __init__(self, db_rows: int, interp: int, c: int, per: int, item_elems: int, seed: bytes):
+        super().__init__(db_rows, interp, c, per, item_elems, seed=0)
+        self.seed = bytes(seed)
+        words = _o.chacha_blocks(self.seed, 1, 0, N // 8).astype(np.uint64).reshape(-1)
+        u64 = [int(words[2 * k]) | (int(words[2 * k + 1]) << 32) for k in range(N)]
+        s = [1] * HAMMING + [-1] * HAMMING + [0] * (N - 2 * HAMMING)
+        for step, i in enumerate(range(N - 1, 0, -1)):
+            j = (u64[step] * (i + 1)) >> 64
+            s[i], s[j] = s[j], s[i]
+        self.s = np.array(s, dtype=np.int8)
+        self.s_raw = (self.s.astype(np.int64) % Q).astype(np.uint64)
+        self.s_ntt = to_ntt(self.s_raw)
+        self._noise, self._next = None, 0
+
+    def noise_raw(self):
+        e = self._noise[self._next]
+        self._next += 1
+        return (e % Q).astype(np.uint64)
+
+    def query(self, buckets, nonce: int = 0):
+        npolys = 6 + len(buckets) * (self.db_rows // N + 6)
+        w = _o.chacha_blocks(self.seed, 2 + nonce, 0, npolys * N)
+        m = np.uint32((1 << 18) - 1)
+        pos = np.bitwise_count(w[:, 0]) + np.bitwise_count(w[:, 1]) + np.bitwise_count(w[:, 2] & m)
+        neg = np.bitwise_count(w[:, 3]) + np.bitwise_count(w[:, 4]) + np.bitwise_count(w[:, 5] & m)
+        self._noise = (pos.astype(np.int64) - neg.astype(np.int64)).reshape(npolys, N)
+        self._next = 0
+        out = super().query(buckets)
+        assert self._next == npolys
+        return out

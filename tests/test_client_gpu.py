@@ -1,0 +1,122 @@
+"""The keyword-PIR client on the GPU (ipr_client_*, KeywordClient).
+
+The device client draws its key and noise deterministically from its seed, so
+its query bytes must equal, bit for bit, those of the oracle's model of the
+same client (`pir_client.SeededClient`: the reference client's query
+construction, client/keyword.rs:137-214, with the same key shuffle and noise
+streams).  Its decryption must equal the model's decryption of the same
+response bytes and the database rows the queries select.  The answering server
+is the device library's, built from a raw DB on the device.
+"""
+import numpy as np
+import pytest
+
+import pir_client as pc
+
+N = 2048
+SEED = bytes(range(1, 33))
+
+
+def test_model_key_and_noise(orc):
+    """the model's key has 256 entries +1 and 256 entries -1; its noise has sigma ~ 6.4"""
+    cl = pc.SeededClient(2048, 8, 1, 16, 608, seed=SEED)
+    assert (cl.s == 1).sum() == 256 and (cl.s == -1).sum() == 256
+    cl.query([3], nonce=1)
+    assert abs(cl._noise.std() - 6.4) < 0.1 and np.abs(cl._noise).max() <= 82
+    other = pc.SeededClient(2048, 8, 1, 16, 608, seed=SEED)
+    other.query([3], nonce=2)
+    assert not np.array_equal(other._noise, cl._noise)  # a fresh nonce draws fresh noise
+
+
+def _small_plan(pkg, db_rows=2048, instances=2, interp=2, per=6):
+    return pkg.Plan(num_items=db_rows * per, entry_size=1216, item_size_bits=9728, dim0=db_rows, db_rows=db_rows,
+                    db_cols=instances * N, instances=instances, interp=interp, c=instances // interp, peak_bytes=0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", ["10k", "rows4096"])
+def test_device_query_bytes_equal_model(pkg, shape):
+    if shape == "10k":
+        plan = pkg.plan_from_shape(10_000, 32, 1184)
+    else:  # two first-dimension polynomials per sub-query
+        plan = _small_plan(pkg, db_rows=4096, instances=4, interp=2, per=4)
+    per = plan.num_items // plan.db_rows
+    model = pc.SeededClient(plan.db_rows, plan.interp, plan.c, per, 608, seed=SEED)
+    with pkg.KeywordClient(plan, SEED) as dev:
+        assert np.array_equal(dev.secret_key(), model.s)
+        for nonce, buckets in ((0, [5, plan.num_items - 1]), (9, [plan.num_items // 2]),
+                               (3, [1, 2 * per + 4, 7 * per + 3])):
+            got = dev.query(buckets, nonce=nonce)
+            want, _ = model.query(buckets, nonce=nonce)
+            assert len(got) == pkg.query_bytes(plan.db_rows, len(buckets))
+            assert got == want, (nonce, buckets)
+
+
+@pytest.mark.gpu
+def test_device_client_round_trip(pkg, orc):
+    """device client -> device server (set up from a raw DB on the device) -> device
+    decryption: equal to the model's decryption and to the DB rows, and extract returns
+    the entries"""
+    plan = pkg.plan_from_shape(10_000, 32, 1184)
+    per = plan.num_items // plan.db_rows
+    rng = np.random.default_rng(12)
+    entries = rng.integers(0, 256, (plan.num_items, plan.entry_size), dtype=np.uint8)
+    pairs = entries[:, :plan.entry_size // 2 * 2].reshape(plan.num_items, -1, 2)
+    pairs[(pairs[..., 0] == 255) & (pairs[..., 1] == 255), 1] = 254  # no DB value 0xFFFF (= 0 mod 65535)
+    occ = np.ones(plan.num_items, dtype=np.uint8)
+    raw = orc.raw_db(entries, occ, plan.entry_size, plan.db_rows, plan.db_cols, per)
+    R = raw.reshape(plan.db_cols, plan.db_rows)
+    buckets = [0 * per + 1, 1234 * per + 2, 2047 * per + 4]  # items inside one DB polynomial
+    model = pc.SeededClient(plan.db_rows, plan.interp, plan.c, per, 608, seed=SEED)
+    with pkg.KeywordServer.setup(plan, raw, raw=True) as srv, pkg.KeywordClient(plan, SEED) as dev:
+        q = dev.query(buckets, nonce=4)
+        resp = srv.respond_to_serialized_query(q)
+        got = dev.decrypt(resp)
+    want = model.decrypt(resp)[0]
+    assert got.shape == (3, plan.c, N)
+    for k, b in enumerate(buckets):
+        np.testing.assert_array_equal(got[k], want[k])
+        row, col, sub = model.target(b)
+        np.testing.assert_array_equal(got[k][0], R[sub * N:(sub + 1) * N, row])
+        assert dev.extract(b, got[k]) == entries[b].tobytes()
+
+
+@pytest.mark.gpu
+def test_device_clients_batch_of_64_at_1m(pkg):
+    """64 device clients, one batched pass of the 1M server set up from a raw DB, 64
+    device decryptions: every result of every client equals the DB row it selects"""
+    plan = pkg.plan_from_shape(1_000_000, 32, 1184, 2_097_152, 2048)
+    per = plan.num_items // plan.db_rows
+    raw = np.random.default_rng(3).integers(0, 65535, plan.db_rows * plan.db_cols, dtype=np.uint16)
+    R = raw.reshape(plan.db_cols, plan.db_rows)
+    rng = np.random.default_rng(99)
+    asks = [[int(x) for x in rng.integers(0, plan.num_items, 2)] for _ in range(64)]
+    clients = [pkg.KeywordClient(plan, bytes([i]) * 32) for i in range(64)]
+    try:
+        qs = [cl.query(b) for cl, b in zip(clients, asks)]
+        with pkg.KeywordServer.setup(plan, raw, raw=True) as srv:
+            batch = srv.respond_batch(qs)
+        for cl, b, resp in zip(clients, asks, batch):
+            pt = cl.decrypt(resp)
+            for k, bucket in enumerate(b):
+                row = bucket // per
+                sub = ((bucket % per) * 608 % (plan.interp * N)) // N
+                for w in range(plan.c):
+                    c0 = (w * plan.interp + sub) * N
+                    np.testing.assert_array_equal(pt[k][w], R[c0:c0 + N, row])
+    finally:
+        for cl in clients:
+            cl.close()
+
+
+@pytest.mark.gpu
+def test_device_client_refuses_bad_input(pkg):
+    plan = pkg.plan_from_shape(10_000, 32, 1184)
+    with pkg.KeywordClient(plan, SEED) as dev:
+        with pytest.raises(pkg.IprError) as e:
+            dev.query([plan.num_items])  # bucket out of range
+        assert e.value.status == -1
+        with pytest.raises(pkg.IprError) as e:
+            dev.decrypt(b"\x01\x00\x00\x00\x05\x00\x00\x00abcde")  # a result of the wrong length
+        assert e.value.status == -5
+        assert dev.decrypt(b"\x00\x00\x00\x00\x00\x00\x00\x00").shape == (0, plan.c, N)
