@@ -421,6 +421,45 @@ def micro_bench(pkg, steps, warmup):
                 except Exception as exc:
                     line["cpu_baseline"] = {"unavailable": str(exc)[:120]}
             lines.append(line)
+    # the client on the GPU (ipr_client_*) at the 1M plan: one payload of 2 sub-queries built
+    # and serialized (host bytes out), and one 2 x 11-result response decrypted (host bytes in)
+    plan = pkg.plan_from_shape(RECORDS, KEY, VALUE, BUCKETS, DIM0)
+    resp_len = 4 + 2 * (4 + plan.c * 12288) + 4
+    rb = bytearray(np.random.default_rng(5).integers(0, 256, resp_len, dtype=np.uint8).tobytes())
+    rb[0:4] = (2).to_bytes(4, "little")
+    for k in range(2):
+        o = 4 + k * (4 + plan.c * 12288)
+        rb[o:o + 4] = (plan.c * 12288).to_bytes(4, "little")
+    rb[-4:] = bytes(4)
+    resp = bytes(rb)
+    buckets = [12345, 1_500_000]
+    with pkg.KeywordClient(plan, bytes(range(32))) as cl:
+        for name, fn in (("query generation", lambda i: cl.query(buckets, nonce=i)),
+                         ("response decryption", lambda i: cl.decrypt(resp))):
+            for i in range(max(warmup, 1)):
+                fn(i)
+            t0 = time.perf_counter()
+            for i in range(steps):
+                fn(1000 + i)
+            ms = (time.perf_counter() - t0) * 1000.0 / steps
+            line = {"metric": f"client {name} on the GPU (1M plan, 2 sub-queries, host bytes)",
+                    "value": 1000.0 / ms, "unit": "payloads/s", "ms_per_call": ms}
+            try:
+                sys.path.insert(0, os.path.join(ROOT, "oracle"))
+                import pir_client as pcl
+                model = pcl.SeededClient(plan.db_rows, plan.interp, plan.c, plan.num_items // plan.db_rows, 608,
+                                         seed=bytes(range(32)))
+                t0 = time.perf_counter()
+                if name == "query generation":
+                    model.query(buckets, nonce=1)
+                else:
+                    model.decrypt(resp)
+                cpu_s = time.perf_counter() - t0
+                line["cpu_baseline"] = {"value": 1.0 / cpu_s, "unit": "payloads/s", "cores": 1, "kind": "port",
+                                        "sample": f"1 payload, oracle model of the client ({cpu_s * 1000:.1f} ms)"}
+            except Exception as exc:
+                line["cpu_baseline"] = {"unavailable": str(exc)[:120]}
+            lines.append(line)
     for ln in lines:
         print(json.dumps(ln))
     return 0
