@@ -283,7 +283,8 @@ int ipr_state_file_plan(const char *path, ipr_plan *out);
  * 256 coefficients +1 and 256 -1, gen_ternary_mat, client/base.rs:126-139) and all noise are
  * drawn deterministically from `seed` with ChaCha20: key placement from stream 1, the noise
  * of a query from stream 2 + nonce (centered binomial, eta = 82: sigma 6.40, the width of the
- * reference's discrete Gaussian).  A nonce must not be reused under one seed. */
+ * reference's discrete Gaussian).  A nonce must not be reused under one seed.  A client
+ * handle keeps per-call scratch: use it from one thread at a time (one handle per thread). */
 typedef struct ipr_client ipr_client;
 
 /* KeywordClient::setup_from_public_params (keyword.rs:60-115) for `plan` */
