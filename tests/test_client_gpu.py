@@ -120,3 +120,27 @@ def test_device_client_refuses_bad_input(pkg):
             dev.decrypt(b"\x01\x00\x00\x00\x05\x00\x00\x00abcde")  # a result of the wrong length
         assert e.value.status == -5
         assert dev.decrypt(b"\x00\x00\x00\x00\x00\x00\x00\x00").shape == (0, plan.c, N)
+
+
+@pytest.mark.gpu
+def test_device_client_zero_queries_and_stash(pkg, orc):
+    """a payload of keys only (0 sub-queries) equals the model's and gets an empty answer;
+    a response with a stash block decrypts its results and leaves the stash to the caller"""
+    plan = _small_plan(pkg)
+    per = plan.num_items // plan.db_rows
+    raw = np.random.default_rng(4).integers(0, 65535, plan.db_rows * plan.db_cols, dtype=np.uint16)
+    stash = [bytes([i]) * plan.entry_size for i in (1, 2, 3)]
+    model = pc.SeededClient(plan.db_rows, plan.interp, plan.c, per, 608, seed=SEED)
+    with pkg.KeywordServer.setup(plan, raw, raw=True, stash=stash) as srv, pkg.KeywordClient(plan, SEED) as dev:
+        q0 = dev.query([], nonce=11)
+        assert q0 == model.query([], nonce=11)[0] and len(q0) == pkg.query_bytes(plan.db_rows, 0)
+        r0 = srv.respond_to_serialized_query(q0)
+        assert pkg.deserialize_keyword_response(r0).responses == []
+        assert dev.decrypt(r0).shape == (0, plan.c, N)
+        b = 321 * per + 4
+        resp = srv.respond_to_serialized_query(dev.query([b], nonce=12))
+    assert pkg.deserialize_keyword_response(resp).stash_entries == stash
+    with pkg.KeywordClient(plan, SEED) as dev2:  # the same seed decrypts the same key's answers
+        pt = dev2.decrypt(resp)
+    row, _, sub = model.target(b)
+    np.testing.assert_array_equal(pt[0][0], raw.reshape(plan.db_cols, plan.db_rows)[sub * N:(sub + 1) * N, row])
