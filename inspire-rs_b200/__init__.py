@@ -590,16 +590,25 @@ class KeywordService:
         _check(_svc_submit_batch(self._h, db, n, ptrs, lens, out), "service_submit_batch")
         return list(out)
 
+    def _buffer(self, cap: int):
+        """a per-thread result buffer, reused across calls (no allocation or zeroing per result)"""
+        import threading
+        tl = self.__dict__.setdefault("_tls", threading.local())
+        buf = getattr(tl, "buf", None)
+        if buf is None or len(buf) < cap:
+            buf = tl.buf = (ctypes.c_uint8 * cap)()
+        return buf
+
     def _collect(self, fn, ticket, *extra):
         cap = self._cap
-        out = (ctypes.c_uint8 * cap)()
+        out = self._buffer(cap)
         n = _sz()
         st = fn(self._h, ticket, *extra, ctypes.cast(out, _u8p), cap, ctypes.byref(n))
         if st == IPR_PENDING:
             return None
         if st == -6 and n.value > cap:  # a larger payload: the result is kept for the retry
             cap = n.value
-            out = (ctypes.c_uint8 * cap)()
+            out = self._buffer(cap)
             st = _svc_poll(self._h, ticket, ctypes.cast(out, _u8p), cap, ctypes.byref(n))
         _check(st, "service_result")
         return ctypes.string_at(out, n.value)
