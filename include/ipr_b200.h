@@ -303,6 +303,11 @@ int ipr_client_decrypt(ipr_client *c, const uint8_t *response, size_t len, uint1
 int ipr_client_secret_key(const ipr_client *c, int8_t *out);
 void ipr_client_destroy(ipr_client *c);
 
+/* Fault injection for tests (process-wide): the next `after` device allocations of servers
+ * succeed and the one after fails as an out-of-memory would (IPR_E_OOM from the call that
+ * needed it); the hook then switches itself off.  after < 0 switches it off at once. */
+int ipr_debug_fail_allocation(int64_t after);
+
 /* Failure detection self-test: launches one CTA that waits, with the bounded wait every
  * tensor-core kernel of this library uses on its mbarriers, on a barrier nothing arrives
  * on.  The wait gives up after `budget` polls; the call returns IPR_E_TIMEOUT (the status a

@@ -179,6 +179,15 @@ class Plan:
         return query_bytes(self.db_rows, 2)
 
 
+_fail_alloc = _sig("ipr_debug_fail_allocation", _i32, ctypes.c_int64)
+
+
+def fail_allocation_after(n: int):
+    """test hook: the next n server device allocations succeed, the one after fails (IPR_E_OOM);
+    n < 0 switches the hook off"""
+    _check(_fail_alloc(n), "ipr_debug_fail_allocation")
+
+
 def selftest_bounded_wait(budget: int = 1 << 16, device: int = 0) -> int:
     """ipr_selftest_bounded_wait: the status of a bounded mbarrier wait that nobody
     satisfies (IPR_E_TIMEOUT = -4 when the failure is detected)"""

@@ -11,6 +11,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -433,6 +434,18 @@ int respond_locked(ipr_server* s, const uint8_t* query, size_t len, uint8_t* out
 
 }  // namespace
 
+namespace ipr {
+namespace {
+std::atomic<int64_t> g_alloc_fault{-1};  // allocations left before the injected failure; -1 = off
+}
+bool alloc_fault_due() {
+    int64_t v = g_alloc_fault.load(std::memory_order_relaxed);
+    while (v >= 0 && !g_alloc_fault.compare_exchange_weak(v, v - 1)) {
+    }
+    return v == 0;
+}
+}  // namespace ipr
+
 int ipr_server::alloc_failed(size_t bytes, cudaError_t e) const {
     return fail(IPR_E_OOM, "cudaMalloc(%zu bytes) failed on device %d: %s", bytes, device, cudaGetErrorString(e));
 }
@@ -600,6 +613,7 @@ static int create_server(int device, const ipr_plan* plan, const ipr_server_data
                          ipr_server** out);
 
 int ipr_server_create(int device, const ipr_plan* plan, const ipr_server_data* data, ipr_server** out) {
+    ipr::NvtxRange nvtx_range("ipr_server_create");
     return create_server(device, plan, data, false, out);
 }
 
@@ -635,8 +649,14 @@ static int create_server(int device, const ipr_plan* plan, const ipr_server_data
     return IPR_OK;
 }
 
+int ipr_debug_fail_allocation(int64_t after) {
+    ipr::g_alloc_fault.store(after < 0 ? -1 : after);
+    return IPR_OK;
+}
+
 int ipr_server_setup(int device, const ipr_plan* plan, const ipr_server_data* data, int db_is_raw,
                      ipr_server** out) {
+    ipr::NvtxRange nvtx_range("ipr_server_setup");
     if (!out || !data || !data->db) return fail(IPR_E_ARGS, "null argument");
     if (data->stash_count && (!data->stash || !data->stash_entry_bytes)) return fail(IPR_E_ARGS, "bad stash");
     *out = nullptr;
@@ -666,6 +686,7 @@ int ipr_server_setup(int device, const ipr_plan* plan, const ipr_server_data* da
 }
 
 int ipr_server_create_synthetic(int device, const ipr_plan* plan, uint64_t seed, ipr_server** out) {
+    ipr::NvtxRange nvtx_range("ipr_server_create_synthetic");
     if (!out) return fail(IPR_E_ARGS, "null output");
     *out = nullptr;
     auto* s = new ipr_server();
@@ -755,6 +776,7 @@ int ipr_server_plan(const ipr_server* s, ipr_plan* out) {
 }
 
 int ipr_server_respond(ipr_server* s, const uint8_t* query, size_t len, uint8_t* out, size_t cap, size_t* out_len) {
+    ipr::NvtxRange nvtx_range("ipr_server_respond");
     if (!s) return fail(IPR_E_ARGS, "null server");
     std::lock_guard<std::mutex> lk(s->mu);
     return respond_locked(s, query, len, out, cap, out_len);
@@ -762,6 +784,7 @@ int ipr_server_respond(ipr_server* s, const uint8_t* query, size_t len, uint8_t*
 
 int ipr_server_respond_batch(ipr_server* s, int n, const uint8_t* const* queries, const size_t* lens,
                              uint8_t* const* outs, const size_t* caps, size_t* out_lens, int* statuses) {
+    ipr::NvtxRange nvtx_range("ipr_server_respond_batch");
     if (!s || n < 0 || (n && (!queries || !lens || !outs || !caps))) return fail(IPR_E_ARGS, "null argument");
     std::lock_guard<std::mutex> lk(s->mu);
     const uint64_t qb = ipr::query_bytes(s->plan.db_rows, 2), rb = s->response_bytes(2);
@@ -816,6 +839,7 @@ int ipr_server_prepare_batch(ipr_server* s, int max_payloads) {
 }
 
 int ipr_server_respond_batch_device(ipr_server* s, int n, const uint8_t* d_queries, uint8_t* d_out) {
+    ipr::NvtxRange nvtx_range("ipr_server_respond_batch_device");
     if (!s || !d_queries || !d_out || n < 1 || n > kMaxBatch) return fail(IPR_E_ARGS, "bad argument (1 <= n <= 64)");
     std::lock_guard<std::mutex> lk(s->mu);
     CU(cudaSetDevice(s->device));
@@ -827,6 +851,7 @@ int ipr_server_respond_batch_device(ipr_server* s, int n, const uint8_t* d_queri
 
 int ipr_server_respond_device(ipr_server* s, const uint8_t* d_query, size_t len, uint8_t* d_out, size_t cap,
                               size_t* out_len) {
+    ipr::NvtxRange nvtx_range("ipr_server_respond_device");
     if (!s || !d_query || !d_out) return fail(IPR_E_ARGS, "null argument");
     std::lock_guard<std::mutex> lk(s->mu);
     CU(cudaSetDevice(s->device));

@@ -12,6 +12,22 @@
 #include "host_math.hpp"
 #include "ipr_b200.h"
 
+#include <nvtx3/nvToolsExt.h>
+
+namespace ipr {
+// a named NVTX range over a host API call (visible in Nsight Systems; inert without a tool)
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
+// allocation-failure injection (ipr_debug_fail_allocation): true for the one device allocation
+// of a server that the armed countdown reaches, which then fails as an out-of-memory would
+bool alloc_fault_due();
+}
+
 namespace ipr {
 void set_last_error(const char* msg);
 }
@@ -75,6 +91,7 @@ struct ipr_server {
     int alloc_failed(size_t bytes, cudaError_t e) const;  // records the message, returns IPR_E_OOM
     template <typename T>
     int alloc(T** p, size_t bytes) {
+        if (ipr::alloc_fault_due()) return alloc_failed(bytes, cudaErrorMemoryAllocation);  // injected
         void* v = nullptr;
         cudaError_t e = cudaMalloc(&v, bytes ? bytes : 16);
         if (e != cudaSuccess)

@@ -165,6 +165,7 @@ void answer_single(ipr_service* v, Lane& ln, Request* r) {
 
 // stage and enqueue one batch into the lane's next free slot
 void launch_batch(ipr_service* v, Lane& ln, std::vector<Request*>& batch) {
+    ipr::NvtxRange nvtx_range("ipr_service batch launch");
     Slot& sl = ln.slot[(ln.head + ln.nbusy) & 1];
     const int B = (int)batch.size();
     for (int b = 0; b < B; b++) std::memcpy(sl.h_q + (size_t)b * ln.qb, batch[b]->query.data(), ln.qb);

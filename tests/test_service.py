@@ -173,3 +173,49 @@ def test_submit_many_answers_each_payload_like_alone(pkg, orc):
             svc.close()
     for q, g in zip(qs, got):
         assert g == orc.respond(sdb, q)
+
+
+@pytest.mark.gpu
+def test_injected_allocation_failures_are_clean(pkg, orc):
+    """every device allocation of server creation, a first respond and batch preparation fails
+    once in turn (ipr_debug_fail_allocation): the call that needed it returns IPR_E_OOM, the
+    server stays usable and bit-exact, and closing everything returns the device memory"""
+    import torch
+    plan = pkg.plan_from_shape(10_000, 32, 1184)
+    sdb = orc.SynthDB(plan.db_rows, plan.instances, plan.interp, plan.c, seed=3)
+    q = orc.synth_query(77, plan.db_rows, 2)
+    want = orc.respond(sdb, q)
+    with pkg.KeywordServer.synthetic(plan, seed=3) as warm:  # first-use tables and context
+        assert warm.respond_to_serialized_query(q) == want
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    fired = 0
+    for n in range(200):
+        pkg.fail_allocation_after(n)
+        srv = None
+        try:
+            srv = pkg.KeywordServer.synthetic(plan, seed=3)
+            for step in (lambda: srv.respond_to_serialized_query(q), lambda: srv.prepare_batch(4),
+                         lambda: srv.respond_batch([q, q])):
+                try:
+                    step()
+                except pkg.IprError as e:
+                    assert e.status == -2, e  # IPR_E_OOM
+                    fired += 1
+        except pkg.IprError as e:
+            assert e.status == -2, e
+            fired += 1
+            continue
+        finally:
+            pkg.fail_allocation_after(-1)
+        try:
+            # after the failure, the same server answers bit-exactly
+            assert srv.respond_to_serialized_query(q) == want
+            assert srv.respond_batch([q, q]) == [want, want]
+        finally:
+            srv.close()
+        if fired < n + 1 and n > 0:  # the countdown outlived every allocation: all points covered
+            break
+    assert fired >= 10
+    torch.cuda.synchronize()
+    assert abs(torch.cuda.mem_get_info()[0] - free0) < (64 << 20)
