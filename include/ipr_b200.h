@@ -299,6 +299,13 @@ int ipr_client_query(ipr_client *c, uint64_t nonce, unsigned n, const uint64_t *
  * *count = responses x c x 2048.  The stash block is not read. */
 int ipr_client_decrypt(ipr_client *c, const uint8_t *response, size_t len, uint16_t *values, size_t cap,
                        size_t *count);
+/* CuckooHash::all_positions (src/pir/keyword/cuckoo.rs:105-131): the num_hashes bucket
+ * positions of a keyword under the server's 16-byte cuckoo seed.  Hash i is SipHash-2-4
+ * with keys (seed[0..8] LE ^ i, seed[8..16] LE ^ (i << 32)) mod num_buckets; the all-zero
+ * seed is the identity layout (last 8 key bytes big-endian, hash 0 into the first half of the
+ * table, hash 1 into the second).  Host only. */
+int ipr_cuckoo_positions(const uint8_t seed[16], uint64_t num_buckets, unsigned num_hashes, const uint8_t *key,
+                         size_t key_len, uint64_t *out);
 /* the client's secret key, 2048 coefficients in {-1, 0, 1} (for tests) */
 int ipr_client_secret_key(const ipr_client *c, int8_t *out);
 void ipr_client_destroy(ipr_client *c);

@@ -673,6 +673,16 @@ _cl_decrypt = _sig("ipr_client_decrypt", _i32, _vp, _u8p, _sz, ctypes.POINTER(ct
                    ctypes.POINTER(_sz))
 _cl_key = _sig("ipr_client_secret_key", _i32, _vp, ctypes.POINTER(ctypes.c_int8))
 _cl_destroy = _sig("ipr_client_destroy", None, _vp)
+_cuckoo = _sig("ipr_cuckoo_positions", _i32, ctypes.c_char_p, _u64, ctypes.c_uint, ctypes.c_char_p, _sz,
+               ctypes.POINTER(_u64))
+
+
+def cuckoo_positions(seed: bytes, num_buckets: int, num_hashes: int, key: bytes) -> List[int]:
+    """CuckooHash::all_positions (cuckoo.rs:105-131): the bucket positions of a keyword"""
+    out = (_u64 * max(num_hashes, 1))()
+    _check(_cuckoo(bytes(seed)[:16].ljust(16, b"\0"), num_buckets, num_hashes, bytes(key), len(key), out),
+           "ipr_cuckoo_positions")
+    return list(out)[:num_hashes]
 
 
 class KeywordClient:
@@ -684,6 +694,7 @@ class KeywordClient:
         if len(seed) != 32:
             raise ValueError("seed must be 32 bytes")
         self.plan, self.device, self._nonce = plan, device, 0
+        self.keyword = None  # the keyword layout, known when built from the public parameters
         self.per = plan.num_items // plan.db_rows
         self.item_elems = plan.item_size_bits // 16
         h = _vp()
@@ -714,6 +725,58 @@ class KeywordClient:
         _check(_cl_decrypt(self._h, buf, len(response), vals.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)),
                            vals.size, ctypes.byref(n)), "ipr_client_decrypt")
         return vals.reshape(-1, self.plan.c, POLY_LEN)
+
+    @classmethod
+    def from_public_params(cls, params: dict, seed: bytes, device: int = 0) -> "KeywordClient":
+        """KeywordClient::setup_from_public_params (keyword.rs:60-115): the plan from the
+        server's public parameters; keeps the keyword layout for query_key / extract_key"""
+        kw = params.get("keyword_pir")
+        if not kw:
+            raise ValueError("server is not in keyword PIR mode")
+        if kw["key_size"] == 0 or kw["value_size"] == 0:
+            raise ValueError("server keyword and value sizes must be non-zero")
+        if kw["entry_size"] < kw["key_size"] + kw["value_size"]:
+            raise ValueError("server entry size is smaller than key_size + value_size")
+        plan = plan_from_shape(max(1, min(kw.get("num_records", 0) or 1, params["num_items"])), kw["key_size"],
+                               kw["value_size"], params["num_items"], params["dim0"])
+        if plan.item_size_bits != params["item_size_bits"]:
+            raise ValueError("public parameters do not match the scheme's shape")
+        c = cls(plan, seed, device)
+        c.keyword = kw
+        return c
+
+    def positions(self, key: bytes) -> List[int]:
+        """positions (keyword.rs:129-137)"""
+        kw = self.keyword
+        if kw is None:
+            raise ValueError("no keyword layout: build the client with from_public_params")
+        if len(key) != kw["key_size"]:
+            raise ValueError(f"expected {kw['key_size']} keyword bytes, got {len(key)}")
+        return cuckoo_positions(bytes(kw["cuckoo_seed"]), self.plan.num_items, kw["num_hashes"], key)
+
+    def query_key(self, key: bytes):
+        """query (keyword.rs:193-200) + serialize_query: (positions, payload bytes)"""
+        pos = self.positions(key)
+        return pos, self.query(pos)
+
+    def extract_key(self, key: bytes, positions: Sequence[int], response: bytes) -> Optional[bytes]:
+        """extract_from_serialized_response (keyword.rs:232-300): the value stored under key, from
+        the decrypted entry of one of its positions or from the stash, else None"""
+        kw = self.keyword
+        if kw is None:
+            raise ValueError("no keyword layout: build the client with from_public_params")
+        if len(key) != kw["key_size"]:
+            return None
+        ks, vs, es = kw["key_size"], kw["value_size"], kw["entry_size"]
+        pts = self.decrypt(response)
+        for pos, pt in zip(positions, pts):
+            entry = self.extract(pos, pt)
+            if entry is not None and len(entry) >= es and entry[:ks] == bytes(key):
+                return entry[ks:ks + vs]
+        for entry in deserialize_keyword_response(response).stash_entries:
+            if len(entry) >= es and entry[:ks] == bytes(key):
+                return entry[ks:ks + vs]
+        return None
 
     def extract(self, bucket: int, plaintext) -> Optional[bytes]:
         """the entry bytes of `bucket` from its sub-query's plaintexts (keyword.rs:246-257);

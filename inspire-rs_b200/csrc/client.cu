@@ -569,6 +569,62 @@ int ipr_client_decrypt(ipr_client* c, const uint8_t* response, size_t len, uint1
     return IPR_OK;
 }
 
+// SipHash-2-4 (Aumasson and Bernstein) of `len` bytes under keys (k0, k1)
+static uint64_t siphash24(uint64_t k0, uint64_t k1, const uint8_t* m, size_t len) {
+    uint64_t v0 = k0 ^ 0x736f6d6570736575ull, v1 = k1 ^ 0x646f72616e646f6dull;
+    uint64_t v2 = k0 ^ 0x6c7967656e657261ull, v3 = k1 ^ 0x7465646279746573ull;
+    auto rotl = [](uint64_t x, int b) { return (x << b) | (x >> (64 - b)); };
+    auto round = [&]() {
+        v0 += v1; v1 = rotl(v1, 13); v1 ^= v0; v0 = rotl(v0, 32);
+        v2 += v3; v3 = rotl(v3, 16); v3 ^= v2;
+        v0 += v3; v3 = rotl(v3, 21); v3 ^= v0;
+        v2 += v1; v1 = rotl(v1, 17); v1 ^= v2; v2 = rotl(v2, 32);
+    };
+    size_t i = 0;
+    for (; i + 8 <= len; i += 8) {
+        uint64_t w = 0;
+        for (int b = 0; b < 8; b++) w |= (uint64_t)m[i + b] << (8 * b);
+        v3 ^= w;
+        round();
+        round();
+        v0 ^= w;
+    }
+    uint64_t last = (uint64_t)(len & 0xff) << 56;
+    for (size_t b = 0; i + b < len; b++) last |= (uint64_t)m[i + b] << (8 * b);
+    v3 ^= last;
+    round();
+    round();
+    v0 ^= last;
+    v2 ^= 0xff;
+    for (int r = 0; r < 4; r++) round();
+    return v0 ^ v1 ^ v2 ^ v3;
+}
+
+int ipr_cuckoo_positions(const uint8_t seed[16], uint64_t num_buckets, unsigned num_hashes, const uint8_t* key,
+                         size_t key_len, uint64_t* out) {
+    if (!seed || !out || (key_len && !key) || num_buckets < 2 || num_hashes < 1 || num_hashes > 255)
+        return fail(IPR_E_ARGS, "bad argument");
+    bool trivial = true;
+    for (int i = 0; i < 16; i++) trivial = trivial && seed[i] == 0;
+    uint64_t s0 = 0, s1 = 0;
+    for (int b = 0; b < 8; b++) {
+        s0 |= (uint64_t)seed[b] << (8 * b);
+        s1 |= (uint64_t)seed[8 + b] << (8 * b);
+    }
+    for (unsigned h = 0; h < num_hashes; h++) {
+        if (trivial) {  // identity: the last 8 key bytes, big-endian, into one half of the table
+            uint64_t idx = 0;
+            const size_t n = key_len < 8 ? key_len : 8, start = key_len - n;
+            for (size_t b = 0; b < n; b++) idx |= (uint64_t)key[start + b] << (8 * (7 - b));
+            const uint64_t half = num_buckets / 2;
+            out[h] = h == 0 ? idx % half : half + idx % half;
+        } else {
+            out[h] = siphash24(s0 ^ h, s1 ^ ((uint64_t)h << 32), key, key_len) % num_buckets;
+        }
+    }
+    return IPR_OK;
+}
+
 int ipr_client_secret_key(const ipr_client* c, int8_t* out) {
     if (!c || !out) return fail(IPR_E_ARGS, "null argument");
     std::memcpy(out, c->s, N);

@@ -289,3 +289,43 @@ class SeededClient(TestClient):
         out = super().query(buckets)
         assert self._next == npolys
         return out
+
+
+# --- cuckoo positions (src/pir/keyword/cuckoo.rs:105-131) -------------------------------------
+_M64 = (1 << 64) - 1
+
+
+def siphash24(k0: int, k1: int, msg: bytes) -> int:
+    """SipHash-2-4 (Aumasson and Bernstein, 2012) of msg under the 64-bit keys k0, k1"""
+    def rotl(x, b):
+        return ((x << b) | (x >> (64 - b))) & _M64
+    v = [k0 ^ 0x736f6d6570736575, k1 ^ 0x646f72616e646f6d, k0 ^ 0x6c7967656e657261, k1 ^ 0x7465646279746573]
+
+    def rnd():
+        v[0] = (v[0] + v[1]) & _M64; v[1] = rotl(v[1], 13) ^ v[0]; v[0] = rotl(v[0], 32)
+        v[2] = (v[2] + v[3]) & _M64; v[3] = rotl(v[3], 16) ^ v[2]
+        v[0] = (v[0] + v[3]) & _M64; v[3] = rotl(v[3], 21) ^ v[0]
+        v[2] = (v[2] + v[1]) & _M64; v[1] = rotl(v[1], 17) ^ v[2]; v[2] = rotl(v[2], 32)
+    full = len(msg) // 8 * 8
+    blocks = [int.from_bytes(msg[i:i + 8], "little") for i in range(0, full, 8)]
+    blocks.append(int.from_bytes(msg[full:], "little") | ((len(msg) & 0xFF) << 56))
+    for m in blocks:
+        v[3] ^= m
+        rnd()
+        rnd()
+        v[0] ^= m
+    v[2] ^= 0xFF
+    for _ in range(4):
+        rnd()
+    return v[0] ^ v[1] ^ v[2] ^ v[3]
+
+
+def cuckoo_positions(seed: bytes, num_buckets: int, num_hashes: int, key: bytes):
+    """CuckooHash::all_positions: SipHash-2-4 with keys (seed[..8] ^ i, seed[8..] ^ (i << 32)) mod
+    num_buckets; the all-zero seed is the identity layout (cuckoo.rs:105-121)"""
+    if bytes(seed) == bytes(16):
+        idx = int.from_bytes(key[-8:].ljust(8, b"\0") if len(key) < 8 else key[-8:], "big")
+        half = num_buckets // 2
+        return [idx % half if i == 0 else half + idx % half for i in range(num_hashes)]
+    s0, s1 = int.from_bytes(seed[:8], "little"), int.from_bytes(seed[8:16], "little")
+    return [siphash24(s0 ^ i, s1 ^ (i << 32), bytes(key)) % num_buckets for i in range(num_hashes)]

@@ -144,3 +144,75 @@ def test_device_client_zero_queries_and_stash(pkg, orc):
         pt = dev2.decrypt(resp)
     row, _, sub = model.target(b)
     np.testing.assert_array_equal(pt[0][0], raw.reshape(plan.db_cols, plan.db_rows)[sub * N:(sub + 1) * N, row])
+
+
+# --- keyword lookup: cuckoo positions, query by ID, extract the value --------------------------
+def test_siphash_paper_vectors():
+    """SipHash-2-4 of the paper (Aumasson, Bernstein 2012), key 00..0f: the empty message and the
+    15-byte message 00..0e"""
+    k0, k1 = int.from_bytes(bytes(range(8)), "little"), int.from_bytes(bytes(range(8, 16)), "little")
+    assert pc.siphash24(k0, k1, b"") == 0x726FDB47DD0E0E31
+    assert pc.siphash24(k0, k1, bytes(range(15))) == 0xA129CA6149BE45E5
+
+
+def test_library_positions_equal_oracle(pkg):
+    rng = np.random.default_rng(8)
+    for seed in (bytes(16), bytes(range(16)), bytes(rng.integers(0, 256, 16, dtype=np.uint8))):
+        for klen in (0, 5, 8, 16, 32, 33):
+            for _ in range(4):
+                key = bytes(rng.integers(0, 256, klen, dtype=np.uint8))
+                for nb in (2, 32768, 2_097_152):
+                    assert pkg.cuckoo_positions(seed, nb, 2, key) == pc.cuckoo_positions(seed, nb, 2, key)
+    assert pkg.cuckoo_positions(bytes(range(16)), 1000, 3, b"abc") == pc.cuckoo_positions(bytes(range(16)), 1000, 3,
+                                                                                         b"abc")
+
+
+def _no_ffff(b):
+    a = np.frombuffer(bytearray(b), dtype=np.uint8).copy()
+    pairs = a[:len(a) // 2 * 2].reshape(-1, 2)
+    pairs[(pairs[:, 0] == 255) & (pairs[:, 1] == 255), 1] = 254  # 0xFFFF reads back as 0 mod 65535
+    return a.tobytes()
+
+
+@pytest.mark.gpu
+def test_keyword_lookup_end_to_end(pkg, orc):
+    """the reference's end-to-end property (tests/e2e_mlkem.rs: the client retrieves the right
+    key): records placed in a cuckoo layout under a non-trivial seed (or in the stash), the
+    server set up on the device, and a device client that queries by 32-byte ID and extracts
+    the 1184-byte value, or None for an absent ID"""
+    plan = pkg.plan_from_shape(10_000, 32, 1184)
+    per, es = plan.num_items // plan.db_rows, plan.entry_size
+    cseed = bytes(range(100, 116))
+    rng = np.random.default_rng(2026)
+    entries = np.zeros((plan.num_items, es), dtype=np.uint8)
+    occ = np.zeros(plan.num_items, dtype=np.uint8)
+    placed, stash = {}, []
+
+    def inside(b):  # the entry lies in one DB polynomial, so one result holds all of it
+        return (b % per) * 608 % N + 608 <= N
+    while len(placed) < 300:
+        key, value = _no_ffff(rng.bytes(32)), _no_ffff(rng.bytes(1184))
+        pos = pc.cuckoo_positions(cseed, plan.num_items, 2, key)
+        free = [p for p in pos if not occ[p] and inside(p)]
+        if free:
+            entries[free[0], :32], entries[free[0], 32:1216] = np.frombuffer(key, np.uint8), np.frombuffer(value,
+                                                                                                           np.uint8)
+            occ[free[0]] = 1
+            placed[key] = value
+        elif len(stash) < 3:
+            stash.append(key + value + bytes(es - 1216))
+            placed[key] = value
+    raw = orc.raw_db(entries, occ, es, plan.db_rows, plan.db_cols, per)
+    with pkg.KeywordServer.setup(plan, raw, raw=True, stash=stash, key_size=32, value_size=1184,
+                                 num_records=len(placed), cuckoo_seed=cseed) as srv:
+        pp = srv.public_params()
+        assert bytes(pp["keyword_pir"]["cuckoo_seed"]) == cseed
+        with pkg.KeywordClient.from_public_params(pp, bytes([9]) * 32) as cl:
+            keys = list(placed)[:6] + [s[:32] for s in stash]
+            for key in keys:
+                pos, q = cl.query_key(key)
+                assert pos == pc.cuckoo_positions(cseed, plan.num_items, 2, key)
+                assert cl.extract_key(key, pos, srv.respond_to_serialized_query(q)) == placed[key]
+            absent = _no_ffff(rng.bytes(32))
+            pos, q = cl.query_key(absent)
+            assert cl.extract_key(absent, pos, srv.respond_to_serialized_query(q)) is None
