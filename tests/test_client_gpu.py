@@ -216,3 +216,15 @@ def test_keyword_lookup_end_to_end(pkg, orc):
             absent = _no_ffff(rng.bytes(32))
             pos, q = cl.query_key(absent)
             assert cl.extract_key(absent, pos, srv.respond_to_serialized_query(q)) is None
+
+
+def test_public_params_are_validated_before_any_device_work(pkg):
+    """setup_from_public_params (keyword.rs:64-79): keyword mode, non-zero sizes, entry size"""
+    base = {"num_items": 32768, "item_size_bits": 9728, "dim0": 2048,
+            "keyword_pir": {"cuckoo_seed": list(range(16)), "num_hashes": 2, "key_size": 32, "value_size": 1184,
+                            "entry_size": 1216, "num_records": 10000}}
+    for bad in ({"keyword_pir": None}, {"keyword_pir": dict(base["keyword_pir"], key_size=0)},
+                {"keyword_pir": dict(base["keyword_pir"], value_size=0)},
+                {"keyword_pir": dict(base["keyword_pir"], entry_size=1000)}, {"item_size_bits": 4096}):
+        with pytest.raises(ValueError):
+            pkg.KeywordClient.from_public_params(dict(base, **bad), bytes(32))
