@@ -905,7 +905,7 @@ int ipr_synth_query(uint64_t seed, uint64_t db_rows, unsigned nq, uint8_t *out, 
     return IPR_OK;
 }
 
-/* ---- setup-time DB layout and encode -------------------------------------- */
+/* ---- setup-time DB layout and encode ----------------------------------------------------- */
 
 /* KeywordCuckooTable::to_raw_db (src/pir/keyword/cuckoo.rs:314-353): raw[(item*ise + j) *
  * db_rows + row] = big-endian u16 of entry bytes (2j, 2j+1) of bucket row*per + item, zero

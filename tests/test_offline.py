@@ -1,4 +1,4 @@
-"""Offline precomputation (SURVEY f1): PirServer::perform_offline_precomputation_simplepir
+"""Offline precomputation: PirServer::perform_offline_precomputation_simplepir
 (src/pir/server/engine.rs:677-1042) -> a_hat, bold_t, bold_t_bar, bold_t_hat.
 
 CPU: the device's algorithm — the packing sums of full_packing_with_preprocessing_offline
