@@ -562,8 +562,11 @@ def main():
     d_batches = [torch.frombuffer(bytearray(b"".join(payloads[k * B:(k + 1) * B])), dtype=torch.uint8).to(dev)
                  for k in range(2)]
     d_out = torch.empty(B * rbytes, dtype=torch.uint8, device=dev)
+    tune = None
     if B > 1:
         srv.prepare_batch(min(B, PASS))
+        # the autotuner times the exact candidate configurations of the batch path and keeps the fastest
+        tune = srv.autotune(min(B, PASS), 5)
 
     def run_device(i):
         d = d_batches[i % 2]
@@ -715,6 +718,7 @@ def main():
                        "records": args.records, "buckets": plan.num_items, "dim0": plan.dim0, "db_rows": plan.db_rows,
                        "db_cols": plan.db_cols, "instances": plan.instances, "interp": plan.interp, "c": plan.c,
                        "batch_payloads": B, "parallelism": f"replica x{world}",
+                       "autotune": ({"chosen": tune["chosen"], "candidates": tune["candidates"]} if tune else None),
                        "l2": "inputs larger than L2 (packing stream of %.1f GB + DB of %.2f GB per step)" % (
                            pack_bytes / 1e9, plan.db_rows * plan.db_cols * 2 / 1e9)},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": B * qbytes, "d2h_bytes_per_step": B * rbytes,

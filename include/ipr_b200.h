@@ -194,6 +194,21 @@ int ipr_server_set_profiling(ipr_server *srv, int on);
  * two accumulators of a tile are double-buffered in TMEM. */
 #define IPR_OPT_GEMV_TILE 4
 int ipr_server_set_option(ipr_server *srv, int option, int64_t value);
+
+/* Autotuner for the batch path: runs `reps` timed batches of `payloads` synthetic payloads
+ * (after one warm-up each) under every candidate of IPR_OPT_PACK_CTA_PAIR {0, 1} x
+ * IPR_OPT_GEMV_TILE {256, 128}, timed with CUDA events on the server's stream, and
+ * leaves the server set to the fastest.  Every candidate gives identical responses.  On an
+ * error the options are restored. */
+#define IPR_AUTOTUNE_MAX 8
+typedef struct {
+    int candidates;                    /* how many were timed */
+    int pack_cta_pair[IPR_AUTOTUNE_MAX];
+    int gemv_tile[IPR_AUTOTUNE_MAX];
+    double ms[IPR_AUTOTUNE_MAX];       /* mean device time per batch */
+    int chosen;                        /* index of the candidate now in force */
+} ipr_autotune_result;
+int ipr_server_autotune(ipr_server *srv, int payloads, int reps, ipr_autotune_result *out);
 int ipr_server_stage_times(ipr_server *srv, double *ms_sum, uint64_t *calls);
 
 const char *ipr_last_error(void);

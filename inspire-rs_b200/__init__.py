@@ -85,6 +85,14 @@ _stage_times = _sig("ipr_server_stage_times", _i32, _vp, ctypes.POINTER(ctypes.c
 _last_error = _sig("ipr_last_error", ctypes.c_char_p)
 
 
+class _AutotuneResult(ctypes.Structure):
+    _fields_ = [("candidates", _i32), ("pack_cta_pair", _i32 * 8), ("gemv_tile", _i32 * 8),
+                ("ms", ctypes.c_double * 8), ("chosen", _i32)]
+
+
+_autotune = _sig("ipr_server_autotune", _i32, _vp, _i32, _i32, ctypes.POINTER(_AutotuneResult))
+
+
 class _ServiceConfig(ctypes.Structure):
     _fields_ = [("max_batch", _i32), ("max_pending", _i32), ("hbm_budget_bytes", _u64)]
 
@@ -499,6 +507,15 @@ class KeywordServer:
         _check(_respond_dev(self._h, _vp(d_query_ptr), length, _vp(d_out_ptr), cap, ctypes.byref(n)),
                "respond_device")
         return n.value
+
+    def autotune(self, payloads: int = 64, reps: int = 3) -> dict:
+        """ipr_server_autotune: time the batch path's candidate configurations on synthetic
+        payloads and keep the fastest (every candidate gives identical responses)"""
+        r = _AutotuneResult()
+        _check(_autotune(self._h, payloads, reps, ctypes.byref(r)), "ipr_server_autotune")
+        cands = [{"pack_cta_pair": r.pack_cta_pair[i], "gemv_tile": r.gemv_tile[i], "ms": r.ms[i]}
+                 for i in range(r.candidates)]
+        return {"candidates": cands, "chosen": cands[r.chosen]}
 
     def stream_handle(self) -> int:
         s = _vp()

@@ -884,6 +884,103 @@ int ipr_server_sync(ipr_server* s) {
     return IPR_OK;
 }
 
+int ipr_server_autotune(ipr_server* s, int payloads, int reps, ipr_autotune_result* out) {
+    ipr::NvtxRange nvtx_range("ipr_server_autotune");
+    if (!s || !out || payloads < 1 || payloads > kMaxBatch || reps < 1 || reps > 100)
+        return fail(IPR_E_ARGS, "bad argument (1 <= payloads <= 64, 1 <= reps <= 100)");
+    std::lock_guard<std::mutex> lk(s->mu);
+    CU(cudaSetDevice(s->device));
+    if (!s->gemv_tc) return fail(IPR_E_STATE, "the batch path needs the tensor-core first dimension");
+    int st = ensure_batch(s, payloads);
+    if (st) return st;
+    // synthetic payloads: a count byte of 2, then 56-bit fields of residues below each prime
+    const uint64_t qb = ipr::query_bytes(s->plan.db_rows, 2);
+    uint64_t x = 0x9E3779B97F4A7C15ull;
+    auto next = [&x]() {
+        uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    };
+    for (int b = 0; b < payloads; b++) {
+        uint8_t* q = s->h_bq + (size_t)b * qb;
+        q[0] = 2;
+        for (uint64_t f = 0; f < (qb - 1) / 7; f++) {
+            const uint64_t v = (next() % 268369921ull) | ((next() % 249561089ull) << 28);
+            for (int k = 0; k < 7; k++) q[1 + 7 * f + k] = (uint8_t)(v >> (8 * k));
+        }
+    }
+    CU(cudaMemcpyAsync(s->d_bq, s->h_bq, (size_t)payloads * qb, cudaMemcpyHostToDevice, s->stream));
+    const int old_pair = s->pack_pair, old_tile = s->g1_tile;
+    static const int pairs[] = {0, 1}, tiles[] = {0, 128};
+    *out = ipr_autotune_result{};
+    for (int pr : pairs)
+        for (int tl : tiles) {
+            out->pack_cta_pair[out->candidates] = pr;
+            out->gemv_tile[out->candidates++] = tl ? tl : 256;
+        }
+    const int nc = out->candidates;
+    // candidates interleaved round-robin, one event pair per timed batch, so that clock drift
+    // under the power cap falls on every candidate alike
+    std::vector<cudaEvent_t> ev((size_t)2 * nc * reps, nullptr);
+    auto cleanup = [&]() {
+        for (cudaEvent_t e : ev)
+            if (e) cudaEventDestroy(e);
+    };
+    for (auto& e : ev)
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            e = nullptr;
+            cleanup();
+            return fail(IPR_E_CUDA, "event");
+        }
+    auto use = [&](int i) {
+        s->pack_pair = out->pack_cta_pair[i];
+        s->g1_tile = out->gemv_tile[i] == 256 ? 0 : out->gemv_tile[i];
+    };
+    cudaMemsetAsync(s->d_err, 0, sizeof(int), s->stream);
+    for (int i = 0; i < nc && !st; i++) {  // one warm-up batch per candidate
+        use(i);
+        st = enqueue_batch(s, payloads, s->d_bq, s->d_bresp, -1);
+    }
+    for (int r = 0; r < reps && !st; r++)
+        for (int i = 0; i < nc && !st; i++) {
+            use(i);
+            cudaEventRecord(ev[(size_t)2 * (r * nc + i)], s->stream);
+            st = enqueue_batch(s, payloads, s->d_bq, s->d_bresp, -1);
+            cudaEventRecord(ev[(size_t)2 * (r * nc + i) + 1], s->stream);
+        }
+    int flag = 0;
+    if (!st && (cudaStreamSynchronize(s->stream) != cudaSuccess ||
+                cudaMemcpy(&flag, s->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess))
+        st = fail(IPR_E_CUDA, "autotune: %s", cudaGetErrorString(cudaGetLastError()));
+    if (!st && flag) st = fail(IPR_E_TIMEOUT, "a device-side wait ran out during autotuning (code %d)", flag);
+    int best = -1;
+    for (int i = 0; i < nc && !st; i++) {
+        double sum = 0;
+        for (int r = 0; r < reps && !st; r++) {
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, ev[(size_t)2 * (r * nc + i)], ev[(size_t)2 * (r * nc + i) + 1]) !=
+                cudaSuccess)
+                st = fail(IPR_E_CUDA, "event timing: %s", cudaGetErrorString(cudaGetLastError()));
+            sum += ms;
+        }
+        out->ms[i] = sum / reps;
+        if (best < 0 || out->ms[i] < out->ms[best]) best = i;
+    }
+    cleanup();
+    if (st) {
+        cudaStreamSynchronize(s->stream);
+        s->pack_pair = old_pair;
+        s->g1_tile = old_tile;
+        return st;
+    }
+    s->pack_pair = out->pack_cta_pair[best];
+    s->g1_tile = out->gemv_tile[best] == 256 ? 0 : out->gemv_tile[best];
+    out->chosen = best;
+    if (s->g1_tile != old_tile) destroy_graphs(s);  // the single-payload graphs bake in the tile
+    return IPR_OK;
+}
+
 int ipr_server_set_option(ipr_server* s, int option, int64_t value) {
     if (!s) return fail(IPR_E_ARGS, "null server");
     std::lock_guard<std::mutex> lk(s->mu);
