@@ -591,8 +591,12 @@ class KeywordService:
     The servers must stay open while the service runs."""
 
     def __init__(self, servers: Sequence["KeywordServer"], max_batch: int = 64, max_pending: int = 0,
-                 hbm_budget_bytes: int = 0):
+                 hbm_budget_bytes: int = 0, autotune: bool = False):
         self._servers = list(servers)
+        if autotune:  # each database's batch path set to its fastest exact configuration first
+            for srv in self._servers:
+                srv.prepare_batch(max_batch)
+                srv.autotune(max_batch)
         arr = (_vp * len(self._servers))(*[s._h.value for s in self._servers])
         cfg = _ServiceConfig(max_batch, max_pending, hbm_budget_bytes)
         self._h = _vp()
