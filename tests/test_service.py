@@ -219,3 +219,17 @@ def test_injected_allocation_failures_are_clean(pkg, orc):
     assert fired >= 10
     torch.cuda.synchronize()
     assert abs(torch.cuda.mem_get_info()[0] - free0) < (64 << 20)
+
+
+@pytest.mark.gpu
+def test_service_with_autotuned_servers_answers_exactly(pkg, orc):
+    plan = pkg.plan_from_shape(10_000, 32, 1184)
+    sdb = orc.SynthDB(plan.db_rows, plan.instances, plan.interp, plan.c, seed=21)
+    qs = [orc.synth_query(300 + i, plan.db_rows, 2) for i in range(12)]
+    with pkg.KeywordServer.synthetic(plan, seed=21) as srv:
+        svc = pkg.KeywordService([srv], max_batch=8, autotune=True)
+        try:
+            got = [svc.wait(t) for t in svc.submit_many(0, qs)]
+        finally:
+            svc.close()
+    assert got == [orc.respond(sdb, q) for q in qs]
