@@ -195,18 +195,22 @@ int ipr_server_set_profiling(ipr_server *srv, int on);
 #define IPR_OPT_GEMV_TILE 4
 int ipr_server_set_option(ipr_server *srv, int option, int64_t value);
 
-/* Autotuner for the batch path: runs `reps` timed batches of `payloads` synthetic payloads
- * (after one warm-up each) under every candidate of IPR_OPT_PACK_CTA_PAIR {0, 1} x
- * IPR_OPT_GEMV_TILE {256, 128}, timed with CUDA events on the server's stream, and
- * leaves the server set to the fastest.  Every candidate gives identical responses.  On an
- * error the options are restored. */
+/* Autotuner for the batch path: runs `reps` timed batches of `payloads` synthetic payloads,
+ * and as many of payloads / 4 (from 4 payloads up), after one warm-up each, under every
+ * candidate of IPR_OPT_PACK_CTA_PAIR {2 (automatic), 0, 1} x IPR_OPT_GEMV_TILE {256, 128},
+ * timed with CUDA events on the server's stream, round-robin.  It leaves the server set
+ * to the candidate with the least device time per payload summed over the two sizes, so a
+ * choice that only suits full batches does not slow the smaller ones a serving loop also
+ * runs.  Every candidate gives identical responses.  On an error the options are restored. */
 #define IPR_AUTOTUNE_MAX 8
 typedef struct {
     int candidates;                    /* how many were timed */
     int pack_cta_pair[IPR_AUTOTUNE_MAX];
     int gemv_tile[IPR_AUTOTUNE_MAX];
-    double ms[IPR_AUTOTUNE_MAX];       /* mean device time per batch */
+    double ms[IPR_AUTOTUNE_MAX];       /* mean device time per batch of `payloads` */
     int chosen;                        /* index of the candidate now in force */
+    int small_payloads;                /* the second batch size timed (0: none) */
+    double ms_small[IPR_AUTOTUNE_MAX]; /* mean device time per batch of small_payloads */
 } ipr_autotune_result;
 int ipr_server_autotune(ipr_server *srv, int payloads, int reps, ipr_autotune_result *out);
 int ipr_server_stage_times(ipr_server *srv, double *ms_sum, uint64_t *calls);
@@ -222,7 +226,8 @@ const char *ipr_version(void);
  * (h_a: db_rows condensed query values; h_c: b_cols results mod q; d_db: the
  * column-major u16 DB on the current device), but the query row and result
  * are staged in a fixed 8.5 MiB device array inside this library (at most
- * 65,536 rows and 1,048,576 columns; larger shapes return IPR_E_ARGS).  Every
+ * 65,536 rows and 1,048,576 columns; larger shapes return IPR_E_ARGS, and so
+ * does a query entry that is not reduced, lo32 >= q0 or hi32 >= q1).  Every
  * GPU that loads the library holds that array until the process exits.  All
  * calls share it, so calls that overlap on the GPU race; issue them one at a
  * time.  The first call on a device resolves the array's address and loads
@@ -330,11 +335,17 @@ void ipr_client_destroy(ipr_client *c);
  * needed it); the hook then switches itself off.  after < 0 switches it off at once. */
 int ipr_debug_fail_allocation(int64_t after);
 
+/* The compute capability the library's device code was compiled for, as the CUDA runtime
+ * reports it for one of its kernels on `device` (100 for sm_100a), without reading the
+ * binary. */
+int ipr_device_binary_version(int device, int *binary_version);
+
 /* Failure detection self-test: launches one CTA that waits, with the bounded wait every
  * tensor-core kernel of this library uses on its mbarriers, on a barrier nothing arrives
- * on.  The wait gives up after `budget` polls; the call returns IPR_E_TIMEOUT (the status a
- * server call returns when one of its kernels' waits runs out) and the device stays usable. */
-int ipr_selftest_bounded_wait(int device, uint32_t budget);
+ * on.  The wait gives up after limit_us microseconds of GPU global time (1 .. 1,000,000,
+ * else IPR_E_ARGS); the call returns IPR_E_TIMEOUT (the status a server call returns when
+ * one of its kernels' waits runs out, after 100 ms there) and the device stays usable. */
+int ipr_selftest_bounded_wait(int device, uint32_t limit_us);
 
 /* Setup-time database layout and encode on device buffers.
  * ipr_cuckoo_to_raw_db: KeywordCuckooTable::to_raw_db (cuckoo.rs:314-353) — bucket

@@ -87,7 +87,8 @@ _last_error = _sig("ipr_last_error", ctypes.c_char_p)
 
 class _AutotuneResult(ctypes.Structure):
     _fields_ = [("candidates", _i32), ("pack_cta_pair", _i32 * 8), ("gemv_tile", _i32 * 8),
-                ("ms", ctypes.c_double * 8), ("chosen", _i32)]
+                ("ms", ctypes.c_double * 8), ("chosen", _i32), ("small_payloads", _i32),
+                ("ms_small", ctypes.c_double * 8)]
 
 
 _autotune = _sig("ipr_server_autotune", _i32, _vp, _i32, _i32, ctypes.POINTER(_AutotuneResult))
@@ -196,10 +197,11 @@ def fail_allocation_after(n: int):
     _check(_fail_alloc(n), "ipr_debug_fail_allocation")
 
 
-def selftest_bounded_wait(budget: int = 1 << 16, device: int = 0) -> int:
+def selftest_bounded_wait(limit_us: int = 20_000, device: int = 0) -> int:
     """ipr_selftest_bounded_wait: the status of a bounded mbarrier wait that nobody
-    satisfies (IPR_E_TIMEOUT = -4 when the failure is detected)"""
-    return int(_wait_selftest(device, budget))
+    satisfies, given up after limit_us microseconds (IPR_E_TIMEOUT = -4 when the failure
+    is detected; IPR_E_ARGS for a limit outside 1 .. 1,000,000)"""
+    return int(_wait_selftest(device, limit_us))
 
 
 def offline_precompute(d_db: int, db_rows: int, instances: int, d_a_hat: int, d_bold_t: int, d_bold_t_bar: int,
@@ -510,12 +512,14 @@ class KeywordServer:
 
     def autotune(self, payloads: int = 64, reps: int = 3) -> dict:
         """ipr_server_autotune: time the batch path's candidate configurations on synthetic
-        payloads and keep the fastest (every candidate gives identical responses)"""
+        batches of `payloads` and of payloads // 4 and keep the one with the least device time
+        per payload over both sizes (every candidate gives identical responses)"""
         r = _AutotuneResult()
         _check(_autotune(self._h, payloads, reps, ctypes.byref(r)), "ipr_server_autotune")
-        cands = [{"pack_cta_pair": r.pack_cta_pair[i], "gemv_tile": r.gemv_tile[i], "ms": r.ms[i]}
+        cands = [{"pack_cta_pair": r.pack_cta_pair[i], "gemv_tile": r.gemv_tile[i], "ms": r.ms[i],
+                  "ms_small": r.ms_small[i] if r.small_payloads else None}
                  for i in range(r.candidates)]
-        return {"candidates": cands, "chosen": cands[r.chosen]}
+        return {"candidates": cands, "chosen": cands[r.chosen], "small_payloads": r.small_payloads}
 
     def stream_handle(self) -> int:
         s = _vp()

@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(G1_THREADS, 1)
             }
             // every tile load issued has landed before the CTA may exit
             for (int s = 0; s < stages; s++)
-                if (last_phase[s] >= 0) umma::mbar_wait(&sh->full[s], (uint32_t)last_phase[s], 1u << 22);
+                if (last_phase[s] >= 0) umma::mbar_wait(&sh->full[s], (uint32_t)last_phase[s], umma::kDrainLimitNs);
         }
     } else if (warp == 1) {
         if (lane == 0) {  // MMA issuer
@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(G1_THREADS, 1)
                 }
             }
             // the last MMAs have completed before TMEM can be released
-            if (last_stage >= 0) umma::mbar_wait(&sh->empty[last_stage], last_parity, 1u << 22);
+            if (last_stage >= 0) umma::mbar_wait(&sh->empty[last_stage], last_parity, umma::kDrainLimitNs);
         }
     } else {
         // epilogue: warps 2..9 -> TMEM lane quarters 2,3,0,1 (twice); the two warps of a quarter

@@ -98,16 +98,16 @@ __global__ void __launch_bounds__(256) k_automorph(const uint64_t* __restrict__ 
 }
 
 // The bounded wait the tensor-core kernels use on their mbarriers (umma::mbar_wait), on a
-// barrier nothing arrives on: the wait gives up after `budget` polls and the kernel reports it
-// instead of hanging, as the GEMM kernels do through their error flags.
-__global__ void k_wait_selftest(uint32_t budget, int* out) {
+// barrier nothing arrives on: the wait gives up after `limit_ns` of global time and the kernel
+// reports it instead of hanging, as the GEMM kernels do through their error flags.
+__global__ void k_wait_selftest(uint64_t limit_ns, int* out) {
     __shared__ uint64_t bar;
     if (threadIdx.x == 0) {
         umma::mbar_init(&bar, 1);
         umma::fence_mbar_init();
     }
     __syncthreads();
-    const bool done = umma::mbar_wait(&bar, 0, budget);  // phase 0 never completes
+    const bool done = umma::mbar_wait(&bar, 0, limit_ns);  // phase 0 never completes
     if (threadIdx.x == 0) *out = done ? 1 : 0;
 }
 
@@ -189,14 +189,29 @@ int ipr_automorph_batch(int device, const uint64_t* d_in, uint64_t count, const 
     return ipr::cuda_status(cudaGetLastError());
 }
 
-int ipr_selftest_bounded_wait(int device, uint32_t budget) {
+int ipr_device_binary_version(int device, int* binary_version) {
+    if (!binary_version) return IPR_E_ARGS;
+    int st = ipr::cuda_status(cudaSetDevice(device));
+    if (st) return st;
+    cudaFuncAttributes a{};
+    st = ipr::cuda_status(cudaFuncGetAttributes(&a, ipr::k_wait_selftest));
+    if (st) return st;
+    *binary_version = a.binaryVersion;
+    return IPR_OK;
+}
+
+int ipr_selftest_bounded_wait(int device, uint32_t limit_us) {
+    if (limit_us == 0 || limit_us > 1000000u) {
+        ipr::set_last_error("ipr_selftest_bounded_wait: limit_us must be in [1, 1000000]");
+        return IPR_E_ARGS;
+    }
     int st = ipr::cuda_status(cudaSetDevice(device));
     if (st) return st;
     int* d = nullptr;
     int h = -1;
     cudaError_t e = cudaMalloc(&d, sizeof(int));
     if (e == cudaSuccess) {
-        ipr::k_wait_selftest<<<1, 32>>>(budget, d);
+        ipr::k_wait_selftest<<<1, 32>>>((uint64_t)limit_us * 1000u, d);
         e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(int), cudaMemcpyDeviceToHost);
         cudaFree(d);

@@ -91,6 +91,11 @@ extern "C" int ipr_gemv_query_noalloc(uint64_t* h_c, const uint64_t* h_a, const 
         return noalloc_fail(IPR_E_ARGS, "db_rows must be a multiple of 256 in [256, 65536]");
     if (b_cols < 16 || (b_cols & 15) || (uint64_t)b_cols > kMaxCols)
         return noalloc_fail(IPR_E_ARGS, "b_cols must be a multiple of 16 in [16, 1048576]");
+    // the kernel's 64-bit partial sums stay exact only for reduced residues (at 65,536 rows a
+    // full 32-bit limb could wrap them), so an unreduced query row is refused
+    for (int k = 0; k < db_rows; k++)
+        if ((uint32_t)h_a[k] >= ipr::Q0 || (uint32_t)(h_a[k] >> 32) >= ipr::Q1)
+            return noalloc_fail(IPR_E_ARGS, "query row entry not reduced (need lo32 < q0 and hi32 < q1)");
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return noalloc_fail(IPR_E_CUDA, "no current device", e);

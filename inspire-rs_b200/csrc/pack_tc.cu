@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
                 }
             }
             for (int s = 0; s < stages; s++)
-                if (last_phase[s] >= 0) umma::mbar_wait(&sh->full[s], (uint32_t)last_phase[s], 1u << 22);
+                if (last_phase[s] >= 0) umma::mbar_wait(&sh->full[s], (uint32_t)last_phase[s], umma::kDrainLimitNs);
         }
     } else if (warp == 1) {
         if (lane == 0) {
@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
                     acc_phase ^= 1;
                 }
             }
-            if (last_stage >= 0) umma::mbar_wait(&sh->empty[last_stage], last_parity, 1u << 22);
+            if (last_stage >= 0) umma::mbar_wait(&sh->empty[last_stage], last_parity, umma::kDrainLimitNs);
         }
     } else {
         // epilogue group t (warps 2+4t .. 5+4t) drains tile t (slot z0 + t).  Warp w reads TMEM
@@ -424,7 +424,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Q_THREADS, 1)
             }
             if (leader)  // every load of either CTA has landed before the pair may exit
                 for (int s = 0; s < stages; s++)
-                    if (last_phase[s] >= 0) umma::mbar_wait(&sh->full[s], (uint32_t)last_phase[s], 1u << 22);
+                    if (last_phase[s] >= 0) umma::mbar_wait(&sh->full[s], (uint32_t)last_phase[s], umma::kDrainLimitNs);
         }
     } else if (warp == 1) {
         if (leader && lane == 0) {
@@ -467,7 +467,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Q_THREADS, 1)
                 buf ^= 1;
                 if (buf == 0) acc_phase ^= 1;
             }
-            if (last_stage >= 0) umma::mbar_wait(&sh->empty[last_stage], last_parity, 1u << 22);
+            if (last_stage >= 0) umma::mbar_wait(&sh->empty[last_stage], last_parity, umma::kDrainLimitNs);
         }
     } else {
         // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 = byte b of outputs mt*32 + lane, slot z0 + rank

@@ -912,7 +912,10 @@ int ipr_server_autotune(ipr_server* s, int payloads, int reps, ipr_autotune_resu
     }
     CU(cudaMemcpyAsync(s->d_bq, s->h_bq, (size_t)payloads * qb, cudaMemcpyHostToDevice, s->stream));
     const int old_pair = s->pack_pair, old_tile = s->g1_tile;
-    static const int pairs[] = {0, 1}, tiles[] = {0, 128};
+    // CTA pairs pay off only for large batches, so the automatic threshold (2) competes with
+    // pairs never (0) and always (1), and every candidate is timed at the requested batch
+    // size and at a quarter of it: the score is the device time per payload summed over both
+    static const int pairs[] = {2, 0, 1}, tiles[] = {0, 128};
     *out = ipr_autotune_result{};
     for (int pr : pairs)
         for (int tl : tiles) {
@@ -920,9 +923,12 @@ int ipr_server_autotune(ipr_server* s, int payloads, int reps, ipr_autotune_resu
             out->gemv_tile[out->candidates++] = tl ? tl : 256;
         }
     const int nc = out->candidates;
+    const int sizes[2] = {payloads, payloads >= 4 ? payloads / 4 : 0};
+    const int nsz = sizes[1] ? 2 : 1;
+    out->small_payloads = sizes[1];
     // candidates interleaved round-robin, one event pair per timed batch, so that clock drift
     // under the power cap falls on every candidate alike
-    std::vector<cudaEvent_t> ev((size_t)2 * nc * reps, nullptr);
+    std::vector<cudaEvent_t> ev((size_t)2 * nc * reps * nsz, nullptr);
     auto cleanup = [&]() {
         for (cudaEvent_t e : ev)
             if (e) cudaEventDestroy(e);
@@ -937,35 +943,45 @@ int ipr_server_autotune(ipr_server* s, int payloads, int reps, ipr_autotune_resu
         s->pack_pair = out->pack_cta_pair[i];
         s->g1_tile = out->gemv_tile[i] == 256 ? 0 : out->gemv_tile[i];
     };
+    auto evi = [&](int z, int r, int i) { return (size_t)2 * ((z * reps + r) * nc + i); };
     cudaMemsetAsync(s->d_err, 0, sizeof(int), s->stream);
-    for (int i = 0; i < nc && !st; i++) {  // one warm-up batch per candidate
-        use(i);
-        st = enqueue_batch(s, payloads, s->d_bq, s->d_bresp, -1);
-    }
-    for (int r = 0; r < reps && !st; r++)
-        for (int i = 0; i < nc && !st; i++) {
+    for (int z = 0; z < nsz; z++)
+        for (int i = 0; i < nc && !st; i++) {  // one warm-up batch per candidate and size
             use(i);
-            cudaEventRecord(ev[(size_t)2 * (r * nc + i)], s->stream);
-            st = enqueue_batch(s, payloads, s->d_bq, s->d_bresp, -1);
-            cudaEventRecord(ev[(size_t)2 * (r * nc + i) + 1], s->stream);
+            st = enqueue_batch(s, sizes[z], s->d_bq, s->d_bresp, -1);
         }
+    for (int r = 0; r < reps && !st; r++)
+        for (int z = 0; z < nsz && !st; z++)
+            for (int i = 0; i < nc && !st; i++) {
+                use(i);
+                cudaEventRecord(ev[evi(z, r, i)], s->stream);
+                st = enqueue_batch(s, sizes[z], s->d_bq, s->d_bresp, -1);
+                cudaEventRecord(ev[evi(z, r, i) + 1], s->stream);
+            }
     int flag = 0;
     if (!st && (cudaStreamSynchronize(s->stream) != cudaSuccess ||
                 cudaMemcpy(&flag, s->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess))
         st = fail(IPR_E_CUDA, "autotune: %s", cudaGetErrorString(cudaGetLastError()));
     if (!st && flag) st = fail(IPR_E_TIMEOUT, "a device-side wait ran out during autotuning (code %d)", flag);
     int best = -1;
+    double best_score = 0;
     for (int i = 0; i < nc && !st; i++) {
-        double sum = 0;
-        for (int r = 0; r < reps && !st; r++) {
-            float ms = 0;
-            if (cudaEventElapsedTime(&ms, ev[(size_t)2 * (r * nc + i)], ev[(size_t)2 * (r * nc + i) + 1]) !=
-                cudaSuccess)
-                st = fail(IPR_E_CUDA, "event timing: %s", cudaGetErrorString(cudaGetLastError()));
-            sum += ms;
+        double score = 0;
+        for (int z = 0; z < nsz && !st; z++) {
+            double sum = 0;
+            for (int r = 0; r < reps && !st; r++) {
+                float ms = 0;
+                if (cudaEventElapsedTime(&ms, ev[evi(z, r, i)], ev[evi(z, r, i) + 1]) != cudaSuccess)
+                    st = fail(IPR_E_CUDA, "event timing: %s", cudaGetErrorString(cudaGetLastError()));
+                sum += ms;
+            }
+            (z ? out->ms_small : out->ms)[i] = sum / reps;
+            score += sum / reps / sizes[z];
         }
-        out->ms[i] = sum / reps;
-        if (best < 0 || out->ms[i] < out->ms[best]) best = i;
+        if (best < 0 || score < best_score) {
+            best = i;
+            best_score = score;
+        }
     }
     cleanup();
     if (st) {

@@ -55,18 +55,40 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* mbar, uint32_t bytes) {
                  : "memory");
 }
 
-// bounded wait for the phase with the given parity; false if the budget ran out
-__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint32_t budget = (1u << 26)) {
+// nanoseconds of the GPU's global timer
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// time limits of the bounded waits: a pipeline wait (a healthy one completes within
+// microseconds) and the drain of a kernel's own copies after a failed wait
+constexpr uint64_t kWaitLimitNs = 100000000ull;  // 100 ms
+constexpr uint64_t kDrainLimitNs = 10000000ull;  // 10 ms
+
+__device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// bounded wait for the phase with the given parity: false once limit_ns of global time have
+// passed without it (a poll count far above any such time backs the clock up)
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint64_t limit_ns = kWaitLimitNs) {
     const uint32_t a = smem_addr(mbar);
-    for (uint32_t it = 0; it < budget; it++) {
-        uint32_t ok;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(ok)
-            : "r"(a), "r"(parity)
-            : "memory");
-        if (ok) return true;
+    if (mbar_try(a, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (uint32_t it = 0; it < (1u << 26); it++) {
+#pragma unroll 1
+        for (int k = 0; k < 8; k++)
+            if (mbar_try(a, parity)) return true;
+        if (global_ns() - t0 >= limit_ns) return false;
     }
     return false;
 }

@@ -358,6 +358,21 @@ def gemv(sdb: SynthDB, a: np.ndarray) -> np.ndarray:
     return c
 
 
+def gemv_db(db: np.ndarray, db_rows: int, a: np.ndarray) -> np.ndarray:
+    """the first-dimension GEMV (ipr_oracle_gemv) over a bare column-major u16 DB
+    [db_cols][db_rows] and one condensed query row, without a server state around it"""
+    dbv = np.ascontiguousarray(db, dtype=np.uint16)
+    assert dbv.size % db_rows == 0
+    d = OracleDB()
+    d.db_rows, d.db_cols, d.num_outputs, d.interp, d.c = db_rows, dbv.size // db_rows, 0, 1, 0
+    d.db = _ptr(dbv)
+    av = np.ascontiguousarray(a, dtype=np.uint64)
+    assert av.size == db_rows
+    c = np.zeros(d.db_cols, dtype=np.uint64)
+    _gemv(ctypes.byref(params()), ctypes.byref(d), _ptr(av), _ptr(c))
+    return c
+
+
 def rotations(y_body: np.ndarray):
     y = np.ascontiguousarray(y_body, dtype=np.uint64)
     ya = np.zeros(NINNER * N, dtype=np.uint64)

@@ -323,20 +323,25 @@ def test_packing_gemm_forms(cfg0, pkg, orc, pair, B):
 
 @pytest.mark.gpu
 def test_every_batch_configuration_is_exact_and_autotune_keeps_one(cfg0, pkg, orc):
-    """the autotuner's candidates (packing GEMM on one CTA or a CTA pair, first-dimension GEMM
-    tile 256 or 128) all answer bit-exactly; autotune times them and leaves the fastest set"""
+    """the autotuner's candidates (packing GEMM on one CTA, a CTA pair or pairs from 48 payloads
+    up; first-dimension GEMM tile 256 or 128) all answer bit-exactly; autotune times them at 64
+    and 16 payloads and leaves the one with the least time per payload over both sizes set"""
     plan, srv, sdb = cfg0
     qs = [orc.synth_query(600 + i, plan.db_rows, 2) for i in range(64)]
     want = [orc.respond(sdb, q) for q in qs[:3]] + [orc.respond(sdb, qs[63])]
-    for pair in (0, 1):
+    for pair in (0, 1, 2):
         for tile in (0, 128):
             srv.set_option(pkg.KeywordServer.OPT_PACK_CTA_PAIR, pair)
             srv.set_option(pkg.KeywordServer.OPT_GEMV_TILE, tile)
             got = srv.respond_batch(qs)
             assert got[:3] + [got[63]] == want, (pair, tile)
     res = srv.autotune(64, 2)
-    ms = [c["ms"] for c in res["candidates"]]
-    assert len(ms) == 4 and all(m > 0 for m in ms) and res["chosen"]["ms"] == min(ms)
+    assert res["small_payloads"] == 16
+    score = [c["ms"] / 64 + c["ms_small"] / 16 for c in res["candidates"]]
+    assert len(score) == 6 and all(c["ms"] > 0 and c["ms_small"] > 0 for c in res["candidates"])
+    chosen = res["chosen"]
+    assert chosen["ms"] / 64 + chosen["ms_small"] / 16 == min(score)
+    assert {c["pack_cta_pair"] for c in res["candidates"]} == {0, 1, 2}
     got = srv.respond_batch(qs)
     assert got[:3] + [got[63]] == want
     assert srv.respond_to_serialized_query(qs[1]) == want[1]

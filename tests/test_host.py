@@ -30,11 +30,15 @@ def test_library_exports_every_declared_symbol(pkg, header):
     assert not missing, missing
 
 
+@pytest.mark.gpu
 def test_library_is_sm100a(pkg):
-    out = subprocess.run(["cuobjdump", "--list-elf", pkg._LIB_PATH], capture_output=True, text=True)
-    if out.returncode != 0:
-        pytest.skip("cuobjdump unavailable")
-    assert "sm_100a" in out.stdout
+    """the runtime reports the library's kernels as built for compute capability 10.0"""
+    v = ctypes.c_int(0)
+    f = pkg.lib.ipr_device_binary_version
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    assert f(0, ctypes.byref(v)) == 0
+    assert v.value == 100
 
 
 SHAPES = [

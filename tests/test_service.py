@@ -147,8 +147,12 @@ def test_bounded_wait_reports_timeout_and_device_stays_usable(pkg, orc):
     """failure detection without a GPU fault: a kernel's bounded mbarrier wait on a barrier
     nothing arrives on gives up and is reported as IPR_E_TIMEOUT; afterwards the same
     process answers a query bit-exactly"""
-    assert pkg.selftest_bounded_wait(1 << 12) == -4
+    import time
+    t0 = time.perf_counter()
+    assert pkg.selftest_bounded_wait(5_000) == -4  # 5 ms limit
+    assert time.perf_counter() - t0 < 5.0
     assert "bounded wait ran out" in (pkg.lib.ipr_last_error() or b"").decode()
+    assert pkg.selftest_bounded_wait(2_000_000) == -1  # limits above one second are refused
     plan = pkg.plan_from_shape(10_000, 32, 1184)
     with pkg.KeywordServer.synthetic(plan, seed=3) as srv:
         sdb = orc.SynthDB(plan.db_rows, plan.instances, plan.interp, plan.c, seed=3)
