@@ -274,7 +274,11 @@ def serve_config4(pkg, rates, seconds):
         svc.wait(t)
     sat = 3 * n_each / (time.perf_counter() - t1)
     poisson_load(svc, None, rates[0], 0.5, per_db=per_db)  # warm-up at the first load, not reported
-    serving = [poisson_load(svc, None, r, seconds, per_db=per_db) for r in rates]
+    clocks = ClockSampler(0)
+    clocks.start()
+    # at least 1,000 arrivals per load, so that a p99 rests on ten or more samples
+    serving = [poisson_load(svc, None, r, max(seconds, 1000.0 / r), per_db=per_db) for r in rates]
+    clk = clocks.stop()
     st = svc.stats()
     free_b, total_b = torch.cuda.mem_get_info()
     hbm = total_b - free_b  # the whole device in use while serving
@@ -288,7 +292,7 @@ def serve_config4(pkg, rates, seconds):
                        "databases": [{"name": c[0], "db_rows": p.db_rows, "db_cols": p.db_cols,
                                       "instances": p.instances, "c": p.c} for c, p in zip(CONFIG4, plans)],
                        "max_batch": st.max_batch, "device_bytes_in_use": hbm, "setup_s": setup_s},
-            "serving": serving}
+            "serving": serving, "clocks": clk}
     print(json.dumps(line))
     return 0
 
@@ -491,6 +495,8 @@ def main():
     ap.add_argument("--dim0", type=int, default=None)
     ap.add_argument("--batch", type=int, default=64, help="payloads per step (1 = batch-1 u64 packing path)")
     ap.add_argument("--no-batch1", action="store_true", help="skip the batch-1 comparison measurement")
+    ap.add_argument("--fold-form", type=int, default=2, choices=[1, 2],
+                    help="2: fold with the packing post-process fused in (default); 1: separate INTT + CRT pass")
     ap.add_argument("--no-serving", action="store_true", help="skip the Poisson serving measurement")
     ap.add_argument("--serve-rates", type=float, nargs="*", default=[1000.0, 2500.0],
                     help="offered Poisson loads (payloads/s) for the serving measurement")
@@ -504,7 +510,7 @@ def main():
     if args.micro:
         return micro_bench(load_package(), max(args.steps, 3), max(args.warmup, 1))
     if args.serve_config4:
-        rates = args.serve_rates if args.serve_rates != [1000.0, 2500.0] else [300.0, 600.0, 1200.0]
+        rates = args.serve_rates if args.serve_rates != [1000.0, 2500.0] else [100.0, 300.0, 1200.0, 2500.0]
         return serve_config4(load_package(), rates, args.serve_seconds)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -547,6 +553,8 @@ def main():
     else:
         plan = pkg.plan_from_shape(RECORDS, KEY, VALUE, BUCKETS, DIM0)
     srv = pkg.KeywordServer.synthetic(plan, seed=7 + rank, device=dev)
+    if args.fold_form != 2:
+        srv.set_option(pkg.KeywordServer.OPT_FOLD_REGISTER_NTT, args.fold_form)
     qbytes = srv.query_bytes(2)
     rbytes = srv.response_bytes(2)
 

@@ -168,11 +168,13 @@ int ipr_server_stream(ipr_server *srv, void **cuda_stream);
 int ipr_server_sync(ipr_server *srv);
 
 /* Per-stage CUDA-event timing on the server stream (stages below), summed
- * over the calls since profiling was enabled. */
+ * over the calls since profiling was enabled.  IPR_STAGE_POST is the step between
+ * the packing sum and the fold: the scaling pass of the fused fold (default), or the
+ * INTT + CRT pass of the separate form (IPR_OPT_FOLD_REGISTER_NTT 0 or 1). */
 #define IPR_STAGE_PARSE 0
 #define IPR_STAGE_GEMV 1
 #define IPR_STAGE_PACK 2
-#define IPR_STAGE_INTT 3
+#define IPR_STAGE_POST 3
 #define IPR_STAGE_FOLD 4
 #define IPR_NSTAGES 5
 int ipr_server_set_profiling(ipr_server *srv, int on);
@@ -181,8 +183,11 @@ int ipr_server_set_profiling(ipr_server *srv, int on);
  * tensor cores over DB byte planes (default where db_rows <= 32768), 0 = the
  * CUDA-core kernel on the u16 DB.  Both give identical results. */
 #define IPR_OPT_TENSOR_GEMV 1
-/* IPR_OPT_FOLD_REGISTER_NTT: 1 = RGSW fold with register-resident NTTs
- * (default), 0 = shared-memory NTTs.  Identical results. */
+/* IPR_OPT_FOLD_REGISTER_NTT: the form of the RGSW fold.  2 (default) = register-
+ * resident NTTs with the packing post-process (INTT + CRT + b add) fused into the
+ * fold's own inverse transforms; 1 = register-resident NTTs after a separate INTT + CRT
+ * pass; 0 = shared-memory NTTs after that pass (single-payload calls only; batches
+ * then use form 1).  Identical results. */
 #define IPR_OPT_FOLD_REGISTER_NTT 2
 /* IPR_OPT_PACK_CTA_PAIR: 1 = the batch path's packing GEMM runs on CTA pairs
  * (tcgen05 cta_group::2, M = 256 across two SMs); 0 = one CTA per unit;

@@ -26,7 +26,7 @@ __all__ = [
 
 POLY_LEN = 2048
 RESULT_BYTES = 12288
-STAGES = ("parse", "gemv", "pack", "intt", "fold")
+STAGES = ("parse", "gemv", "pack", "post", "fold")
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libipr_b200.so")

@@ -1,0 +1,422 @@
+// fold3.cu — RGSW interpolation fold with the packing post-process fused in, plus the
+// modulus switch, on register-resident NTTs.
+//
+// Restates, per (query, fold group wp), the fold closure of KeywordServer::respond
+// (rkdud007/inspire-rs src/pir/server/keyword.rs:543-581)
+//   s = 0; for i = interp-1 .. 0:  s = from_ntt(CT * to_ntt(G^-1(s))) + packed[wp*interp + i]  (mod q)
+// followed by switch_and_keep (src/pir/modulus_switch.rs:45-73), where the packed
+// ciphertexts are the online-packing post-process (src/pir/gpu/packing_online.rs:359-397):
+//   packed[j] = (a_hat[j], from_ntt(S[j]) + c[j*N .. (j+1)*N]).
+// from_ntt is linear, so INTT(CT * NTT(G^-1(s)))[row 1] + INTT(S[j]) is one inverse
+// transform of the sum: the packing output S[j] joins the fold's own row-1 accumulator
+// in the NTT domain and no separate INTT + CRT pass (nor its u64 output array) exists.
+//
+// Layout of the work: a CTA of 512 threads takes two fold groups (chains) of one query;
+// each team of 256 threads runs one chain alone (its own named barrier), both teams
+// sharing the query's six RGSW bodies in shared memory.  A thread owns 8 coefficients
+// (layout A of ntt_regs.cuh, e = t + 256 m) of both rows of s as u64 values mod q, kept
+// in a shared-memory slot only that thread touches, and runs the transforms of both CRT
+// limbs itself, so the CRT compose, the packed-row add and the gadget decomposition need
+// no exchange between threads.
+//
+// Arithmetic: the inverse transforms are Gentleman-Sande butterflies with the plain
+// inverse twiddles (the reference pre-halves them, ntt.rs:93-96, to fold in N^-1);
+// here N^-1 is folded into the operands instead: into row 0 of the RGSW matrix and the
+// query's bodies (once per chain) and into S (by k_fold_prep).  Inverse transforms are
+// unique, so the canonical outputs equal the reference's.  The forward transforms of the
+// gadget digits (< 2^19) skip the conditional subtraction in their first seven stages,
+// where the values provably stay below 2^19 + 14q < 16q < 2^32.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "ipr_device.cuh"
+#include "kernels.cuh"
+#include "ntt_regs.cuh"
+
+namespace ipr {
+
+namespace {
+
+constexpr int F3_TEAM = 256;
+constexpr int F3_THREADS = 2 * F3_TEAM;
+constexpr int EPT = nttr::EPT;
+constexpr int XP = 4;  // polynomials per team exchange buffer
+
+using nttr::csub;
+using nttr::eA;
+using nttr::eB;
+using nttr::eC;
+using nttr::eD;
+
+// forward butterfly by stage: MODE 0 leaves x unreduced (x < 2^19 + 2q * stage), MODE 1
+// brings x < 16q down to [0, 2q) with three conditional subtractions, MODE 2 is the
+// Harvey form (x < 4q -> [0, 2q)).  Outputs: x + w*y, x - w*y (+2q), w*y in [0, 2q).
+template <int MODE>
+__device__ __forceinline__ void fwd_b(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wp, uint32_t q) {
+    const uint32_t two_q = 2 * q;
+    uint32_t xx = x;
+    if (MODE == 1) xx = csub(csub(csub(x, 8 * q), 4 * q), two_q);
+    if (MODE == 2) xx = csub(x, two_q);
+    const uint32_t qn = shoup_lazy(y, w, wp, q);
+    x = xx + qn;
+    y = xx + two_q - qn;
+}
+
+template <int P, int MODE, typename E>
+__device__ __forceinline__ void fstage(uint32_t (&v)[P][EPT], int mm, int dd, E e, const uint32_t* __restrict__ w_t,
+                                       const uint32_t* __restrict__ wp_t, uint32_t q) {
+#pragma unroll
+    for (int k = 0; k < EPT; k++) {
+        if (k & dd) continue;
+        const int idx = (1 << mm) + (e(k) >> (11 - mm));
+        const uint32_t w = __ldg(w_t + idx), wp = __ldg(wp_t + idx);
+#pragma unroll
+        for (int p = 0; p < P; p++) fwd_b<MODE>(v[p][k], v[p][k + dd], w, wp, q);
+    }
+}
+
+// forward NTT of P gadget-digit polynomials (< 2^19) of one limb: layout A in, layout D out
+// in [0, 2q); xbuf holds XP >= P polynomials of this team
+template <int P>
+__device__ __forceinline__ void forward_digits(uint32_t (&v)[P][EPT], int t, uint32_t* xbuf, int bar,
+                                               const uint32_t* __restrict__ fw, const uint32_t* __restrict__ fwp,
+                                               uint32_t q) {
+    const int l = t & 31;
+    uint32_t* wb = xbuf + (t >> 5) * 256;
+    auto fa = [&](int k) { return eA(t, k); };
+    auto fb = [&](int k) { return eB(t, k); };
+    auto fc = [&](int k) { return eC(t, k); };
+    auto fd = [&](int k) { return eD(t, k); };
+    fstage<P, 0>(v, 0, 4, fa, fw, fwp, q);
+    fstage<P, 0>(v, 1, 2, fa, fw, fwp, q);
+    fstage<P, 0>(v, 2, 1, fa, fw, fwp, q);
+    nttr::exchange<P, true>(v, t, xbuf, bar);
+    fstage<P, 0>(v, 3, 4, fb, fw, fwp, q);
+    fstage<P, 0>(v, 4, 2, fb, fw, fwp, q);
+    fstage<P, 0>(v, 5, 1, fb, fw, fwp, q);
+    nttr::b_to_c<P>(v, l, wb);
+    fstage<P, 0>(v, 6, 4, fc, fw, fwp, q);
+    fstage<P, 1>(v, 7, 2, fc, fw, fwp, q);
+    fstage<P, 2>(v, 8, 1, fc, fw, fwp, q);
+    nttr::c_to_d<P>(v, l, wb);
+    fstage<P, 2>(v, 9, 2, fd, fw, fwp, q);
+    fstage<P, 2>(v, 10, 1, fd, fw, fwp, q);
+#pragma unroll
+    for (int p = 0; p < P; p++)
+#pragma unroll
+        for (int k = 0; k < EPT; k++) v[p][k] = csub(v[p][k], 2 * q);
+}
+
+// Gentleman-Sande butterfly with a plain inverse twiddle: x + y, (x - y) * w; inputs below
+// 2q (below q on the first stage, where x + y needs no reduction), outputs in [0, 2q)
+template <bool FIRST>
+__device__ __forceinline__ void inv_b(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wp, uint32_t q) {
+    const uint32_t two_q = 2 * q;
+    const uint32_t s = x + y;
+    const uint32_t d = x + two_q - y;
+    x = FIRST ? s : csub(s, two_q);
+    y = shoup_lazy(d, w, wp, q);
+}
+
+// one inverse stage over 2 * PL polynomials: [0, PL) of limb 0, [PL, 2 PL) of limb 1
+template <int PL, bool FIRST, typename E>
+__device__ __forceinline__ void istage(uint32_t (&v)[2 * PL][EPT], int mm, int dd, E e,
+                                       const uint32_t* __restrict__ iw, const uint32_t* __restrict__ iwp) {
+#pragma unroll
+    for (int k = 0; k < EPT; k++) {
+        if (k & dd) continue;
+        const int idx = (1 << mm) + (e(k) >> (11 - mm));
+        const uint32_t w0 = __ldg(iw + idx), wp0 = __ldg(iwp + idx);
+        const uint32_t w1 = __ldg(iw + N + idx), wp1 = __ldg(iwp + N + idx);
+#pragma unroll
+        for (int p = 0; p < PL; p++) inv_b<FIRST>(v[p][k], v[p][k + dd], w0, wp0, Q0);
+#pragma unroll
+        for (int p = PL; p < 2 * PL; p++) inv_b<FIRST>(v[p][k], v[p][k + dd], w1, wp1, Q1);
+    }
+}
+
+// N * INTT of 2 * PL canonical polynomials (PL per limb): layout D in, layout A canonical out
+template <int PL>
+__device__ __forceinline__ void inverse_limbs(uint32_t (&v)[2 * PL][EPT], int t, uint32_t* xbuf, int bar,
+                                              const uint32_t* __restrict__ iw, const uint32_t* __restrict__ iwp) {
+    const int l = t & 31;
+    uint32_t* wb = xbuf + (t >> 5) * 256;
+    auto fa = [&](int k) { return eA(t, k); };
+    auto fb = [&](int k) { return eB(t, k); };
+    auto fc = [&](int k) { return eC(t, k); };
+    auto fd = [&](int k) { return eD(t, k); };
+    istage<PL, true>(v, 10, 1, fd, iw, iwp);
+    istage<PL, false>(v, 9, 2, fd, iw, iwp);
+    nttr::d_to_c<2 * PL>(v, l, wb);
+    istage<PL, false>(v, 8, 1, fc, iw, iwp);
+    istage<PL, false>(v, 7, 2, fc, iw, iwp);
+    istage<PL, false>(v, 6, 4, fc, iw, iwp);
+    nttr::c_to_b<2 * PL>(v, l, wb);
+    istage<PL, false>(v, 5, 1, fb, iw, iwp);
+    istage<PL, false>(v, 4, 2, fb, iw, iwp);
+    istage<PL, false>(v, 3, 4, fb, iw, iwp);
+    nttr::exchange<2 * PL, false>(v, t, xbuf, bar);
+    istage<PL, false>(v, 2, 1, fa, iw, iwp);
+    istage<PL, false>(v, 1, 2, fa, iw, iwp);
+    istage<PL, false>(v, 0, 4, fa, iw, iwp);
+#pragma unroll
+    for (int p = 0; p < 2 * PL; p++)
+#pragma unroll
+        for (int k = 0; k < EPT; k++) v[p][k] = csub(v[p][k], p < PL ? Q0 : Q1);
+}
+
+// the 8 consecutive words of layout D held by thread t (two 16-byte loads)
+__device__ __forceinline__ void load_d8(uint32_t (&r)[EPT], const uint32_t* __restrict__ p) {
+    const uint4 a = __ldg(reinterpret_cast<const uint4*>(p)), b = __ldg(reinterpret_cast<const uint4*>(p) + 1);
+    r[0] = a.x; r[1] = a.y; r[2] = a.z; r[3] = a.w;
+    r[4] = b.x; r[5] = b.y; r[6] = b.z; r[7] = b.w;
+}
+
+__device__ __forceinline__ uint32_t mul_canon(uint32_t x, uint32_t w, uint32_t wp, uint32_t q) {
+    return csub(shoup_lazy(x, w, wp, q), q);
+}
+
+__device__ __forceinline__ uint64_t add_q(uint64_t a, uint64_t b) {  // a, b < q
+    const uint64_t v = a + b;
+    return v >= QQ ? v - QQ : v;
+}
+
+__device__ __forceinline__ uint64_t rescale_q(uint64_t v, uint64_t out_mod) {
+    // rescale (src/core/arith.rs:436-452) of a canonical v in [0, q)
+    const uint64_t half = QQ / 2;
+    const bool neg = v >= half;
+    const uint64_t u = neg ? QQ - v : v;
+    const unsigned __int128 num = (unsigned __int128)u * out_mod + half;
+    const uint64_t rr = (uint64_t)(num / QQ);
+    const uint64_t rm = rr % out_mod;
+    return neg ? (rm ? out_mod - rm : 0) : rm;
+}
+
+}  // namespace
+
+// N^-1 mod q_l and its Shoup companion, per limb
+struct NInv {
+    uint32_t w[2], wp[2];
+};
+
+// S[f][l][z] <- (S[f][l][z] + sum_k zb[f / instances][k][z] * That[f % instances][k][z]) * N^-1 mod q_l
+// (the z_body x That term of packing_online_kernel.cu:76-83, then the N^-1 the fold's inverse
+// transforms leave out); zb null: the scaling alone.  One thread per 4 slots of one output.
+__global__ void __launch_bounds__(256) k_fold_prep(uint32_t* __restrict__ S, int64_t count,
+                                                   const uint64_t* __restrict__ zb, const uint64_t* __restrict__ bth,
+                                                   int instances, NInv ni) {
+    const int64_t n4 = count * (N / 4);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t f = i / (N / 4);
+        const int z0 = (int)(i % (N / 4)) * 4;
+        uint4* s0 = reinterpret_cast<uint4*>(S + (f * 2) * N + z0);
+        uint4* s1 = reinterpret_cast<uint4*>(S + (f * 2 + 1) * N + z0);
+        const uint4 a = *s0, b = *s1;
+        uint64_t acc0[4] = {a.x, a.y, a.z, a.w}, acc1[4] = {b.x, b.y, b.z, b.w};
+        if (zb) {
+            const uint64_t* zc = zb + (f / instances) * T_EXP * N + z0;
+            const uint64_t* th = bth + (f % instances) * T_EXP * N + z0;
+#pragma unroll
+            for (int k = 0; k < T_EXP; k++) {
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const ulonglong2 zv = __ldg(reinterpret_cast<const ulonglong2*>(zc + k * N) + h);
+                    const ulonglong2 tv = __ldg(reinterpret_cast<const ulonglong2*>(th + k * N) + h);
+                    acc0[2 * h] += (uint64_t)(uint32_t)zv.x * (uint32_t)tv.x;
+                    acc0[2 * h + 1] += (uint64_t)(uint32_t)zv.y * (uint32_t)tv.y;
+                    acc1[2 * h] += (zv.x >> 32) * (tv.x >> 32);
+                    acc1[2 * h + 1] += (zv.y >> 32) * (tv.y >> 32);
+                }
+            }
+        }
+        uint32_t o0[4], o1[4];
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            o0[m] = mul_canon(mod64(acc0[m], Q0, BR0), ni.w[0], ni.wp[0], Q0);
+            o1[m] = mul_canon(mod64(acc1[m], Q1, BR1), ni.w[1], ni.wp[1], Q1);
+        }
+        *s0 = make_uint4(o0[0], o0[1], o0[2], o0[3]);
+        *s1 = make_uint4(o1[0], o1[1], o1[2], o1[3]);
+    }
+}
+
+// chains: blockIdx.x = fold-group pair (groups 2x, 2x + 1), blockIdx.y = query qg (global over
+// the batch); query qg belongs to payload qg / qpp.  S: the prepared packing outputs
+// (k_fold_prep) of payload p at S + p * s_payload_stride, [instances][2][N].
+__global__ void __launch_bounds__(F3_THREADS, 1)
+    k_fold3(const uint32_t* __restrict__ row0s, const uint32_t* __restrict__ gsw, const uint64_t* __restrict__ a_hat,
+            const uint32_t* __restrict__ S, int64_t s_payload_stride, const uint64_t* __restrict__ cvec,
+            const uint32_t* __restrict__ fw, const uint32_t* __restrict__ fwp, const uint32_t* __restrict__ iwu,
+            const uint32_t* __restrict__ iwup, NInv ni, int interp, int c_groups, int64_t db_cols, int qpp,
+            uint8_t* __restrict__ resp, int64_t resp_payload_stride, int64_t resp_query_stride) {
+    extern __shared__ uint32_t f3_smem[];
+    uint32_t* sbody = f3_smem;  // [6 gadget rows][2 limbs][N]: N^-1 x the query's RGSW bodies
+    const int team = threadIdx.x >> 8, t = threadIdx.x & (F3_TEAM - 1);
+    uint32_t* xbuf = f3_smem + 12 * N + team * XP * N;
+    // s of this team: [row][m][t] u64, word (row, m) of thread t read back only by thread t
+    uint64_t* sst = reinterpret_cast<uint64_t*>(f3_smem + (12 + 2 * XP) * N) + team * 2 * N;
+    auto S_AT = [&](int row, int m) -> uint64_t& { return sst[(row * EPT + m) * F3_TEAM + t]; };
+    const int qg = blockIdx.y;
+    const int wp = 2 * blockIdx.x + team;
+    {
+        const uint4* gb = reinterpret_cast<const uint4*>(gsw + (int64_t)qg * 12 * N);
+        uint4* sb = reinterpret_cast<uint4*>(sbody);
+        for (int i = threadIdx.x; i < 12 * N / 4; i += F3_THREADS) {
+            const int lb = ((4 * i) / N) & 1;  // word (p * 2 + l) * N + z
+            const uint32_t q = lb ? Q1 : Q0, w = ni.w[lb], wq = ni.wp[lb];
+            const uint4 b = __ldg(gb + i);
+            sb[i] = make_uint4(mul_canon(b.x, w, wq, q), mul_canon(b.y, w, wq, q), mul_canon(b.z, w, wq, q),
+                               mul_canon(b.w, w, wq, q));
+        }
+    }
+    __syncthreads();
+    if (wp >= c_groups) return;  // the second team of an odd group count has no chain
+    const int bar = 1 + team;
+    const int payload = qg / qpp, qin = qg % qpp;
+    const uint32_t* Sq = S + (int64_t)payload * s_payload_stride;
+    const uint64_t* cq = cvec + (int64_t)qg * db_cols;
+    const uint64_t mask = (1ull << GADGET_BITS) - 1;
+    const int zd = eD(t, 0);
+
+    {  // first step: G^-1(0) = 0, so s = (a_hat[j], INTT(S[j]) + c[j]) mod q
+        const int j = wp * interp + interp - 1;
+        uint32_t pr[2][EPT];
+        load_d8(pr[0], Sq + ((int64_t)j * 2) * N + zd);
+        load_d8(pr[1], Sq + ((int64_t)j * 2 + 1) * N + zd);
+        uint64_t pc[EPT];
+#pragma unroll
+        for (int m = 0; m < EPT; m++) {
+            S_AT(0, m) = __ldg(a_hat + (int64_t)j * N + eA(t, m));
+            pc[m] = __ldg(cq + (int64_t)j * N + eA(t, m));
+        }
+        inverse_limbs<1>(pr, t, xbuf, bar, iwu, iwup);
+#pragma unroll
+        for (int m = 0; m < EPT; m++) S_AT(1, m) = add_q(crt2(pr[0][m], pr[1][m], Q0INV, BR1), pc[m]);
+    }
+
+    for (int step = interp - 2; step >= 0; step--) {
+        const int j = wp * interp + step;
+        uint32_t pr[4][EPT];  // [row 0 limb 0, row 1 limb 0, row 0 limb 1, row 1 limb 1]
+#pragma unroll
+        for (int l = 0; l < 2; l++) {
+            const uint32_t q = l ? Q1 : Q0;
+            const uint64_t br = l ? BR1 : BR0;
+            uint32_t sv[EPT];
+            load_d8(sv, Sq + ((int64_t)j * 2 + l) * N + zd);
+            uint32_t acc0[EPT], acc1[EPT];  // acc1 reduced after every batch of three digits
+#pragma unroll
+            for (int m = 0; m < EPT; m++) {
+                acc0[m] = 0;
+                acc1[m] = sv[m];
+            }
+#pragma unroll 1
+            for (int r = 0; r < 2; r++) {  // gadget rows p = r + 2k hold digit k of row r (gadget.rs:44-58)
+                uint32_t v[3][EPT];
+#pragma unroll
+                for (int m = 0; m < EPT; m++) {
+                    const uint64_t x = S_AT(r, m);
+#pragma unroll
+                    for (int k = 0; k < 3; k++) v[k][m] = (uint32_t)((x >> (k * GADGET_BITS)) & mask);
+                }
+                forward_digits<3>(v, t, xbuf, bar, fw + l * N, fwp + l * N, q);
+                uint64_t part[EPT];
+#pragma unroll
+                for (int m = 0; m < EPT; m++) part[m] = acc1[m];
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    const uint4* bp = reinterpret_cast<const uint4*>(sbody + ((r + 2 * k) * 2 + l) * N + zd);
+                    const uint4 b0 = bp[0], b1 = bp[1];
+                    const uint32_t bv[EPT] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+                    for (int m = 0; m < EPT; m++) {
+                        acc0[m] += v[k][m];                    // 6 terms < 12q < 2^32
+                        part[m] += (uint64_t)bv[m] * v[k][m];  // q + 3 terms < q + 6 q^2 < 2^60
+                    }
+                }
+#pragma unroll
+                for (int m = 0; m < EPT; m++) acc1[m] = mod64(part[m], q, br);
+            }
+            uint32_t r0[EPT];
+            load_d8(r0, row0s + l * N + zd);
+            if (l == 0) {
+#pragma unroll
+                for (int m = 0; m < EPT; m++) {
+                    pr[0][m] = mod64((uint64_t)r0[m] * acc0[m], q, br);
+                    pr[1][m] = acc1[m];
+                }
+            } else {
+#pragma unroll
+                for (int m = 0; m < EPT; m++) {
+                    pr[2][m] = mod64((uint64_t)r0[m] * acc0[m], q, br);
+                    pr[3][m] = acc1[m];
+                }
+            }
+        }
+        uint64_t pa[EPT], pc[EPT];  // packed row j, fetched while the inverse transforms run
+#pragma unroll
+        for (int m = 0; m < EPT; m++) {
+            pa[m] = __ldg(a_hat + (int64_t)j * N + eA(t, m));
+            pc[m] = __ldg(cq + (int64_t)j * N + eA(t, m));
+        }
+        inverse_limbs<2>(pr, t, xbuf, bar, iwu, iwup);
+#pragma unroll
+        for (int m = 0; m < EPT; m++) {
+            S_AT(0, m) = add_q(crt2(pr[0][m], pr[2][m], Q0INV, BR1), pa[m]);
+            S_AT(1, m) = add_q(crt2(pr[1][m], pr[3][m], Q0INV, BR1), pc[m]);
+        }
+    }
+
+    // switch_and_keep: row 0 -> 28-bit fields (2 per 7 bytes), row 1 -> 20-bit fields (2 per 5
+    // bytes), LSB first; coefficient e + 1 sits in the next lane of the same warp
+    uint8_t* out = resp + (int64_t)payload * resp_payload_stride + 8 + (int64_t)qin * resp_query_stride +
+                   (int64_t)wp * RESULT_BYTES;
+#pragma unroll
+    for (int m = 0; m < EPT; m++) {
+        const uint64_t a = rescale_q(S_AT(0, m), QP2), b = rescale_q(S_AT(1, m), QP1);
+        const uint64_t an = __shfl_down_sync(0xffffffffu, a, 1), bn = __shfl_down_sync(0xffffffffu, b, 1);
+        if (!(t & 1)) {
+            const int tt = eA(t, m) >> 1;
+            const uint64_t v = a | (an << 28), w = b | (bn << 20);
+#pragma unroll
+            for (int x = 0; x < 7; x++) out[7 * tt + x] = (uint8_t)(v >> (8 * x));
+#pragma unroll
+            for (int x = 0; x < 5; x++) out[7 * N / 2 + 5 * tt + x] = (uint8_t)(w >> (8 * x));
+        }
+    }
+}
+
+// RGSW bodies 96 KB + two team exchange buffers of 4 polynomials (2 x 32 KB) + the two
+// teams' s (2 x 32 KB) = 224 KB
+constexpr int FOLD3_SMEM = (12 + 2 * XP) * N * 4 + 2 * 2 * N * 8;
+
+cudaError_t init_fold3_kernel() {
+    return cudaFuncSetAttribute(k_fold3, cudaFuncAttributeMaxDynamicSharedMemorySize, FOLD3_SMEM);
+}
+
+cudaError_t launch_fold_prep(uint32_t* S, int64_t count, const uint64_t* zb, const uint64_t* bth, int instances,
+                             const uint32_t ninv[4], int sm_count, cudaStream_t st) {
+    if (count < 1 || (zb && instances < 1)) return cudaErrorInvalidValue;
+    NInv ni{{ninv[0], ninv[2]}, {ninv[1], ninv[3]}};
+    const int64_t n4 = count * (N / 4);
+    const int64_t blocks = std::min<int64_t>((n4 + 255) / 256, (int64_t)sm_count * 8);
+    k_fold_prep<<<(unsigned)blocks, 256, 0, st>>>(S, count, zb, bth, instances, ni);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fold3(const uint32_t* row0s, const uint32_t* gsw, const uint64_t* a_hat, const uint32_t* S,
+                         int64_t s_payload_stride, const uint64_t* cvec, const uint32_t* fw, const uint32_t* fwp,
+                         const uint32_t* iwu, const uint32_t* iwup, const uint32_t ninv[4], int interp, int c_groups,
+                         int num_queries, int64_t db_cols, int qpp, uint8_t* resp, int64_t resp_payload_stride,
+                         int64_t resp_query_stride, cudaStream_t st) {
+    if (interp < 1 || c_groups < 1 || num_queries < 1 || num_queries > 65535 || qpp < 1) return cudaErrorInvalidValue;
+    NInv ni{{ninv[0], ninv[2]}, {ninv[1], ninv[3]}};
+    dim3 grid((c_groups + 1) / 2, num_queries);
+    k_fold3<<<grid, F3_THREADS, FOLD3_SMEM, st>>>(row0s, gsw, a_hat, S, s_payload_stride, cvec, fw, fwp, iwu, iwup,
+                                                   ni, interp, c_groups, db_cols, qpp, resp, resp_payload_stride,
+                                                   resp_query_stride);
+    return cudaGetLastError();
+}
+
+}  // namespace ipr

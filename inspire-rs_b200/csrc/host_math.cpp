@@ -232,6 +232,20 @@ void host_params_init(HostParams& p) {
     forward_ntt_u64(p, a.data());
     p.row0.resize(2 * kN);
     for (int i = 0; i < 2 * kN; i++) p.row0[i] = (uint32_t)a[i];
+    p.iwu.assign(2 * kN, 0);
+    p.iwup.assign(2 * kN, 0);
+    p.row0s.assign(2 * kN, 0);
+    for (int l = 0; l < 2; l++) {
+        const uint64_t m = p.q[l], ninv = inverse(kN, m);
+        p.ninv[2 * l] = (uint32_t)ninv;
+        p.ninv[2 * l + 1] = (uint32_t)((ninv << 32) / m);
+        for (int i = 0; i < kN; i++) {
+            const uint64_t w = (2 * (uint64_t)p.iw[l * kN + i]) % m;
+            p.iwu[l * kN + i] = (uint32_t)w;
+            p.iwup[l * kN + i] = (uint32_t)((w << 32) / m);
+            p.row0s[l * kN + i] = (uint32_t)mulmod(p.row0[l * kN + i], ninv, m);
+        }
+    }
 }
 
 namespace {

@@ -22,6 +22,11 @@ struct HostParams {
     // their Shoup companions; inverse powers pre-halved and companions
     std::vector<uint32_t> fw, fwp, iw, iwp;
     std::vector<uint32_t> row0;  // [2][N] NTT(-a), a from ChaCha20Rng([7;32])
+    // for inverse transforms that leave out N^-1 (the fold folds it into its operands):
+    // plain inverse twiddles (2 x the pre-halved ones) with Shoup companions, row 0 times
+    // N^-1, and N^-1 mod q_l with its companion as {w0, wp0, w1, wp1}
+    std::vector<uint32_t> iwu, iwup, row0s;
+    uint32_t ninv[4];
 };
 
 void host_params_init(HostParams& p);

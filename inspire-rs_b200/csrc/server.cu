@@ -153,13 +153,21 @@ int enqueue(ipr_server* s, unsigned nq, const uint8_t* d_query, uint8_t* d_resp,
         rec(2);
         CU(ipr::launch_pack(s->d_bt, s->d_btb, s->d_bth, s->d_y, s->d_z, s->d_S, (int)p.instances, st));
         rec(3);
-        CU(ipr::launch_intt_crt(s->d_S, s->d_iw, s->d_iwp, s->d_R, (int)p.instances, st));
-        rec(4);
-        if (s->fold_regs) {
+        if (s->fold_mode == 2) {
+            CU(ipr::launch_fold_prep(s->d_S, (int64_t)p.instances, nullptr, nullptr, 1, s->hp.ninv, s->sm_count, st));
+            rec(4);
+            CU(ipr::launch_fold3(s->d_row0s, s->d_gsw, s->d_ahat, s->d_S, 0, s->d_c, s->d_fw, s->d_fwp, s->d_iwu,
+                                 s->d_iwup, s->hp.ninv, (int)p.interp, (int)p.c, (int)nq, (int64_t)p.db_cols, (int)nq,
+                                 d_resp, 0, (int64_t)(4 + s->per_query_bytes()), st));
+        } else if (s->fold_mode == 1) {
+            CU(ipr::launch_intt_crt(s->d_S, s->d_iw, s->d_iwp, s->d_R, (int)p.instances, st));
+            rec(4);
             CU(ipr::launch_fold2(s->d_row0, s->d_gsw, s->d_ahat, s->d_R, 0, s->d_c, s->d_fw, s->d_fwp, s->d_iw,
                                  s->d_iwp, (int)p.interp, (int)p.c, (int)nq, (int64_t)p.db_cols, (int)nq, d_resp, 0,
                                  (int64_t)(4 + s->per_query_bytes()), st));
         } else {
+            CU(ipr::launch_intt_crt(s->d_S, s->d_iw, s->d_iwp, s->d_R, (int)p.instances, st));
+            rec(4);
             CU(ipr::launch_fold_switch(s->d_row0, s->d_gsw, s->d_ahat, s->d_R, s->d_c, s->d_fw, s->d_fwp, s->d_iw,
                                        s->d_iwp, (int)p.interp, (int)p.c, (int)nq, (int64_t)p.db_cols, d_resp + 8,
                                        (int64_t)(4 + s->per_query_bytes()), st));
@@ -232,9 +240,11 @@ int ensure_batch(ipr_server* s, int B) {
     const uint64_t qb = ipr::query_bytes(s->plan.db_rows, 2), rb = s->response_bytes(2);
     const uint64_t no = s->plan.instances;
     s->y8_np = ipr::pack_mma_nt(B);
+    s->d_bR = nullptr;
     if ((st = s->alloc(&s->d_bq, (size_t)B * qb)) || (st = s->alloc(&s->d_ybs, (size_t)B * 3 * kN * 8)) ||
         (st = s->alloc(&s->d_zbs, (size_t)B * 3 * kN * 8)) || (st = s->alloc(&s->d_y8, (size_t)2 * s->y8_np * 3 * kN)) ||
-        (st = s->alloc(&s->d_bS, (size_t)B * no * 2 * kN * 4)) || (st = s->alloc(&s->d_bR, (size_t)B * no * kN * 8)) ||
+        (st = s->alloc(&s->d_bS, (size_t)B * no * 2 * kN * 4)) ||
+        (s->fold_mode != 2 && (st = s->alloc(&s->d_bR, (size_t)B * no * kN * 8))) ||
         (st = s->alloc(&s->d_bresp, (size_t)B * rb)))
         return st;
     CU(cudaMallocHost(&s->h_bq, (size_t)B * qb));
@@ -290,12 +300,22 @@ int enqueue_batch(ipr_server* s, int B, const uint8_t* d_queries, uint8_t* d_res
                                     st));
     }
     rec(3);
-    CU(ipr::launch_intt_crt(s->d_bS, s->d_iw, s->d_iwp, s->d_bR, (int)(B * p.instances), st, s->d_zbs, s->d_bth,
-                            (int)p.instances));
-    rec(4);
-    CU(ipr::launch_fold2(s->d_row0, s->d_gsw, s->d_ahat, s->d_bR, (int64_t)(p.instances * kN), s->d_c, s->d_fw,
-                         s->d_fwp, s->d_iw, s->d_iwp, (int)p.interp, (int)p.c, nqt, (int64_t)p.db_cols, 2, d_resps, rb,
-                         (int64_t)(4 + s->per_query_bytes()), st));
+    if (s->fold_mode == 2) {
+        CU(ipr::launch_fold_prep(s->d_bS, (int64_t)B * p.instances, s->d_zbs, s->d_bth, (int)p.instances, s->hp.ninv,
+                                 s->sm_count, st));
+        rec(4);
+        CU(ipr::launch_fold3(s->d_row0s, s->d_gsw, s->d_ahat, s->d_bS, (int64_t)(p.instances * 2 * kN), s->d_c,
+                             s->d_fw, s->d_fwp, s->d_iwu, s->d_iwup, s->hp.ninv, (int)p.interp, (int)p.c, nqt,
+                             (int64_t)p.db_cols, 2, d_resps, rb, (int64_t)(4 + s->per_query_bytes()), st));
+    } else {
+        if (!s->d_bR) return fail(IPR_E_STATE, "batch scratch lacks the INTT output (fold form changed mid-batch)");
+        CU(ipr::launch_intt_crt(s->d_bS, s->d_iw, s->d_iwp, s->d_bR, (int)(B * p.instances), st, s->d_zbs, s->d_bth,
+                                (int)p.instances));
+        rec(4);
+        CU(ipr::launch_fold2(s->d_row0, s->d_gsw, s->d_ahat, s->d_bR, (int64_t)(p.instances * kN), s->d_c, s->d_fw,
+                             s->d_fwp, s->d_iw, s->d_iwp, (int)p.interp, (int)p.c, nqt, (int64_t)p.db_cols, 2, d_resps,
+                             rb, (int64_t)(4 + s->per_query_bytes()), st));
+    }
     CU(ipr::launch_response_frame(d_resps, 2, (int64_t)s->per_query_bytes(), s->d_stash, (int64_t)s->stash_count,
                                   (int64_t)s->stash_entry, st, B, rb));
     rec(5);
@@ -363,6 +383,7 @@ int init_common(ipr_server* s, int device, const ipr_plan* plan) {
     CU(ipr::init_device_kernels());
     CU(ipr::init_gemm1_kernel());
     CU(ipr::init_fold2_kernel());
+    CU(ipr::init_fold3_kernel());
     CU(ipr::init_pack_mma_kernel());
     CU(ipr::init_pack_pair_kernel());
     ipr::host_params_init(s->hp);
@@ -370,8 +391,12 @@ int init_common(ipr_server* s, int device, const ipr_plan* plan) {
     int st;
     const size_t tb = 2 * kN * 4;
     if ((st = s->alloc(&s->d_fw, tb)) || (st = s->alloc(&s->d_fwp, tb)) || (st = s->alloc(&s->d_iw, tb)) ||
-        (st = s->alloc(&s->d_iwp, tb)) || (st = s->alloc(&s->d_row0, tb)))
+        (st = s->alloc(&s->d_iwp, tb)) || (st = s->alloc(&s->d_row0, tb)) || (st = s->alloc(&s->d_iwu, tb)) ||
+        (st = s->alloc(&s->d_iwup, tb)) || (st = s->alloc(&s->d_row0s, tb)))
         return st;
+    CU(cudaMemcpy(s->d_iwu, s->hp.iwu.data(), tb, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(s->d_iwup, s->hp.iwup.data(), tb, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(s->d_row0s, s->hp.row0s.data(), tb, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(s->d_fw, s->hp.fw.data(), tb, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(s->d_fwp, s->hp.fwp.data(), tb, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(s->d_iw, s->hp.iw.data(), tb, cudaMemcpyHostToDevice));
@@ -472,7 +497,7 @@ uint64_t server_batch_bytes(const ipr_server* s, int B) {
     const uint64_t scratch = ipr::query_bytes(rows, (unsigned)nq) + 16 + (nq + 1) / 2 * rows * 16 + nq * 12 * kN * 4 +
                              nq * cols * 8 + s->response_bytes((unsigned)nq) + qb_rows((unsigned)nq) * rows;
     const uint64_t batch = B * qb + 2ull * B * 3 * kN * 8 + 2ull * ipr::pack_mma_nt(B) * 3 * kN +
-                           B * no * 2 * kN * 4 + B * no * kN * 8 + B * rb;
+                           B * no * 2 * kN * 4 + (s->fold_mode != 2 ? B * no * kN * 8 : 0) + B * rb;
     return tpp + scratch + batch;
 }
 
@@ -1007,10 +1032,17 @@ int ipr_server_set_option(ipr_server* s, int option, int64_t value) {
             s->gemv_tc = value != 0;
             destroy_graphs(s);
             return IPR_OK;
-        case IPR_OPT_FOLD_REGISTER_NTT:
-            s->fold_regs = value != 0;
+        case IPR_OPT_FOLD_REGISTER_NTT: {
+            if (value < 0 || value > 2) return fail(IPR_E_ARGS, "IPR_OPT_FOLD_REGISTER_NTT takes 0, 1 or 2");
+            const bool had_r = s->fold_mode != 2;
+            s->fold_mode = (int)value;
             destroy_graphs(s);
+            if ((s->fold_mode != 2) != had_r && s->bcap) {  // the batch scratch changes shape
+                CU(cudaStreamSynchronize(s->stream));
+                s->bcap = 0;
+            }
             return IPR_OK;
+        }
         case IPR_OPT_PACK_CTA_PAIR:
             if (value < 0 || value > 2) return fail(IPR_E_ARGS, "IPR_OPT_PACK_CTA_PAIR takes 0, 1 or 2");
             s->pack_pair = (int)value;

@@ -43,7 +43,7 @@ struct ipr_server {
     uint8_t* d_db8 = nullptr;  // [2][db_cols][db_rows] byte planes for the tensor-core GEMM
     CUtensorMap tm_db;
     bool gemv_tc = false;      // first dimension on tcgen05 (db_rows <= 32768)
-    bool fold_regs = true;     // fold with register-resident NTTs (k_fold2) vs shared-memory NTTs
+    int fold_mode = 2;         // 2 fused fold (k_fold_prep + k_fold3), 1 k_intt_crt + k_fold2, 0 smem fold
     int pack_pair = 2;         // batch packing GEMM on CTA pairs: 0 never, 1 always, 2 from 48 payloads up
     int g1_tile = 0;           // first-dimension GEMM query-byte tile height cap (0 = 256)
     std::map<int, CUtensorMap> tm_qb;  // per query-byte tile height
@@ -51,6 +51,7 @@ struct ipr_server {
     uint8_t* d_stash = nullptr;
     uint64_t stash_count = 0, stash_entry = 0;
     uint32_t *d_fw = nullptr, *d_fwp = nullptr, *d_iw = nullptr, *d_iwp = nullptr, *d_row0 = nullptr;
+    uint32_t *d_iwu = nullptr, *d_iwup = nullptr, *d_row0s = nullptr;  // the fused fold's tables
     // per-request scratch
     unsigned cap_q = 0;
     uint8_t* d_query = nullptr;
