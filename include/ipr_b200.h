@@ -352,6 +352,19 @@ int ipr_device_binary_version(int device, int *binary_version);
  * one of its kernels' waits runs out, after 100 ms there) and the device stays usable. */
 int ipr_selftest_bounded_wait(int device, uint32_t limit_us);
 
+/* Dataset generation on the GPU: DatasetGenerator::generate_record (src/dataset/generator.rs:
+ * 171-193) for records first .. first + count - 1 of the dataset with `seed` and KEM
+ * ML-KEM-`kem` (512, 768 or 1024).  Record i is id (32 bytes) || pk (800 / 1184 / 1568
+ * bytes), written to d_records + i * (32 + pk_len): pk the FIPS 203 encapsulation key from
+ * d = the ChaCha20Rng::seed_from_u64(seed) keystream block number first + i (kem.rs:27-44),
+ * id = SHA3-256("pq-key:v1:" || "ml-kem-<kem>" || pk) (dataset.rs:36-46).  Enqueued on
+ * `stream` (a cudaStream_t, NULL = legacy default). */
+int ipr_dataset_generate(int device, int kem, uint64_t seed, uint64_t first, uint64_t count, uint8_t *d_records,
+                         void *stream);
+/* The same records into host memory h_records (count * (32 + pk_len) bytes), generated in
+ * device batches of up to 65,536 records; returns when they are copied. */
+int ipr_dataset_generate_host(int device, int kem, uint64_t seed, uint64_t first, uint64_t count, uint8_t *h_records);
+
 /* Setup-time database layout and encode on device buffers.
  * ipr_cuckoo_to_raw_db: KeywordCuckooTable::to_raw_db (cuckoo.rs:314-353) — bucket
  * entries (num_buckets x entry_size bytes, row-major) and occupancy flags (one byte

@@ -22,6 +22,8 @@ __all__ = [
     "deserialize_keyword_response", "POLY_LEN", "RESULT_BYTES", "KeywordService", "ServiceStats",
     "shard_plan", "merge_responses", "ShardedKeywordServer", "ntt_batch", "automorph_batch", "encode_db",
     "cuckoo_to_raw_db", "state_file_plan", "offline_precompute", "InspiringPacker",
+    "DatasetGenerator", "Dataset", "DatasetRecord", "derive_public_key_id", "public_key_matches_id",
+    "build_cuckoo_table", "setup_keyword_server",
 ]
 
 POLY_LEN = 2048
@@ -953,3 +955,176 @@ def cuckoo_to_raw_db(d_entries: int, d_occupied: int, num_buckets: int, entry_si
     """ipr_cuckoo_to_raw_db on device buffers"""
     _check(_raw_db(device, _vp(d_entries), _vp(d_occupied), num_buckets, entry_size, db_rows, db_cols, per,
                    _vp(d_raw), _vp(stream)), "cuckoo_to_raw_db")
+
+
+# --- dataset generation and keyword-server setup from a dataset ------------------------------
+# DatasetGenerator / Dataset (src/dataset/generator.rs:16-193, dataset.rs:20-46) and
+# setup_keyword_server (src/dataset/keyword.rs:29-44) over the device generator
+# ipr_dataset_generate and the device setup path.
+
+KEM_PUBLIC_KEY_LEN = {"ml-kem-512": 800, "ml-kem-768": 1184, "ml-kem-1024": 1568}  # kem.rs:47-54
+PUBLIC_KEY_ID_LEN = 32
+PUBLIC_KEY_ID_DOMAIN = b"pq-key:v1:"
+DEFAULT_DATASET_BATCH_SIZE = 100_000
+# CuckooParams of build_cuckoo_table (server/keyword.rs:33-47; cuckoo.rs:29-31, 48-65)
+DETERMINISTIC_SEED = bytes([0xDE, 0xAD, 0xBE, 0xEF, 0xCA, 0xFE, 0xBA, 0xBE,
+                            0x01, 0x23, 0x45, 0x67, 0x89, 0xAB, 0xCD, 0xEF])
+CUCKOO_NUM_HASHES = 2
+CUCKOO_MAX_EVICTIONS = 500
+
+_dataset_gen = _sig("ipr_dataset_generate", _i32, _i32, _i32, _u64, _u64, _u64, _vp, _vp)
+_dataset_gen_host = _sig("ipr_dataset_generate_host", _i32, _i32, _i32, _u64, _u64, _u64, _vp)
+
+
+def derive_public_key_id(public_key: bytes, kem_name: str) -> bytes:
+    """SHA3-256(domain || kem_name || public_key) (dataset.rs:36-46)"""
+    import hashlib
+    return hashlib.sha3_256(PUBLIC_KEY_ID_DOMAIN + kem_name.encode() + bytes(public_key)).digest()
+
+
+def public_key_matches_id(public_key_id: bytes, public_key: bytes, kem_name: str) -> bool:
+    """dataset/keyword.rs:22-24"""
+    return derive_public_key_id(public_key, kem_name) == bytes(public_key_id)
+
+
+@dataclass
+class DatasetRecord:
+    public_key_id: bytes
+    public_key: bytes
+
+
+@dataclass
+class Dataset:
+    kem_name: str
+    public_key_len: int
+    records: List[DatasetRecord]
+
+
+class DatasetGenerator:
+    """DatasetGenerator (generator.rs:16-193): seeded ML-KEM public keys with their IDs,
+    generated on the GPU (ipr_dataset_generate)."""
+
+    def __init__(self, kem: str, count: int):
+        if kem not in KEM_PUBLIC_KEY_LEN:
+            raise ValueError(f"unknown KEM {kem!r}")
+        self.kem, self.count, self.seed, self.batch_size = kem, count, 1, DEFAULT_DATASET_BATCH_SIZE
+
+    def with_seed(self, seed: int) -> "DatasetGenerator":
+        self.seed = seed
+        return self
+
+    def with_batch_size(self, batch_size: int) -> "DatasetGenerator":
+        self.batch_size = batch_size
+        return self
+
+    @property
+    def public_key_len(self) -> int:
+        return KEM_PUBLIC_KEY_LEN[self.kem]
+
+    @property
+    def record_size(self) -> int:
+        return PUBLIC_KEY_ID_LEN + self.public_key_len
+
+    def _validate(self):  # generator.rs:150-164
+        if self.count == 0:
+            raise ValueError("count must be greater than zero")
+        if self.batch_size == 0:
+            raise ValueError("batch_size must be greater than zero")
+
+    def generate_device(self, d_records: int, first: int = 0, count: Optional[int] = None, device: int = 0,
+                        stream: int = 0):
+        """records first .. first + count - 1 as id || pk rows into device memory"""
+        n = self.count - first if count is None else count
+        _check(_dataset_gen(device, int(self.kem.split("-")[-1]), self.seed, first, n, _vp(d_records), _vp(stream)),
+               "ipr_dataset_generate")
+
+    def generate_records(self, device: int = 0):
+        """all records as one host array [count][32 + pk_len] (uint8), generated on the device
+        (ipr_dataset_generate_host)"""
+        import numpy as np
+        self._validate()
+        out = np.empty((self.count, self.record_size), dtype=np.uint8)
+        _check(_dataset_gen_host(device, int(self.kem.split("-")[-1]), self.seed, 0, self.count, _vp(out.ctypes.data)),
+               "ipr_dataset_generate_host")
+        return out
+
+    def generate_in_memory(self, device: int = 0) -> Dataset:
+        """generate_in_memory (generator.rs:59-87): the whole dataset on the host; a duplicate
+        id is an error, as in the reference"""
+        rows = self.generate_records(device)
+        ids = set()
+        records = []
+        for row in rows:
+            rid, pk = row[:PUBLIC_KEY_ID_LEN].tobytes(), row[PUBLIC_KEY_ID_LEN:].tobytes()
+            if rid in ids:
+                raise ValueError("duplicate public key id generated")
+            ids.add(rid)
+            records.append(DatasetRecord(rid, pk))
+        return Dataset(self.kem, self.public_key_len, records)
+
+
+def build_cuckoo_table(keys: Sequence[bytes], values: Sequence[bytes], num_buckets: int, key_size: int,
+                       value_size: int, seed: bytes = DETERMINISTIC_SEED, eviction_seed: int = 0):
+    """build_cuckoo_table (server/keyword.rs:33-47) with CuckooTable::insert (cuckoo.rs:199-246):
+    each record goes to its first free position of the two SipHash-2-4 positions, else
+    evicts at a random hash position up to 500 times, else joins the stash.  The reference
+    draws the eviction choice from the unseeded rand::rng(); here it is a seeded generator,
+    so the table is reproducible.  Returns (entries [num_buckets][entry] uint8, occupied
+    uint8 [num_buckets], stash list of entry bytes)."""
+    import random
+    import numpy as np
+    es = key_size + value_size
+    entries = np.zeros((num_buckets, es), dtype=np.uint8)
+    occ = np.zeros(num_buckets, dtype=np.uint8)
+    stash = []
+    rng = random.Random(eviction_seed)
+
+    def positions(k):
+        return cuckoo_positions(seed, num_buckets, CUCKOO_NUM_HASHES, k)
+
+    for key, value in zip(keys, values):
+        entry = np.zeros(es, dtype=np.uint8)
+        entry[:key_size] = np.frombuffer(bytes(key), dtype=np.uint8)
+        entry[key_size:key_size + len(value)] = np.frombuffer(bytes(value), dtype=np.uint8)
+        placed = False
+        for p in positions(bytes(key)):
+            if not occ[p]:
+                entries[p], occ[p], placed = entry, 1, True
+                break
+        for _ in range(0 if placed else CUCKOO_MAX_EVICTIONS):
+            p = positions(entry[:key_size].tobytes())[rng.randrange(CUCKOO_NUM_HASHES)]
+            evicted = entries[p].copy()
+            entries[p], occ[p] = entry, 1
+            entry = evicted
+            for q in positions(entry[:key_size].tobytes()):
+                if not occ[q]:
+                    entries[q], occ[q], placed = entry, 1, True
+                    break
+            if placed:
+                break
+        if not placed:
+            stash.append(entry.tobytes())
+    return entries, occ, stash
+
+
+def setup_keyword_server(dataset: Dataset, buckets: Optional[int] = None, dim0: Optional[int] = None,
+                         device: int = 0) -> "KeywordServer":
+    """setup_keyword_server (dataset/keyword.rs:29-44): records (id -> public key) in a cuckoo
+    table under DETERMINISTIC_SEED, its raw DB (to_raw_db, on the device), then
+    KeywordServer::setup on the GPU (encode + offline precomputation)."""
+    import torch
+    plan = plan_from_shape(len(dataset.records), PUBLIC_KEY_ID_LEN, dataset.public_key_len, buckets, dim0)
+    entries, occ, stash = build_cuckoo_table([r.public_key_id for r in dataset.records],
+                                             [r.public_key for r in dataset.records], plan.num_items,
+                                             PUBLIC_KEY_ID_LEN, dataset.public_key_len)
+    dev = f"cuda:{device}"
+    d_entries = torch.from_numpy(entries.reshape(-1)).to(dev)
+    d_occ = torch.from_numpy(occ).to(dev)
+    d_raw = torch.empty(plan.db_rows * plan.db_cols, dtype=torch.int16, device=dev)
+    cuckoo_to_raw_db(d_entries.data_ptr(), d_occ.data_ptr(), plan.num_items, plan.entry_size, plan.db_rows,
+                     plan.db_cols, plan.num_items // plan.db_rows, d_raw.data_ptr(), device=device)
+    torch.cuda.synchronize(device)
+    raw = d_raw.cpu().numpy().view("uint16")
+    return KeywordServer.setup(plan, raw, raw=True, stash=stash, key_size=PUBLIC_KEY_ID_LEN,
+                               value_size=dataset.public_key_len, num_records=len(dataset.records),
+                               cuckoo_seed=DETERMINISTIC_SEED, device=device)

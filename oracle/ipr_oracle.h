@@ -191,6 +191,17 @@ int ipr_oracle_offline_instance(const ipr_params *p, const uint16_t *db, uint64_
 
 int ipr_oracle_threads(void);
 
+/* dataset generation (ipr_dataset.c): FIPS 202 hashes, FIPS 203 encapsulation keys, the
+ * rand_core record-seed key and one DatasetGenerator record (id || pk) */
+void ipr_keccakf(uint64_t a[25]);
+void ipr_sha3_256(const uint8_t *m, size_t n, uint8_t out[32]);
+void ipr_sha3_512(const uint8_t *m, size_t n, uint8_t out[64]);
+void ipr_shake128(const uint8_t *m, size_t n, uint8_t *out, size_t outlen);
+void ipr_shake256(const uint8_t *m, size_t n, uint8_t *out, size_t outlen);
+void ipr_mlkem_ek(int k, const uint8_t d[32], uint8_t *ek);
+void ipr_seed_from_u64(uint64_t state, uint8_t key[32]);
+void ipr_dataset_record(int kem_k, uint64_t seed, uint64_t idx, uint8_t *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -540,3 +540,71 @@ def inspiring_pack(lwe: np.ndarray, y_body: np.ndarray, z_body: np.ndarray) -> n
     sdb.stash, sdb._stash_buf = [], np.zeros(1, dtype=np.uint8)
     S = packing_sum(sdb, y_body, z_body)
     return postprocess(sdb, S, lwe[N])[0]
+
+
+# --- dataset generation (ipr_dataset.c): FIPS 202 / FIPS 203 / rand seeds ------------------
+_sha3_256 = _sig("ipr_sha3_256", None, _p, _sz, _p)
+_sha3_512 = _sig("ipr_sha3_512", None, _p, _sz, _p)
+_shake128 = _sig("ipr_shake128", None, _p, _sz, _p, _sz)
+_shake256 = _sig("ipr_shake256", None, _p, _sz, _p, _sz)
+_mlkem_ek = _sig("ipr_mlkem_ek", None, ctypes.c_int, _p, _p)
+_seed_u64 = _sig("ipr_seed_from_u64", None, _u64, _p)
+_record = _sig("ipr_dataset_record", None, ctypes.c_int, _u64, _u64, _p)
+
+KEM_K = {"ml-kem-512": 2, "ml-kem-768": 3, "ml-kem-1024": 4}
+
+
+def _bufp(b: bytes):
+    a = np.frombuffer(bytes(b) or b"\0", dtype=np.uint8).copy()
+    return a, _ptr(a)
+
+
+def sha3_256(m: bytes) -> bytes:
+    a, p = _bufp(m)
+    out = np.zeros(32, dtype=np.uint8)
+    _sha3_256(p, len(m), _ptr(out))
+    return out.tobytes()
+
+
+def sha3_512(m: bytes) -> bytes:
+    a, p = _bufp(m)
+    out = np.zeros(64, dtype=np.uint8)
+    _sha3_512(p, len(m), _ptr(out))
+    return out.tobytes()
+
+
+def shake128(m: bytes, n: int) -> bytes:
+    a, p = _bufp(m)
+    out = np.zeros(max(n, 1), dtype=np.uint8)
+    _shake128(p, len(m), _ptr(out), n)
+    return out[:n].tobytes()
+
+
+def shake256(m: bytes, n: int) -> bytes:
+    a, p = _bufp(m)
+    out = np.zeros(max(n, 1), dtype=np.uint8)
+    _shake256(p, len(m), _ptr(out), n)
+    return out[:n].tobytes()
+
+
+def mlkem_ek(kem: str, d: bytes) -> bytes:
+    """FIPS 203 K-PKE.KeyGen(d) encapsulation key (ML-KEM.KeyGen_internal's ek)"""
+    k = KEM_K[kem]
+    a, p = _bufp(d[:32])
+    out = np.zeros(384 * k + 32, dtype=np.uint8)
+    _mlkem_ek(k, p, _ptr(out))
+    return out.tobytes()
+
+
+def seed_from_u64(seed: int) -> bytes:
+    out = np.zeros(32, dtype=np.uint8)
+    _seed_u64(seed, _ptr(out))
+    return out.tobytes()
+
+
+def dataset_record(kem: str, seed: int, idx: int):
+    """(id, public key) of record idx of DatasetGenerator(kem).with_seed(seed)"""
+    k = KEM_K[kem]
+    out = np.zeros(32 + 384 * k + 32, dtype=np.uint8)
+    _record(k, seed, idx, _ptr(out))
+    return out[:32].tobytes(), out[32:].tobytes()

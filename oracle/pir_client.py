@@ -329,3 +329,30 @@ def cuckoo_positions(seed: bytes, num_buckets: int, num_hashes: int, key: bytes)
         return [idx % half if i == 0 else half + idx % half for i in range(num_hashes)]
     s0, s1 = int.from_bytes(seed[:8], "little"), int.from_bytes(seed[8:16], "little")
     return [siphash24(s0 ^ i, s1 ^ (i << 32), bytes(key)) % num_buckets for i in range(num_hashes)]
+
+
+# --- the e2e test's target selection (tests/e2e_mlkem.rs:17-19) -------------------------------
+def chacha_u32_stream(seed_u64: int):
+    """next_u32 of ChaCha20Rng::seed_from_u64(seed) (rand_core's PCG32 key expansion, then the
+    keystream words in order); a restatement of the crates' published algorithms"""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    import oracle as orc
+    key = orc.seed_from_u64(seed_u64)
+    ctr = 0
+    while True:
+        for w in orc.chacha_blocks(key, 0, ctr, 1)[0]:
+            yield int(w)
+        ctr += 1
+
+
+def random_range_u32(words, n: int) -> int:
+    """a uniform index in [0, n) from u32 words by the widening multiply with one
+    bias-correcting step (the single-sample integer method of rand 0.9 / 0.10 for ranges
+    that fit u32); which record the e2e test picks does not change what it checks"""
+    hi, lo = divmod(next(words) * n, 1 << 32)
+    if lo > (-n) % (1 << 32):
+        hi2 = (next(words) * n) >> 32
+        hi += (lo + hi2) >> 32
+    return hi
