@@ -665,24 +665,50 @@ def main():
         svc.close()
 
     # ---- the plain batch-1 u64 path on the same GPU (CUDA-core GEMV + packing) ----------
-    b1 = {}
+    # the CUDA-core GEMV is timed in each of its forms (DB columns per warp); the fastest is
+    # the u64 figure, its stage time against HBM (2 bytes per DB element, both queries in one
+    # pass) is its roofline
+    b1, u64_forms = {}, []
     if B > 1 and not args.no_batch1:
         d1 = torch.frombuffer(bytearray(payloads[0]), dtype=torch.uint8).to(dev)
         d1o = torch.empty(rbytes, dtype=torch.uint8, device=dev)
-        for mode, tc in (("u64", 0), ("tensor_gemv", 1)):
-            srv.set_option(pkg.KeywordServer.OPT_TENSOR_GEMV, tc)
+        k1 = max(5, min(args.steps, 20))
+
+        def single_rate():
             for _ in range(2):
                 srv.respond_device(d1.data_ptr(), qbytes, d1o.data_ptr(), rbytes)
             srv.sync()
-            k1 = max(5, min(args.steps, 20))
             a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a0.record(stream)
             for _ in range(k1):
                 srv.respond_device(d1.data_ptr(), qbytes, d1o.data_ptr(), rbytes)
             a1.record(stream)
             srv.sync()
-            b1[mode] = k1 / (a0.elapsed_time(a1) / 1000.0)
+            return k1 / (a0.elapsed_time(a1) / 1000.0)
+
+        def single_gemv_ms():
+            srv.set_profiling(True)
+            for _ in range(k1):
+                srv.respond_device(d1.data_ptr(), qbytes, d1o.data_ptr(), rbytes)
+            srv.sync()
+            st_ms, n_calls = srv.stage_times()
+            srv.set_profiling(False)
+            return st_ms["gemv"] / max(n_calls, 1)
+
+        srv.set_option(pkg.KeywordServer.OPT_TENSOR_GEMV, 0)
+        gemv_bytes = 2 * plan.db_rows * plan.db_cols
+        for cols in (8, 4, 2):
+            srv.set_option(pkg.KeywordServer.OPT_GEMV_COLS, cols)
+            rate = single_rate()
+            gms = single_gemv_ms()
+            u64_forms.append({"cols_per_warp": cols, "payloads_per_s": rate, "gemv_ms": gms,
+                              "gemv_gbs": gemv_bytes / (gms / 1000.0) / 1e9})
+        best = min(u64_forms, key=lambda f: f["gemv_ms"])
+        srv.set_option(pkg.KeywordServer.OPT_GEMV_COLS, best["cols_per_warp"])
+        b1["u64"] = max(f["payloads_per_s"] for f in u64_forms)
         srv.set_option(pkg.KeywordServer.OPT_TENSOR_GEMV, 1)
+        b1["tensor_gemv"] = single_rate()
+        b1["u64_gemv"] = dict(best, bytes=gemv_bytes)
 
     t = torch.tensor([dev_ms, e2e_ms], dtype=torch.float64, device=dev)
     if dist is not None:
@@ -753,7 +779,14 @@ def main():
                     "blocking_batch_call_payloads_per_s": args.steps * B / (blocking_ms / 1000.0)},
             "serving": serving or None,
             "batch1": ({"u64_payloads_per_s": b1["u64"], "tensor_gemv_payloads_per_s": b1["tensor_gemv"],
-                        "speedup_vs_batch1_u64": value / world / b1["u64"]} if b1 else None),
+                        "speedup_vs_batch1_u64": value / world / b1["u64"],
+                        "u64_gemv_roofline": {"bound": "hbm", "kernel": "k_gemv (u64, CUDA cores)",
+                                              "cols_per_warp": b1["u64_gemv"]["cols_per_warp"],
+                                              "avg_launch_ms": b1["u64_gemv"]["gemv_ms"],
+                                              "algorithmic_bytes": b1["u64_gemv"]["bytes"],
+                                              "achieved": b1["u64_gemv"]["gemv_gbs"], "peak": peak, "unit": "GB/s",
+                                              "frac": b1["u64_gemv"]["gemv_gbs"] / peak},
+                        "u64_forms": u64_forms} if b1 else None),
             "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": ("measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                                          else "fallback 6.65 TB/s (MEASURED_PEAKS.json absent)"),

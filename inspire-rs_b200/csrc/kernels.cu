@@ -109,14 +109,17 @@ __global__ void k_parse_query(const uint8_t* __restrict__ qb_all, int nq, int db
 // D is column-major [db_cols][db_rows] u16 (the reference layout).  A warp owns
 // COLS consecutive columns; lane l reads 16 B (8 rows) of each column per
 // 256-row stripe, so every load instruction covers 512 contiguous bytes.
-// Per-lane u64 partial sums are combined by a 31-shuffle transpose-reduce.
+// Per-lane u64 partial sums (NV = COLS * NQ * 2 of them) are folded across lane
+// groups down to NV lanes and combined by a transpose-reduce.  Fewer columns per
+// warp mean fewer accumulators, so more warps fit on an SM (MINB CTAs of 256) to
+// keep loads in flight.
 // ---------------------------------------------------------------------------
-template <int NQ, int COLS>
-__global__ void __launch_bounds__(256) k_gemv(const uint16_t* __restrict__ db, int db_rows,
-                                              int64_t db_cols, const uint32_t* __restrict__ a_il,
-                                              uint64_t* __restrict__ c) {
-    constexpr int NV = COLS * NQ * 2;  // values reduced per warp task (must be 32)
-    static_assert(NV == 32, "transpose-reduce expects 32 values per lane");
+template <int NQ, int COLS, int MINB = 1>
+__global__ void __launch_bounds__(256, MINB) k_gemv(const uint16_t* __restrict__ db, int db_rows,
+                                                    int64_t db_cols, const uint32_t* __restrict__ a_il,
+                                                    uint64_t* __restrict__ c) {
+    constexpr int NV = COLS * NQ * 2;  // values reduced per warp task
+    static_assert(NV == 8 || NV == 16 || NV == 32, "8, 16 or 32 values per lane");
     const int lane = threadIdx.x & 31;
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -158,9 +161,14 @@ __global__ void __launch_bounds__(256) k_gemv(const uint16_t* __restrict__ db, i
                 }
             }
         }
-        // transpose-reduce: lane v ends with the warp-wide sum of value v
+        // fold lane groups down to NV lanes, then transpose-reduce: lane v (< NV) ends with the
+        // warp-wide sum of value v (lanes v + NV, v + 2 NV, ... hold copies)
 #pragma unroll
-        for (int s = 16; s >= 1; s >>= 1) {
+        for (int s = 16; s >= NV; s >>= 1)
+#pragma unroll
+            for (int i = 0; i < NV; i++) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], s);
+#pragma unroll
+        for (int s = NV / 2; s >= 1; s >>= 1) {
             const bool upper = lane & s;
 #pragma unroll
             for (int i = 0; i < s; i++) {
@@ -173,7 +181,7 @@ __global__ void __launch_bounds__(256) k_gemv(const uint16_t* __restrict__ db, i
         const int l = lane & 1;
         const uint32_t r = modq(acc[0], l);
         const uint32_t other = __shfl_xor_sync(0xffffffffu, r, 1);
-        if (l == 0) {
+        if (l == 0 && lane < NV) {
             const int q = (lane >> 1) % NQ, cc = lane / (NQ * 2);
             c[(int64_t)q * db_cols + col0 + cc] = crt2(r, other, c_q0inv, c_br[1]);
         }
@@ -588,9 +596,11 @@ cudaError_t launch_parse_batch(const uint8_t* qb, int npay, int64_t pstride, int
 }
 
 cudaError_t launch_gemv(const uint16_t* db, int db_rows, int64_t db_cols, int nq, const uint32_t* a_il,
-                        uint64_t* c, int sm_count, cudaStream_t st) {
+                        uint64_t* c, int sm_count, cudaStream_t st, int cols) {
     const int blocks = sm_count * 4;
-    if (nq == 2) k_gemv<2, 8><<<blocks, 256, 0, st>>>(db, db_rows, db_cols, a_il, c);
+    if (nq == 2 && cols == 8) k_gemv<2, 8><<<blocks, 256, 0, st>>>(db, db_rows, db_cols, a_il, c);
+    else if (nq == 2 && cols == 4) k_gemv<2, 4, 2><<<sm_count * 2, 256, 0, st>>>(db, db_rows, db_cols, a_il, c);
+    else if (nq == 2 && cols == 2) k_gemv<2, 2, 3><<<sm_count * 3, 256, 0, st>>>(db, db_rows, db_cols, a_il, c);
     else if (nq == 1) k_gemv<1, 16><<<blocks, 256, 0, st>>>(db, db_rows, db_cols, a_il, c);
     else return cudaErrorInvalidValue;
     return cudaGetLastError();

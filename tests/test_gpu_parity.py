@@ -89,10 +89,12 @@ def test_first_dimension_paths(cfg0, pkg, orc, tensor, nq):
         srv.set_option(pkg.KeywordServer.OPT_TENSOR_GEMV, 1)
 
 
-@pytest.mark.parametrize("regs", [0, 1])
+@pytest.mark.parametrize("regs", [0, 1, 2])
 @pytest.mark.parametrize("instances,interp", [(8, 8), (8, 1), (6, 2)])
 def test_fold_kernels(pkg, orc, regs, instances, interp):
-    """register-resident-NTT fold and shared-memory fold give the oracle's bytes"""
+    """the three fold forms (shared-memory NTTs, register NTTs after a separate INTT + CRT
+    pass, register NTTs with that pass fused in) give the oracle's bytes, for one, eight and
+    three fold groups (an odd count leaves the fused fold's second team of a CTA idle)"""
     plan = _plan(pkg, instances, interp)
     with pkg.KeywordServer.synthetic(plan, seed=50 + instances + interp) as srv:
         srv.set_option(pkg.KeywordServer.OPT_FOLD_REGISTER_NTT, regs)
@@ -100,6 +102,21 @@ def test_fold_kernels(pkg, orc, regs, instances, interp):
         for nq in (1, 2, 3):
             q = orc.synth_query(60 + nq, plan.db_rows, nq)
             assert srv.respond_to_serialized_query(q) == orc.respond(sdb, q)
+
+
+@pytest.mark.parametrize("cols", [2, 4, 8])
+def test_u64_gemv_forms(cfg0, pkg, orc, cols):
+    """the CUDA-core GEMV with 2, 4 or 8 DB columns per warp gives the oracle's bytes"""
+    plan, srv, sdb = cfg0
+    srv.set_option(pkg.KeywordServer.OPT_TENSOR_GEMV, 0)
+    srv.set_option(pkg.KeywordServer.OPT_GEMV_COLS, cols)
+    try:
+        for nq in (1, 2, 3):
+            q = orc.synth_query(70 + nq + cols, plan.db_rows, nq)
+            assert srv.respond_to_serialized_query(q) == orc.respond(sdb, q)
+    finally:
+        srv.set_option(pkg.KeywordServer.OPT_GEMV_COLS, 8)
+        srv.set_option(pkg.KeywordServer.OPT_TENSOR_GEMV, 1)
 
 
 def test_first_dimension_tensor_wide_rows(pkg, orc):
