@@ -495,6 +495,10 @@ def main():
     ap.add_argument("--dim0", type=int, default=None)
     ap.add_argument("--batch", type=int, default=64, help="payloads per step (1 = batch-1 u64 packing path)")
     ap.add_argument("--no-batch1", action="store_true", help="skip the batch-1 comparison measurement")
+    ap.add_argument("--shard", action="store_true",
+                    help="under torchrun: one database split by fold groups over the ranks (each rank answers its "
+                         "groups of every payload; NCCL broadcast of the queries and gather of the parts) "
+                         "instead of one replica per rank")
     ap.add_argument("--fold-form", type=int, default=2, choices=[1, 2],
                     help="2: fold with the packing post-process fused in (default); 1: separate INTT + CRT pass")
     ap.add_argument("--no-serving", action="store_true", help="skip the Poisson serving measurement")
@@ -552,7 +556,12 @@ def main():
         plan = pkg.plan_from_shape(args.records, KEY, VALUE, args.buckets, args.dim0)
     else:
         plan = pkg.plan_from_shape(RECORDS, KEY, VALUE, BUCKETS, DIM0)
-    srv = pkg.KeywordServer.synthetic(plan, seed=7 + rank, device=dev)
+    shard = args.shard and world > 1
+    if shard:  # this rank's fold groups of one synthetic database
+        srv = pkg.KeywordServer.synthetic_shard(plan, world, rank, seed=7, device=dev)
+    else:
+        srv = pkg.KeywordServer.synthetic(plan, seed=7 + rank, device=dev)
+    local = srv.plan  # the rank's share: the whole plan for a replica, a fold-group slice for a shard
     if args.fold_form != 2:
         srv.set_option(pkg.KeywordServer.OPT_FOLD_REGISTER_NTT, args.fold_form)
     qbytes = srv.query_bytes(2)
@@ -575,7 +584,7 @@ def main():
     PASS = 64
     passes = (B + PASS - 1) // PASS if B > 1 else 1
     npay = max(2 * B, 4)
-    payloads = [synth_payload(1000 * rank + i) for i in range(npay)]
+    payloads = [synth_payload((0 if shard else 1000 * rank) + i) for i in range(npay)]
     assert len(payloads[0]) == qbytes
     stream = torch.cuda.ExternalStream(srv.stream_handle(), device=dev)
     # HBM-resident inputs: two distinct batches of B payloads, alternated
@@ -627,12 +636,13 @@ def main():
     barrier()
     dev_ms = e0.elapsed_time(e1)
     stage_ms, calls = srv.stage_times()
+    plan_response_bytes = 4 + 2 * (4 + plan.c * 12288) + 4  # the merged (whole-database) response
     srv.set_profiling(False)
     clk = clocks.stop()
 
     # ---- end-to-end through the serving API: host buffers, H2D + D2H of every batch ---------
     # (KeywordService: continuous batching, pinned staging, copies overlapped with compute)
-    svc = pkg.KeywordService([srv], max_batch=min(B, PASS)) if B > 1 else None
+    svc = pkg.KeywordService([srv], max_batch=min(B, PASS)) if B > 1 and not shard else None
     barrier()
     # the blocking call (ipr_server_respond_batch / ipr_server_respond), for comparison
     t0 = time.perf_counter()
@@ -640,6 +650,18 @@ def main():
         run_host(i)
     blocking_ms = (time.perf_counter() - t0) * 1000
     e2e_ms = blocking_ms
+    if shard:
+        # the public sharded API: rank 0's host payloads broadcast over NCCL, every rank answers
+        # its groups (ipr_server_respond_batch, host bytes), the parts gathered and merged on rank 0
+        sks = pkg.ShardedKeywordServer(srv.respond_to_serialized_query, device=torch.device("cuda", dev))
+        sks.respond_batch(payloads[:B] if rank == 0 else None, srv.respond_batch)
+        barrier()
+        t0 = time.perf_counter()
+        for i in range(args.steps):
+            batch = payloads[(i % 2) * B:(i % 2 + 1) * B]
+            sks.respond_batch(batch if rank == 0 else None, srv.respond_batch)
+        barrier()
+        e2e_ms = (time.perf_counter() - t0) * 1000
     if svc is not None:
         for t in [svc.submit(0, payloads[i % npay]) for i in range(2 * B)]:
             svc.wait(t)
@@ -669,7 +691,7 @@ def main():
     # the u64 figure, its stage time against HBM (2 bytes per DB element, both queries in one
     # pass) is its roofline
     b1, u64_forms = {}, []
-    if B > 1 and not args.no_batch1:
+    if B > 1 and not args.no_batch1 and not shard:
         d1 = torch.frombuffer(bytearray(payloads[0]), dtype=torch.uint8).to(dev)
         d1o = torch.empty(rbytes, dtype=torch.uint8, device=dev)
         k1 = max(5, min(args.steps, 20))
@@ -714,17 +736,17 @@ def main():
     if dist is not None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     dev_ms, e2e_ms = float(t[0]), float(t[1])
-    total = args.steps * B * world
+    total = args.steps * B * (1 if shard else world)  # a shard answers part of every payload
     value = total / (dev_ms / 1000.0)
     e2e = total / (e2e_ms / 1000.0)
 
     peak, peak_kind = read_peaks()
     pack_ms = stage_ms["pack"] / max(calls, 1)
     if B > 1:  # the packing GEMM streams the slot-indexed precomputation once per batch
-        pack_bytes = N * 2 * ((plan.instances + 31) // 32) * 128 * 3 * N  # [slot][limb][tile][128 rows][6144]
+        pack_bytes = N * 2 * ((local.instances + 31) // 32) * 128 * 3 * N  # [slot][limb][tile][128 rows][6144]
         kname = "k_pack_mma_pair" if min(B, PASS) >= 48 else "k_pack_mma"  # the server's default choice of form
     else:
-        pack_bytes = plan.instances * (2 * 3069 + 3) * N * 8  # bold_t + bold_t_bar + bold_t_hat per launch
+        pack_bytes = local.instances * (2 * 3069 + 3) * N * 8  # bold_t + bold_t_bar + bold_t_hat per launch
         kname = "k_pack"
     achieved = pack_bytes / (pack_ms / 1000.0) / 1e9
     tensor = None
@@ -764,18 +786,23 @@ def main():
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u8 limbs -> s32 / u64" if B > 1 else "u64",
+            "scaling": "strong" if shard else "weak", "vs_baseline": None,
+            "dtype": "u8 limbs -> s32 / u64" if B > 1 else "u64",
             "data": "synthetic",
             "config": {"workload": wl if not small else f"{args.records} ML-KEM-768 records (profiling case)",
                        "records": args.records, "buckets": plan.num_items, "dim0": plan.dim0, "db_rows": plan.db_rows,
                        "db_cols": plan.db_cols, "instances": plan.instances, "interp": plan.interp, "c": plan.c,
-                       "batch_payloads": B, "parallelism": f"replica x{world}",
+                       "batch_payloads": B,
+                       "parallelism": f"fold-group shards x{world}" if shard else f"replica x{world}",
+                       "rank0_share": {"instances": local.instances, "c": local.c, "db_cols": local.db_cols},
                        "autotune": ({"chosen": tune["chosen"], "candidates": tune["candidates"]} if tune else None),
                        "l2": "inputs larger than L2 (packing stream of %.1f GB + DB of %.2f GB per step)" % (
                            pack_bytes / 1e9, plan.db_rows * plan.db_cols * 2 / 1e9)},
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": B * qbytes, "d2h_bytes_per_step": B * rbytes,
-                    "api": (f"KeywordService (ipr_service_submit_batch per {B} payloads / ipr_service_wait)" if B > 1
-                            else "ipr_server_respond"),
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": B * qbytes,
+                    "d2h_bytes_per_step": B * (plan_response_bytes if shard else rbytes),
+                    "api": ("ShardedKeywordServer.respond_batch (NCCL broadcast / gather, ipr_response_merge)" if shard
+                            else f"KeywordService (ipr_service_submit_batch per {B} payloads / ipr_service_wait)"
+                            if B > 1 else "ipr_server_respond"),
                     "blocking_batch_call_payloads_per_s": args.steps * B / (blocking_ms / 1000.0)},
             "serving": serving or None,
             "batch1": ({"u64_payloads_per_s": b1["u64"], "tensor_gemv_payloads_per_s": b1["tensor_gemv"],

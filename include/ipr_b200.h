@@ -122,6 +122,12 @@ int ipr_server_setup(int device, const ipr_plan *plan, const ipr_server_data *da
  * (uniform u16 < 65535, uniform residues), the timing mode the reference
  * itself uses (online_only, src/pir/server/engine.rs:693-729). */
 int ipr_server_create_synthetic(int device, const ipr_plan *plan, uint64_t seed, ipr_server **out);
+/* Shard `shard` of `num_shards` (ipr_plan_shard) of the synthetic server that
+ * ipr_server_create_synthetic(full, seed) builds: the same elements of DB and
+ * precomputation, generated alone, so the shards' merged responses equal the full
+ * server's. */
+int ipr_server_create_synthetic_shard(int device, const ipr_plan *full, int num_shards, int shard, uint64_t seed,
+                                      ipr_server **out);
 
 void ipr_server_destroy(ipr_server *srv);
 

@@ -68,6 +68,8 @@ _plan_from_shape = _sig("ipr_plan_from_shape", _i32, _u64, _u64, _u64, _u64, _u6
 _query_bytes = _sig("ipr_query_bytes", _u64, _u64, ctypes.c_uint)
 _create = _sig("ipr_server_create", _i32, _i32, ctypes.POINTER(_Plan), ctypes.POINTER(_ServerData), ctypes.POINTER(_vp))
 _create_synth = _sig("ipr_server_create_synthetic", _i32, _i32, ctypes.POINTER(_Plan), _u64, ctypes.POINTER(_vp))
+_create_synth_shard = _sig("ipr_server_create_synthetic_shard", _i32, _i32, ctypes.c_void_p, _i32, _i32, _u64,
+                           ctypes.POINTER(_vp))
 _destroy = _sig("ipr_server_destroy", None, _vp)
 _pp_json = _sig("ipr_server_public_params_json", _i32, _vp, ctypes.c_char_p, _sz, ctypes.POINTER(_sz))
 _srv_qbytes = _sig("ipr_server_query_bytes", _u64, _vp, ctypes.c_uint)
@@ -421,6 +423,17 @@ class KeywordServer:
         pc = plan._c()
         _check(_create_synth(device, ctypes.byref(pc), seed, ctypes.byref(h)), "ipr_server_create_synthetic")
         return cls(h.value, plan, device)
+
+    @classmethod
+    def synthetic_shard(cls, full: Plan, num_shards: int, shard: int, seed: int = 7,
+                        device: int = 0) -> "KeywordServer":
+        """shard `shard` of `num_shards` (fold groups, ipr_plan_shard) of synthetic(full, seed),
+        generated alone on the device: the shards' merged responses are the full server's"""
+        h = _vp()
+        pc = full._c()
+        _check(_create_synth_shard(device, ctypes.byref(pc), num_shards, shard, seed, ctypes.byref(h)),
+               "ipr_server_create_synthetic_shard")
+        return cls(h.value, shard_plan(full, num_shards, shard)[0], device)
 
     @classmethod
     def load(cls, path: str, device: int = 0) -> "KeywordServer":
@@ -931,6 +944,36 @@ class ShardedKeywordServer:
         part = self._answer(q)
         parts = self._gather_bytes(part)
         return merge_responses(parts) if parts is not None else None
+
+    def respond_batch(self, queries: Optional[Sequence[bytes]], answer_batch=None) -> Optional[List[bytes]]:
+        """collective batch form: rank 0's payloads travel in one broadcast, every rank answers
+        them with `answer_batch` (list -> list, e.g. its KeywordServer.respond_batch; default:
+        `answer` per payload), the parts come back in one gather and rank 0 merges each
+        payload's parts (other ranks return None)"""
+        import struct
+        if self.rank == 0:
+            blob = struct.pack("<I", len(queries)) + b"".join(struct.pack("<Q", len(q)) + bytes(q) for q in queries)
+        else:
+            blob = None
+        blob = self._bcast_bytes(blob)
+        n, off, qs = struct.unpack_from("<I", blob)[0], 4, []
+        for _ in range(n):
+            k = struct.unpack_from("<Q", blob, off)[0]
+            qs.append(blob[off + 8:off + 8 + k])
+            off += 8 + k
+        mine = answer_batch(qs) if answer_batch is not None else [self._answer(q) for q in qs]
+        parts = self._gather_bytes(b"".join(struct.pack("<Q", len(r)) + r for r in mine))
+        if parts is None:
+            return None
+        per_rank = []
+        for blob_r in parts:
+            rs, o = [], 0
+            while o < len(blob_r):
+                k = struct.unpack_from("<Q", blob_r, o)[0]
+                rs.append(blob_r[o + 8:o + 8 + k])
+                o += 8 + k
+            per_rank.append(rs)
+        return [merge_responses([rs[i] for rs in per_rank]) for i in range(n)]
 
 
 # ---------------------------------------------------------------------------

@@ -555,21 +555,23 @@ __device__ __forceinline__ uint64_t synth(uint64_t seed, uint64_t stream, uint64
     return x;
 }
 
-__global__ void k_synth_db(uint16_t* db, int64_t n, uint64_t seed) {
+// element i of the output is element idx0 + i of the whole synthetic array (a fold-group
+// shard of a larger synthetic server is generated alone)
+__global__ void k_synth_db(uint16_t* db, int64_t n, uint64_t seed, uint64_t idx0) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        db[i] = (uint16_t)(synth(seed, 1, (uint64_t)i) % PT);
+        db[i] = (uint16_t)(synth(seed, 1, idx0 + (uint64_t)i) % PT);
 }
 
-__global__ void k_synth_condensed(uint64_t* out, int64_t n, uint64_t seed, uint64_t stream) {
+__global__ void k_synth_condensed(uint64_t* out, int64_t n, uint64_t seed, uint64_t stream, uint64_t idx0) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint64_t x = synth(seed, stream, (uint64_t)i);
+        const uint64_t x = synth(seed, stream, idx0 + (uint64_t)i);
         out[i] = ((x & 0xffffffffull) % Q0) | (((x >> 32) % Q1) << 32);
     }
 }
 
-__global__ void k_synth_modq(uint64_t* out, int64_t n, uint64_t seed, uint64_t stream) {
+__global__ void k_synth_modq(uint64_t* out, int64_t n, uint64_t seed, uint64_t stream, uint64_t idx0) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        out[i] = synth(seed, stream, (uint64_t)i) % QQ;
+        out[i] = synth(seed, stream, idx0 + (uint64_t)i) % QQ;
 }
 
 // ---------------------------------------------------------------------------
@@ -662,16 +664,18 @@ cudaError_t launch_ntt_batch(uint64_t* data, int npairs, int forward, const uint
     return cudaGetLastError();
 }
 
-cudaError_t launch_synth_db(uint16_t* db, int64_t n, uint64_t seed, cudaStream_t st) {
-    k_synth_db<<<148 * 8, 256, 0, st>>>(db, n, seed);
+cudaError_t launch_synth_db(uint16_t* db, int64_t n, uint64_t seed, cudaStream_t st, uint64_t idx0) {
+    k_synth_db<<<148 * 8, 256, 0, st>>>(db, n, seed, idx0);
     return cudaGetLastError();
 }
-cudaError_t launch_synth_condensed(uint64_t* out, int64_t n, uint64_t seed, uint64_t stream, cudaStream_t st) {
-    k_synth_condensed<<<148 * 8, 256, 0, st>>>(out, n, seed, stream);
+cudaError_t launch_synth_condensed(uint64_t* out, int64_t n, uint64_t seed, uint64_t stream, cudaStream_t st,
+                                   uint64_t idx0) {
+    k_synth_condensed<<<148 * 8, 256, 0, st>>>(out, n, seed, stream, idx0);
     return cudaGetLastError();
 }
-cudaError_t launch_synth_modq(uint64_t* out, int64_t n, uint64_t seed, uint64_t stream, cudaStream_t st) {
-    k_synth_modq<<<148 * 8, 256, 0, st>>>(out, n, seed, stream);
+cudaError_t launch_synth_modq(uint64_t* out, int64_t n, uint64_t seed, uint64_t stream, cudaStream_t st,
+                              uint64_t idx0) {
+    k_synth_modq<<<148 * 8, 256, 0, st>>>(out, n, seed, stream, idx0);
     return cudaGetLastError();
 }
 

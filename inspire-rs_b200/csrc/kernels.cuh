@@ -57,9 +57,12 @@ cudaError_t launch_pack_materialized(const uint64_t* bt, const uint64_t* btb, co
                                      int num_outputs, int n_rot, uint64_t* out, cudaStream_t st);
 cudaError_t launch_ntt_batch(uint64_t* data, int npairs, int forward, const uint32_t* w, const uint32_t* wp,
                              cudaStream_t st);
-cudaError_t launch_synth_db(uint16_t* db, int64_t n, uint64_t seed, cudaStream_t st);
-cudaError_t launch_synth_condensed(uint64_t* out, int64_t n, uint64_t seed, uint64_t stream, cudaStream_t st);
-cudaError_t launch_synth_modq(uint64_t* out, int64_t n, uint64_t seed, uint64_t stream, cudaStream_t st);
+// seeded synthetic arrays; element i is element idx0 + i of the whole array
+cudaError_t launch_synth_db(uint16_t* db, int64_t n, uint64_t seed, cudaStream_t st, uint64_t idx0 = 0);
+cudaError_t launch_synth_condensed(uint64_t* out, int64_t n, uint64_t seed, uint64_t stream, cudaStream_t st,
+                                   uint64_t idx0 = 0);
+cudaError_t launch_synth_modq(uint64_t* out, int64_t n, uint64_t seed, uint64_t stream, cudaStream_t st,
+                              uint64_t idx0 = 0);
 
 // tensor-core first-dimension GEMM (gemm_tc.cu)
 cudaError_t make_u8_tile_map(CUtensorMap* map, const void* base, uint64_t row_bytes, uint64_t rows, uint32_t box_rows);

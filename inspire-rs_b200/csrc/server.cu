@@ -710,8 +710,9 @@ int ipr_server_setup(int device, const ipr_plan* plan, const ipr_server_data* da
     return IPR_OK;
 }
 
-int ipr_server_create_synthetic(int device, const ipr_plan* plan, uint64_t seed, ipr_server** out) {
-    ipr::NvtxRange nvtx_range("ipr_server_create_synthetic");
+namespace {
+// a synthetic server holding instances [first, first + plan->instances) of a synthetic state
+int create_synthetic(int device, const ipr_plan* plan, uint64_t seed, uint64_t first, ipr_server** out) {
     if (!out) return fail(IPR_E_ARGS, "null output");
     *out = nullptr;
     auto* s = new ipr_server();
@@ -721,16 +722,18 @@ int ipr_server_create_synthetic(int device, const ipr_plan* plan, uint64_t seed,
         return st;
     }
     const int64_t no = (int64_t)plan->instances;
+    const uint64_t f = first;
     cudaStream_t t = s->stream;
     auto chk = [&](cudaError_t e) -> int {
         if (e != cudaSuccess) return fail(IPR_E_CUDA, "synthetic fill: %s", cudaGetErrorString(e));
         return IPR_OK;
     };
-    if ((st = chk(ipr::launch_synth_db(s->d_db, (int64_t)(plan->db_rows * plan->db_cols), seed, t))) ||
-        (st = chk(ipr::launch_synth_modq(s->d_ahat, no * kN, seed, 2, t))) ||
-        (st = chk(ipr::launch_synth_condensed(s->d_bt, no * kNInner * kN, seed, 3, t))) ||
-        (st = chk(ipr::launch_synth_condensed(s->d_btb, no * kNInner * kN, seed, 4, t))) ||
-        (st = chk(ipr::launch_synth_condensed(s->d_bth, no * 3 * kN, seed, 5, t))) ||
+    if ((st = chk(ipr::launch_synth_db(s->d_db, (int64_t)(plan->db_rows * plan->db_cols), seed, t,
+                                       f * kN * plan->db_rows))) ||
+        (st = chk(ipr::launch_synth_modq(s->d_ahat, no * kN, seed, 2, t, f * kN))) ||
+        (st = chk(ipr::launch_synth_condensed(s->d_bt, no * kNInner * kN, seed, 3, t, f * kNInner * kN))) ||
+        (st = chk(ipr::launch_synth_condensed(s->d_btb, no * kNInner * kN, seed, 4, t, f * kNInner * kN))) ||
+        (st = chk(ipr::launch_synth_condensed(s->d_bth, no * 3 * kN, seed, 5, t, f * 3 * kN))) ||
         (st = chk(ipr::launch_db_to_planes(s->d_db, s->d_db8, (int64_t)(plan->db_rows * plan->db_cols), t))) ||
         (st = chk(cudaStreamSynchronize(t)))) {
         ipr_server_destroy(s);
@@ -740,6 +743,23 @@ int ipr_server_create_synthetic(int device, const ipr_plan* plan, uint64_t seed,
     s->value_size = plan->entry_size > 32 ? plan->entry_size - 32 : 0;
     *out = s;
     return IPR_OK;
+}
+}  // namespace
+
+int ipr_server_create_synthetic(int device, const ipr_plan* plan, uint64_t seed, ipr_server** out) {
+    ipr::NvtxRange nvtx_range("ipr_server_create_synthetic");
+    return create_synthetic(device, plan, seed, 0, out);
+}
+
+int ipr_server_create_synthetic_shard(int device, const ipr_plan* full, int num_shards, int shard, uint64_t seed,
+                                      ipr_server** out) {
+    ipr::NvtxRange nvtx_range("ipr_server_create_synthetic_shard");
+    if (!full || !out) return fail(IPR_E_ARGS, "null argument");
+    ipr_plan sub;
+    uint64_t first = 0;
+    int st = ipr_plan_shard(full, num_shards, shard, &sub, &first);
+    if (st) return st;
+    return create_synthetic(device, &sub, seed, first, out);
 }
 
 void ipr_server_destroy(ipr_server* s) {

@@ -98,6 +98,10 @@ def _rank_main(rank, world, port, out_q):
                 results.append(r == orc.respond(full, orc.synth_query(seed, plan.db_rows, nq)))
             else:
                 results.append(r is None)
+        # the batch collective: one broadcast of three payloads, one gather of the parts
+        qs = [orc.synth_query(10 + i, plan.db_rows, 2) for i in range(3)]
+        rb = srv.respond_batch(qs if rank == 0 else None, lambda batch: [orc.respond(mine, q) for q in batch])
+        results.append(rb == [orc.respond(full, q) for q in qs] if rank == 0 else rb is None)
         out_q.put((rank, results))
     finally:
         dist.destroy_process_group()
@@ -114,8 +118,8 @@ def test_sharded_server_gloo_two_ranks():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    assert got[0] == [True, True, True]
-    assert got[1] == [True, True, True]
+    assert got[0] == [True, True, True, True]
+    assert got[1] == [True, True, True, True]
 
 
 @pytest.mark.gpu
@@ -157,3 +161,26 @@ def test_synth_shard_of_equals_slice(orc):
         assert np.array_equal(getattr(alone, a), getattr(view, a)), a
     q = orc.synth_query(3, 2048, 2)
     assert orc.respond(alone, q) == orc.respond(view, q)
+
+
+@pytest.mark.gpu
+def test_synthetic_shards_merge_to_full_synthetic(pkg):
+    """ipr_server_create_synthetic_shard: each shard generates its own slice of the synthetic
+    state on the device; merged, the shards answer like the full synthetic server (single and
+    batch paths).  This is how a sharded run builds its per-GPU servers."""
+    import numpy as np  # noqa: F401
+    sys_orc = __import__("oracle")
+    plan = _plan(pkg, 6, 2)
+    with pkg.KeywordServer.synthetic(plan, seed=12) as whole:
+        for shards in (2, 3):
+            parts = [pkg.KeywordServer.synthetic_shard(plan, shards, k, seed=12) for k in range(shards)]
+            try:
+                qs = [sys_orc.synth_query(80 + i, plan.db_rows, 2) for i in range(4)]
+                want = whole.respond_batch(qs)
+                for i, q in enumerate(qs[:2]):
+                    assert pkg.merge_responses([s.respond_to_serialized_query(q) for s in parts]) == want[i]
+                per = [s.respond_batch(qs) for s in parts]
+                assert [pkg.merge_responses(list(x)) for x in zip(*per)] == want
+            finally:
+                for s in parts:
+                    s.close()
