@@ -35,6 +35,13 @@ void gpu_encode_db_from_host(const uint16_t *h_db_in, uint16_t *h_db_out, int db
                              int interp_degree, int gamma, int c, uint32_t modulus, uint32_t num_inv);
 const uint16_t *gpu_encode_get_device_db(void);
 void gpu_encode_free_device_db(void);
+/* src/pir/gpu/encode.rs:20-31 (native/cuda/encode_kernel.cu:452-516): encode a new host DB
+ * into a secondary device slot (uploaded in 256 MB pieces on the per-thread stream) while
+ * the primary keeps serving; get its pointer; free the primary and promote the secondary. */
+void gpu_encode_db_from_host_fold(const uint16_t *h_db_in, int db_rows, int db_cols, int interp_degree, int gamma,
+                                  int c, uint32_t modulus, uint32_t num_inv);
+const uint16_t *gpu_encode_get_device_db_fold(void);
+void gpu_encode_swap_primary(void);
 
 /* src/pir/gpu/gemv.rs:5-25 (native/cuda/gemv_kernel.cu:106-194) */
 void gpu_gemv_upload_db(const uint16_t *h_db, uint16_t **d_db_out, size_t db_size_bytes);

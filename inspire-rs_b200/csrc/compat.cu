@@ -35,7 +35,8 @@ uint64_t *d_bold_t = nullptr, *d_bold_t_bar = nullptr, *d_bold_t_hat = nullptr, 
 uint64_t *d_y_all = nullptr, *d_y_bar_all = nullptr, *d_z_body = nullptr;
 bool g_adopted = false;
 int g_n_inner = 0, g_poly_len = 0;
-uint16_t* g_encoded_db = nullptr;  // gpu_encode_db_from_host's result, kept on the device
+uint16_t* g_encoded_db = nullptr;      // gpu_encode_db_from_host's result, kept on the device
+uint16_t* g_encoded_db_new = nullptr;  // gpu_encode_db_from_host_fold's result until the swap
 
 bool report(const char* tag, cudaError_t e, int line) {
     if (e == cudaSuccess) return false;
@@ -145,6 +146,50 @@ void gpu_encode_free_device_db(void) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (g_encoded_db) cudaFree(g_encoded_db);
     g_encoded_db = nullptr;
+}
+
+// encode_kernel.cu:452-516: encode a new DB into the secondary slot while the primary keeps
+// serving; the upload goes in 256 MB pieces on the per-thread stream so that query copies
+// on other streams interleave with it
+void gpu_encode_db_from_host_fold(const uint16_t* h_db_in, int db_rows, int db_cols, int interp_degree, int gamma,
+                                  int c, uint32_t modulus, uint32_t num_inv) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    const size_t bytes = (size_t)db_rows * (size_t)db_cols * sizeof(uint16_t);
+    uint16_t *d_in = nullptr, *d_out = nullptr;
+    if (report("GPU Encode Fold", cudaMalloc(&d_in, bytes), __LINE__) ||
+        report("GPU Encode Fold", cudaMalloc(&d_out, bytes), __LINE__)) {
+        if (d_in) cudaFree(d_in);
+        if (d_out) cudaFree(d_out);
+        return;
+    }
+    const size_t chunk = 256ull << 20;
+    for (size_t off = 0; off < bytes; off += chunk) {
+        const size_t n = off + chunk <= bytes ? chunk : bytes - off;
+        if (report("GPU Encode Fold",
+                   cudaMemcpyAsync(reinterpret_cast<uint8_t*>(d_in) + off, reinterpret_cast<const uint8_t*>(h_db_in) + off,
+                                   n, cudaMemcpyHostToDevice, cudaStreamPerThread),
+                   __LINE__)) {
+            cudaStreamSynchronize(cudaStreamPerThread);
+            cudaFree(d_in);
+            cudaFree(d_out);
+            return;
+        }
+    }
+    cudaStreamSynchronize(cudaStreamPerThread);
+    gpu_encode_db(d_in, d_out, db_rows, db_cols, interp_degree, gamma, c, modulus, num_inv);
+    cudaFree(d_in);
+    if (g_encoded_db_new && g_encoded_db_new != d_out) cudaFree(g_encoded_db_new);
+    g_encoded_db_new = d_out;
+}
+
+const uint16_t* gpu_encode_get_device_db_fold(void) { return g_encoded_db_new; }
+
+// free the primary encoded DB and promote the secondary one
+void gpu_encode_swap_primary(void) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_encoded_db && g_encoded_db != g_encoded_db_new) cudaFree(g_encoded_db);
+    g_encoded_db = g_encoded_db_new;
+    g_encoded_db_new = nullptr;
 }
 
 void gpu_trim_memory_pool(void) {

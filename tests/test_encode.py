@@ -150,3 +150,43 @@ def test_server_from_raw_answers_like_encoded(pkg, orc):
         sdb.db[:] = enc  # the oracle answers over the encoded DB
         assert ra == orc.respond(sdb, q)
         assert a.respond_batch([q, q]) == [ra, ra]
+
+
+@pytest.mark.gpu
+def test_compat_encode_fold_and_swap(pkg, orc):
+    """gpu_encode_db_from_host_fold / gpu_encode_get_device_db_fold / gpu_encode_swap_primary
+    (encode_kernel.cu:452-516): a second DB is encoded into the secondary slot while the
+    primary stays as it was; the swap promotes it"""
+    from cuda.bindings import runtime as rt
+    lib = pkg.lib
+    sig = [ctypes.c_void_p] + [ctypes.c_int] * 5 + [ctypes.c_uint32, ctypes.c_uint32]
+    lib.gpu_encode_db_from_host.argtypes = [ctypes.c_void_p] + sig
+    lib.gpu_encode_db_from_host_fold.argtypes = sig
+    lib.gpu_encode_get_device_db.restype = ctypes.c_void_p
+    lib.gpu_encode_get_device_db_fold.restype = ctypes.c_void_p
+    db_rows, interp, c = 64, 8, 2
+    cols = interp * N * c
+    inv = pow(interp, -1, P)
+    rng = np.random.default_rng(19)
+    a = rng.integers(0, P, cols * db_rows, dtype=np.uint16)
+    b = rng.integers(0, P, cols * db_rows, dtype=np.uint16)
+
+    def dev(ptr):
+        got = np.zeros_like(a)
+        err, = rt.cudaMemcpy(got.ctypes.data, ptr, got.nbytes, rt.cudaMemcpyKind.cudaMemcpyDeviceToHost)
+        assert err == rt.cudaError_t.cudaSuccess
+        return got
+
+    lib.gpu_encode_db_from_host(a.ctypes.data, None, db_rows, cols, interp, N, c, P, inv)
+    primary = lib.gpu_encode_get_device_db()
+    lib.gpu_encode_db_from_host_fold(b.ctypes.data, db_rows, cols, interp, N, c, P, inv)
+    second = lib.gpu_encode_get_device_db_fold()
+    assert primary and second and primary != second
+    assert lib.gpu_encode_get_device_db() == primary
+    assert np.array_equal(dev(primary), orc.encode_db(a, db_rows, cols, interp))
+    assert np.array_equal(dev(second), orc.encode_db(b, db_rows, cols, interp))
+    lib.gpu_encode_swap_primary()
+    assert lib.gpu_encode_get_device_db() == second and not lib.gpu_encode_get_device_db_fold()
+    assert np.array_equal(dev(second), orc.encode_db(b, db_rows, cols, interp))
+    lib.gpu_encode_free_device_db()
+    assert not lib.gpu_encode_get_device_db()
