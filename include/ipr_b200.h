@@ -429,6 +429,11 @@ typedef struct ipr_service_stats {
 
 int ipr_service_create(ipr_server *const *servers, int num_servers, const ipr_service_config *cfg,
                        ipr_service **out);
+/* Admit one more database to a running service (up to 64 in all): its batch size is the
+ * largest B <= max_batch whose batch-path memory and I/O slots fit what the earlier
+ * databases left of the HBM budget (IPR_E_OOM if even B = 1 does not fit); *db is its
+ * index for submit.  The databases already served keep running meanwhile. */
+int ipr_service_add_database(ipr_service *svc, ipr_server *server, int *db);
 /* Queue one serialized KeywordQueryPayload for database `db`; *ticket names it. */
 int ipr_service_submit(ipr_service *svc, int db, const uint8_t *query, size_t len, uint64_t *ticket);
 /* n payloads queued atomically (all or none: IPR_E_BUSY if the queue cannot take all,

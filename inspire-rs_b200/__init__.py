@@ -134,6 +134,7 @@ _state_plan = _sig("ipr_state_file_plan", _i32, ctypes.c_char_p, ctypes.POINTER(
 _svc_create = _sig("ipr_service_create", _i32, ctypes.POINTER(_vp), _i32, ctypes.POINTER(_ServiceConfig),
                    ctypes.POINTER(_vp))
 _svc_submit = _sig("ipr_service_submit", _i32, _vp, _i32, _u8p, _sz, ctypes.POINTER(_u64))
+_svc_add_db = _sig("ipr_service_add_database", _i32, _vp, _vp, ctypes.POINTER(_i32))
 _svc_submit_batch = _sig("ipr_service_submit_batch", _i32, _vp, _i32, _i32, ctypes.POINTER(_u8p),
                          ctypes.POINTER(_sz), ctypes.POINTER(_u64))
 _svc_poll = _sig("ipr_service_poll", _i32, _vp, _u64, _u8p, _sz, ctypes.POINTER(_sz))
@@ -622,6 +623,15 @@ class KeywordService:
         self._h = _vp()
         _check(_svc_create(arr, len(self._servers), ctypes.byref(cfg), ctypes.byref(self._h)), "service_create")
         self._cap = max(s.response_bytes(2) for s in self._servers)
+
+    def add_database(self, server: "KeywordServer") -> int:
+        """ipr_service_add_database: serve one more database (admitted under what is left of
+        the HBM budget); returns its index for submit"""
+        db = _i32()
+        _check(_svc_add_db(self._h, server._h, ctypes.byref(db)), "service_add_database")
+        self._servers.append(server)
+        self._cap = max(self._cap, server.response_bytes(2))
+        return db.value
 
     def submit(self, db: int, query: bytes) -> int:
         t = _u64()

@@ -12,12 +12,15 @@
 //
 // Admission: the batch size is the largest B <= max_batch whose batch-path
 // device memory (slot-indexed precomputation + scratch + I/O slots) fits the
-// HBM budget for all databases together; submissions beyond max_pending
-// queued requests are refused with IPR_E_BUSY.  Responses are byte-identical
+// HBM budget for all databases together; a database added later
+// (ipr_service_add_database) gets the largest batch size that still fits what is
+// left of the budget.  Submissions beyond max_pending queued requests are refused
+// with IPR_E_BUSY.  Responses are byte-identical
 // to ipr_server_respond: the batch path is bit-exact per payload.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstdio>
@@ -36,6 +39,7 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 constexpr size_t kBatchLog = 4096;
+constexpr int kMaxDatabases = 64;  // lanes are allocated once, so adding one never moves the others
 
 int svc_fail(int code, const std::string& msg) {
     ipr::set_last_error(msg.c_str());
@@ -97,9 +101,12 @@ struct Lane {
 }  // namespace
 
 struct ipr_service {
-    std::vector<Lane> lanes;
+    std::vector<Lane> lanes;          // kMaxDatabases entries; [0, nlanes) are in use
+    std::atomic<int> nlanes{0};       // published after a lane is fully set up
+    uint64_t budget = 0;              // the HBM budget the admissions share
     ipr_service_config cfg{};
     std::mutex mu;
+    std::mutex add_mu;  // serialises ipr_service_add_database
     std::condition_variable cv_work, cv_done;
     std::unordered_map<uint64_t, Request*> reqs;
     uint64_t next_ticket = 1;
@@ -113,7 +120,7 @@ struct ipr_service {
     std::vector<ipr_service_batch> log;  // ring of the most recent batches
     uint64_t log_next = 0;
     uint64_t timed_batches = 0, queued_requests = 0;
-    uint64_t hbm = 0;
+    std::atomic<uint64_t> hbm{0};  // device bytes of the batch paths and I/O slots
     int admitted_batch = 0;
 };
 
@@ -259,7 +266,9 @@ void scheduler(ipr_service* v) {
     for (;;) {
         bool progressed = false;
         // 1. finished batches, oldest first per database
-        for (Lane& ln : v->lanes) {
+        const int nl = v->nlanes.load(std::memory_order_acquire);
+        for (int li = 0; li < nl; li++) {
+            Lane& ln = v->lanes[li];
             while (ln.nbusy > 0) {
                 Slot& sl = ln.slot[ln.head];
                 {
@@ -277,8 +286,8 @@ void scheduler(ipr_service* v) {
         // staging lead), so it carries everything that arrived meanwhile.
         Clock::time_point wake = Clock::time_point::max();
         const auto now = Clock::now();
-        for (size_t i = 0; i < v->lanes.size(); i++) {
-            Lane& ln = v->lanes[(rr + i) % v->lanes.size()];
+        for (int i = 0; i < nl; i++) {
+            Lane& ln = v->lanes[(rr + i) % nl];
             while (ln.max_batch == 0 || ln.nbusy < 2) {
                 if (ln.max_batch > 0 && ln.nbusy == 1) {
                     const auto lead = std::chrono::microseconds(
@@ -325,7 +334,8 @@ void scheduler(ipr_service* v) {
         std::unique_lock<std::mutex> lk(v->mu);
         auto ready = [&] {
             if (v->stop) return true;
-            for (Lane& ln : v->lanes) {
+            for (int li = 0; li < v->nlanes.load(std::memory_order_acquire); li++) {
+                const Lane& ln = v->lanes[li];
                 if (ln.nbusy > 0 && ln.slot[ln.head].ready) return true;
                 if (!ln.pending.empty() && (ln.max_batch == 0 || ln.nbusy == 0)) return true;
             }
@@ -335,12 +345,12 @@ void scheduler(ipr_service* v) {
         else v->cv_work.wait_until(lk, wake, ready);
         if (v->stop) {
             bool busy = false;
-            for (Lane& ln : v->lanes) busy = busy || ln.nbusy > 0;
+            for (int li = 0; li < nl; li++) busy = busy || v->lanes[li].nbusy > 0;
             if (!busy) break;
             // let the batches in flight finish before leaving
             lk.unlock();
-            for (Lane& ln : v->lanes)
-                if (ln.nbusy) cudaStreamSynchronize(ln.down);
+            for (int li = 0; li < nl; li++)
+                if (v->lanes[li].nbusy) cudaStreamSynchronize(v->lanes[li].down);
         }
     }
 }
@@ -437,7 +447,12 @@ int ipr_service_create(ipr_server* const* servers, int num_servers, const ipr_se
     auto* v = new ipr_service();
     v->cfg = c;
     v->admitted_batch = B;
-    v->lanes.resize(num_servers);
+    if (num_servers > kMaxDatabases) {
+        delete v;
+        return svc_fail(IPR_E_ARGS, "more than 64 databases");
+    }
+    v->budget = budget;
+    v->lanes.resize(kMaxDatabases);
     for (int i = 0; i < num_servers; i++) {
         Lane& ln = v->lanes[i];
         ln.s = servers[i];
@@ -452,14 +467,69 @@ int ipr_service_create(ipr_server* const* servers, int num_servers, const ipr_se
             return st;
         }
     }
+    v->nlanes.store(num_servers, std::memory_order_release);
     v->sched = std::thread(scheduler, v);
     *out = v;
     return IPR_OK;
 }
 
+int ipr_service_add_database(ipr_service* v, ipr_server* server, int* db) {
+    if (!v || !server || !db) return svc_fail(IPR_E_ARGS, "null argument");
+    std::lock_guard<std::mutex> add_lk(v->add_mu);  // one admission at a time
+    const int n = v->nlanes.load(std::memory_order_acquire);
+    if (n >= kMaxDatabases) return svc_fail(IPR_E_ARGS, "the service holds 64 databases already");
+    for (int i = 0; i < n; i++)
+        if (v->lanes[i].s == server) return svc_fail(IPR_E_ARGS, "server already served");
+    uint64_t used;
+    {
+        std::lock_guard<std::mutex> lk(v->mu);
+        if (v->stop) return svc_fail(IPR_E_STATE, "service is shutting down");
+        used = v->hbm.load();
+    }
+    const uint64_t left = v->budget > used ? v->budget - used : 0;
+    int B = 0;
+    if (server->gemv_tc) {
+        auto need = [&](int b) {
+            return ipr::server_batch_bytes(server, b) +
+                   2ull * b * (ipr::query_bytes(server->plan.db_rows, 2) + server->response_bytes(2));
+        };
+        B = v->cfg.max_batch;
+        while (B > 0 && need(B) > left) B--;
+        if (B == 0) {
+            char msg[256];
+            snprintf(msg, sizeof msg, "HBM budget has %llu bytes left; one payload of this database needs %llu",
+                     (unsigned long long)left, (unsigned long long)need(1));
+            return svc_fail(IPR_E_OOM, msg);
+        }
+    }
+    Lane& ln = v->lanes[n];  // not visible to the scheduler until nlanes is raised
+    ln.s = server;
+    ln.max_batch = B;
+    ln.qb = ipr::query_bytes(server->plan.db_rows, 2);
+    ln.rb = server->response_bytes(2);
+    uint64_t batch_bytes = B ? ipr::server_batch_bytes(server, B) : 0;
+    const uint64_t hbm_before = v->hbm.load();
+    int st = setup_lane(v, ln);
+    if (st) {
+        free_lane(ln);
+        ln = Lane();
+        std::lock_guard<std::mutex> lk(v->mu);
+        v->hbm.store(hbm_before);
+        return st;
+    }
+    {
+        std::lock_guard<std::mutex> lk(v->mu);
+        v->hbm += batch_bytes;
+    }
+    v->nlanes.store(n + 1, std::memory_order_release);
+    *db = n;
+    v->cv_work.notify_one();
+    return IPR_OK;
+}
+
 int ipr_service_submit(ipr_service* v, int db, const uint8_t* query, size_t len, uint64_t* ticket) {
     if (!v || !query || !ticket) return svc_fail(IPR_E_ARGS, "null argument");
-    if (db < 0 || db >= (int)v->lanes.size()) return svc_fail(IPR_E_ARGS, "no such database");
+    if (db < 0 || db >= v->nlanes.load(std::memory_order_acquire)) return svc_fail(IPR_E_ARGS, "no such database");
     Lane& ln = v->lanes[db];
     if (len < 1) return svc_fail(IPR_E_FORMAT, "empty query");
     const uint64_t want = ipr_server_query_bytes(ln.s, query[0]);
@@ -494,7 +564,7 @@ int ipr_service_submit(ipr_service* v, int db, const uint8_t* query, size_t len,
 int ipr_service_submit_batch(ipr_service* v, int db, int n, const uint8_t* const* queries, const size_t* lens,
                              uint64_t* tickets) {
     if (!v || n < 0 || (n && (!queries || !lens || !tickets))) return svc_fail(IPR_E_ARGS, "null argument");
-    if (db < 0 || db >= (int)v->lanes.size()) return svc_fail(IPR_E_ARGS, "no such database");
+    if (db < 0 || db >= v->nlanes.load(std::memory_order_acquire)) return svc_fail(IPR_E_ARGS, "no such database");
     Lane& ln = v->lanes[db];
     std::vector<Request*> rs;
     rs.reserve((size_t)n);
@@ -595,7 +665,7 @@ int ipr_service_get_stats(ipr_service* v, ipr_service_stats* out) {
         out->pending = v->npending;
         out->in_flight = v->in_flight;
         out->max_batch = v->admitted_batch;
-        out->hbm_bytes = v->hbm;
+        out->hbm_bytes = v->hbm.load();
         lat = v->lat_us;
     }
     out->p50_us = out->p99_us = out->mean_us = out->max_us = 0;
@@ -655,7 +725,7 @@ void ipr_service_destroy(ipr_service* v) {
     {
         std::lock_guard<std::mutex> lk(v->mu);
         v->stop = true;
-        for (Lane& ln : v->lanes) ln.pending.clear();  // never started; freed below
+        for (int li = 0; li < v->nlanes.load(); li++) v->lanes[li].pending.clear();  // never started; freed below
         v->npending = 0;
     }
     v->cv_work.notify_all();

@@ -123,6 +123,38 @@ def test_admission_by_hbm_budget_and_queue(pkg, orc, dbs):
 
 
 @pytest.mark.gpu
+def test_database_added_to_a_running_service(pkg, orc, dbs):
+    """ipr_service_add_database: a second database joins while the first one's traffic runs;
+    both answer exactly, and a database that does not fit what is left of the budget is
+    refused with IPR_E_OOM"""
+    (p0, s0, d0), (p1, s1, d1) = dbs
+    q0 = [orc.synth_query(1100 + i, p0.db_rows, 2) for i in range(10)]
+    q1 = [orc.synth_query(1200 + i, p1.db_rows, 2) for i in range(6)] + [orc.synth_query(1300, p1.db_rows, 1)]
+    want0 = [s0.respond_to_serialized_query(q) for q in q0]
+    want1 = [s1.respond_to_serialized_query(q) for q in q1]
+    assert want1[-1] == orc.respond(d1, q1[-1])
+    with pkg.KeywordService([s0], max_batch=8, hbm_budget_bytes=1 << 40) as svc:
+        first = [svc.submit(0, q) for q in q0[:5]]
+        db = svc.add_database(s1)
+        assert db == 1
+        second = [svc.submit(1, q) for q in q1] + [svc.submit(0, q) for q in q0[5:]]
+        assert [svc.wait(t) for t in first] == want0[:5]
+        got = [svc.wait(t) for t in second]
+        assert got[:len(q1)] == want1 and got[len(q1):] == want0[5:]
+        with pytest.raises(pkg.IprError):
+            svc.add_database(s1)  # already served
+    s0.prepare_batch(2)
+    s1.prepare_batch(2)
+    with pkg.KeywordService([s0], max_batch=2, hbm_budget_bytes=1 << 40) as probe:
+        need = probe.stats().hbm_bytes
+    with pkg.KeywordService([s0], max_batch=2, hbm_budget_bytes=need) as svc:
+        with pytest.raises(pkg.IprError) as ei:
+            svc.add_database(s1)
+        assert ei.value.status == -2  # IPR_E_OOM: nothing of the budget is left
+        assert svc.wait(svc.submit(0, q0[0])) == want0[0]
+
+
+@pytest.mark.gpu
 def test_service_errors_and_poll(pkg, orc, dbs):
     plan, srv, _ = dbs[0]
     with pkg.KeywordService([srv]) as svc:
