@@ -439,6 +439,33 @@ def micro_bench(pkg, steps, warmup):
                 except Exception as exc:
                     line["cpu_baseline"] = {"unavailable": str(exc)[:120]}
             lines.append(line)
+    # dataset generation (DatasetGenerator): 1M ML-KEM-768 records (id || key) into device memory
+    gen = pkg.DatasetGenerator("ml-kem-768", RECORDS).with_seed(7)
+    recs = torch.empty(RECORDS * gen.record_size, dtype=torch.uint8, device="cuda")
+    gen.generate_device(recs.data_ptr(), 0, 65536)  # warm-up
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    gen.generate_device(recs.data_ptr())
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    line = {"metric": "dataset generation: 1M ML-KEM-768 records (ChaCha20 seed, FIPS 203 key, SHA3-256 id)",
+            "value": RECORDS / (ms / 1000.0), "unit": "records/s", "ms_total": ms}
+    try:  # the oracle's restatement of the same records on the host cores (one thread per call)
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as orc
+        n_cpu = 2000
+        t0 = time.perf_counter()
+        for i in range(n_cpu):
+            orc.dataset_record("ml-kem-768", 7, i)
+        cpu_s = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": n_cpu / cpu_s, "unit": "records/s", "cores": 1, "kind": "port",
+                                "sample": f"{n_cpu} records on one host thread ({cpu_s:.1f} s)"}
+    except Exception as exc:
+        line["cpu_baseline"] = {"unavailable": str(exc)[:120]}
+    lines.append(line)
+    del recs
     # the client on the GPU (ipr_client_*) at the 1M plan: one payload of 2 sub-queries built
     # and serialized (host bytes out), and one 2 x 11-result response decrypted (host bytes in)
     plan = pkg.plan_from_shape(RECORDS, KEY, VALUE, BUCKETS, DIM0)
