@@ -519,6 +519,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--records", type=int, default=RECORDS, help="workload override (profiling small cases)")
     ap.add_argument("--buckets", type=int, default=None)
+    ap.add_argument("--plan", type=int, nargs=2, metavar=("INSTANCES", "INTERP"), default=None,
+                    help="profiling case: a synthetic plan of INSTANCES packing outputs and interpolation degree "
+                         "INTERP (db_rows 2048, INSTANCES / INTERP fold groups) instead of a record count")
     ap.add_argument("--dim0", type=int, default=None)
     ap.add_argument("--batch", type=int, default=64, help="payloads per step (1 = batch-1 u64 packing path)")
     ap.add_argument("--no-batch1", action="store_true", help="skip the batch-1 comparison measurement")
@@ -537,7 +540,7 @@ def main():
     ap.add_argument("--micro", action="store_true",
                     help="kernel microbenchmarks (batched NTT / INTT, Galois automorphisms) instead of the step")
     args = ap.parse_args()
-    small = args.records != RECORDS
+    small = args.records != RECORDS or args.plan is not None
     if args.micro:
         return micro_bench(load_package(), max(args.steps, 3), max(args.warmup, 1))
     if args.serve_config4:
@@ -579,7 +582,11 @@ def main():
     dev = torch.cuda.current_device()
 
     pkg = load_package()
-    if small:
+    if args.plan is not None:
+        inst, interp = args.plan
+        plan = pkg.Plan(num_items=32768, entry_size=KEY + VALUE, item_size_bits=8 * (KEY + VALUE), dim0=2048,
+                        db_rows=2048, db_cols=inst * N, instances=inst, interp=interp, c=inst // interp, peak_bytes=0)
+    elif small:
         plan = pkg.plan_from_shape(args.records, KEY, VALUE, args.buckets, args.dim0)
     else:
         plan = pkg.plan_from_shape(RECORDS, KEY, VALUE, BUCKETS, DIM0)
@@ -816,7 +823,9 @@ def main():
             "scaling": "strong" if shard else "weak", "vs_baseline": None,
             "dtype": "u8 limbs -> s32 / u64" if B > 1 else "u64",
             "data": "synthetic",
-            "config": {"workload": wl if not small else f"{args.records} ML-KEM-768 records (profiling case)",
+            "config": {"workload": wl if not small else (
+                           f"profiling case: {plan.instances} packing outputs, interp {plan.interp}"
+                           if args.plan is not None else f"{args.records} ML-KEM-768 records (profiling case)"),
                        "records": args.records, "buckets": plan.num_items, "dim0": plan.dim0, "db_rows": plan.db_rows,
                        "db_cols": plan.db_cols, "instances": plan.instances, "interp": plan.interp, "c": plan.c,
                        "batch_payloads": B,
