@@ -77,6 +77,40 @@ __device__ __forceinline__ void fstage(uint32_t (&v)[P][EPT], int mm, int dd, E 
     }
 }
 
+// Team exchanges through xbuf.  The intra-warp transposes (B <-> C <-> D) use only the warp's
+// own 256-word region of each polynomial and synchronise only the warp, so the cross-warp
+// exchanges are fenced by where they write: A -> B stores into every warp's region, so a
+// team barrier first lets every warp finish with its region; its loads read the warp's own
+// region, which nothing else writes before the next such barrier.  B -> A stores into the
+// warp's own region (no other warp reads it until the barrier) and loads from all regions,
+// which nothing writes before the next A -> B barrier.
+template <int P>
+__device__ __forceinline__ void xchg_a2b(uint32_t (&v)[P][EPT], int t, uint32_t* xbuf, int bar) {
+    nttr::group_bar(bar);
+#pragma unroll
+    for (int p = 0; p < P; p++)
+#pragma unroll
+        for (int m = 0; m < EPT; m++) xbuf[p * N + eA(t, m)] = v[p][m];
+    nttr::group_bar(bar);
+#pragma unroll
+    for (int p = 0; p < P; p++)
+#pragma unroll
+        for (int m = 0; m < EPT; m++) v[p][m] = xbuf[p * N + eB(t, m)];
+}
+
+template <int P>
+__device__ __forceinline__ void xchg_b2a(uint32_t (&v)[P][EPT], int t, uint32_t* xbuf, int bar) {
+#pragma unroll
+    for (int p = 0; p < P; p++)
+#pragma unroll
+        for (int m = 0; m < EPT; m++) xbuf[p * N + eB(t, m)] = v[p][m];
+    nttr::group_bar(bar);
+#pragma unroll
+    for (int p = 0; p < P; p++)
+#pragma unroll
+        for (int m = 0; m < EPT; m++) v[p][m] = xbuf[p * N + eA(t, m)];
+}
+
 // forward NTT of P gadget-digit polynomials (< 2^19) of one limb: layout A in, layout D out
 // in [0, 2q); xbuf holds XP >= P polynomials of this team
 template <int P>
@@ -92,7 +126,7 @@ __device__ __forceinline__ void forward_digits(uint32_t (&v)[P][EPT], int t, uin
     fstage<P, 0>(v, 0, 4, fa, fw, fwp, q);
     fstage<P, 0>(v, 1, 2, fa, fw, fwp, q);
     fstage<P, 0>(v, 2, 1, fa, fw, fwp, q);
-    nttr::exchange<P, true>(v, t, xbuf, bar);
+    xchg_a2b<P>(v, t, xbuf, bar);
     fstage<P, 0>(v, 3, 4, fb, fw, fwp, q);
     fstage<P, 0>(v, 4, 2, fb, fw, fwp, q);
     fstage<P, 0>(v, 5, 1, fb, fw, fwp, q);
@@ -157,7 +191,7 @@ __device__ __forceinline__ void inverse_limbs(uint32_t (&v)[2 * PL][EPT], int t,
     istage<PL, false>(v, 5, 1, fb, iw, iwp);
     istage<PL, false>(v, 4, 2, fb, iw, iwp);
     istage<PL, false>(v, 3, 4, fb, iw, iwp);
-    nttr::exchange<2 * PL, false>(v, t, xbuf, bar);
+    xchg_b2a<2 * PL>(v, t, xbuf, bar);
     istage<PL, false>(v, 2, 1, fa, iw, iwp);
     istage<PL, false>(v, 1, 2, fa, iw, iwp);
     istage<PL, false>(v, 0, 4, fa, iw, iwp);

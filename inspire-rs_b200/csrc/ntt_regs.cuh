@@ -66,11 +66,17 @@ __device__ __forceinline__ void inv_bfly(uint32_t& x, uint32_t& y, uint32_t w, u
 __device__ __forceinline__ uint32_t canon(uint32_t v, uint32_t q) { return csub(csub(v, 2 * q), q); }
 
 // A <-> B exchange of P polynomials through xbuf (XP * 2048 words, XP <= P polynomials at a
-// time), group barrier id bar
+// time), group barrier id bar.  The intra-warp transposes use only the warp's own 256-word
+// region of each polynomial and synchronise only the warp.  A -> B stores into every warp's
+// region, so its barrier comes before the stores (every warp of the group is done with its
+// region, e.g. the transposes of a previous transform) and its loads read the warp's own
+// region; B -> A stores into the warp's own region and loads from all regions, so its second
+// barrier lets every warp finish loading before anything writes there again.
 template <int P, bool A_TO_B, int XP = P>
 __device__ __forceinline__ void exchange(uint32_t (&v)[P][EPT], int t, uint32_t* xbuf, int bar) {
 #pragma unroll
     for (int c0 = 0; c0 < P; c0 += XP) {
+        if (A_TO_B) group_bar(bar);
 #pragma unroll
         for (int p = c0; p < c0 + XP && p < P; p++)
 #pragma unroll
@@ -80,7 +86,7 @@ __device__ __forceinline__ void exchange(uint32_t (&v)[P][EPT], int t, uint32_t*
         for (int p = c0; p < c0 + XP && p < P; p++)
 #pragma unroll
             for (int m = 0; m < EPT; m++) v[p][m] = xbuf[(p - c0) * N + (A_TO_B ? eB(t, m) : eA(t, m))];
-        group_bar(bar);
+        if (!A_TO_B) group_bar(bar);
     }
 }
 
