@@ -753,14 +753,16 @@ def main():
 
         srv.set_option(pkg.KeywordServer.OPT_TENSOR_GEMV, 0)
         gemv_bytes = 2 * plan.db_rows * plan.db_cols
-        for cols in (8, 4, 2):
-            srv.set_option(pkg.KeywordServer.OPT_GEMV_COLS, cols)
+        forms = {0: "8 columns per warp, registers", 1: "4 columns per warp, registers",
+                 2: "2 columns per warp, registers", 3: "8 columns per warp, cp.async ring in shared memory"}
+        for form, name in forms.items():
+            srv.set_option(pkg.KeywordServer.OPT_GEMV_FORM, form)
             rate = single_rate()
             gms = single_gemv_ms()
-            u64_forms.append({"cols_per_warp": cols, "payloads_per_s": rate, "gemv_ms": gms,
+            u64_forms.append({"form": form, "name": name, "payloads_per_s": rate, "gemv_ms": gms,
                               "gemv_gbs": gemv_bytes / (gms / 1000.0) / 1e9})
         best = min(u64_forms, key=lambda f: f["gemv_ms"])
-        srv.set_option(pkg.KeywordServer.OPT_GEMV_COLS, best["cols_per_warp"])
+        srv.set_option(pkg.KeywordServer.OPT_GEMV_FORM, best["form"])
         b1["u64"] = max(f["payloads_per_s"] for f in u64_forms)
         srv.set_option(pkg.KeywordServer.OPT_TENSOR_GEMV, 1)
         b1["tensor_gemv"] = single_rate()
@@ -844,7 +846,7 @@ def main():
             "batch1": ({"u64_payloads_per_s": b1["u64"], "tensor_gemv_payloads_per_s": b1["tensor_gemv"],
                         "speedup_vs_batch1_u64": value / world / b1["u64"],
                         "u64_gemv_roofline": {"bound": "hbm", "kernel": "k_gemv (u64, CUDA cores)",
-                                              "cols_per_warp": b1["u64_gemv"]["cols_per_warp"],
+                                              "form": b1["u64_gemv"]["name"],
                                               "avg_launch_ms": b1["u64_gemv"]["gemv_ms"],
                                               "algorithmic_bytes": b1["u64_gemv"]["bytes"],
                                               "achieved": b1["u64_gemv"]["gemv_gbs"], "peak": peak, "unit": "GB/s",

@@ -204,10 +204,11 @@ int ipr_server_set_profiling(ipr_server *srv, int on);
  * (N of each MMA: 16, 32, 64, 128 or 256; 0 = 256, the default).  Up to 128 the
  * two accumulators of a tile are double-buffered in TMEM. */
 #define IPR_OPT_GEMV_TILE 4
-/* IPR_OPT_GEMV_COLS: DB columns per warp of the CUDA-core first-dimension GEMV
- * (IPR_OPT_TENSOR_GEMV 0): 2, 4 or 8.  Fewer columns hold fewer partial sums per
- * thread, so more warps fit on an SM.  Identical results. */
-#define IPR_OPT_GEMV_COLS 5
+/* IPR_OPT_GEMV_FORM: form of the CUDA-core first-dimension GEMV (IPR_OPT_TENSOR_GEMV 0)
+ * for two queries: 0 (default) / 1 / 2 = 8 / 4 / 2 DB columns per warp loaded into
+ * registers (fewer columns, fewer partial sums per thread, more warps per SM); 3 = 8 columns
+ * per warp streamed through a 4-stage shared-memory ring by cp.async.  Identical results. */
+#define IPR_OPT_GEMV_FORM 5
 int ipr_server_set_option(ipr_server *srv, int option, int64_t value);
 
 /* Autotuner for the batch path: runs `reps` timed batches of `payloads` synthetic payloads,

@@ -549,7 +549,7 @@ class KeywordServer:
     OPT_FOLD_REGISTER_NTT = 2
     OPT_PACK_CTA_PAIR = 3
     OPT_GEMV_TILE = 4
-    OPT_GEMV_COLS = 5
+    OPT_GEMV_FORM = 5
 
     def set_option(self, option: int, value: int):
         """ipr_server_set_option: e.g. OPT_TENSOR_GEMV 0/1 selects the CUDA-core or

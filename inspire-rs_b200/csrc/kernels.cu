@@ -188,6 +188,97 @@ __global__ void __launch_bounds__(256, MINB) k_gemv(const uint16_t* __restrict__
     }
 }
 
+// The two-query GEMV with each warp's DB stripes staged through shared memory: a warp owns 8
+// consecutive columns per task (as k_gemv<2, 8>) and streams its (task, stripe) sequence
+// through a private ring of STAGES stripes with 16-byte cp.async copies, so the HBM reads of
+// the next STAGES - 1 stripes are in flight while one is multiplied.  Each lane reads back only
+// the slots it copied itself, so the ring needs no warp synchronisation.
+constexpr int GS_COLS = 8, GS_WARPS = 8;
+
+__device__ __forceinline__ void gs_cp16(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+
+template <int STAGES>
+__global__ void __launch_bounds__(GS_WARPS * 32, 1)
+    k_gemv_staged(const uint16_t* __restrict__ db, int db_rows, int64_t db_cols, const uint32_t* __restrict__ a_il,
+                  uint64_t* __restrict__ c) {
+    constexpr int NQ = 2, NV = GS_COLS * NQ * 2;  // 32 values per lane
+    extern __shared__ uint4 gs_ring[];              // [warp][stage][column][lane]
+    const int lane = threadIdx.x & 31;
+    uint4* ring = gs_ring + (threadIdx.x >> 5) * STAGES * GS_COLS * 32;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t ntasks = db_cols / GS_COLS;
+    const int stripes = db_rows >> 8;
+    const int64_t my_tasks = warp < ntasks ? (ntasks - 1 - warp) / nwarps + 1 : 0;
+    const int64_t items = my_tasks * stripes;  // (task, stripe) pairs of this warp, in order
+    auto issue = [&](int64_t u) {
+        if (u < items) {
+            const int64_t col0 = (warp + (u / stripes) * nwarps) * GS_COLS;
+            const int k0 = (int)(u % stripes) * 256 + lane * 8;
+            uint4* dst = ring + (int)(u % STAGES) * GS_COLS * 32 + lane;
+#pragma unroll
+            for (int cc = 0; cc < GS_COLS; cc++) gs_cp16(dst + cc * 32, db + (col0 + cc) * (int64_t)db_rows + k0);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");  // one group per item, empty past the end
+    };
+#pragma unroll
+    for (int u = 0; u < STAGES - 1; u++) issue(u);
+    uint64_t acc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) acc[v] = 0;
+    for (int64_t u = 0; u < items; u++) {
+        asm volatile("cp.async.wait_group %0;" ::"n"(STAGES - 2) : "memory");  // item u has landed
+        const uint4* src = ring + (int)(u % STAGES) * GS_COLS * 32 + lane;
+        uint4 d[GS_COLS];
+#pragma unroll
+        for (int cc = 0; cc < GS_COLS; cc++) d[cc] = src[cc * 32];
+        issue(u + STAGES - 1);  // into the stage item u - 1 used, already read
+        const int it = (int)(u % stripes);
+        const int k0 = it * 256 + lane * 8;
+#pragma unroll
+        for (int kk = 0; kk < 8; kk++) {
+            const uint4 t = __ldg(reinterpret_cast<const uint4*>(a_il) + (k0 + kk));
+            const uint32_t av[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+            for (int cc = 0; cc < GS_COLS; cc++) {
+                const uint32_t w = (&d[cc].x)[kk >> 1];
+                const uint32_t dv = (kk & 1) ? (w >> 16) : (w & 0xffffu);
+#pragma unroll
+                for (int v = 0; v < 4; v++) acc[cc * 4 + v] += (uint64_t)av[v] * dv;
+            }
+        }
+        if (it == stripes - 1) {  // the task's last stripe: reduce across the warp and write
+#pragma unroll
+            for (int s = 16; s >= 1; s >>= 1) {
+                const bool upper = lane & s;
+#pragma unroll
+                for (int i = 0; i < s; i++) {
+                    const uint64_t send = upper ? acc[i] : acc[i + s];
+                    const uint64_t keep = upper ? acc[i + s] : acc[i];
+                    acc[i] = keep + __shfl_xor_sync(0xffffffffu, send, s);
+                }
+            }
+            const int l = lane & 1;
+            const uint32_t r = modq(acc[0], l);
+            const uint32_t other = __shfl_xor_sync(0xffffffffu, r, 1);
+            if (l == 0) {
+                const int q = (lane >> 1) % NQ, cc = lane / (NQ * 2);
+                const int64_t col0 = (warp + (u / stripes) * nwarps) * GS_COLS;
+                c[(int64_t)q * db_cols + col0 + cc] = crt2(r, other, c_q0inv, c_br[1]);
+            }
+#pragma unroll
+            for (int v = 0; v < NV; v++) acc[v] = 0;
+        }
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+constexpr int GS_STAGES = 4;
+constexpr int GS_SMEM = GS_WARPS * GS_STAGES * GS_COLS * 32 * 16;  // 128 KB
+
 // ---------------------------------------------------------------------------
 // Packing inner product, rotations fused.  For output j, NTT slot z, limb l:
 //   S[j][l][z] = sum_{i<1023,k<3} y_l[k][rot_i(z)] T_l[j][i,k][z]
@@ -582,6 +673,8 @@ __global__ void k_synth_modq(uint64_t* out, int64_t n, uint64_t seed, uint64_t s
 cudaError_t init_device_kernels() {
     cudaError_t e = cudaFuncSetAttribute(k_pack, cudaFuncAttributeMaxDynamicSharedMemorySize, T_EXP * N * 8);
     if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_gemv_staged<GS_STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, GS_SMEM);
+    if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_fold_switch, cudaFuncAttributeMaxDynamicSharedMemorySize, 12 * N * 4);
 }
 
@@ -598,11 +691,13 @@ cudaError_t launch_parse_batch(const uint8_t* qb, int npay, int64_t pstride, int
 }
 
 cudaError_t launch_gemv(const uint16_t* db, int db_rows, int64_t db_cols, int nq, const uint32_t* a_il,
-                        uint64_t* c, int sm_count, cudaStream_t st, int cols) {
+                        uint64_t* c, int sm_count, cudaStream_t st, int form) {
     const int blocks = sm_count * 4;
-    if (nq == 2 && cols == 8) k_gemv<2, 8><<<blocks, 256, 0, st>>>(db, db_rows, db_cols, a_il, c);
-    else if (nq == 2 && cols == 4) k_gemv<2, 4, 2><<<sm_count * 2, 256, 0, st>>>(db, db_rows, db_cols, a_il, c);
-    else if (nq == 2 && cols == 2) k_gemv<2, 2, 3><<<sm_count * 3, 256, 0, st>>>(db, db_rows, db_cols, a_il, c);
+    if (nq == 2 && form == 0) k_gemv<2, 8><<<blocks, 256, 0, st>>>(db, db_rows, db_cols, a_il, c);
+    else if (nq == 2 && form == 1) k_gemv<2, 4, 2><<<sm_count * 2, 256, 0, st>>>(db, db_rows, db_cols, a_il, c);
+    else if (nq == 2 && form == 2) k_gemv<2, 2, 3><<<sm_count * 3, 256, 0, st>>>(db, db_rows, db_cols, a_il, c);
+    else if (nq == 2 && form == 3)
+        k_gemv_staged<GS_STAGES><<<sm_count, GS_WARPS * 32, GS_SMEM, st>>>(db, db_rows, db_cols, a_il, c);
     else if (nq == 1) k_gemv<1, 16><<<blocks, 256, 0, st>>>(db, db_rows, db_cols, a_il, c);
     else return cudaErrorInvalidValue;
     return cudaGetLastError();

@@ -14,10 +14,11 @@ cudaError_t init_device_kernels();
 // this payload's queries starting at global query index qbase
 cudaError_t launch_parse_query(const uint8_t* qb, int nq, int db_rows, uint64_t* y, uint64_t* z,
                                uint32_t* a_il, uint32_t* gsw, uint8_t* qbytes, int qbase, cudaStream_t st);
-// nq must be 1 or 2; a_il points at the pair group, c at [nq][db_cols]; cols: DB columns per
-// warp for two queries (2, 4 or 8; one query always takes 16)
+// nq must be 1 or 2; a_il points at the pair group, c at [nq][db_cols]; form of the two-query
+// kernel: 0 / 1 / 2 = 8 / 4 / 2 DB columns per warp loaded into registers, 3 = 8 columns per
+// warp staged through shared memory by cp.async (one query always takes 16 columns per warp)
 cudaError_t launch_gemv(const uint16_t* db, int db_rows, int64_t db_cols, int nq, const uint32_t* a_il,
-                        uint64_t* c, int sm_count, cudaStream_t st, int cols = 8);
+                        uint64_t* c, int sm_count, cudaStream_t st, int form = 0);
 cudaError_t launch_pack(const uint64_t* bt, const uint64_t* btb, const uint64_t* bth, const uint64_t* y,
                         const uint64_t* z, uint32_t* S, int num_outputs, cudaStream_t st);
 // R = from_ntt(S) per (client, output) polynomial pair; with z_bodies non-null the

@@ -147,7 +147,7 @@ int enqueue(ipr_server* s, unsigned nq, const uint8_t* d_query, uint8_t* d_resp,
                 const int ng = nq - 2 * g >= 2 ? 2 : 1;
                 CU(ipr::launch_gemv(s->d_db, (int)p.db_rows, (int64_t)p.db_cols, ng,
                                     s->d_ail + (size_t)g * p.db_rows * 4, s->d_c + (size_t)2 * g * p.db_cols,
-                                    s->sm_count, st, s->gemv_cols));
+                                    s->sm_count, st, s->gemv_form));
             }
         }
         rec(2);
@@ -1063,9 +1063,9 @@ int ipr_server_set_option(ipr_server* s, int option, int64_t value) {
             }
             return IPR_OK;
         }
-        case IPR_OPT_GEMV_COLS:
-            if (value != 2 && value != 4 && value != 8) return fail(IPR_E_ARGS, "IPR_OPT_GEMV_COLS takes 2, 4 or 8");
-            s->gemv_cols = (int)value;
+        case IPR_OPT_GEMV_FORM:
+            if (value < 0 || value > 3) return fail(IPR_E_ARGS, "IPR_OPT_GEMV_FORM takes 0 to 3");
+            s->gemv_form = (int)value;
             destroy_graphs(s);
             return IPR_OK;
         case IPR_OPT_PACK_CTA_PAIR:

@@ -104,18 +104,19 @@ def test_fold_kernels(pkg, orc, regs, instances, interp):
             assert srv.respond_to_serialized_query(q) == orc.respond(sdb, q)
 
 
-@pytest.mark.parametrize("cols", [2, 4, 8])
-def test_u64_gemv_forms(cfg0, pkg, orc, cols):
-    """the CUDA-core GEMV with 2, 4 or 8 DB columns per warp gives the oracle's bytes"""
+@pytest.mark.parametrize("form", [0, 1, 2, 3])
+def test_u64_gemv_forms(cfg0, pkg, orc, form):
+    """the CUDA-core GEMV forms (8 / 4 / 2 DB columns per warp in registers, 8 columns staged
+    through a shared-memory ring) give the oracle's bytes"""
     plan, srv, sdb = cfg0
     srv.set_option(pkg.KeywordServer.OPT_TENSOR_GEMV, 0)
-    srv.set_option(pkg.KeywordServer.OPT_GEMV_COLS, cols)
+    srv.set_option(pkg.KeywordServer.OPT_GEMV_FORM, form)
     try:
         for nq in (1, 2, 3):
-            q = orc.synth_query(70 + nq + cols, plan.db_rows, nq)
+            q = orc.synth_query(70 + nq + form, plan.db_rows, nq)
             assert srv.respond_to_serialized_query(q) == orc.respond(sdb, q)
     finally:
-        srv.set_option(pkg.KeywordServer.OPT_GEMV_COLS, 8)
+        srv.set_option(pkg.KeywordServer.OPT_GEMV_FORM, 0)
         srv.set_option(pkg.KeywordServer.OPT_TENSOR_GEMV, 1)
 
 
