@@ -64,16 +64,17 @@ __device__ __forceinline__ void fwd_b(uint32_t& x, uint32_t& y, uint32_t w, uint
     y = xx + two_q - qn;
 }
 
+// twiddle tables interleaved with their Shoup companions ([limb][N] of (w, wp)): one 8-byte
+// load per twiddle, half the L1 requests of two separate tables
 template <int P, int MODE, typename E>
-__device__ __forceinline__ void fstage(uint32_t (&v)[P][EPT], int mm, int dd, E e, const uint32_t* __restrict__ w_t,
-                                       const uint32_t* __restrict__ wp_t, uint32_t q) {
+__device__ __forceinline__ void fstage(uint32_t (&v)[P][EPT], int mm, int dd, E e, const uint2* __restrict__ tw,
+                                       uint32_t q) {
 #pragma unroll
     for (int k = 0; k < EPT; k++) {
         if (k & dd) continue;
-        const int idx = (1 << mm) + (e(k) >> (11 - mm));
-        const uint32_t w = __ldg(w_t + idx), wp = __ldg(wp_t + idx);
+        const uint2 w = __ldg(tw + (1 << mm) + (e(k) >> (11 - mm)));
 #pragma unroll
-        for (int p = 0; p < P; p++) fwd_b<MODE>(v[p][k], v[p][k + dd], w, wp, q);
+        for (int p = 0; p < P; p++) fwd_b<MODE>(v[p][k], v[p][k + dd], w.x, w.y, q);
     }
 }
 
@@ -115,28 +116,27 @@ __device__ __forceinline__ void xchg_b2a(uint32_t (&v)[P][EPT], int t, uint32_t*
 // in [0, 2q); xbuf holds XP >= P polynomials of this team
 template <int P>
 __device__ __forceinline__ void forward_digits(uint32_t (&v)[P][EPT], int t, uint32_t* xbuf, int bar,
-                                               const uint32_t* __restrict__ fw, const uint32_t* __restrict__ fwp,
-                                               uint32_t q) {
+                                               const uint2* __restrict__ tw, uint32_t q) {
     const int l = t & 31;
     uint32_t* wb = xbuf + (t >> 5) * 256;
     auto fa = [&](int k) { return eA(t, k); };
     auto fb = [&](int k) { return eB(t, k); };
     auto fc = [&](int k) { return eC(t, k); };
     auto fd = [&](int k) { return eD(t, k); };
-    fstage<P, 0>(v, 0, 4, fa, fw, fwp, q);
-    fstage<P, 0>(v, 1, 2, fa, fw, fwp, q);
-    fstage<P, 0>(v, 2, 1, fa, fw, fwp, q);
+    fstage<P, 0>(v, 0, 4, fa, tw, q);
+    fstage<P, 0>(v, 1, 2, fa, tw, q);
+    fstage<P, 0>(v, 2, 1, fa, tw, q);
     xchg_a2b<P>(v, t, xbuf, bar);
-    fstage<P, 0>(v, 3, 4, fb, fw, fwp, q);
-    fstage<P, 0>(v, 4, 2, fb, fw, fwp, q);
-    fstage<P, 0>(v, 5, 1, fb, fw, fwp, q);
+    fstage<P, 0>(v, 3, 4, fb, tw, q);
+    fstage<P, 0>(v, 4, 2, fb, tw, q);
+    fstage<P, 0>(v, 5, 1, fb, tw, q);
     nttr::b_to_c<P>(v, l, wb);
-    fstage<P, 0>(v, 6, 4, fc, fw, fwp, q);
-    fstage<P, 1>(v, 7, 2, fc, fw, fwp, q);
-    fstage<P, 2>(v, 8, 1, fc, fw, fwp, q);
+    fstage<P, 0>(v, 6, 4, fc, tw, q);
+    fstage<P, 1>(v, 7, 2, fc, tw, q);
+    fstage<P, 2>(v, 8, 1, fc, tw, q);
     nttr::c_to_d<P>(v, l, wb);
-    fstage<P, 2>(v, 9, 2, fd, fw, fwp, q);
-    fstage<P, 2>(v, 10, 1, fd, fw, fwp, q);
+    fstage<P, 2>(v, 9, 2, fd, tw, q);
+    fstage<P, 2>(v, 10, 1, fd, tw, q);
 #pragma unroll
     for (int p = 0; p < P; p++)
 #pragma unroll
@@ -156,45 +156,43 @@ __device__ __forceinline__ void inv_b(uint32_t& x, uint32_t& y, uint32_t w, uint
 
 // one inverse stage over 2 * PL polynomials: [0, PL) of limb 0, [PL, 2 PL) of limb 1
 template <int PL, bool FIRST, typename E>
-__device__ __forceinline__ void istage(uint32_t (&v)[2 * PL][EPT], int mm, int dd, E e,
-                                       const uint32_t* __restrict__ iw, const uint32_t* __restrict__ iwp) {
+__device__ __forceinline__ void istage(uint32_t (&v)[2 * PL][EPT], int mm, int dd, E e, const uint2* __restrict__ iw) {
 #pragma unroll
     for (int k = 0; k < EPT; k++) {
         if (k & dd) continue;
         const int idx = (1 << mm) + (e(k) >> (11 - mm));
-        const uint32_t w0 = __ldg(iw + idx), wp0 = __ldg(iwp + idx);
-        const uint32_t w1 = __ldg(iw + N + idx), wp1 = __ldg(iwp + N + idx);
+        const uint2 w0 = __ldg(iw + idx), w1 = __ldg(iw + N + idx);
 #pragma unroll
-        for (int p = 0; p < PL; p++) inv_b<FIRST>(v[p][k], v[p][k + dd], w0, wp0, Q0);
+        for (int p = 0; p < PL; p++) inv_b<FIRST>(v[p][k], v[p][k + dd], w0.x, w0.y, Q0);
 #pragma unroll
-        for (int p = PL; p < 2 * PL; p++) inv_b<FIRST>(v[p][k], v[p][k + dd], w1, wp1, Q1);
+        for (int p = PL; p < 2 * PL; p++) inv_b<FIRST>(v[p][k], v[p][k + dd], w1.x, w1.y, Q1);
     }
 }
 
 // N * INTT of 2 * PL canonical polynomials (PL per limb): layout D in, layout A canonical out
 template <int PL>
 __device__ __forceinline__ void inverse_limbs(uint32_t (&v)[2 * PL][EPT], int t, uint32_t* xbuf, int bar,
-                                              const uint32_t* __restrict__ iw, const uint32_t* __restrict__ iwp) {
+                                              const uint2* __restrict__ iw) {
     const int l = t & 31;
     uint32_t* wb = xbuf + (t >> 5) * 256;
     auto fa = [&](int k) { return eA(t, k); };
     auto fb = [&](int k) { return eB(t, k); };
     auto fc = [&](int k) { return eC(t, k); };
     auto fd = [&](int k) { return eD(t, k); };
-    istage<PL, true>(v, 10, 1, fd, iw, iwp);
-    istage<PL, false>(v, 9, 2, fd, iw, iwp);
+    istage<PL, true>(v, 10, 1, fd, iw);
+    istage<PL, false>(v, 9, 2, fd, iw);
     nttr::d_to_c<2 * PL>(v, l, wb);
-    istage<PL, false>(v, 8, 1, fc, iw, iwp);
-    istage<PL, false>(v, 7, 2, fc, iw, iwp);
-    istage<PL, false>(v, 6, 4, fc, iw, iwp);
+    istage<PL, false>(v, 8, 1, fc, iw);
+    istage<PL, false>(v, 7, 2, fc, iw);
+    istage<PL, false>(v, 6, 4, fc, iw);
     nttr::c_to_b<2 * PL>(v, l, wb);
-    istage<PL, false>(v, 5, 1, fb, iw, iwp);
-    istage<PL, false>(v, 4, 2, fb, iw, iwp);
-    istage<PL, false>(v, 3, 4, fb, iw, iwp);
+    istage<PL, false>(v, 5, 1, fb, iw);
+    istage<PL, false>(v, 4, 2, fb, iw);
+    istage<PL, false>(v, 3, 4, fb, iw);
     xchg_b2a<2 * PL>(v, t, xbuf, bar);
-    istage<PL, false>(v, 2, 1, fa, iw, iwp);
-    istage<PL, false>(v, 1, 2, fa, iw, iwp);
-    istage<PL, false>(v, 0, 4, fa, iw, iwp);
+    istage<PL, false>(v, 2, 1, fa, iw);
+    istage<PL, false>(v, 1, 2, fa, iw);
+    istage<PL, false>(v, 0, 4, fa, iw);
 #pragma unroll
     for (int p = 0; p < 2 * PL; p++)
 #pragma unroll
@@ -282,8 +280,8 @@ __global__ void __launch_bounds__(256) k_fold_prep(uint32_t* __restrict__ S, int
 __global__ void __launch_bounds__(F3_THREADS, 1)
     k_fold3(const uint32_t* __restrict__ row0s, const uint32_t* __restrict__ gsw, const uint64_t* __restrict__ a_hat,
             const uint32_t* __restrict__ S, int64_t s_payload_stride, const uint64_t* __restrict__ cvec,
-            const uint32_t* __restrict__ fw, const uint32_t* __restrict__ fwp, const uint32_t* __restrict__ iwu,
-            const uint32_t* __restrict__ iwup, NInv ni, int interp, int c_groups, int64_t db_cols, int qpp,
+            const uint2* __restrict__ fwi, const uint2* __restrict__ iwi, NInv ni, int interp, int c_groups,
+            int64_t db_cols, int qpp,
             uint8_t* __restrict__ resp, int64_t resp_payload_stride, int64_t resp_query_stride) {
     extern __shared__ uint32_t f3_smem[];
     uint32_t* sbody = f3_smem;  // [6 gadget rows][2 limbs][N]: N^-1 x the query's RGSW bodies
@@ -325,7 +323,7 @@ __global__ void __launch_bounds__(F3_THREADS, 1)
             S_AT(0, m) = __ldg(a_hat + (int64_t)j * N + eA(t, m));
             pc[m] = __ldg(cq + (int64_t)j * N + eA(t, m));
         }
-        inverse_limbs<1>(pr, t, xbuf, bar, iwu, iwup);
+        inverse_limbs<1>(pr, t, xbuf, bar, iwi);
 #pragma unroll
         for (int m = 0; m < EPT; m++) S_AT(1, m) = add_q(crt2(pr[0][m], pr[1][m], Q0INV, BR1), pc[m]);
     }
@@ -354,7 +352,7 @@ __global__ void __launch_bounds__(F3_THREADS, 1)
 #pragma unroll
                     for (int k = 0; k < 3; k++) v[k][m] = (uint32_t)((x >> (k * GADGET_BITS)) & mask);
                 }
-                forward_digits<3>(v, t, xbuf, bar, fw + l * N, fwp + l * N, q);
+                forward_digits<3>(v, t, xbuf, bar, fwi + l * N, q);
                 uint64_t part[EPT];
 #pragma unroll
                 for (int m = 0; m < EPT; m++) part[m] = acc1[m];
@@ -394,7 +392,7 @@ __global__ void __launch_bounds__(F3_THREADS, 1)
             pa[m] = __ldg(a_hat + (int64_t)j * N + eA(t, m));
             pc[m] = __ldg(cq + (int64_t)j * N + eA(t, m));
         }
-        inverse_limbs<2>(pr, t, xbuf, bar, iwu, iwup);
+        inverse_limbs<2>(pr, t, xbuf, bar, iwi);
 #pragma unroll
         for (int m = 0; m < EPT; m++) {
             S_AT(0, m) = add_q(crt2(pr[0][m], pr[2][m], Q0INV, BR1), pa[m]);
@@ -440,16 +438,17 @@ cudaError_t launch_fold_prep(uint32_t* S, int64_t count, const uint64_t* zb, con
 }
 
 cudaError_t launch_fold3(const uint32_t* row0s, const uint32_t* gsw, const uint64_t* a_hat, const uint32_t* S,
-                         int64_t s_payload_stride, const uint64_t* cvec, const uint32_t* fw, const uint32_t* fwp,
-                         const uint32_t* iwu, const uint32_t* iwup, const uint32_t ninv[4], int interp, int c_groups,
+                         int64_t s_payload_stride, const uint64_t* cvec, const uint32_t* fwi, const uint32_t* iwi,
+                         const uint32_t ninv[4], int interp, int c_groups,
                          int num_queries, int64_t db_cols, int qpp, uint8_t* resp, int64_t resp_payload_stride,
                          int64_t resp_query_stride, cudaStream_t st) {
     if (interp < 1 || c_groups < 1 || num_queries < 1 || num_queries > 65535 || qpp < 1) return cudaErrorInvalidValue;
     NInv ni{{ninv[0], ninv[2]}, {ninv[1], ninv[3]}};
     dim3 grid((c_groups + 1) / 2, num_queries);
-    k_fold3<<<grid, F3_THREADS, FOLD3_SMEM, st>>>(row0s, gsw, a_hat, S, s_payload_stride, cvec, fw, fwp, iwu, iwup,
-                                                   ni, interp, c_groups, db_cols, qpp, resp, resp_payload_stride,
-                                                   resp_query_stride);
+    k_fold3<<<grid, F3_THREADS, FOLD3_SMEM, st>>>(row0s, gsw, a_hat, S, s_payload_stride, cvec,
+                                                   reinterpret_cast<const uint2*>(fwi),
+                                                   reinterpret_cast<const uint2*>(iwi), ni, interp, c_groups, db_cols,
+                                                   qpp, resp, resp_payload_stride, resp_query_stride);
     return cudaGetLastError();
 }
 

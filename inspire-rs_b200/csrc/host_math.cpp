@@ -246,6 +246,14 @@ void host_params_init(HostParams& p) {
             p.row0s[l * kN + i] = (uint32_t)mulmod(p.row0[l * kN + i], ninv, m);
         }
     }
+    p.fwi.assign(4 * kN, 0);
+    p.iwi.assign(4 * kN, 0);
+    for (int i = 0; i < 2 * kN; i++) {
+        p.fwi[2 * i] = p.fw[i];
+        p.fwi[2 * i + 1] = p.fwp[i];
+        p.iwi[2 * i] = p.iwu[i];
+        p.iwi[2 * i + 1] = p.iwup[i];
+    }
 }
 
 namespace {

@@ -27,6 +27,8 @@ struct HostParams {
     // N^-1, and N^-1 mod q_l with its companion as {w0, wp0, w1, wp1}
     std::vector<uint32_t> iwu, iwup, row0s;
     uint32_t ninv[4];
+    // the forward and plain inverse twiddles interleaved with their companions: [limb][N][2]
+    std::vector<uint32_t> fwi, iwi;
 };
 
 void host_params_init(HostParams& p);

@@ -84,14 +84,15 @@ cudaError_t launch_fold2(const uint32_t* row0, const uint32_t* gsw, const uint64
 // fold with the packing post-process fused in (fold3.cu).  ninv = {N^-1 mod q0, its Shoup
 // companion, N^-1 mod q1, companion}.  launch_fold_prep turns the packing outputs S
 // ([count][2][N] u32) in place into (S + z_body x That) * N^-1 (zb null: the scaling alone;
-// zb / bth indexed by f / instances and f % instances); launch_fold3 then folds with the plain
-// inverse twiddles iwu / iwup and row0s = row 0 x N^-1, S of payload p at S + p * s_payload_stride.
+// zb / bth indexed by f / instances and f % instances); launch_fold3 then folds with the forward
+// twiddles fwi and the plain inverse twiddles iwi, both [limb][N] pairs (w, Shoup companion),
+// and row0s = row 0 x N^-1, S of payload p at S + p * s_payload_stride.
 cudaError_t init_fold3_kernel();
 cudaError_t launch_fold_prep(uint32_t* S, int64_t count, const uint64_t* zb, const uint64_t* bth, int instances,
                              const uint32_t ninv[4], int sm_count, cudaStream_t st);
 cudaError_t launch_fold3(const uint32_t* row0s, const uint32_t* gsw, const uint64_t* a_hat, const uint32_t* S,
-                         int64_t s_payload_stride, const uint64_t* cvec, const uint32_t* fw, const uint32_t* fwp,
-                         const uint32_t* iwu, const uint32_t* iwup, const uint32_t ninv[4], int interp, int c_groups,
+                         int64_t s_payload_stride, const uint64_t* cvec, const uint32_t* fwi, const uint32_t* iwi,
+                         const uint32_t ninv[4], int interp, int c_groups,
                          int num_queries, int64_t db_cols, int qpp, uint8_t* resp, int64_t resp_payload_stride,
                          int64_t resp_query_stride, cudaStream_t st);
 

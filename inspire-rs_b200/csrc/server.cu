@@ -156,9 +156,9 @@ int enqueue(ipr_server* s, unsigned nq, const uint8_t* d_query, uint8_t* d_resp,
         if (s->fold_mode == 2) {
             CU(ipr::launch_fold_prep(s->d_S, (int64_t)p.instances, nullptr, nullptr, 1, s->hp.ninv, s->sm_count, st));
             rec(4);
-            CU(ipr::launch_fold3(s->d_row0s, s->d_gsw, s->d_ahat, s->d_S, 0, s->d_c, s->d_fw, s->d_fwp, s->d_iwu,
-                                 s->d_iwup, s->hp.ninv, (int)p.interp, (int)p.c, (int)nq, (int64_t)p.db_cols, (int)nq,
-                                 d_resp, 0, (int64_t)(4 + s->per_query_bytes()), st));
+            CU(ipr::launch_fold3(s->d_row0s, s->d_gsw, s->d_ahat, s->d_S, 0, s->d_c, s->d_fwi, s->d_iwi, s->hp.ninv,
+                                 (int)p.interp, (int)p.c, (int)nq, (int64_t)p.db_cols, (int)nq, d_resp, 0,
+                                 (int64_t)(4 + s->per_query_bytes()), st));
         } else if (s->fold_mode == 1) {
             CU(ipr::launch_intt_crt(s->d_S, s->d_iw, s->d_iwp, s->d_R, (int)p.instances, st));
             rec(4);
@@ -305,8 +305,8 @@ int enqueue_batch(ipr_server* s, int B, const uint8_t* d_queries, uint8_t* d_res
                                  s->sm_count, st));
         rec(4);
         CU(ipr::launch_fold3(s->d_row0s, s->d_gsw, s->d_ahat, s->d_bS, (int64_t)(p.instances * 2 * kN), s->d_c,
-                             s->d_fw, s->d_fwp, s->d_iwu, s->d_iwup, s->hp.ninv, (int)p.interp, (int)p.c, nqt,
-                             (int64_t)p.db_cols, 2, d_resps, rb, (int64_t)(4 + s->per_query_bytes()), st));
+                             s->d_fwi, s->d_iwi, s->hp.ninv, (int)p.interp, (int)p.c, nqt, (int64_t)p.db_cols, 2,
+                             d_resps, rb, (int64_t)(4 + s->per_query_bytes()), st));
     } else {
         if (!s->d_bR) return fail(IPR_E_STATE, "batch scratch lacks the INTT output (fold form changed mid-batch)");
         CU(ipr::launch_intt_crt(s->d_bS, s->d_iw, s->d_iwp, s->d_bR, (int)(B * p.instances), st, s->d_zbs, s->d_bth,
@@ -391,11 +391,11 @@ int init_common(ipr_server* s, int device, const ipr_plan* plan) {
     int st;
     const size_t tb = 2 * kN * 4;
     if ((st = s->alloc(&s->d_fw, tb)) || (st = s->alloc(&s->d_fwp, tb)) || (st = s->alloc(&s->d_iw, tb)) ||
-        (st = s->alloc(&s->d_iwp, tb)) || (st = s->alloc(&s->d_row0, tb)) || (st = s->alloc(&s->d_iwu, tb)) ||
-        (st = s->alloc(&s->d_iwup, tb)) || (st = s->alloc(&s->d_row0s, tb)))
+        (st = s->alloc(&s->d_iwp, tb)) || (st = s->alloc(&s->d_row0, tb)) || (st = s->alloc(&s->d_fwi, 2 * tb)) ||
+        (st = s->alloc(&s->d_iwi, 2 * tb)) || (st = s->alloc(&s->d_row0s, tb)))
         return st;
-    CU(cudaMemcpy(s->d_iwu, s->hp.iwu.data(), tb, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(s->d_iwup, s->hp.iwup.data(), tb, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(s->d_fwi, s->hp.fwi.data(), 2 * tb, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(s->d_iwi, s->hp.iwi.data(), 2 * tb, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(s->d_row0s, s->hp.row0s.data(), tb, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(s->d_fw, s->hp.fw.data(), tb, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(s->d_fwp, s->hp.fwp.data(), tb, cudaMemcpyHostToDevice));

@@ -52,7 +52,7 @@ struct ipr_server {
     uint8_t* d_stash = nullptr;
     uint64_t stash_count = 0, stash_entry = 0;
     uint32_t *d_fw = nullptr, *d_fwp = nullptr, *d_iw = nullptr, *d_iwp = nullptr, *d_row0 = nullptr;
-    uint32_t *d_iwu = nullptr, *d_iwup = nullptr, *d_row0s = nullptr;  // the fused fold's tables
+    uint32_t *d_fwi = nullptr, *d_iwi = nullptr, *d_row0s = nullptr;  // the fused fold's tables
     // per-request scratch
     unsigned cap_q = 0;
     uint8_t* d_query = nullptr;
