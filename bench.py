@@ -59,29 +59,47 @@ def load_oracle():
 
 
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    """nvidia-smi samples of SM clock, power and throttle reasons.  Each sample carries the
+    driver's own timestamp, so that the summary covers only [begin(), end()] when those are
+    marked: the 20 ms samples taken before and after the timed region run at idle clocks."""
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, interval_ms=20):
         self.gpu = gpu_index
+        self.interval = interval_ms
         self.proc = None
         self.lines = []
+        self.t0 = self.t1 = None
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", str(self.interval)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except Exception:
             self.proc = None
 
+    def begin(self):
+        self.t0 = time.time()
+
+    def end(self):
+        self.t1 = time.time()
+
     def _read(self):
         for ln in self.proc.stdout:
             self.lines.append(ln.strip())
+
+    @staticmethod
+    def _when(ts):
+        import datetime
+        try:
+            return datetime.datetime.strptime(ts, "%Y/%m/%d %H:%M:%S.%f").timestamp()
+        except ValueError:
+            return None
 
     def stop(self):
         if not self.proc:
@@ -92,22 +110,32 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        rows = []
         for ln in self.lines:
             f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
+            if len(f) < 10:
                 continue
             try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
+                rows.append((self._when(f[0]), float(f[2]), float(f[3]), float(f[4]), f[6:10]))
             except ValueError:
                 continue
-            for nm, v in zip(names, f[5:9]):
+        window = "whole run"
+        if self.t0 is not None and self.t1 is not None:
+            inside = [r for r in rows if r[0] is not None and self.t0 <= r[0] <= self.t1]
+            if inside:
+                rows, window = inside, "timed region"
+        sm = [r[1] for r in rows]
+        mx = rows[-1][2] if rows else None
+        power = [r[3] for r in rows]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for nm, v in zip(names, r[4]):
                 if v.lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "sm_mhz_min": min(sm) if sm else None, "power_w": statistics.median(power) if power else None,
+                "reasons": sorted(reasons), "samples": len(sm), "window": window}
 
 
 def read_peaks():
@@ -184,6 +212,31 @@ def cpu_sample(orc, payloads=3):
     return s.describe(statistics.median(per), payloads)
 
 
+SERVICE_WAIT_S = 120.0  # no request of these loads waits that long unless the service is stuck
+
+
+def svc_wait(svc, ticket, timeout_s=SERVICE_WAIT_S):
+    """a service response within timeout_s; otherwise the service's counters and its last
+    batches go to stderr and the process ends (a stuck wait would hold the GPU indefinitely)"""
+    r = svc.wait(ticket, int(timeout_s * 1000))
+    if r is None:
+        try:
+            st = svc.stats()
+            print(f"service wait timed out after {timeout_s:.0f} s on ticket {ticket}: {st}", file=sys.stderr)
+            print(svc.diagnose(), file=sys.stderr)
+            for b in svc.batch_log(16):
+                print(f"  batch {b}", file=sys.stderr)
+            sys.stderr.flush()
+            smi = subprocess.run(["nvidia-smi", "--query-gpu=utilization.gpu,clocks.sm,power.draw,memory.used",
+                                  "--format=csv"], capture_output=True, text=True, timeout=30)
+            print(smi.stdout, file=sys.stderr)
+        finally:
+            sys.stderr.flush()
+            sys.stdout.flush()
+            os._exit(3)
+    return r
+
+
 def poisson_load(svc, payloads, rate, seconds, per_db=None):
     """Poisson arrivals at `rate` payloads/s for `seconds`; latency = submit -> response ready
     inside the service (p50/p99 over all requests), throughput = completions / elapsed.
@@ -202,25 +255,27 @@ def poisson_load(svc, payloads, rate, seconds, per_db=None):
             t = q.get()
             if t is None:
                 return
-            svc.wait(t)
+            svc_wait(svc, t)
             done.append(time.perf_counter())
 
-    th = threading.Thread(target=collector)
+    th = threading.Thread(target=collector, daemon=True)
     th.start()
     t_start = time.perf_counter()
     t_next = t_start
-    for i in range(n):
-        t_next += rng.expovariate(rate)
-        d = t_next - time.perf_counter()
-        if d > 0:
-            time.sleep(d)
-        if per_db:
-            db = pick.randrange(len(per_db))
-            q.put(svc.submit(db, per_db[db][i % len(per_db[db])]))
-        else:
-            q.put(svc.submit(0, payloads[i % len(payloads)]))
-    offered_s = time.perf_counter() - t_start
-    q.put(None)
+    try:
+        for i in range(n):
+            t_next += rng.expovariate(rate)
+            d = t_next - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            if per_db:
+                db = pick.randrange(len(per_db))
+                q.put(svc.submit(db, per_db[db][i % len(per_db[db])]))
+            else:
+                q.put(svc.submit(0, payloads[i % len(payloads)]))
+        offered_s = time.perf_counter() - t_start
+    finally:
+        q.put(None)  # the collector ends even when a submission raised
     th.join()
     st = svc.stats()
     return {"offered_payloads_per_s": rate, "arrived_payloads_per_s": n / offered_s, "payloads": n,
@@ -247,6 +302,10 @@ def serve_config4(pkg, rates, seconds):
     torch.cuda.set_device(0)
     servers, plans, per_db = [], [], []
     t0 = time.perf_counter()
+
+    def progress(what):  # phase marks on stderr: the JSON line on stdout comes only at the end
+        print(f"[serve-config4 {time.perf_counter() - t0:7.1f} s] {what}", file=sys.stderr, flush=True)
+
     for name, rec, key, val, buckets, seed in CONFIG4:
         plan = pkg.plan_from_shape(rec, key, val, buckets, 8192)
         srv = pkg.KeywordServer.synthetic(plan, seed=seed)
@@ -263,21 +322,33 @@ def serve_config4(pkg, rates, seconds):
         per_db.append(pays)
     svc = pkg.KeywordService(servers, max_batch=64)
     setup_s = time.perf_counter() - t0
+    progress("three databases and the service are up")
     for db in range(3):
         for t in [svc.submit(db, per_db[db][i % 32]) for i in range(64)]:
-            svc.wait(t)
-    # saturation: every database kept full
-    n_each = 6 * 64
-    t1 = time.perf_counter()
-    tickets = [svc.submit(i % 3, per_db[i % 3][(i // 3) % 32]) for i in range(3 * n_each)]
-    for t in tickets:
-        svc.wait(t)
-    sat = 3 * n_each / (time.perf_counter() - t1)
+            svc_wait(svc, t)
+    # saturation: every database kept full, 16 batches of 64 per database; the median of
+    # three repetitions (a single short burst varies with host scheduling)
+    n_each = 16 * 64
+    sat_runs = []
+    for _ in range(3):
+        t1 = time.perf_counter()
+        tickets = [svc.submit(i % 3, per_db[i % 3][(i // 3) % 32]) for i in range(3 * n_each)]
+        for t in tickets:
+            svc_wait(svc, t)
+        sat_runs.append(3 * n_each / (time.perf_counter() - t1))
+    sat = statistics.median(sat_runs)
+    progress(f"saturation runs {[round(x) for x in sat_runs]} payloads/s")
     poisson_load(svc, None, rates[0], 0.5, per_db=per_db)  # warm-up at the first load, not reported
-    clocks = ClockSampler(0)
+    clocks = ClockSampler(0, interval_ms=100)
     clocks.start()
+    time.sleep(0.5)
+    clocks.begin()
     # at least 1,000 arrivals per load, so that a p99 rests on ten or more samples
-    serving = [poisson_load(svc, None, r, max(seconds, 1000.0 / r), per_db=per_db) for r in rates]
+    serving = []
+    for r in rates:
+        serving.append(poisson_load(svc, None, r, max(seconds, 1000.0 / r), per_db=per_db))
+        progress(f"Poisson load {r:g}/s: p99 {serving[-1]['p99_ms']:.1f} ms")
+    clocks.end()
     clk = clocks.stop()
     st = svc.stats()
     free_b, total_b = torch.cuda.mem_get_info()
@@ -291,7 +362,8 @@ def serve_config4(pkg, rates, seconds):
             "config": {"workload": "config 4: " + ", ".join(c[0] for c in CONFIG4) + ", dim0 8192",
                        "databases": [{"name": c[0], "db_rows": p.db_rows, "db_cols": p.db_cols,
                                       "instances": p.instances, "c": p.c} for c, p in zip(CONFIG4, plans)],
-                       "max_batch": st.max_batch, "device_bytes_in_use": hbm, "setup_s": setup_s},
+                       "max_batch": st.max_batch, "device_bytes_in_use": hbm, "setup_s": setup_s,
+                       "saturation_runs": sat_runs, "saturation_payloads_per_run": 3 * n_each},
             "serving": serving, "clocks": clk}
     print(json.dumps(line))
     return 0
@@ -529,8 +601,9 @@ def main():
                     help="under torchrun: one database split by fold groups over the ranks (each rank answers its "
                          "groups of every payload; NCCL broadcast of the queries and gather of the parts) "
                          "instead of one replica per rank")
-    ap.add_argument("--fold-form", type=int, default=2, choices=[1, 2],
-                    help="2: fold with the packing post-process fused in (default); 1: separate INTT + CRT pass")
+    ap.add_argument("--fold-form", type=int, default=3, choices=[1, 2, 3],
+                    help="3: fold with the packing post-process fused in, one chain per CTA (default); 2: the "
+                         "same on two chains per CTA; 1: separate INTT + CRT pass")
     ap.add_argument("--no-serving", action="store_true", help="skip the Poisson serving measurement")
     ap.add_argument("--serve-rates", type=float, nargs="*", default=[1000.0, 2500.0],
                     help="offered Poisson loads (payloads/s) for the serving measurement")
@@ -596,7 +669,7 @@ def main():
     else:
         srv = pkg.KeywordServer.synthetic(plan, seed=7 + rank, device=dev)
     local = srv.plan  # the rank's share: the whole plan for a replica, a fold-group slice for a shard
-    if args.fold_form != 2:
+    if args.fold_form != 3:
         srv.set_option(pkg.KeywordServer.OPT_FOLD_REGISTER_NTT, args.fold_form)
     qbytes = srv.query_bytes(2)
     rbytes = srv.response_bytes(2)
@@ -651,22 +724,26 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
+    # the clock sampler runs from the warm-up on (nvidia-smi takes a moment to start); its
+    # summary keeps only the samples inside the timed region
+    clocks = ClockSampler(dev if world == 1 else local)
+    clocks.start()
     for i in range(args.warmup):
         run_device(i)
         run_host(i)
     srv.sync()
 
     # ---- device-resident timed region -------------------------------------------------
-    clocks = ClockSampler(dev if world == 1 else local)
-    clocks.start()
     srv.set_profiling(True)
     barrier()
+    clocks.begin()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for i in range(args.steps):
         run_device(i)
     e1.record(stream)
     srv.sync()
+    clocks.end()
     barrier()
     dev_ms = e0.elapsed_time(e1)
     stage_ms, calls = srv.stage_times()
@@ -698,7 +775,7 @@ def main():
         e2e_ms = (time.perf_counter() - t0) * 1000
     if svc is not None:
         for t in [svc.submit(0, payloads[i % npay]) for i in range(2 * B)]:
-            svc.wait(t)
+            svc_wait(svc, t)
         barrier()
         t0 = time.perf_counter()
         # handed over a batch's worth at a time (ipr_service_submit_batch): the first dispatch
@@ -707,7 +784,7 @@ def main():
         for s0 in range(0, args.steps * B, B):
             tickets += svc.submit_many(0, [payloads[i % npay] for i in range(s0, min(s0 + B, args.steps * B))])
         for t in tickets:
-            svc.wait(t)
+            svc_wait(svc, t)
         e2e_ms = (time.perf_counter() - t0) * 1000
     barrier()
 

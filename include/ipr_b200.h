@@ -189,11 +189,14 @@ int ipr_server_set_profiling(ipr_server *srv, int on);
  * tensor cores over DB byte planes (default where db_rows <= 32768), 0 = the
  * CUDA-core kernel on the u16 DB.  Both give identical results. */
 #define IPR_OPT_TENSOR_GEMV 1
-/* IPR_OPT_FOLD_REGISTER_NTT: the form of the RGSW fold.  2 (default) = register-
+/* IPR_OPT_FOLD_REGISTER_NTT: the form of the RGSW fold.  3 (default) = register-
  * resident NTTs with the packing post-process (INTT + CRT + b add) fused into the
- * fold's own inverse transforms; 1 = register-resident NTTs after a separate INTT + CRT
- * pass; 0 = shared-memory NTTs after that pass (single-payload calls only; batches
- * then use form 1).  Identical results. */
+ * fold's own inverse transforms, one chain per CTA and two CTAs per SM, the query's
+ * RGSW bodies staged from global memory; 2 = the same fused fold on two chains of one
+ * query per CTA sharing the bodies in shared memory (an odd fold-group count leaves
+ * half a CTA idle); 1 = register-resident NTTs after a separate INTT + CRT pass;
+ * 0 = shared-memory NTTs after that pass (single-payload calls only; batches then
+ * use form 1).  Identical results. */
 #define IPR_OPT_FOLD_REGISTER_NTT 2
 /* IPR_OPT_PACK_CTA_PAIR: 1 = the batch path's packing GEMM runs on CTA pairs
  * (tcgen05 cta_group::2, M = 256 across two SMs); 0 = one CTA per unit;
@@ -458,6 +461,11 @@ typedef struct ipr_service_batch {
 } ipr_service_batch;
 int ipr_service_batch_log(ipr_service *svc, ipr_service_batch *out, int cap, int *n);
 int ipr_service_reset_stats(ipr_service *svc);
+/* A text snapshot of every database lane for diagnosing a stalled service: queued
+ * requests, busy I/O slots, and whether each slot's upload and compute events and the
+ * lane's server and download streams have completed (CUDA queries, no waiting).
+ * NUL-terminated, truncated to cap bytes. */
+int ipr_service_diagnose(ipr_service *svc, char *out, size_t cap);
 /* Finishes the batches in flight, drops queued and uncollected requests. */
 void ipr_service_destroy(ipr_service *svc);
 

@@ -141,6 +141,7 @@ _svc_poll = _sig("ipr_service_poll", _i32, _vp, _u64, _u8p, _sz, ctypes.POINTER(
 _svc_wait = _sig("ipr_service_wait", _i32, _vp, _u64, _i32, _u8p, _sz, ctypes.POINTER(_sz))
 _svc_stats = _sig("ipr_service_get_stats", _i32, _vp, ctypes.POINTER(_ServiceStats))
 _svc_reset = _sig("ipr_service_reset_stats", _i32, _vp)
+_svc_diagnose = _sig("ipr_service_diagnose", _i32, _vp, ctypes.c_char_p, _sz)
 
 
 class _ServiceBatch(ctypes.Structure):
@@ -688,6 +689,13 @@ class KeywordService:
 
     def reset_stats(self):
         _check(_svc_reset(self._h), "service_reset_stats")
+
+    def diagnose(self) -> str:
+        """ipr_service_diagnose: per database lane, the queue, busy slots and the completion
+        state of their uploads, compute and streams"""
+        buf = ctypes.create_string_buffer(1 << 14)
+        _check(_svc_diagnose(self._h, buf, len(buf)), "service_diagnose")
+        return buf.value.decode()
 
     def batch_log(self, cap: int = 4096):
         """the most recent batches, oldest first: dicts of db, payloads, launch/start/ready ms, queue_ms_max"""

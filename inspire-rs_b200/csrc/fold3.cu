@@ -50,18 +50,21 @@ using nttr::eB;
 using nttr::eC;
 using nttr::eD;
 
-// forward butterfly by stage: MODE 0 leaves x unreduced (x < 2^19 + 2q * stage), MODE 1
-// brings x < 16q down to [0, 2q) with three conditional subtractions, MODE 2 is the
-// Harvey form (x < 4q -> [0, 2q)).  Outputs: x + w*y, x - w*y (+2q), w*y in [0, 2q).
+// Barrett reduction with m = floor(2^32 / q): any 32-bit x to [0, 2q) (the quotient estimate
+// umulhi(x, m) is at most one below floor(x / q) because 2^32 - m q < q)
+constexpr uint32_t BM0 = (uint32_t)((1ull << 32) / Q0), BM1 = (uint32_t)((1ull << 32) / Q1);
+__device__ __forceinline__ uint32_t bred(uint32_t x, uint32_t q) {
+    return x - q * __umulhi(x, q == Q0 ? BM0 : BM1);
+}
+
+// forward butterfly by stage: MODE 0 leaves x unreduced (the bound grows by 2q), MODE 1
+// first brings x (any 32-bit value) to [0, 2q).  Outputs: x + w*y, x - w*y + 2q, w*y in [0, 2q).
 template <int MODE>
 __device__ __forceinline__ void fwd_b(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wp, uint32_t q) {
-    const uint32_t two_q = 2 * q;
-    uint32_t xx = x;
-    if (MODE == 1) xx = csub(csub(csub(x, 8 * q), 4 * q), two_q);
-    if (MODE == 2) xx = csub(x, two_q);
+    const uint32_t xx = MODE == 1 ? bred(x, q) : x;
     const uint32_t qn = shoup_lazy(y, w, wp, q);
     x = xx + qn;
-    y = xx + two_q - qn;
+    y = xx + 2 * q - qn;
 }
 
 // twiddle tables interleaved with their Shoup companions ([limb][N] of (w, wp)): one 8-byte
@@ -99,21 +102,29 @@ __device__ __forceinline__ void xchg_a2b(uint32_t (&v)[P][EPT], int t, uint32_t*
         for (int m = 0; m < EPT; m++) v[p][m] = xbuf[p * N + eB(t, m)];
 }
 
-template <int P>
+// XB < P: the buffer holds XB polynomials, moved XB at a time; a later chunk's stores wait at
+// a team barrier for every warp to finish loading the previous chunk from this warp's region
+template <int P, int XB = P>
 __device__ __forceinline__ void xchg_b2a(uint32_t (&v)[P][EPT], int t, uint32_t* xbuf, int bar) {
 #pragma unroll
-    for (int p = 0; p < P; p++)
+    for (int c0 = 0; c0 < P; c0 += XB) {
+        if (c0) nttr::group_bar(bar);
 #pragma unroll
-        for (int m = 0; m < EPT; m++) xbuf[p * N + eB(t, m)] = v[p][m];
-    nttr::group_bar(bar);
+        for (int p = c0; p < c0 + XB && p < P; p++)
 #pragma unroll
-    for (int p = 0; p < P; p++)
+            for (int m = 0; m < EPT; m++) xbuf[(p - c0) * N + eB(t, m)] = v[p][m];
+        nttr::group_bar(bar);
 #pragma unroll
-        for (int m = 0; m < EPT; m++) v[p][m] = xbuf[p * N + eA(t, m)];
+        for (int p = c0; p < c0 + XB && p < P; p++)
+#pragma unroll
+            for (int m = 0; m < EPT; m++) v[p][m] = xbuf[(p - c0) * N + eA(t, m)];
+    }
 }
 
 // forward NTT of P gadget-digit polynomials (< 2^19) of one limb: layout A in, layout D out
-// in [0, 2q); xbuf holds XP >= P polynomials of this team
+// in [0, 2q); xbuf holds XP >= P polynomials of this team.  Bounds: after stage s <= 6 every
+// value is below 2^19 + 2q (s + 1) <= 2^19 + 14q; stage 7 reduces x first (outputs < 4q);
+// stages 8..10 add 2q each (< 10q < 2^32); one reduction at the end.
 template <int P>
 __device__ __forceinline__ void forward_digits(uint32_t (&v)[P][EPT], int t, uint32_t* xbuf, int bar,
                                                const uint2* __restrict__ tw, uint32_t q) {
@@ -133,29 +144,29 @@ __device__ __forceinline__ void forward_digits(uint32_t (&v)[P][EPT], int t, uin
     nttr::b_to_c<P>(v, l, wb);
     fstage<P, 0>(v, 6, 4, fc, tw, q);
     fstage<P, 1>(v, 7, 2, fc, tw, q);
-    fstage<P, 2>(v, 8, 1, fc, tw, q);
+    fstage<P, 0>(v, 8, 1, fc, tw, q);
     nttr::c_to_d<P>(v, l, wb);
-    fstage<P, 2>(v, 9, 2, fd, tw, q);
-    fstage<P, 2>(v, 10, 1, fd, tw, q);
+    fstage<P, 0>(v, 9, 2, fd, tw, q);
+    fstage<P, 0>(v, 10, 1, fd, tw, q);
 #pragma unroll
     for (int p = 0; p < P; p++)
 #pragma unroll
-        for (int k = 0; k < EPT; k++) v[p][k] = csub(v[p][k], 2 * q);
+        for (int k = 0; k < EPT; k++) v[p][k] = bred(v[p][k], q);
 }
 
-// Gentleman-Sande butterfly with a plain inverse twiddle: x + y, (x - y) * w; inputs below
-// 2q (below q on the first stage, where x + y needs no reduction), outputs in [0, 2q)
-template <bool FIRST>
+// Gentleman-Sande butterfly with a plain inverse twiddle: x + y, (x - y) * w.  Inputs below
+// OFF * q; the difference is taken as x + OFF q - y (< 2 OFF q <= 16q < 2^32); the product
+// lands in [0, 2q); the sum (< 2 OFF q) is Barrett-reduced to [0, 2q) when RED.
+template <int OFF, bool RED>
 __device__ __forceinline__ void inv_b(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wp, uint32_t q) {
-    const uint32_t two_q = 2 * q;
     const uint32_t s = x + y;
-    const uint32_t d = x + two_q - y;
-    x = FIRST ? s : csub(s, two_q);
+    const uint32_t d = x + OFF * q - y;
+    x = RED ? bred(s, q) : s;
     y = shoup_lazy(d, w, wp, q);
 }
 
 // one inverse stage over 2 * PL polynomials: [0, PL) of limb 0, [PL, 2 PL) of limb 1
-template <int PL, bool FIRST, typename E>
+template <int PL, int OFF, bool RED, typename E>
 __device__ __forceinline__ void istage(uint32_t (&v)[2 * PL][EPT], int mm, int dd, E e, const uint2* __restrict__ iw) {
 #pragma unroll
     for (int k = 0; k < EPT; k++) {
@@ -163,14 +174,16 @@ __device__ __forceinline__ void istage(uint32_t (&v)[2 * PL][EPT], int mm, int d
         const int idx = (1 << mm) + (e(k) >> (11 - mm));
         const uint2 w0 = __ldg(iw + idx), w1 = __ldg(iw + N + idx);
 #pragma unroll
-        for (int p = 0; p < PL; p++) inv_b<FIRST>(v[p][k], v[p][k + dd], w0.x, w0.y, Q0);
+        for (int p = 0; p < PL; p++) inv_b<OFF, RED>(v[p][k], v[p][k + dd], w0.x, w0.y, Q0);
 #pragma unroll
-        for (int p = PL; p < 2 * PL; p++) inv_b<FIRST>(v[p][k], v[p][k + dd], w1.x, w1.y, Q1);
+        for (int p = PL; p < 2 * PL; p++) inv_b<OFF, RED>(v[p][k], v[p][k + dd], w1.x, w1.y, Q1);
     }
 }
 
-// N * INTT of 2 * PL canonical polynomials (PL per limb): layout D in, layout A canonical out
-template <int PL>
+// N * INTT of 2 * PL canonical polynomials (PL per limb): layout D in, layout A canonical out;
+// xbuf holds XB polynomials.  Value bounds entering each stage: q, 2q, 4q, 8q (then the sums
+// are reduced), 2q, 4q, 8q (reduced), 2q, 4q, 8q (reduced), 2q; below 4q at the end.
+template <int PL, int XB = 2 * PL>
 __device__ __forceinline__ void inverse_limbs(uint32_t (&v)[2 * PL][EPT], int t, uint32_t* xbuf, int bar,
                                               const uint2* __restrict__ iw) {
     const int l = t & 31;
@@ -179,24 +192,27 @@ __device__ __forceinline__ void inverse_limbs(uint32_t (&v)[2 * PL][EPT], int t,
     auto fb = [&](int k) { return eB(t, k); };
     auto fc = [&](int k) { return eC(t, k); };
     auto fd = [&](int k) { return eD(t, k); };
-    istage<PL, true>(v, 10, 1, fd, iw);
-    istage<PL, false>(v, 9, 2, fd, iw);
-    nttr::d_to_c<2 * PL>(v, l, wb);
-    istage<PL, false>(v, 8, 1, fc, iw);
-    istage<PL, false>(v, 7, 2, fc, iw);
-    istage<PL, false>(v, 6, 4, fc, iw);
-    nttr::c_to_b<2 * PL>(v, l, wb);
-    istage<PL, false>(v, 5, 1, fb, iw);
-    istage<PL, false>(v, 4, 2, fb, iw);
-    istage<PL, false>(v, 3, 4, fb, iw);
-    xchg_b2a<2 * PL>(v, t, xbuf, bar);
-    istage<PL, false>(v, 2, 1, fa, iw);
-    istage<PL, false>(v, 1, 2, fa, iw);
-    istage<PL, false>(v, 0, 4, fa, iw);
+    istage<PL, 1, false>(v, 10, 1, fd, iw);
+    istage<PL, 2, false>(v, 9, 2, fd, iw);
+    nttr::d_to_c<2 * PL, XB>(v, l, wb);
+    istage<PL, 4, false>(v, 8, 1, fc, iw);
+    istage<PL, 8, true>(v, 7, 2, fc, iw);
+    istage<PL, 2, false>(v, 6, 4, fc, iw);
+    nttr::c_to_b<2 * PL, XB>(v, l, wb);
+    istage<PL, 4, false>(v, 5, 1, fb, iw);
+    istage<PL, 8, true>(v, 4, 2, fb, iw);
+    istage<PL, 2, false>(v, 3, 4, fb, iw);
+    xchg_b2a<2 * PL, XB>(v, t, xbuf, bar);
+    istage<PL, 4, false>(v, 2, 1, fa, iw);
+    istage<PL, 8, true>(v, 1, 2, fa, iw);
+    istage<PL, 2, false>(v, 0, 4, fa, iw);
 #pragma unroll
     for (int p = 0; p < 2 * PL; p++)
 #pragma unroll
-        for (int k = 0; k < EPT; k++) v[p][k] = csub(v[p][k], p < PL ? Q0 : Q1);
+        for (int k = 0; k < EPT; k++) {
+            const uint32_t q = p < PL ? Q0 : Q1;
+            v[p][k] = csub(csub(v[p][k], 2 * q), q);
+        }
 }
 
 // the 8 consecutive words of layout D held by thread t (two 16-byte loads)
@@ -226,6 +242,44 @@ __device__ __forceinline__ uint64_t rescale_q(uint64_t v, uint64_t out_mod) {
     return neg ? (rm ? out_mod - rm : 0) : rm;
 }
 
+// switch_and_keep (src/pir/modulus_switch.rs:45-73) of thread t's coefficients e = t + 256 m of s:
+// row 0 -> 28-bit fields (2 per 7 bytes), row 1 -> 20-bit fields (2 per 5 bytes), LSB first;
+// coefficient e + 1 sits in the next lane of the same warp
+template <typename SA>
+__device__ __forceinline__ void switch_keep(SA S_AT, int t, uint8_t* __restrict__ out) {
+#pragma unroll
+    for (int m = 0; m < EPT; m++) {
+        const uint64_t a = rescale_q(S_AT(0, m), QP2), b = rescale_q(S_AT(1, m), QP1);
+        const uint64_t an = __shfl_down_sync(0xffffffffu, a, 1), bn = __shfl_down_sync(0xffffffffu, b, 1);
+        if (!(t & 1)) {
+            const int tt = eA(t, m) >> 1;
+            const uint64_t v = a | (an << 28), w = b | (bn << 20);
+#pragma unroll
+            for (int x = 0; x < 7; x++) out[7 * tt + x] = (uint8_t)(v >> (8 * x));
+#pragma unroll
+            for (int x = 0; x < 5; x++) out[7 * N / 2 + 5 * tt + x] = (uint8_t)(w >> (8 * x));
+        }
+    }
+}
+
+// 16- and 8-byte asynchronous copies global -> shared (sm_80+ cp.async); a thread waits for
+// its own copies with cp_wait
+__device__ __forceinline__ void cp16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int PENDING>
+__device__ __forceinline__ void cp_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(PENDING) : "memory");
+}
+
 }  // namespace
 
 // N^-1 mod q_l and its Shoup companion, per limb
@@ -238,7 +292,19 @@ struct NInv {
 // transforms leave out); zb null: the scaling alone.  One thread per 4 slots of one output.
 __global__ void __launch_bounds__(256) k_fold_prep(uint32_t* __restrict__ S, int64_t count,
                                                    const uint64_t* __restrict__ zb, const uint64_t* __restrict__ bth,
-                                                   int instances, NInv ni) {
+                                                   int instances, NInv ni, uint32_t* __restrict__ gsw,
+                                                   int64_t gsw_words) {
+    // the queries' RGSW bodies [query][6 gadget rows][2 limbs][N], scaled by N^-1 in place for
+    // the fold form that reads them straight from global memory
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < gsw_words / 4;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int lb = (int)((4 * i / N) & 1);
+        const uint32_t q = lb ? Q1 : Q0, w = ni.w[lb], wq = ni.wp[lb];
+        uint4* g = reinterpret_cast<uint4*>(gsw) + i;
+        const uint4 b = *g;
+        *g = make_uint4(mul_canon(b.x, w, wq, q), mul_canon(b.y, w, wq, q), mul_canon(b.z, w, wq, q),
+                        mul_canon(b.w, w, wq, q));
+    }
     const int64_t n4 = count * (N / 4);
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t f = i / (N / 4);
@@ -400,23 +466,151 @@ __global__ void __launch_bounds__(F3_THREADS, 1)
         }
     }
 
-    // switch_and_keep: row 0 -> 28-bit fields (2 per 7 bytes), row 1 -> 20-bit fields (2 per 5
-    // bytes), LSB first; coefficient e + 1 sits in the next lane of the same warp
-    uint8_t* out = resp + (int64_t)payload * resp_payload_stride + 8 + (int64_t)qin * resp_query_stride +
-                   (int64_t)wp * RESULT_BYTES;
+    switch_keep(S_AT, t, resp + (int64_t)payload * resp_payload_stride + 8 + (int64_t)qin * resp_query_stride +
+                             (int64_t)wp * RESULT_BYTES);
+}
+
+// One chain (query qg = blockIdx.y, fold group wp = blockIdx.x) per CTA of 256 threads, two
+// CTAs per SM, so that the grid's c x queries chains fill the SMs' 296 chain slots in waves
+// without the idle half-CTAs of an odd group count.  The RGSW bodies (already scaled by N^-1,
+// k_fold_prep) stay in global memory (L2-resident: 48 KB per query per limb); each batch of
+// three gadget digits stages the matching three bodies, with the packing output and row 0 of
+// its limb, through cp.async into shared memory while its forward transforms run, and the
+// packed row j (a_hat, c) lands in s's own slots while the inverse transforms run.
+// Shared memory: exchange buffer of 3 polynomials (24 KB), s (32 KB), staging (40 KB).
+constexpr int F4_THREADS = nttr::EPT * 32;  // 256: one chain, 8 coefficients per thread
+constexpr int F4_XB = 3;
+constexpr int F4_SMEM = F4_XB * N * 4 + 2 * N * 8 + 5 * N * 4;
+
+__global__ void __launch_bounds__(F4_THREADS, 2)
+    k_fold4(const uint32_t* __restrict__ row0s, const uint32_t* __restrict__ gsw, const uint64_t* __restrict__ a_hat,
+            const uint32_t* __restrict__ S, int64_t s_payload_stride, const uint64_t* __restrict__ cvec,
+            const uint2* __restrict__ fwi, const uint2* __restrict__ iwi, int interp, int c_groups, int64_t db_cols,
+            int qpp, uint8_t* __restrict__ resp, int64_t resp_payload_stride, int64_t resp_query_stride) {
+    extern __shared__ uint4 f4_smem[];
+    uint32_t* xbuf = reinterpret_cast<uint32_t*>(f4_smem);  // [F4_XB][N]
+    uint64_t* sst = reinterpret_cast<uint64_t*>(xbuf + F4_XB * N);  // [row][m][t]: read back only by thread t
+    uint32_t* stg = xbuf + F4_XB * N + 4 * N;  // [5][N]: bodies of digits 0..2, row 0, packing output
+    const int t = threadIdx.x;
+    auto S_AT = [&](int row, int m) -> uint64_t& { return sst[(row * EPT + m) * F4_THREADS + t]; };
+    const int wp = blockIdx.x, qg = blockIdx.y;
+    if (wp >= c_groups) return;
+    constexpr int bar = 1;
+    const int payload = qg / qpp, qin = qg % qpp;
+    const uint32_t* Sq = S + (int64_t)payload * s_payload_stride;
+    const uint64_t* cq = cvec + (int64_t)qg * db_cols;
+    const uint32_t* gq = gsw + (int64_t)qg * 12 * N;
+    const int z8 = 8 * t;  // layout D: thread t's 8 consecutive words (eD(t, k) = 8 t + k)
+    const uint64_t mask = (1ull << GADGET_BITS) - 1;
+
+    {  // first step: G^-1(0) = 0, so s = (a_hat[j], INTT(S[j]) + c[j]) mod q
+        const int j = wp * interp + interp - 1;
+        uint32_t pr[2][EPT];
+        load_d8(pr[0], Sq + ((int64_t)j * 2) * N + z8);
+        load_d8(pr[1], Sq + ((int64_t)j * 2 + 1) * N + z8);
+        uint64_t pc[EPT];
 #pragma unroll
-    for (int m = 0; m < EPT; m++) {
-        const uint64_t a = rescale_q(S_AT(0, m), QP2), b = rescale_q(S_AT(1, m), QP1);
-        const uint64_t an = __shfl_down_sync(0xffffffffu, a, 1), bn = __shfl_down_sync(0xffffffffu, b, 1);
-        if (!(t & 1)) {
-            const int tt = eA(t, m) >> 1;
-            const uint64_t v = a | (an << 28), w = b | (bn << 20);
+        for (int m = 0; m < EPT; m++) {
+            S_AT(0, m) = __ldg(a_hat + (int64_t)j * N + eA(t, m));
+            pc[m] = __ldg(cq + (int64_t)j * N + eA(t, m));
+        }
+        inverse_limbs<1, 2>(pr, t, xbuf, bar, iwi);
 #pragma unroll
-            for (int x = 0; x < 7; x++) out[7 * tt + x] = (uint8_t)(v >> (8 * x));
+        for (int m = 0; m < EPT; m++) S_AT(1, m) = add_q(crt2(pr[0][m], pr[1][m], Q0INV, BR1), pc[m]);
+    }
+
+    for (int step = interp - 2; step >= 0; step--) {
+        const int j = wp * interp + step;
+        uint32_t pr[4][EPT];  // [row 0 limb 0, row 1 limb 0, row 0 limb 1, row 1 limb 1]
 #pragma unroll
-            for (int x = 0; x < 5; x++) out[7 * N / 2 + 5 * tt + x] = (uint8_t)(w >> (8 * x));
+        for (int l = 0; l < 2; l++) {
+            const uint32_t q = l ? Q1 : Q0;
+            const uint64_t br = l ? BR1 : BR0;
+            uint32_t acc0[EPT], acc1[EPT];  // acc1 reduced after every batch of three digits
+#pragma unroll
+            for (int m = 0; m < EPT; m++) acc0[m] = 0;
+#pragma unroll 1
+            for (int r = 0; r < 2; r++) {  // gadget rows p = r + 2k hold digit k of row r (gadget.rs:44-58)
+                // every thread's reads of the staging area (the previous batch) are done
+                nttr::group_bar(bar);
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    const uint32_t* src = gq + (int64_t)((r + 2 * k) * 2 + l) * N + z8;
+                    cp16(stg + k * N + z8, src);
+                    cp16(stg + k * N + z8 + 4, src + 4);
+                }
+                if (r == 0) {
+                    cp16(stg + 3 * N + z8, row0s + l * N + z8);
+                    cp16(stg + 3 * N + z8 + 4, row0s + l * N + z8 + 4);
+                    const uint32_t* sp = Sq + ((int64_t)j * 2 + l) * N + z8;
+                    cp16(stg + 4 * N + z8, sp);
+                    cp16(stg + 4 * N + z8 + 4, sp + 4);
+                }
+                cp_commit();
+                uint32_t v[3][EPT];
+#pragma unroll
+                for (int m = 0; m < EPT; m++) {
+                    const uint64_t x = S_AT(r, m);
+#pragma unroll
+                    for (int k = 0; k < 3; k++) v[k][m] = (uint32_t)((x >> (k * GADGET_BITS)) & mask);
+                }
+                forward_digits<3>(v, t, xbuf, bar, fwi + l * N, q);
+                if (l == 1 && r == 1) {
+                    // s is consumed (the team barriers of the transforms ordered every read of
+                    // it): the packed row j lands in its slots while the inverse transforms run
+#pragma unroll
+                    for (int m = 0; m < EPT; m++) {
+                        cp8(&S_AT(0, m), a_hat + (int64_t)j * N + eA(t, m));
+                        cp8(&S_AT(1, m), cq + (int64_t)j * N + eA(t, m));
+                    }
+                    cp_commit();
+                    cp_wait<1>();
+                } else {
+                    cp_wait<0>();
+                }
+                if (r == 0) {
+                    const uint4 a = *reinterpret_cast<const uint4*>(stg + 4 * N + z8);
+                    const uint4 b = *reinterpret_cast<const uint4*>(stg + 4 * N + z8 + 4);
+                    acc1[0] = a.x; acc1[1] = a.y; acc1[2] = a.z; acc1[3] = a.w;
+                    acc1[4] = b.x; acc1[5] = b.y; acc1[6] = b.z; acc1[7] = b.w;
+                }
+                uint64_t part[EPT];
+#pragma unroll
+                for (int m = 0; m < EPT; m++) part[m] = acc1[m];
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    const uint4 b0 = *reinterpret_cast<const uint4*>(stg + k * N + z8);
+                    const uint4 b1 = *reinterpret_cast<const uint4*>(stg + k * N + z8 + 4);
+                    const uint32_t bv[EPT] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+                    for (int m = 0; m < EPT; m++) {
+                        acc0[m] += v[k][m];                    // 6 terms < 12q < 2^32
+                        part[m] += (uint64_t)bv[m] * v[k][m];  // q + 3 terms < q + 6 q^2 < 2^60
+                    }
+                }
+#pragma unroll
+                for (int m = 0; m < EPT; m++) acc1[m] = mod64(part[m], q, br);
+            }
+            const uint4 ra = *reinterpret_cast<const uint4*>(stg + 3 * N + z8);
+            const uint4 rb = *reinterpret_cast<const uint4*>(stg + 3 * N + z8 + 4);
+            const uint32_t r0[EPT] = {ra.x, ra.y, ra.z, ra.w, rb.x, rb.y, rb.z, rb.w};
+#pragma unroll
+            for (int m = 0; m < EPT; m++) {
+                pr[2 * l][m] = mod64((uint64_t)r0[m] * acc0[m], q, br);
+                pr[2 * l + 1][m] = acc1[m];
+            }
+        }
+        inverse_limbs<2, 2>(pr, t, xbuf, bar, iwi);
+        cp_wait<0>();  // the packed row j in s's slots
+#pragma unroll
+        for (int m = 0; m < EPT; m++) {
+            S_AT(0, m) = add_q(crt2(pr[0][m], pr[2][m], Q0INV, BR1), S_AT(0, m));
+            S_AT(1, m) = add_q(crt2(pr[1][m], pr[3][m], Q0INV, BR1), S_AT(1, m));
         }
     }
+
+    switch_keep(S_AT, t, resp + (int64_t)payload * resp_payload_stride + 8 + (int64_t)qin * resp_query_stride +
+                             (int64_t)wp * RESULT_BYTES);
 }
 
 // RGSW bodies 96 KB + two team exchange buffers of 4 polynomials (2 x 32 KB) + the two
@@ -424,16 +618,19 @@ __global__ void __launch_bounds__(F3_THREADS, 1)
 constexpr int FOLD3_SMEM = (12 + 2 * XP) * N * 4 + 2 * 2 * N * 8;
 
 cudaError_t init_fold3_kernel() {
-    return cudaFuncSetAttribute(k_fold3, cudaFuncAttributeMaxDynamicSharedMemorySize, FOLD3_SMEM);
+    cudaError_t e = cudaFuncSetAttribute(k_fold3, cudaFuncAttributeMaxDynamicSharedMemorySize, FOLD3_SMEM);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_fold4, cudaFuncAttributeMaxDynamicSharedMemorySize, F4_SMEM);
 }
 
 cudaError_t launch_fold_prep(uint32_t* S, int64_t count, const uint64_t* zb, const uint64_t* bth, int instances,
-                             const uint32_t ninv[4], int sm_count, cudaStream_t st) {
-    if (count < 1 || (zb && instances < 1)) return cudaErrorInvalidValue;
+                             const uint32_t ninv[4], int sm_count, cudaStream_t st, uint32_t* gsw, int gsw_queries) {
+    if (count < 1 || (zb && instances < 1) || (gsw && gsw_queries < 1)) return cudaErrorInvalidValue;
     NInv ni{{ninv[0], ninv[2]}, {ninv[1], ninv[3]}};
     const int64_t n4 = count * (N / 4);
     const int64_t blocks = std::min<int64_t>((n4 + 255) / 256, (int64_t)sm_count * 8);
-    k_fold_prep<<<(unsigned)blocks, 256, 0, st>>>(S, count, zb, bth, instances, ni);
+    const int64_t gsw_words = gsw ? (int64_t)gsw_queries * 12 * N : 0;
+    k_fold_prep<<<(unsigned)blocks, 256, 0, st>>>(S, count, zb, bth, instances, ni, gsw, gsw_words);
     return cudaGetLastError();
 }
 
@@ -449,6 +646,19 @@ cudaError_t launch_fold3(const uint32_t* row0s, const uint32_t* gsw, const uint6
                                                    reinterpret_cast<const uint2*>(fwi),
                                                    reinterpret_cast<const uint2*>(iwi), ni, interp, c_groups, db_cols,
                                                    qpp, resp, resp_payload_stride, resp_query_stride);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fold4(const uint32_t* row0s, const uint32_t* gsw_scaled, const uint64_t* a_hat, const uint32_t* S,
+                         int64_t s_payload_stride, const uint64_t* cvec, const uint32_t* fwi, const uint32_t* iwi,
+                         int interp, int c_groups, int num_queries, int64_t db_cols, int qpp, uint8_t* resp,
+                         int64_t resp_payload_stride, int64_t resp_query_stride, cudaStream_t st) {
+    if (interp < 1 || c_groups < 1 || num_queries < 1 || num_queries > 65535 || qpp < 1) return cudaErrorInvalidValue;
+    dim3 grid(c_groups, num_queries);
+    k_fold4<<<grid, F4_THREADS, F4_SMEM, st>>>(row0s, gsw_scaled, a_hat, S, s_payload_stride, cvec,
+                                                reinterpret_cast<const uint2*>(fwi), reinterpret_cast<const uint2*>(iwi),
+                                                interp, c_groups, db_cols, qpp, resp, resp_payload_stride,
+                                                resp_query_stride);
     return cudaGetLastError();
 }
 

@@ -153,12 +153,19 @@ int enqueue(ipr_server* s, unsigned nq, const uint8_t* d_query, uint8_t* d_resp,
         rec(2);
         CU(ipr::launch_pack(s->d_bt, s->d_btb, s->d_bth, s->d_y, s->d_z, s->d_S, (int)p.instances, st));
         rec(3);
-        if (s->fold_mode == 2) {
-            CU(ipr::launch_fold_prep(s->d_S, (int64_t)p.instances, nullptr, nullptr, 1, s->hp.ninv, s->sm_count, st));
+        if (s->fold_mode >= 2) {
+            const bool chain = s->fold_mode == 3;
+            CU(ipr::launch_fold_prep(s->d_S, (int64_t)p.instances, nullptr, nullptr, 1, s->hp.ninv, s->sm_count, st,
+                                     chain ? s->d_gsw : nullptr, (int)nq));
             rec(4);
-            CU(ipr::launch_fold3(s->d_row0s, s->d_gsw, s->d_ahat, s->d_S, 0, s->d_c, s->d_fwi, s->d_iwi, s->hp.ninv,
-                                 (int)p.interp, (int)p.c, (int)nq, (int64_t)p.db_cols, (int)nq, d_resp, 0,
-                                 (int64_t)(4 + s->per_query_bytes()), st));
+            if (chain)
+                CU(ipr::launch_fold4(s->d_row0s, s->d_gsw, s->d_ahat, s->d_S, 0, s->d_c, s->d_fwi, s->d_iwi,
+                                     (int)p.interp, (int)p.c, (int)nq, (int64_t)p.db_cols, (int)nq, d_resp, 0,
+                                     (int64_t)(4 + s->per_query_bytes()), st));
+            else
+                CU(ipr::launch_fold3(s->d_row0s, s->d_gsw, s->d_ahat, s->d_S, 0, s->d_c, s->d_fwi, s->d_iwi,
+                                     s->hp.ninv, (int)p.interp, (int)p.c, (int)nq, (int64_t)p.db_cols, (int)nq, d_resp,
+                                     0, (int64_t)(4 + s->per_query_bytes()), st));
         } else if (s->fold_mode == 1) {
             CU(ipr::launch_intt_crt(s->d_S, s->d_iw, s->d_iwp, s->d_R, (int)p.instances, st));
             rec(4);
@@ -244,7 +251,7 @@ int ensure_batch(ipr_server* s, int B) {
     if ((st = s->alloc(&s->d_bq, (size_t)B * qb)) || (st = s->alloc(&s->d_ybs, (size_t)B * 3 * kN * 8)) ||
         (st = s->alloc(&s->d_zbs, (size_t)B * 3 * kN * 8)) || (st = s->alloc(&s->d_y8, (size_t)2 * s->y8_np * 3 * kN)) ||
         (st = s->alloc(&s->d_bS, (size_t)B * no * 2 * kN * 4)) ||
-        (s->fold_mode != 2 && (st = s->alloc(&s->d_bR, (size_t)B * no * kN * 8))) ||
+        (s->fold_mode < 2 && (st = s->alloc(&s->d_bR, (size_t)B * no * kN * 8))) ||
         (st = s->alloc(&s->d_bresp, (size_t)B * rb)))
         return st;
     CU(cudaMallocHost(&s->h_bq, (size_t)B * qb));
@@ -300,13 +307,19 @@ int enqueue_batch(ipr_server* s, int B, const uint8_t* d_queries, uint8_t* d_res
                                     st));
     }
     rec(3);
-    if (s->fold_mode == 2) {
+    if (s->fold_mode >= 2) {
+        const bool chain = s->fold_mode == 3;
         CU(ipr::launch_fold_prep(s->d_bS, (int64_t)B * p.instances, s->d_zbs, s->d_bth, (int)p.instances, s->hp.ninv,
-                                 s->sm_count, st));
+                                 s->sm_count, st, chain ? s->d_gsw : nullptr, nqt));
         rec(4);
-        CU(ipr::launch_fold3(s->d_row0s, s->d_gsw, s->d_ahat, s->d_bS, (int64_t)(p.instances * 2 * kN), s->d_c,
-                             s->d_fwi, s->d_iwi, s->hp.ninv, (int)p.interp, (int)p.c, nqt, (int64_t)p.db_cols, 2,
-                             d_resps, rb, (int64_t)(4 + s->per_query_bytes()), st));
+        if (chain)
+            CU(ipr::launch_fold4(s->d_row0s, s->d_gsw, s->d_ahat, s->d_bS, (int64_t)(p.instances * 2 * kN), s->d_c,
+                                 s->d_fwi, s->d_iwi, (int)p.interp, (int)p.c, nqt, (int64_t)p.db_cols, 2, d_resps, rb,
+                                 (int64_t)(4 + s->per_query_bytes()), st));
+        else
+            CU(ipr::launch_fold3(s->d_row0s, s->d_gsw, s->d_ahat, s->d_bS, (int64_t)(p.instances * 2 * kN), s->d_c,
+                                 s->d_fwi, s->d_iwi, s->hp.ninv, (int)p.interp, (int)p.c, nqt, (int64_t)p.db_cols, 2,
+                                 d_resps, rb, (int64_t)(4 + s->per_query_bytes()), st));
     } else {
         if (!s->d_bR) return fail(IPR_E_STATE, "batch scratch lacks the INTT output (fold form changed mid-batch)");
         CU(ipr::launch_intt_crt(s->d_bS, s->d_iw, s->d_iwp, s->d_bR, (int)(B * p.instances), st, s->d_zbs, s->d_bth,
@@ -497,7 +510,7 @@ uint64_t server_batch_bytes(const ipr_server* s, int B) {
     const uint64_t scratch = ipr::query_bytes(rows, (unsigned)nq) + 16 + (nq + 1) / 2 * rows * 16 + nq * 12 * kN * 4 +
                              nq * cols * 8 + s->response_bytes((unsigned)nq) + qb_rows((unsigned)nq) * rows;
     const uint64_t batch = B * qb + 2ull * B * 3 * kN * 8 + 2ull * ipr::pack_mma_nt(B) * 3 * kN +
-                           B * no * 2 * kN * 4 + (s->fold_mode != 2 ? B * no * kN * 8 : 0) + B * rb;
+                           B * no * 2 * kN * 4 + (s->fold_mode < 2 ? B * no * kN * 8 : 0) + B * rb;
     return tpp + scratch + batch;
 }
 
@@ -1053,11 +1066,11 @@ int ipr_server_set_option(ipr_server* s, int option, int64_t value) {
             destroy_graphs(s);
             return IPR_OK;
         case IPR_OPT_FOLD_REGISTER_NTT: {
-            if (value < 0 || value > 2) return fail(IPR_E_ARGS, "IPR_OPT_FOLD_REGISTER_NTT takes 0, 1 or 2");
-            const bool had_r = s->fold_mode != 2;
+            if (value < 0 || value > 3) return fail(IPR_E_ARGS, "IPR_OPT_FOLD_REGISTER_NTT takes 0 to 3");
+            const bool had_r = s->fold_mode < 2;
             s->fold_mode = (int)value;
             destroy_graphs(s);
-            if ((s->fold_mode != 2) != had_r && s->bcap) {  // the batch scratch changes shape
+            if ((s->fold_mode < 2) != had_r && s->bcap) {  // the batch scratch changes shape
                 CU(cudaStreamSynchronize(s->stream));
                 s->bcap = 0;
             }

@@ -720,6 +720,46 @@ int ipr_service_reset_stats(ipr_service* v) {
     return IPR_OK;
 }
 
+int ipr_service_diagnose(ipr_service* v, char* out, size_t cap) {
+    if (!v || !out || cap == 0) return svc_fail(IPR_E_ARGS, "null argument");
+    auto q = [](cudaError_t e) { return e == cudaSuccess ? "done" : e == cudaErrorNotReady ? "busy" : "error"; };
+    std::string txt;
+    char line[320];
+    const int nl = v->nlanes.load(std::memory_order_acquire);
+    for (int li = 0; li < nl; li++) {
+        Lane& ln = v->lanes[li];
+        size_t pending;
+        bool ready[2];
+        size_t nb[2];
+        {
+            std::lock_guard<std::mutex> lk(v->mu);
+            pending = ln.pending.size();
+            for (int k = 0; k < 2; k++) {
+                ready[k] = ln.slot[k].ready;
+                nb[k] = ln.slot[k].batch.size();
+            }
+        }
+        // the scheduler owns nbusy / head; a racing read only misstates this one line
+        std::snprintf(line, sizeof line, "db %d: max_batch %d, %zu pending, %d slots busy (head %d); server stream %s, "
+                                         "download stream %s\n",
+                      li, ln.max_batch, pending, ln.nbusy, ln.head, q(cudaStreamQuery(ln.s->stream)),
+                      ln.down ? q(cudaStreamQuery(ln.down)) : "none");
+        txt += line;
+        for (int k = 0; k < 2 && ln.max_batch > 0; k++) {
+            const Slot& sl = ln.slot[k];
+            const double age = std::chrono::duration<double, std::milli>(Clock::now() - sl.t_launch).count();
+            std::snprintf(line, sizeof line, "  slot %d: %zu payloads, uploaded %s, computed %s, ready %d, launched %.1f ms ago\n",
+                          k, nb[k], sl.up ? q(cudaEventQuery(sl.up)) : "none",
+                          sl.computed ? q(cudaEventQuery(sl.computed)) : "none", (int)ready[k], age);
+            txt += line;
+        }
+    }
+    const size_t n = std::min(cap - 1, txt.size());
+    std::memcpy(out, txt.data(), n);
+    out[n] = 0;
+    return IPR_OK;
+}
+
 void ipr_service_destroy(ipr_service* v) {
     if (!v) return;
     {

@@ -89,12 +89,13 @@ def test_first_dimension_paths(cfg0, pkg, orc, tensor, nq):
         srv.set_option(pkg.KeywordServer.OPT_TENSOR_GEMV, 1)
 
 
-@pytest.mark.parametrize("regs", [0, 1, 2])
+@pytest.mark.parametrize("regs", [0, 1, 2, 3])
 @pytest.mark.parametrize("instances,interp", [(8, 8), (8, 1), (6, 2)])
 def test_fold_kernels(pkg, orc, regs, instances, interp):
-    """the three fold forms (shared-memory NTTs, register NTTs after a separate INTT + CRT
-    pass, register NTTs with that pass fused in) give the oracle's bytes, for one, eight and
-    three fold groups (an odd count leaves the fused fold's second team of a CTA idle)"""
+    """the four fold forms (shared-memory NTTs, register NTTs after a separate INTT + CRT
+    pass, register NTTs with that pass fused in on two chains or one chain per CTA) give the
+    oracle's bytes, for one, eight and three fold groups (an odd count leaves the two-chain
+    form's second team of a CTA idle)"""
     plan = _plan(pkg, instances, interp)
     with pkg.KeywordServer.synthetic(plan, seed=50 + instances + interp) as srv:
         srv.set_option(pkg.KeywordServer.OPT_FOLD_REGISTER_NTT, regs)
@@ -297,6 +298,22 @@ def test_respond_batch_other_shapes(pkg, orc, instances, interp):
         got = srv.respond_batch(qs)
         for q, g in zip(qs, got):
             assert g == orc.respond(sdb, q)
+
+
+@pytest.mark.parametrize("form", [1, 2, 3])
+def test_respond_batch_fold_forms(pkg, orc, form):
+    """the batch path's fold forms give the oracle's bytes at an odd fold-group count (40 / 8 = 5)
+    with 9 payloads = 18 queries, 90 chains"""
+    plan = _plan(pkg, 40, 8)
+    sdb = orc.SynthDB(plan.db_rows, 40, 8, plan.c, seed=95)
+    with pkg.KeywordServer.synthetic(plan, seed=95) as srv:
+        srv.set_option(pkg.KeywordServer.OPT_FOLD_REGISTER_NTT, form)
+        qs = [orc.synth_query(4500 + 11 * form + i, plan.db_rows, 2) for i in range(9)]
+        got = srv.respond_batch(qs)
+        for q, g in zip(qs, got):
+            assert g == orc.respond(sdb, q)
+        # the scaled RGSW bodies of one batch do not leak into the next
+        assert srv.respond_batch(qs[:3]) == got[:3]
 
 
 def test_respond_batch_device_entry(cfg0, orc):
