@@ -68,14 +68,25 @@ __device__ __forceinline__ void fwd_b(uint32_t& x, uint32_t& y, uint32_t w, uint
 }
 
 // twiddle tables interleaved with their Shoup companions ([limb][N] of (w, wp)): one 8-byte
-// load per twiddle, half the L1 requests of two separate tables
-template <int P, int MODE, typename E>
-__device__ __forceinline__ void fstage(uint32_t (&v)[P][EPT], int mm, int dd, E e, const uint2* __restrict__ tw,
+// load per twiddle, half the L1 requests of two separate tables.  The twiddle of element k of
+// a thread is (1 << mm) + (e >> (11 - mm)) with e = hi + k * RS + lo in every layout: hi, the
+// thread's part, is a multiple of 2^(11 - mm) at the stages run in that layout, and lo (the
+// thread bits below the register stride RS) never carries into the shifted value.  So the
+// index is the thread's base plus a compile-time constant, and the elements of one stage that
+// share a twiddle share its load.  Layout A: hi = 0, RS = 256; B: hi = 256 w, RS = 32;
+// C: hi = 256 w + 32 (l / 4), RS = 4; D: hi = 256 w + 8 l, RS = 1 (w = t / 32, l = t % 32).
+template <int RS>
+__device__ __forceinline__ int tw_idx(int mm, int hi, int k) {
+    return (1 << mm) + (hi >> (11 - mm)) + ((k * RS) >> (11 - mm));
+}
+
+template <int P, int MODE, int RS>
+__device__ __forceinline__ void fstage(uint32_t (&v)[P][EPT], int mm, int dd, int hi, const uint2* __restrict__ tw,
                                        uint32_t q) {
 #pragma unroll
     for (int k = 0; k < EPT; k++) {
         if (k & dd) continue;
-        const uint2 w = __ldg(tw + (1 << mm) + (e(k) >> (11 - mm)));
+        const uint2 w = __ldg(tw + tw_idx<RS>(mm, hi, k));
 #pragma unroll
         for (int p = 0; p < P; p++) fwd_b<MODE>(v[p][k], v[p][k + dd], w.x, w.y, q);
     }
@@ -128,26 +139,23 @@ __device__ __forceinline__ void xchg_b2a(uint32_t (&v)[P][EPT], int t, uint32_t*
 template <int P>
 __device__ __forceinline__ void forward_digits(uint32_t (&v)[P][EPT], int t, uint32_t* xbuf, int bar,
                                                const uint2* __restrict__ tw, uint32_t q) {
-    const int l = t & 31;
-    uint32_t* wb = xbuf + (t >> 5) * 256;
-    auto fa = [&](int k) { return eA(t, k); };
-    auto fb = [&](int k) { return eB(t, k); };
-    auto fc = [&](int k) { return eC(t, k); };
-    auto fd = [&](int k) { return eD(t, k); };
-    fstage<P, 0>(v, 0, 4, fa, tw, q);
-    fstage<P, 0>(v, 1, 2, fa, tw, q);
-    fstage<P, 0>(v, 2, 1, fa, tw, q);
+    const int l = t & 31, w = t >> 5;
+    uint32_t* wb = xbuf + w * 256;
+    const int hb = 256 * w, hc = 256 * w + 32 * (l >> 2), hd = 256 * w + 8 * l;
+    fstage<P, 0, 256>(v, 0, 4, 0, tw, q);
+    fstage<P, 0, 256>(v, 1, 2, 0, tw, q);
+    fstage<P, 0, 256>(v, 2, 1, 0, tw, q);
     xchg_a2b<P>(v, t, xbuf, bar);
-    fstage<P, 0>(v, 3, 4, fb, tw, q);
-    fstage<P, 0>(v, 4, 2, fb, tw, q);
-    fstage<P, 0>(v, 5, 1, fb, tw, q);
+    fstage<P, 0, 32>(v, 3, 4, hb, tw, q);
+    fstage<P, 0, 32>(v, 4, 2, hb, tw, q);
+    fstage<P, 0, 32>(v, 5, 1, hb, tw, q);
     nttr::b_to_c<P>(v, l, wb);
-    fstage<P, 0>(v, 6, 4, fc, tw, q);
-    fstage<P, 1>(v, 7, 2, fc, tw, q);
-    fstage<P, 0>(v, 8, 1, fc, tw, q);
+    fstage<P, 0, 4>(v, 6, 4, hc, tw, q);
+    fstage<P, 1, 4>(v, 7, 2, hc, tw, q);
+    fstage<P, 0, 4>(v, 8, 1, hc, tw, q);
     nttr::c_to_d<P>(v, l, wb);
-    fstage<P, 0>(v, 9, 2, fd, tw, q);
-    fstage<P, 0>(v, 10, 1, fd, tw, q);
+    fstage<P, 0, 1>(v, 9, 2, hd, tw, q);
+    fstage<P, 0, 1>(v, 10, 1, hd, tw, q);
 #pragma unroll
     for (int p = 0; p < P; p++)
 #pragma unroll
@@ -166,12 +174,12 @@ __device__ __forceinline__ void inv_b(uint32_t& x, uint32_t& y, uint32_t w, uint
 }
 
 // one inverse stage over 2 * PL polynomials: [0, PL) of limb 0, [PL, 2 PL) of limb 1
-template <int PL, int OFF, bool RED, typename E>
-__device__ __forceinline__ void istage(uint32_t (&v)[2 * PL][EPT], int mm, int dd, E e, const uint2* __restrict__ iw) {
+template <int PL, int OFF, bool RED, int RS>
+__device__ __forceinline__ void istage(uint32_t (&v)[2 * PL][EPT], int mm, int dd, int hi, const uint2* __restrict__ iw) {
 #pragma unroll
     for (int k = 0; k < EPT; k++) {
         if (k & dd) continue;
-        const int idx = (1 << mm) + (e(k) >> (11 - mm));
+        const int idx = tw_idx<RS>(mm, hi, k);
         const uint2 w0 = __ldg(iw + idx), w1 = __ldg(iw + N + idx);
 #pragma unroll
         for (int p = 0; p < PL; p++) inv_b<OFF, RED>(v[p][k], v[p][k + dd], w0.x, w0.y, Q0);
@@ -186,26 +194,23 @@ __device__ __forceinline__ void istage(uint32_t (&v)[2 * PL][EPT], int mm, int d
 template <int PL, int XB = 2 * PL>
 __device__ __forceinline__ void inverse_limbs(uint32_t (&v)[2 * PL][EPT], int t, uint32_t* xbuf, int bar,
                                               const uint2* __restrict__ iw) {
-    const int l = t & 31;
-    uint32_t* wb = xbuf + (t >> 5) * 256;
-    auto fa = [&](int k) { return eA(t, k); };
-    auto fb = [&](int k) { return eB(t, k); };
-    auto fc = [&](int k) { return eC(t, k); };
-    auto fd = [&](int k) { return eD(t, k); };
-    istage<PL, 1, false>(v, 10, 1, fd, iw);
-    istage<PL, 2, false>(v, 9, 2, fd, iw);
+    const int l = t & 31, w = t >> 5;
+    uint32_t* wb = xbuf + w * 256;
+    const int hb = 256 * w, hc = 256 * w + 32 * (l >> 2), hd = 256 * w + 8 * l;
+    istage<PL, 1, false, 1>(v, 10, 1, hd, iw);
+    istage<PL, 2, false, 1>(v, 9, 2, hd, iw);
     nttr::d_to_c<2 * PL, XB>(v, l, wb);
-    istage<PL, 4, false>(v, 8, 1, fc, iw);
-    istage<PL, 8, true>(v, 7, 2, fc, iw);
-    istage<PL, 2, false>(v, 6, 4, fc, iw);
+    istage<PL, 4, false, 4>(v, 8, 1, hc, iw);
+    istage<PL, 8, true, 4>(v, 7, 2, hc, iw);
+    istage<PL, 2, false, 4>(v, 6, 4, hc, iw);
     nttr::c_to_b<2 * PL, XB>(v, l, wb);
-    istage<PL, 4, false>(v, 5, 1, fb, iw);
-    istage<PL, 8, true>(v, 4, 2, fb, iw);
-    istage<PL, 2, false>(v, 3, 4, fb, iw);
+    istage<PL, 4, false, 32>(v, 5, 1, hb, iw);
+    istage<PL, 8, true, 32>(v, 4, 2, hb, iw);
+    istage<PL, 2, false, 32>(v, 3, 4, hb, iw);
     xchg_b2a<2 * PL, XB>(v, t, xbuf, bar);
-    istage<PL, 4, false>(v, 2, 1, fa, iw);
-    istage<PL, 8, true>(v, 1, 2, fa, iw);
-    istage<PL, 2, false>(v, 0, 4, fa, iw);
+    istage<PL, 4, false, 256>(v, 2, 1, 0, iw);
+    istage<PL, 8, true, 256>(v, 1, 2, 0, iw);
+    istage<PL, 2, false, 256>(v, 0, 4, 0, iw);
 #pragma unroll
     for (int p = 0; p < 2 * PL; p++)
 #pragma unroll
