@@ -283,13 +283,19 @@ void scheduler(ipr_service* v) {
         }
         // 2. dispatch.  An idle database takes what is pending at once; with one batch in
         // flight the second slot is filled only when that batch is about to end (the
-        // staging lead), so it carries everything that arrived meanwhile.
+        // staging lead), so it carries everything that arrived meanwhile -- unless a full
+        // batch is already waiting, which gains nothing by waiting and is staged at once.
         Clock::time_point wake = Clock::time_point::max();
         const auto now = Clock::now();
         for (int i = 0; i < nl; i++) {
             Lane& ln = v->lanes[(rr + i) % nl];
             while (ln.max_batch == 0 || ln.nbusy < 2) {
+                bool full = false;
                 if (ln.max_batch > 0 && ln.nbusy == 1) {
+                    std::lock_guard<std::mutex> lk(v->mu);
+                    full = ln.pending.size() >= (size_t)ln.max_batch;
+                }
+                if (ln.max_batch > 0 && ln.nbusy == 1 && !full) {
                     const auto lead = std::chrono::microseconds(
                         (int64_t)std::max(1500.0, 250.0 * ln.estimate(ln.max_batch)));
                     if (now + lead < ln.free_at) {

@@ -212,6 +212,33 @@ def test_submit_many_answers_each_payload_like_alone(pkg, orc):
 
 
 @pytest.mark.gpu
+def test_full_batches_staged_at_once_and_diagnose(pkg, orc, dbs):
+    """a queue holding several full batches fills both I/O slots at once (no staging lead);
+    every response equals the payload answered alone, and ipr_service_diagnose reports the
+    lane idle afterwards"""
+    plan, srv, sdb = dbs[0]
+    qs = [orc.synth_query(900 + i, plan.db_rows, 2) for i in range(40)]
+    alone = [srv.respond_to_serialized_query(q) for q in qs]
+    svc = pkg.KeywordService([srv], max_batch=8)
+    try:
+        tickets = svc.submit_many(0, qs)
+        got = [svc.wait(t, 60_000) for t in tickets]
+        for _ in range(100):  # the scheduler frees the last slot just after completing its requests
+            text = svc.diagnose()
+            if "0 slots busy" in text:
+                break
+            time.sleep(0.01)
+        st = svc.stats()
+    finally:
+        svc.close()
+    assert got == alone
+    assert got[0] == orc.respond(sdb, qs[0]) and got[-1] == orc.respond(sdb, qs[-1])
+    assert st.batches >= 5 and st.pending == 0 and st.in_flight == 0
+    assert "db 0: max_batch 8, 0 pending, 0 slots busy" in text
+    assert "slot 0:" in text and "slot 1:" in text and "server stream done" in text
+
+
+@pytest.mark.gpu
 def test_injected_allocation_failures_are_clean(pkg, orc):
     """every device allocation of server creation, a first respond and batch preparation fails
     once in turn (ipr_debug_fail_allocation): the call that needed it returns IPR_E_OOM, the
