@@ -366,6 +366,25 @@ int ipr_device_binary_version(int device, int *binary_version);
  * one of its kernels' waits runs out, after 100 ms there) and the device stays usable. */
 int ipr_selftest_bounded_wait(int device, uint32_t limit_us);
 
+/* Bounds-checked debug build (libipr_b200_dbg.so, built with -DIPR_BOUNDS_CHECK by
+ * `make -C inspire-rs_b200 debug`).  ipr_bounds_checked_build returns 1 in that build and
+ * 0 in the release library.  In the debug build every launch of the respond() path first
+ * checks each buffer argument's byte range, computed from the launch's parameters, against
+ * the device allocation holding it (a launch outside fails with IPR_E_CUDA), and the fold
+ * and its scaling pass check every global index against the extents they are given,
+ * skipping the access and recording a site id instead of faulting.  ipr_bounds_report
+ * synchronises the current device, writes one line per failure since the last report
+ * (NUL-terminated, truncated to cap) and returns their count; 0 in the release build. */
+int ipr_bounds_checked_build(void);
+int ipr_bounds_report(char *out, size_t cap);
+/* Debug build only (IPR_E_STATE in the release library): ipr_debug_check_extent runs the
+ * launch-argument check on [d_ptr, d_ptr + bytes) (IPR_OK inside one device allocation,
+ * IPR_E_ARGS outside, recorded for ipr_bounds_report); ipr_debug_cut_fold_extent(words)
+ * makes every later fold launch believe its packing-output buffer is `words` words shorter
+ * than it is, so that the fold's own index checks trip on allocated memory (0 restores). */
+int ipr_debug_check_extent(const void *d_ptr, uint64_t bytes);
+int ipr_debug_cut_fold_extent(int64_t words);
+
 /* Dataset generation on the GPU: DatasetGenerator::generate_record (src/dataset/generator.rs:
  * 171-193) for records first .. first + count - 1 of the dataset with `seed` and KEM
  * ML-KEM-`kem` (512, 768 or 1024).  Record i is id (32 bytes) || pk (800 / 1184 / 1568

@@ -23,7 +23,8 @@ __all__ = [
     "shard_plan", "merge_responses", "ShardedKeywordServer", "ntt_batch", "automorph_batch", "encode_db",
     "cuckoo_to_raw_db", "state_file_plan", "offline_precompute", "InspiringPacker",
     "DatasetGenerator", "Dataset", "DatasetRecord", "derive_public_key_id", "public_key_matches_id",
-    "build_cuckoo_table", "setup_keyword_server",
+    "build_cuckoo_table", "setup_keyword_server", "BOUNDS_CHECK", "bounds_checked_build", "bounds_report",
+    "debug_check_extent", "debug_cut_fold_extent",
 ]
 
 POLY_LEN = 2048
@@ -31,12 +32,15 @@ RESULT_BYTES = 12288
 STAGES = ("parse", "gemv", "pack", "post", "fold")
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB_PATH = os.path.join(_HERE, "libipr_b200.so")
+# IPR_B200_BOUNDS_CHECK=1 selects the bounds-checked debug build (`make -C inspire-rs_b200 debug`)
+BOUNDS_CHECK = os.environ.get("IPR_B200_BOUNDS_CHECK", "0") == "1"
+_LIB_NAME = "libipr_b200_dbg.so" if BOUNDS_CHECK else "libipr_b200.so"
+_LIB_PATH = os.path.join(_HERE, _LIB_NAME)
 
 if not os.path.exists(_LIB_PATH):
     raise ImportError(
-        f"libipr_b200.so not built at {_LIB_PATH}; run `make -C inspire-rs_b200` "
-        "(the respond() path has no CPU fallback)")
+        f"{_LIB_NAME} not built at {_LIB_PATH}; run `make -C inspire-rs_b200`"
+        + (" debug" if BOUNDS_CHECK else "") + " (the respond() path has no CPU fallback)")
 lib = ctypes.CDLL(_LIB_PATH)
 
 _u64, _i32, _sz = ctypes.c_uint64, ctypes.c_int, ctypes.c_size_t
@@ -124,6 +128,10 @@ _create_raw = _sig("ipr_server_create_from_raw", _i32, _i32, ctypes.POINTER(_Pla
 _encode = _sig("ipr_encode_db", _i32, _i32, _vp, _vp, _u64, _u64, _u64, _vp)
 _raw_db = _sig("ipr_cuckoo_to_raw_db", _i32, _i32, _vp, _vp, _u64, _u64, _u64, _u64, _u64, _vp, _vp)
 _wait_selftest = _sig("ipr_selftest_bounded_wait", _i32, _i32, ctypes.c_uint32)
+_bounds_build = _sig("ipr_bounds_checked_build", _i32)
+_bounds_report = _sig("ipr_bounds_report", _i32, ctypes.c_char_p, _sz)
+_dbg_extent = _sig("ipr_debug_check_extent", _i32, _vp, _u64)
+_dbg_cut = _sig("ipr_debug_cut_fold_extent", _i32, ctypes.c_int64)
 _offline = _sig("ipr_offline_precompute", _i32, _i32, _vp, _u64, _u64, _vp, _vp, _vp, _vp, _u64, _vp)
 _insp_create = _sig("ipr_inspiring_create", _i32, _i32, _i32, ctypes.POINTER(_vp))
 _insp_pack = _sig("ipr_inspiring_pack", _i32, _vp, _i32, _vp, _vp, _vp, _vp, _vp)
@@ -201,6 +209,31 @@ def fail_allocation_after(n: int):
     """test hook: the next n server device allocations succeed, the one after fails (IPR_E_OOM);
     n < 0 switches the hook off"""
     _check(_fail_alloc(n), "ipr_debug_fail_allocation")
+
+
+def bounds_checked_build() -> bool:
+    """ipr_bounds_checked_build: True for the bounds-checked debug library"""
+    return bool(_bounds_build())
+
+
+def bounds_report():
+    """ipr_bounds_report: (number of failed checks since the last report, their lines); the
+    debug build synchronises the current device first, the release build reports (0, "")"""
+    buf = ctypes.create_string_buffer(1 << 13)
+    n = _bounds_report(buf, len(buf))
+    return int(n), buf.value.decode()
+
+
+def debug_check_extent(d_ptr: int, nbytes: int) -> int:
+    """ipr_debug_check_extent (debug build): the launch-argument range check on
+    [d_ptr, d_ptr + nbytes); IPR_OK inside one allocation, IPR_E_ARGS outside"""
+    return int(_dbg_extent(d_ptr, nbytes))
+
+
+def debug_cut_fold_extent(words: int) -> int:
+    """ipr_debug_cut_fold_extent (debug build): later fold launches believe their packing
+    output buffer is `words` words shorter, so the fold's own index checks trip; 0 restores"""
+    return int(_dbg_cut(words))
 
 
 def selftest_bounded_wait(limit_us: int = 20_000, device: int = 0) -> int:

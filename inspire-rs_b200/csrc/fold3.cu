@@ -31,6 +31,7 @@
 #include <algorithm>
 #include <cstdint>
 
+#include "bounds.cuh"
 #include "ipr_device.cuh"
 #include "kernels.cuh"
 #include "ntt_regs.cuh"
@@ -298,7 +299,7 @@ struct NInv {
 __global__ void __launch_bounds__(256) k_fold_prep(uint32_t* __restrict__ S, int64_t count,
                                                    const uint64_t* __restrict__ zb, const uint64_t* __restrict__ bth,
                                                    int instances, NInv ni, uint32_t* __restrict__ gsw,
-                                                   int64_t gsw_words) {
+                                                   int64_t gsw_words, int64_t zb_words, int64_t bth_words) {
     // the queries' RGSW bodies [query][6 gadget rows][2 limbs][N], scaled by N^-1 in place for
     // the fold form that reads them straight from global memory
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < gsw_words / 4;
@@ -318,7 +319,8 @@ __global__ void __launch_bounds__(256) k_fold_prep(uint32_t* __restrict__ S, int
         uint4* s1 = reinterpret_cast<uint4*>(S + (f * 2 + 1) * N + z0);
         const uint4 a = *s0, b = *s1;
         uint64_t acc0[4] = {a.x, a.y, a.z, a.w}, acc1[4] = {b.x, b.y, b.z, b.w};
-        if (zb) {
+        if (zb && in_bounds((f / instances + 1) * T_EXP * N <= zb_words, kSitePrepZb) &&
+            in_bounds((f % instances + 1) * T_EXP * N <= bth_words, kSitePrepBth)) {
             const uint64_t* zc = zb + (f / instances) * T_EXP * N + z0;
             const uint64_t* th = bth + (f % instances) * T_EXP * N + z0;
 #pragma unroll
@@ -491,7 +493,8 @@ __global__ void __launch_bounds__(F4_THREADS, 2)
     k_fold4(const uint32_t* __restrict__ row0s, const uint32_t* __restrict__ gsw, const uint64_t* __restrict__ a_hat,
             const uint32_t* __restrict__ S, int64_t s_payload_stride, const uint64_t* __restrict__ cvec,
             const uint2* __restrict__ fwi, const uint2* __restrict__ iwi, int interp, int c_groups, int64_t db_cols,
-            int qpp, uint8_t* __restrict__ resp, int64_t resp_payload_stride, int64_t resp_query_stride) {
+            int qpp, uint8_t* __restrict__ resp, int64_t resp_payload_stride, int64_t resp_query_stride,
+            FoldExtents ext) {
     extern __shared__ uint4 f4_smem[];
     uint32_t* xbuf = reinterpret_cast<uint32_t*>(f4_smem);  // [F4_XB][N]
     uint64_t* sst = reinterpret_cast<uint64_t*>(xbuf + F4_XB * N);  // [row][m][t]: read back only by thread t
@@ -507,17 +510,27 @@ __global__ void __launch_bounds__(F4_THREADS, 2)
     const uint32_t* gq = gsw + (int64_t)qg * 12 * N;
     const int z8 = 8 * t;  // layout D: thread t's 8 consecutive words (eD(t, k) = 8 t + k)
     const uint64_t mask = (1ull << GADGET_BITS) - 1;
+    // the debug build's index checks (bounds.cuh); the release build keeps none of them
+    const int64_t s_off = (int64_t)payload * s_payload_stride, c_off = (int64_t)qg * db_cols;
+    auto s_ok = [&](int64_t row) { return in_bounds(s_off + (row + 1) * N <= ext.s_words, kSiteFoldS); };
+    auto ac_ok = [&](int j) {  // rows j of a_hat and of this query's c, every word this thread reads
+        const bool a = in_bounds(((int64_t)j + 1) * N <= ext.ahat_words, kSiteFoldAhat);
+        return in_bounds(c_off + ((int64_t)j + 1) * N <= ext.c_words, kSiteFoldC) && a;
+    };
 
     {  // first step: G^-1(0) = 0, so s = (a_hat[j], INTT(S[j]) + c[j]) mod q
         const int j = wp * interp + interp - 1;
-        uint32_t pr[2][EPT];
-        load_d8(pr[0], Sq + ((int64_t)j * 2) * N + z8);
-        load_d8(pr[1], Sq + ((int64_t)j * 2 + 1) * N + z8);
+        uint32_t pr[2][EPT] = {};
+        if (s_ok((int64_t)j * 2 + 1)) {
+            load_d8(pr[0], Sq + ((int64_t)j * 2) * N + z8);
+            load_d8(pr[1], Sq + ((int64_t)j * 2 + 1) * N + z8);
+        }
         uint64_t pc[EPT];
+        const bool acj = ac_ok(j);
 #pragma unroll
         for (int m = 0; m < EPT; m++) {
-            S_AT(0, m) = __ldg(a_hat + (int64_t)j * N + eA(t, m));
-            pc[m] = __ldg(cq + (int64_t)j * N + eA(t, m));
+            S_AT(0, m) = acj ? __ldg(a_hat + (int64_t)j * N + eA(t, m)) : 0;
+            pc[m] = acj ? __ldg(cq + (int64_t)j * N + eA(t, m)) : 0;
         }
         inverse_limbs<1, 2>(pr, t, xbuf, bar, iwi);
 #pragma unroll
@@ -540,6 +553,8 @@ __global__ void __launch_bounds__(F4_THREADS, 2)
                 nttr::group_bar(bar);
 #pragma unroll
                 for (int k = 0; k < 3; k++) {
+                    const int64_t row = (int64_t)qg * 12 + (r + 2 * k) * 2 + l;
+                    if (!in_bounds((row + 1) * N <= ext.gsw_words, kSiteFoldGsw)) continue;
                     const uint32_t* src = gq + (int64_t)((r + 2 * k) * 2 + l) * N + z8;
                     cp16(stg + k * N + z8, src);
                     cp16(stg + k * N + z8 + 4, src + 4);
@@ -547,9 +562,11 @@ __global__ void __launch_bounds__(F4_THREADS, 2)
                 if (r == 0) {
                     cp16(stg + 3 * N + z8, row0s + l * N + z8);
                     cp16(stg + 3 * N + z8 + 4, row0s + l * N + z8 + 4);
-                    const uint32_t* sp = Sq + ((int64_t)j * 2 + l) * N + z8;
-                    cp16(stg + 4 * N + z8, sp);
-                    cp16(stg + 4 * N + z8 + 4, sp + 4);
+                    if (s_ok((int64_t)j * 2 + l)) {
+                        const uint32_t* sp = Sq + ((int64_t)j * 2 + l) * N + z8;
+                        cp16(stg + 4 * N + z8, sp);
+                        cp16(stg + 4 * N + z8 + 4, sp + 4);
+                    }
                 }
                 cp_commit();
                 uint32_t v[3][EPT];
@@ -563,10 +580,12 @@ __global__ void __launch_bounds__(F4_THREADS, 2)
                 if (l == 1 && r == 1) {
                     // s is consumed (the team barriers of the transforms ordered every read of
                     // it): the packed row j lands in its slots while the inverse transforms run
+                    if (ac_ok(j)) {
 #pragma unroll
-                    for (int m = 0; m < EPT; m++) {
-                        cp8(&S_AT(0, m), a_hat + (int64_t)j * N + eA(t, m));
-                        cp8(&S_AT(1, m), cq + (int64_t)j * N + eA(t, m));
+                        for (int m = 0; m < EPT; m++) {
+                            cp8(&S_AT(0, m), a_hat + (int64_t)j * N + eA(t, m));
+                            cp8(&S_AT(1, m), cq + (int64_t)j * N + eA(t, m));
+                        }
                     }
                     cp_commit();
                     cp_wait<1>();
@@ -614,8 +633,9 @@ __global__ void __launch_bounds__(F4_THREADS, 2)
         }
     }
 
-    switch_keep(S_AT, t, resp + (int64_t)payload * resp_payload_stride + 8 + (int64_t)qin * resp_query_stride +
-                             (int64_t)wp * RESULT_BYTES);
+    const int64_t o = (int64_t)payload * resp_payload_stride + 8 + (int64_t)qin * resp_query_stride +
+                      (int64_t)wp * RESULT_BYTES;
+    if (in_bounds(o + RESULT_BYTES <= ext.resp_bytes, kSiteFoldResp)) switch_keep(S_AT, t, resp + o);
 }
 
 // RGSW bodies 96 KB + two team exchange buffers of 4 polynomials (2 x 32 KB) + the two
@@ -635,7 +655,16 @@ cudaError_t launch_fold_prep(uint32_t* S, int64_t count, const uint64_t* zb, con
     const int64_t n4 = count * (N / 4);
     const int64_t blocks = std::min<int64_t>((n4 + 255) / 256, (int64_t)sm_count * 8);
     const int64_t gsw_words = gsw ? (int64_t)gsw_queries * 12 * N : 0;
-    k_fold_prep<<<(unsigned)blocks, 256, 0, st>>>(S, count, zb, bth, instances, ni, gsw, gsw_words);
+    const int64_t zb_words = zb ? (count + instances - 1) / instances * T_EXP * N : 0;
+    const int64_t bth_words = zb ? (int64_t)instances * T_EXP * N : 0;
+    cudaError_t e;
+    if ((e = check_extent(S, (uint64_t)count * 2 * N * 4, "fold scaling: packing outputs")) != cudaSuccess ||
+        (e = check_extent(zb, (uint64_t)zb_words * 8, "fold scaling: z bodies")) != cudaSuccess ||
+        (e = check_extent(bth, (uint64_t)bth_words * 8, "fold scaling: condensed T-hat")) != cudaSuccess ||
+        (e = check_extent(gsw, (uint64_t)gsw_words * 4, "fold scaling: RGSW bodies")) != cudaSuccess)
+        return e;
+    k_fold_prep<<<(unsigned)blocks, 256, 0, st>>>(S, count, zb, bth, instances, ni, gsw, gsw_words, zb_words,
+                                                  bth_words);
     return cudaGetLastError();
 }
 
@@ -657,13 +686,24 @@ cudaError_t launch_fold3(const uint32_t* row0s, const uint32_t* gsw, const uint6
 cudaError_t launch_fold4(const uint32_t* row0s, const uint32_t* gsw_scaled, const uint64_t* a_hat, const uint32_t* S,
                          int64_t s_payload_stride, const uint64_t* cvec, const uint32_t* fwi, const uint32_t* iwi,
                          int interp, int c_groups, int num_queries, int64_t db_cols, int qpp, uint8_t* resp,
-                         int64_t resp_payload_stride, int64_t resp_query_stride, cudaStream_t st) {
+                         int64_t resp_payload_stride, int64_t resp_query_stride, const FoldExtents& ext,
+                         cudaStream_t st) {
     if (interp < 1 || c_groups < 1 || num_queries < 1 || num_queries > 65535 || qpp < 1) return cudaErrorInvalidValue;
+    cudaError_t e;
+    if ((e = check_extent(row0s, 2ull * N * 4, "fold: row 0")) != cudaSuccess ||
+        (e = check_extent(gsw_scaled, (uint64_t)ext.gsw_words * 4, "fold: RGSW bodies")) != cudaSuccess ||
+        (e = check_extent(a_hat, (uint64_t)ext.ahat_words * 8, "fold: a_hat")) != cudaSuccess ||
+        (e = check_extent(S, (uint64_t)ext.s_words * 4, "fold: packing outputs")) != cudaSuccess ||
+        (e = check_extent(cvec, (uint64_t)ext.c_words * 8, "fold: first-dimension outputs")) != cudaSuccess ||
+        (e = check_extent(fwi, 2ull * N * 8, "fold: forward twiddles")) != cudaSuccess ||
+        (e = check_extent(iwi, 2ull * N * 8, "fold: inverse twiddles")) != cudaSuccess ||
+        (e = check_extent(resp, (uint64_t)ext.resp_bytes, "fold: responses")) != cudaSuccess)
+        return e;
     dim3 grid(c_groups, num_queries);
     k_fold4<<<grid, F4_THREADS, F4_SMEM, st>>>(row0s, gsw_scaled, a_hat, S, s_payload_stride, cvec,
                                                 reinterpret_cast<const uint2*>(fwi), reinterpret_cast<const uint2*>(iwi),
                                                 interp, c_groups, db_cols, qpp, resp, resp_payload_stride,
-                                                resp_query_stride);
+                                                resp_query_stride, ext);
     return cudaGetLastError();
 }
 

@@ -24,6 +24,7 @@
 
 #include <cstdint>
 
+#include "bounds.cuh"
 #include "ipr_device.cuh"
 #include "kernels.cuh"
 #include "umma.cuh"
@@ -293,6 +294,8 @@ cudaError_t launch_gemm1(const CUtensorMap* tm_db, const CUtensorMap* tm_qb, int
                          int n_tiles, int num_queries, uint64_t* c, int* err_flag, int sm_count, cudaStream_t st) {
     if (nt < 16 || nt > 256 || (nt & 15) || (db_rows % TILE_K) || db_rows > 32768 || (db_cols % TILE_M))
         return cudaErrorInvalidValue;
+    cudaError_t e = check_extent(c, (uint64_t)num_queries * db_cols * 8, "first dimension: outputs");
+    if (e != cudaSuccess) return e;
     const int stages = gemm1_stages(nt);
     const int64_t total = (db_cols / TILE_M) * n_tiles;
     const int grid = (int)(total < sm_count ? total : sm_count);

@@ -15,6 +15,7 @@
 
 #include <cstdint>
 
+#include "bounds.cuh"
 #include "ipr_device.cuh"
 #include "kernels.cuh"
 #include "ntt_regs.cuh"
@@ -678,14 +679,42 @@ cudaError_t init_device_kernels() {
     return cudaFuncSetAttribute(k_fold_switch, cudaFuncAttributeMaxDynamicSharedMemorySize, 12 * N * 4);
 }
 
+namespace {
+// the byte ranges one parse launch reads and writes (the bounds-checked build checks them
+// against the allocations; the release build compiles the checks away)
+cudaError_t parse_extents(const uint8_t* qb, int npay, int64_t pstride, int nq, int db_rows, const uint64_t* y,
+                          const uint64_t* z, const uint32_t* a_il, const uint32_t* gsw, const uint8_t* qbytes,
+                          int qbase) {
+    const uint64_t fpp = 2ull * T_EXP * N + (uint64_t)nq * ((uint64_t)db_rows + 2ull * T_EXP * N);
+    const uint64_t keys = (uint64_t)npay * T_EXP * N * 8;
+    cudaError_t e;
+    if ((e = check_extent(qb, (uint64_t)(npay - 1) * pstride + 1 + 7 * fpp, "parse: payloads")) != cudaSuccess ||
+        (e = check_extent(y, keys, "parse: y bodies")) != cudaSuccess ||
+        (e = check_extent(z, keys, "parse: z bodies")) != cudaSuccess ||
+        (e = check_extent(gsw, (uint64_t)npay * nq * 12 * N * 4, "parse: RGSW bodies")) != cudaSuccess)
+        return e;
+    if (a_il && (e = check_extent(a_il, (uint64_t)(nq + 1) / 2 * db_rows * 4 * 4, "parse: GEMV operand")) != cudaSuccess)
+        return e;
+    if (qbytes &&
+        (e = check_extent(qbytes, ((uint64_t)qbase + (uint64_t)npay * nq) * 8 * db_rows, "parse: query byte rows")) !=
+            cudaSuccess)
+        return e;
+    return cudaSuccess;
+}
+}  // namespace
+
 cudaError_t launch_parse_query(const uint8_t* qb, int nq, int db_rows, uint64_t* y, uint64_t* z,
                                uint32_t* a_il, uint32_t* gsw, uint8_t* qbytes, int qbase, cudaStream_t st) {
+    cudaError_t e = parse_extents(qb, 1, 0, nq, db_rows, y, z, a_il, gsw, qbytes, qbase);
+    if (e != cudaSuccess) return e;
     k_parse_query<<<2 * 148, 256, 0, st>>>(qb, nq, db_rows, y, z, a_il, gsw, qbytes, qbase, 1, 0);
     return cudaGetLastError();
 }
 
 cudaError_t launch_parse_batch(const uint8_t* qb, int npay, int64_t pstride, int nq, int db_rows, uint64_t* y,
                                uint64_t* z, uint32_t* gsw, uint8_t* qbytes, cudaStream_t st) {
+    cudaError_t e = parse_extents(qb, npay, pstride, nq, db_rows, y, z, nullptr, gsw, qbytes, 0);
+    if (e != cudaSuccess) return e;
     k_parse_query<<<8 * 148, 256, 0, st>>>(qb, nq, db_rows, y, z, nullptr, gsw, qbytes, 0, npay, pstride);
     return cudaGetLastError();
 }
@@ -734,6 +763,11 @@ cudaError_t launch_fold_switch(const uint32_t* row0, const uint32_t* gsw, const 
 cudaError_t launch_response_frame(uint8_t* resp, int nq, int64_t per_query, const uint8_t* stash,
                                   int64_t stash_count, int64_t stash_entry, cudaStream_t st, int npay,
                                   int64_t pstride) {
+    const uint64_t frame = 4 + (uint64_t)nq * (4 + per_query) + 4 + (uint64_t)stash_count * (4 + stash_entry);
+    cudaError_t e;
+    if ((e = check_extent(resp, (uint64_t)(npay - 1) * pstride + frame, "frame: responses")) != cudaSuccess ||
+        (e = check_extent(stash, (uint64_t)stash_count * stash_entry, "frame: stash")) != cudaSuccess)
+        return e;
     k_response_frame<<<dim3(8, npay), 256, 0, st>>>(resp, nq, per_query, stash, stash_count, stash_entry, pstride);
     return cudaGetLastError();
 }

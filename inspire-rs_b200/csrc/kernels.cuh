@@ -98,9 +98,20 @@ cudaError_t launch_fold3(const uint32_t* row0s, const uint32_t* gsw, const uint6
                          const uint32_t ninv[4], int interp, int c_groups,
                          int num_queries, int64_t db_cols, int qpp, uint8_t* resp, int64_t resp_payload_stride,
                          int64_t resp_query_stride, cudaStream_t st);
+// The extents (in elements of each buffer's type, from its base pointer) of the buffers the
+// one-chain fold reads and writes: checked against the allocations before the launch and
+// against every index inside the kernel in the bounds-checked debug build (bounds.cuh).
+struct FoldExtents {
+    int64_t s_words;     // u32 packing outputs
+    int64_t gsw_words;   // u32 RGSW bodies, scaled by N^-1
+    int64_t ahat_words;  // u64 a_hat rows
+    int64_t c_words;     // u64 first-dimension outputs
+    int64_t resp_bytes;  // response bytes
+};
 cudaError_t launch_fold4(const uint32_t* row0s, const uint32_t* gsw_scaled, const uint64_t* a_hat, const uint32_t* S,
                          int64_t s_payload_stride, const uint64_t* cvec, const uint32_t* fwi, const uint32_t* iwi,
                          int interp, int c_groups, int num_queries, int64_t db_cols, int qpp, uint8_t* resp,
-                         int64_t resp_payload_stride, int64_t resp_query_stride, cudaStream_t st);
+                         int64_t resp_payload_stride, int64_t resp_query_stride, const FoldExtents& ext,
+                         cudaStream_t st);
 
 }  // namespace ipr

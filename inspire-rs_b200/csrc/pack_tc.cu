@@ -27,6 +27,7 @@
 
 #include <cstdint>
 
+#include "bounds.cuh"
 #include "ipr_device.cuh"
 #include "kernels.cuh"
 #include "umma.cuh"
@@ -614,6 +615,8 @@ cudaError_t launch_pack_mma_pair(const CUtensorMap* tm_t, const CUtensorMap* tm_
                                  int np, uint32_t* S, int* err_flag, int sm_count, cudaStream_t st) {
     const int nt = pack_mma_nt(clients);
     if (clients < 1 || clients > 64 || np < nt) return cudaErrorInvalidValue;
+    cudaError_t e = check_extent(S, (uint64_t)clients * instances * 2 * N * 4, "packing: outputs");
+    if (e != cudaSuccess) return e;
     const int mt_count = (instances + 31) / 32;
     const int grid = 2 * pack_pair_resident(nt, sm_count);
     k_pack_mma_pair<<<grid, Q_THREADS, pack_pair_smem(nt), st>>>(*tm_t, *tm_y_half, instances, mt_count, clients, np,
@@ -637,7 +640,11 @@ cudaError_t launch_relayout_tpp(const uint64_t* bt, const uint64_t* btb, uint8_t
 }
 
 cudaError_t launch_build_y8(const uint64_t* y_bodies, uint8_t* y8, int clients, int np, cudaStream_t st) {
-    cudaError_t e = cudaMemsetAsync(y8, 0, (size_t)2 * np * P_K, st);
+    cudaError_t e;
+    if ((e = check_extent(y_bodies, (uint64_t)clients * T_EXP * N * 8, "client operand: y bodies")) != cudaSuccess ||
+        (e = check_extent(y8, (uint64_t)2 * np * P_K, "client operand: byte rows")) != cudaSuccess)
+        return e;
+    e = cudaMemsetAsync(y8, 0, (size_t)2 * np * P_K, st);
     if (e != cudaSuccess) return e;
     k_build_y8<<<148 * 4, 256, 0, st>>>(y_bodies, y8, clients, np);
     return cudaGetLastError();
@@ -647,6 +654,8 @@ cudaError_t launch_pack_mma(const CUtensorMap* tm_t, const CUtensorMap* tm_y, in
                             uint32_t* S, int* err_flag, int sm_count, cudaStream_t st) {
     const int nt = pack_mma_nt(clients);
     if (clients < 1 || clients > 64 || np < nt) return cudaErrorInvalidValue;
+    cudaError_t e = check_extent(S, (uint64_t)clients * instances * 2 * N * 4, "packing: outputs");
+    if (e != cudaSuccess) return e;
     const int mt_count = (instances + 31) / 32;
     const int stages = pack_mma_stages(nt);
     k_pack_mma<<<sm_count, P_THREADS, pack_mma_smem(nt), st>>>(*tm_t, *tm_y, instances, mt_count, clients, np, nt,

@@ -20,6 +20,7 @@
 
 #include "host_math.hpp"
 #include "ipr_b200.h"
+#include "bounds.cuh"
 #include "kernels.cuh"
 #include "server_internal.hpp"
 
@@ -158,10 +159,15 @@ int enqueue(ipr_server* s, unsigned nq, const uint8_t* d_query, uint8_t* d_resp,
             CU(ipr::launch_fold_prep(s->d_S, (int64_t)p.instances, nullptr, nullptr, 1, s->hp.ninv, s->sm_count, st,
                                      chain ? s->d_gsw : nullptr, (int)nq));
             rec(4);
-            if (chain)
+            if (chain) {
+                ipr::FoldExtents ext{(int64_t)p.instances * 2 * kN, (int64_t)nq * 12 * kN,
+                                     (int64_t)p.instances * kN, (int64_t)nq * (int64_t)p.db_cols,
+                                     (int64_t)s->response_bytes(nq)};
+                if (ipr::kBoundsChecked) ext.s_words -= ipr::g_fold_extent_cut.load();
                 CU(ipr::launch_fold4(s->d_row0s, s->d_gsw, s->d_ahat, s->d_S, 0, s->d_c, s->d_fwi, s->d_iwi,
                                      (int)p.interp, (int)p.c, (int)nq, (int64_t)p.db_cols, (int)nq, d_resp, 0,
-                                     (int64_t)(4 + s->per_query_bytes()), st));
+                                     (int64_t)(4 + s->per_query_bytes()), ext, st));
+            }
             else
                 CU(ipr::launch_fold3(s->d_row0s, s->d_gsw, s->d_ahat, s->d_S, 0, s->d_c, s->d_fwi, s->d_iwi,
                                      s->hp.ninv, (int)p.interp, (int)p.c, (int)nq, (int64_t)p.db_cols, (int)nq, d_resp,
@@ -312,10 +318,14 @@ int enqueue_batch(ipr_server* s, int B, const uint8_t* d_queries, uint8_t* d_res
         CU(ipr::launch_fold_prep(s->d_bS, (int64_t)B * p.instances, s->d_zbs, s->d_bth, (int)p.instances, s->hp.ninv,
                                  s->sm_count, st, chain ? s->d_gsw : nullptr, nqt));
         rec(4);
-        if (chain)
+        if (chain) {
+            ipr::FoldExtents ext{(int64_t)B * (int64_t)p.instances * 2 * kN, (int64_t)nqt * 12 * kN,
+                                 (int64_t)p.instances * kN, (int64_t)nqt * (int64_t)p.db_cols, (int64_t)B * rb};
+            if (ipr::kBoundsChecked) ext.s_words -= ipr::g_fold_extent_cut.load();
             CU(ipr::launch_fold4(s->d_row0s, s->d_gsw, s->d_ahat, s->d_bS, (int64_t)(p.instances * 2 * kN), s->d_c,
                                  s->d_fwi, s->d_iwi, (int)p.interp, (int)p.c, nqt, (int64_t)p.db_cols, 2, d_resps, rb,
-                                 (int64_t)(4 + s->per_query_bytes()), st));
+                                 (int64_t)(4 + s->per_query_bytes()), ext, st));
+        }
         else
             CU(ipr::launch_fold3(s->d_row0s, s->d_gsw, s->d_ahat, s->d_bS, (int64_t)(p.instances * 2 * kN), s->d_c,
                                  s->d_fwi, s->d_iwi, s->hp.ninv, (int)p.interp, (int)p.c, nqt, (int64_t)p.db_cols, 2,

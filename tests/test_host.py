@@ -30,6 +30,25 @@ def test_library_exports_every_declared_symbol(pkg, header):
     assert not missing, missing
 
 
+@pytest.mark.parametrize("header", ["ipr_b200.h", "ipr_b200_compat.h"])
+def test_debug_library_exports_the_same_symbols_and_release_checks_nothing(pkg, header):
+    """the bounds-checked debug build exports every declared symbol too and says what it is;
+    in the release library the debug entry points refuse and the report is empty (no GPU)"""
+    dbg = os.path.join(os.path.dirname(pkg._LIB_PATH), "libipr_b200_dbg.so")
+    assert os.path.exists(dbg), "run make -C inspire-rs_b200 debug"
+    out = subprocess.run(["nm", "-D", "--defined-only", dbg], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (\S+)", out))
+    missing = [n for n in _declared(header) if n not in exported]
+    assert not missing, missing
+    d = ctypes.CDLL(dbg)
+    assert d.ipr_bounds_checked_build() == 1
+    if not pkg.BOUNDS_CHECK:
+        assert pkg.bounds_checked_build() is False
+        assert pkg.bounds_report() == (0, "")
+        assert pkg.debug_cut_fold_extent(2048) == -7  # IPR_E_STATE: not a bounds-checked build
+        assert pkg.debug_check_extent(0, 16) == -7
+
+
 @pytest.mark.gpu
 def test_library_is_sm100a(pkg):
     """the runtime reports the library's kernels as built for compute capability 10.0"""
