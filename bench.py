@@ -601,9 +601,10 @@ def main():
                     help="under torchrun: one database split by fold groups over the ranks (each rank answers its "
                          "groups of every payload; NCCL broadcast of the queries and gather of the parts) "
                          "instead of one replica per rank")
-    ap.add_argument("--fold-form", type=int, default=3, choices=[1, 2, 3],
-                    help="3: fold with the packing post-process fused in, one chain per CTA (default); 2: the "
-                         "same on two chains per CTA; 1: separate INTT + CRT pass")
+    ap.add_argument("--fold-form", type=int, default=3, choices=[1, 2, 3, 4, 5],
+                    help="3: fold with the packing post-process fused in, one chain per CTA, two or three CTAs "
+                         "per SM by chain count (default); 4 / 5: always three / two per SM; 2: the same on two "
+                         "chains per CTA; 1: separate INTT + CRT pass")
     ap.add_argument("--no-serving", action="store_true", help="skip the Poisson serving measurement")
     ap.add_argument("--serve-rates", type=float, nargs="*", default=[1000.0, 2500.0],
                     help="offered Poisson loads (payloads/s) for the serving measurement")

@@ -191,8 +191,10 @@ int ipr_server_set_profiling(ipr_server *srv, int on);
 #define IPR_OPT_TENSOR_GEMV 1
 /* IPR_OPT_FOLD_REGISTER_NTT: the form of the RGSW fold.  3 (default) = register-
  * resident NTTs with the packing post-process (INTT + CRT + b add) fused into the
- * fold's own inverse transforms, one chain per CTA and two CTAs per SM, the query's
- * RGSW bodies staged from global memory; 2 = the same fused fold on two chains of one
+ * fold's own inverse transforms, one chain per CTA, chosen per call between two CTAs
+ * per SM (the query's RGSW bodies staged through shared memory) and three per SM (the
+ * bodies read from L2 where they are used) by the rounds each needs for the call's
+ * chains; 4 = always three per SM; 5 = always two per SM; 2 = the same fused fold on two chains of one
  * query per CTA sharing the bodies in shared memory (an odd fold-group count leaves
  * half a CTA idle); 1 = register-resident NTTs after a separate INTT + CRT pass;
  * 0 = shared-memory NTTs after that pass (single-payload calls only; batches then

@@ -488,8 +488,12 @@ __global__ void __launch_bounds__(F3_THREADS, 1)
 constexpr int F4_THREADS = nttr::EPT * 32;  // 256: one chain, 8 coefficients per thread
 constexpr int F4_XB = 3;
 constexpr int F4_SMEM = F4_XB * N * 4 + 2 * N * 8 + 5 * N * 4;
+// without the staging area (STAGE false: bodies, packing output and row 0 read straight from
+// global memory where they are used) a CTA needs 56 KB and three fit on an SM
+constexpr int F4_SMEM_UNSTAGED = F4_XB * N * 4 + 2 * N * 8;
 
-__global__ void __launch_bounds__(F4_THREADS, 2)
+template <bool STAGE>
+__global__ void __launch_bounds__(F4_THREADS, STAGE ? 2 : 3)
     k_fold4(const uint32_t* __restrict__ row0s, const uint32_t* __restrict__ gsw, const uint64_t* __restrict__ a_hat,
             const uint32_t* __restrict__ S, int64_t s_payload_stride, const uint64_t* __restrict__ cvec,
             const uint2* __restrict__ fwi, const uint2* __restrict__ iwi, int interp, int c_groups, int64_t db_cols,
@@ -549,26 +553,28 @@ __global__ void __launch_bounds__(F4_THREADS, 2)
             for (int m = 0; m < EPT; m++) acc0[m] = 0;
 #pragma unroll 1
             for (int r = 0; r < 2; r++) {  // gadget rows p = r + 2k hold digit k of row r (gadget.rs:44-58)
-                // every thread's reads of the staging area (the previous batch) are done
-                nttr::group_bar(bar);
+                if constexpr (STAGE) {
+                    // every thread's reads of the staging area (the previous batch) are done
+                    nttr::group_bar(bar);
 #pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    const int64_t row = (int64_t)qg * 12 + (r + 2 * k) * 2 + l;
-                    if (!in_bounds((row + 1) * N <= ext.gsw_words, kSiteFoldGsw)) continue;
-                    const uint32_t* src = gq + (int64_t)((r + 2 * k) * 2 + l) * N + z8;
-                    cp16(stg + k * N + z8, src);
-                    cp16(stg + k * N + z8 + 4, src + 4);
-                }
-                if (r == 0) {
-                    cp16(stg + 3 * N + z8, row0s + l * N + z8);
-                    cp16(stg + 3 * N + z8 + 4, row0s + l * N + z8 + 4);
-                    if (s_ok((int64_t)j * 2 + l)) {
-                        const uint32_t* sp = Sq + ((int64_t)j * 2 + l) * N + z8;
-                        cp16(stg + 4 * N + z8, sp);
-                        cp16(stg + 4 * N + z8 + 4, sp + 4);
+                    for (int k = 0; k < 3; k++) {
+                        const int64_t row = (int64_t)qg * 12 + (r + 2 * k) * 2 + l;
+                        if (!in_bounds((row + 1) * N <= ext.gsw_words, kSiteFoldGsw)) continue;
+                        const uint32_t* src = gq + (int64_t)((r + 2 * k) * 2 + l) * N + z8;
+                        cp16(stg + k * N + z8, src);
+                        cp16(stg + k * N + z8 + 4, src + 4);
                     }
+                    if (r == 0) {
+                        cp16(stg + 3 * N + z8, row0s + l * N + z8);
+                        cp16(stg + 3 * N + z8 + 4, row0s + l * N + z8 + 4);
+                        if (s_ok((int64_t)j * 2 + l)) {
+                            const uint32_t* sp = Sq + ((int64_t)j * 2 + l) * N + z8;
+                            cp16(stg + 4 * N + z8, sp);
+                            cp16(stg + 4 * N + z8 + 4, sp + 4);
+                        }
+                    }
+                    cp_commit();
                 }
-                cp_commit();
                 uint32_t v[3][EPT];
 #pragma unroll
                 for (int m = 0; m < EPT; m++) {
@@ -588,23 +594,40 @@ __global__ void __launch_bounds__(F4_THREADS, 2)
                         }
                     }
                     cp_commit();
-                    cp_wait<1>();
-                } else {
+                    if constexpr (STAGE) cp_wait<1>();
+                } else if constexpr (STAGE) {
                     cp_wait<0>();
                 }
                 if (r == 0) {
-                    const uint4 a = *reinterpret_cast<const uint4*>(stg + 4 * N + z8);
-                    const uint4 b = *reinterpret_cast<const uint4*>(stg + 4 * N + z8 + 4);
-                    acc1[0] = a.x; acc1[1] = a.y; acc1[2] = a.z; acc1[3] = a.w;
-                    acc1[4] = b.x; acc1[5] = b.y; acc1[6] = b.z; acc1[7] = b.w;
+                    if constexpr (STAGE) {
+                        const uint4 a = *reinterpret_cast<const uint4*>(stg + 4 * N + z8);
+                        const uint4 b = *reinterpret_cast<const uint4*>(stg + 4 * N + z8 + 4);
+                        acc1[0] = a.x; acc1[1] = a.y; acc1[2] = a.z; acc1[3] = a.w;
+                        acc1[4] = b.x; acc1[5] = b.y; acc1[6] = b.z; acc1[7] = b.w;
+                    } else {
+#pragma unroll
+                        for (int m = 0; m < EPT; m++) acc1[m] = 0;
+                        if (s_ok((int64_t)j * 2 + l)) load_d8(acc1, Sq + ((int64_t)j * 2 + l) * N + z8);
+                    }
                 }
                 uint64_t part[EPT];
 #pragma unroll
                 for (int m = 0; m < EPT; m++) part[m] = acc1[m];
 #pragma unroll
                 for (int k = 0; k < 3; k++) {
-                    const uint4 b0 = *reinterpret_cast<const uint4*>(stg + k * N + z8);
-                    const uint4 b1 = *reinterpret_cast<const uint4*>(stg + k * N + z8 + 4);
+                    uint4 b0, b1;
+                    if constexpr (STAGE) {
+                        b0 = *reinterpret_cast<const uint4*>(stg + k * N + z8);
+                        b1 = *reinterpret_cast<const uint4*>(stg + k * N + z8 + 4);
+                    } else {
+                        const int64_t row = (int64_t)qg * 12 + (r + 2 * k) * 2 + l;
+                        b0 = b1 = make_uint4(0, 0, 0, 0);
+                        if (in_bounds((row + 1) * N <= ext.gsw_words, kSiteFoldGsw)) {
+                            const uint4* src = reinterpret_cast<const uint4*>(gq + (int64_t)((r + 2 * k) * 2 + l) * N + z8);
+                            b0 = __ldg(src);
+                            b1 = __ldg(src + 1);
+                        }
+                    }
                     const uint32_t bv[EPT] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
 #pragma unroll
                     for (int m = 0; m < EPT; m++) {
@@ -615,9 +638,15 @@ __global__ void __launch_bounds__(F4_THREADS, 2)
 #pragma unroll
                 for (int m = 0; m < EPT; m++) acc1[m] = mod64(part[m], q, br);
             }
-            const uint4 ra = *reinterpret_cast<const uint4*>(stg + 3 * N + z8);
-            const uint4 rb = *reinterpret_cast<const uint4*>(stg + 3 * N + z8 + 4);
-            const uint32_t r0[EPT] = {ra.x, ra.y, ra.z, ra.w, rb.x, rb.y, rb.z, rb.w};
+            uint32_t r0[EPT];
+            if constexpr (STAGE) {
+                const uint4 ra = *reinterpret_cast<const uint4*>(stg + 3 * N + z8);
+                const uint4 rb = *reinterpret_cast<const uint4*>(stg + 3 * N + z8 + 4);
+                r0[0] = ra.x; r0[1] = ra.y; r0[2] = ra.z; r0[3] = ra.w;
+                r0[4] = rb.x; r0[5] = rb.y; r0[6] = rb.z; r0[7] = rb.w;
+            } else {
+                load_d8(r0, row0s + l * N + z8);
+            }
 #pragma unroll
             for (int m = 0; m < EPT; m++) {
                 pr[2 * l][m] = mod64((uint64_t)r0[m] * acc0[m], q, br);
@@ -645,7 +674,9 @@ constexpr int FOLD3_SMEM = (12 + 2 * XP) * N * 4 + 2 * 2 * N * 8;
 cudaError_t init_fold3_kernel() {
     cudaError_t e = cudaFuncSetAttribute(k_fold3, cudaFuncAttributeMaxDynamicSharedMemorySize, FOLD3_SMEM);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_fold4, cudaFuncAttributeMaxDynamicSharedMemorySize, F4_SMEM);
+    if ((e = cudaFuncSetAttribute(k_fold4<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, F4_SMEM)) != cudaSuccess)
+        return e;
+    return cudaFuncSetAttribute(k_fold4<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, F4_SMEM_UNSTAGED);
 }
 
 cudaError_t launch_fold_prep(uint32_t* S, int64_t count, const uint64_t* zb, const uint64_t* bth, int instances,
@@ -687,7 +718,7 @@ cudaError_t launch_fold4(const uint32_t* row0s, const uint32_t* gsw_scaled, cons
                          int64_t s_payload_stride, const uint64_t* cvec, const uint32_t* fwi, const uint32_t* iwi,
                          int interp, int c_groups, int num_queries, int64_t db_cols, int qpp, uint8_t* resp,
                          int64_t resp_payload_stride, int64_t resp_query_stride, const FoldExtents& ext,
-                         cudaStream_t st) {
+                         cudaStream_t st, bool staged) {
     if (interp < 1 || c_groups < 1 || num_queries < 1 || num_queries > 65535 || qpp < 1) return cudaErrorInvalidValue;
     cudaError_t e;
     if ((e = check_extent(row0s, 2ull * N * 4, "fold: row 0")) != cudaSuccess ||
@@ -700,10 +731,16 @@ cudaError_t launch_fold4(const uint32_t* row0s, const uint32_t* gsw_scaled, cons
         (e = check_extent(resp, (uint64_t)ext.resp_bytes, "fold: responses")) != cudaSuccess)
         return e;
     dim3 grid(c_groups, num_queries);
-    k_fold4<<<grid, F4_THREADS, F4_SMEM, st>>>(row0s, gsw_scaled, a_hat, S, s_payload_stride, cvec,
-                                                reinterpret_cast<const uint2*>(fwi), reinterpret_cast<const uint2*>(iwi),
-                                                interp, c_groups, db_cols, qpp, resp, resp_payload_stride,
-                                                resp_query_stride, ext);
+    if (staged)
+        k_fold4<true><<<grid, F4_THREADS, F4_SMEM, st>>>(
+            row0s, gsw_scaled, a_hat, S, s_payload_stride, cvec, reinterpret_cast<const uint2*>(fwi),
+            reinterpret_cast<const uint2*>(iwi), interp, c_groups, db_cols, qpp, resp, resp_payload_stride,
+            resp_query_stride, ext);
+    else
+        k_fold4<false><<<grid, F4_THREADS, F4_SMEM_UNSTAGED, st>>>(
+            row0s, gsw_scaled, a_hat, S, s_payload_stride, cvec, reinterpret_cast<const uint2*>(fwi),
+            reinterpret_cast<const uint2*>(iwi), interp, c_groups, db_cols, qpp, resp, resp_payload_stride,
+            resp_query_stride, ext);
     return cudaGetLastError();
 }
 

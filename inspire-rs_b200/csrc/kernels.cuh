@@ -112,6 +112,6 @@ cudaError_t launch_fold4(const uint32_t* row0s, const uint32_t* gsw_scaled, cons
                          int64_t s_payload_stride, const uint64_t* cvec, const uint32_t* fwi, const uint32_t* iwi,
                          int interp, int c_groups, int num_queries, int64_t db_cols, int qpp, uint8_t* resp,
                          int64_t resp_payload_stride, int64_t resp_query_stride, const FoldExtents& ext,
-                         cudaStream_t st);
+                         cudaStream_t st, bool staged = true);
 
 }  // namespace ipr

@@ -124,6 +124,20 @@ int ensure_scratch(ipr_server* s, unsigned nq) {
     return IPR_OK;
 }
 
+// The one-chain fold's occupancy for `chains` chains: two CTAs per SM staging the RGSW bodies
+// in shared memory, or three per SM reading them from L2 (more warps to hide latency, 80
+// registers).  Chains run in rounds of (CTAs per SM x SMs); a round of three per SM takes
+// about 1.22x as long as one of two per SM (measured at the 1M shape), so the three-per-SM
+// form wins where it needs fewer rounds in proportion, e.g. 1,408 chains (64 payloads) on
+// 148 SMs: 4 rounds x 1.22 against 5 rounds.  Forms 4 / 5 force one occupancy.
+bool fold_staged(const ipr_server* s, int chains) {
+    if (s->fold_mode == 4) return false;
+    if (s->fold_mode == 5) return true;
+    const int sm = s->sm_count > 0 ? s->sm_count : 1;
+    const int64_t r2 = (chains + 2 * sm - 1) / (2 * sm), r3 = (chains + 3 * sm - 1) / (3 * sm);
+    return r3 * 122 >= r2 * 100;
+}
+
 // enqueue the device pipeline for one payload; `prof` = event slot base or -1
 int enqueue(ipr_server* s, unsigned nq, const uint8_t* d_query, uint8_t* d_resp, int prof) {
     cudaStream_t st = s->stream;
@@ -155,7 +169,7 @@ int enqueue(ipr_server* s, unsigned nq, const uint8_t* d_query, uint8_t* d_resp,
         CU(ipr::launch_pack(s->d_bt, s->d_btb, s->d_bth, s->d_y, s->d_z, s->d_S, (int)p.instances, st));
         rec(3);
         if (s->fold_mode >= 2) {
-            const bool chain = s->fold_mode == 3;
+            const bool chain = s->fold_mode >= 3;
             CU(ipr::launch_fold_prep(s->d_S, (int64_t)p.instances, nullptr, nullptr, 1, s->hp.ninv, s->sm_count, st,
                                      chain ? s->d_gsw : nullptr, (int)nq));
             rec(4);
@@ -166,7 +180,8 @@ int enqueue(ipr_server* s, unsigned nq, const uint8_t* d_query, uint8_t* d_resp,
                 if (ipr::kBoundsChecked) ext.s_words -= ipr::g_fold_extent_cut.load();
                 CU(ipr::launch_fold4(s->d_row0s, s->d_gsw, s->d_ahat, s->d_S, 0, s->d_c, s->d_fwi, s->d_iwi,
                                      (int)p.interp, (int)p.c, (int)nq, (int64_t)p.db_cols, (int)nq, d_resp, 0,
-                                     (int64_t)(4 + s->per_query_bytes()), ext, st));
+                                     (int64_t)(4 + s->per_query_bytes()), ext, st,
+                                     fold_staged(s, (int)(nq * p.c))));
             }
             else
                 CU(ipr::launch_fold3(s->d_row0s, s->d_gsw, s->d_ahat, s->d_S, 0, s->d_c, s->d_fwi, s->d_iwi,
@@ -314,7 +329,7 @@ int enqueue_batch(ipr_server* s, int B, const uint8_t* d_queries, uint8_t* d_res
     }
     rec(3);
     if (s->fold_mode >= 2) {
-        const bool chain = s->fold_mode == 3;
+        const bool chain = s->fold_mode >= 3;
         CU(ipr::launch_fold_prep(s->d_bS, (int64_t)B * p.instances, s->d_zbs, s->d_bth, (int)p.instances, s->hp.ninv,
                                  s->sm_count, st, chain ? s->d_gsw : nullptr, nqt));
         rec(4);
@@ -324,7 +339,7 @@ int enqueue_batch(ipr_server* s, int B, const uint8_t* d_queries, uint8_t* d_res
             if (ipr::kBoundsChecked) ext.s_words -= ipr::g_fold_extent_cut.load();
             CU(ipr::launch_fold4(s->d_row0s, s->d_gsw, s->d_ahat, s->d_bS, (int64_t)(p.instances * 2 * kN), s->d_c,
                                  s->d_fwi, s->d_iwi, (int)p.interp, (int)p.c, nqt, (int64_t)p.db_cols, 2, d_resps, rb,
-                                 (int64_t)(4 + s->per_query_bytes()), ext, st));
+                                 (int64_t)(4 + s->per_query_bytes()), ext, st, fold_staged(s, (int)(nqt * p.c))));
         }
         else
             CU(ipr::launch_fold3(s->d_row0s, s->d_gsw, s->d_ahat, s->d_bS, (int64_t)(p.instances * 2 * kN), s->d_c,
@@ -1076,7 +1091,7 @@ int ipr_server_set_option(ipr_server* s, int option, int64_t value) {
             destroy_graphs(s);
             return IPR_OK;
         case IPR_OPT_FOLD_REGISTER_NTT: {
-            if (value < 0 || value > 3) return fail(IPR_E_ARGS, "IPR_OPT_FOLD_REGISTER_NTT takes 0 to 3");
+            if (value < 0 || value > 5) return fail(IPR_E_ARGS, "IPR_OPT_FOLD_REGISTER_NTT takes 0 to 5");
             const bool had_r = s->fold_mode < 2;
             s->fold_mode = (int)value;
             destroy_graphs(s);

@@ -43,7 +43,8 @@ struct ipr_server {
     uint8_t* d_db8 = nullptr;  // [2][db_cols][db_rows] byte planes for the tensor-core GEMM
     CUtensorMap tm_db;
     bool gemv_tc = false;      // first dimension on tcgen05 (db_rows <= 32768)
-    int fold_mode = 3;         // 3 fused fold, one chain per CTA (k_fold_prep + k_fold4), 2 fused fold
+    int fold_mode = 3;         // 3 fused fold, one chain per CTA (k_fold_prep + k_fold4), two or three
+                               // CTAs per SM by chain count (4: three, 5: two), 2 fused fold
                                // on two chains per CTA (k_fold_prep + k_fold3), 1 k_intt_crt + k_fold2,
                                // 0 smem fold
     int pack_pair = 2;         // batch packing GEMM on CTA pairs: 0 never, 1 always, 2 from 48 payloads up

@@ -89,7 +89,7 @@ def test_first_dimension_paths(cfg0, pkg, orc, tensor, nq):
         srv.set_option(pkg.KeywordServer.OPT_TENSOR_GEMV, 1)
 
 
-@pytest.mark.parametrize("regs", [0, 1, 2, 3])
+@pytest.mark.parametrize("regs", [0, 1, 2, 3, 4, 5])
 @pytest.mark.parametrize("instances,interp", [(8, 8), (8, 1), (6, 2)])
 def test_fold_kernels(pkg, orc, regs, instances, interp):
     """the four fold forms (shared-memory NTTs, register NTTs after a separate INTT + CRT
@@ -300,7 +300,7 @@ def test_respond_batch_other_shapes(pkg, orc, instances, interp):
             assert g == orc.respond(sdb, q)
 
 
-@pytest.mark.parametrize("form", [1, 2, 3])
+@pytest.mark.parametrize("form", [1, 2, 3, 4, 5])
 def test_respond_batch_fold_forms(pkg, orc, form):
     """the batch path's fold forms give the oracle's bytes at an odd fold-group count (40 / 8 = 5)
     with 9 payloads = 18 queries, 90 chains"""
