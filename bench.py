@@ -836,7 +836,9 @@ def main():
         srv.set_option(pkg.KeywordServer.OPT_TENSOR_GEMV, 0)
         gemv_bytes = 2 * plan.db_rows * plan.db_cols
         forms = {0: "8 columns per warp, registers", 1: "4 columns per warp, registers",
-                 2: "2 columns per warp, registers", 3: "8 columns per warp, cp.async ring in shared memory"}
+                 2: "2 columns per warp, registers", 3: "8 columns per warp, cp.async ring in shared memory",
+                 4: "8 columns per warp, exact products on the FP64 pipe",
+                 5: "8 columns per warp, cp.async ring, FP64 pipe, residues converted once into shared memory"}
         for form, name in forms.items():
             srv.set_option(pkg.KeywordServer.OPT_GEMV_FORM, form)
             rate = single_rate()

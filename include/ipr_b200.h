@@ -210,9 +210,14 @@ int ipr_server_set_profiling(ipr_server *srv, int on);
  * two accumulators of a tile are double-buffered in TMEM. */
 #define IPR_OPT_GEMV_TILE 4
 /* IPR_OPT_GEMV_FORM: form of the CUDA-core first-dimension GEMV (IPR_OPT_TENSOR_GEMV 0)
- * for two queries: 0 (default) / 1 / 2 = 8 / 4 / 2 DB columns per warp loaded into
+ * for two queries: 0 / 1 / 2 = 8 / 4 / 2 DB columns per warp loaded into
  * registers (fewer columns, fewer partial sums per thread, more warps per SM); 3 = 8 columns
- * per warp streamed through a 4-stage shared-memory ring by cp.async.  Identical results. */
+ * per warp streamed through a 4-stage shared-memory ring by cp.async; 4 = form 0 with the
+ * products on the FP64 pipe (exact: every partial sum is an integer below 2^53); 5 (default)
+ * = form 3's shared-memory ring with the products on the FP64 pipe, the query residues
+ * converted to doubles once per CTA and the DB entries turned into doubles by integer
+ * operations (up to 4,096 DB rows; above, form 4).  Forms 4 and 5 run as form 0 above
+ * 16,384 DB rows.  Identical results. */
 #define IPR_OPT_GEMV_FORM 5
 int ipr_server_set_option(ipr_server *srv, int option, int64_t value);
 

@@ -115,11 +115,23 @@ __global__ void k_parse_query(const uint8_t* __restrict__ qb_all, int nq, int db
 // warp mean fewer accumulators, so more warps fit on an SM (MINB CTAs of 256) to
 // keep loads in flight.
 // ---------------------------------------------------------------------------
-template <int NQ, int COLS, int MINB = 1>
+//
+// FP selects the pipe of the products: 0 = u64 integer multiply-adds (IMAD.WIDE), 1 = the
+// FP64 pipe (fused multiply-adds of doubles).  The FP64 products
+// are exact integer arithmetic: a DB entry (< 2^16) and a residue (< 2^28) are converted
+// exactly (2^52 + x, less 2^52), each product is below 2^44 and a lane sums db_rows / 32 of
+// them, below 2^53 while db_rows <= 16384, so every partial sum is an exactly represented
+// integer, converted exactly to u64 before the cross-lane reduction.
+__device__ __forceinline__ double exact_dbl(uint32_t x) {  // x as a double, exactly, on the FP64 pipe
+    return __hiloint2double(0x43300000, (int)x) - 4503599627370496.0;
+}
+
+template <int NQ, int COLS, int MINB = 1, int FP = 0>
 __global__ void __launch_bounds__(256, MINB) k_gemv(const uint16_t* __restrict__ db, int db_rows,
                                                     int64_t db_cols, const uint32_t* __restrict__ a_il,
                                                     uint64_t* __restrict__ c) {
     constexpr int NV = COLS * NQ * 2;  // values reduced per warp task
+    auto on_fp = [](int) { return FP == 1; };
     static_assert(NV == 8 || NV == 16 || NV == 32, "8, 16 or 32 values per lane");
     const int lane = threadIdx.x & 31;
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
@@ -129,8 +141,12 @@ __global__ void __launch_bounds__(256, MINB) k_gemv(const uint16_t* __restrict__
     for (int64_t task = warp; task < ntasks; task += nwarps) {
         const int64_t col0 = task * COLS;
         uint64_t acc[NV];
+        double accd[NV];
 #pragma unroll
-        for (int v = 0; v < NV; v++) acc[v] = 0;
+        for (int v = 0; v < NV; v++) {
+            acc[v] = 0;
+            accd[v] = 0.0;
+        }
         for (int it = 0; it < stripes; it++) {
             const int k0 = it * 256 + lane * 8;
             uint4 d[COLS];
@@ -152,15 +168,26 @@ __global__ void __launch_bounds__(256, MINB) k_gemv(const uint16_t* __restrict__
                     uint2 t = __ldg(reinterpret_cast<const uint2*>(a_il) + (k0 + kk));
                     av[0] = t.x; av[1] = t.y;
                 }
+                double ad[NQ * 2];
+#pragma unroll
+                for (int v = 0; v < NQ * 2; v++) ad[v] = on_fp(v) ? exact_dbl(av[v]) : 0.0;
 #pragma unroll
                 for (int cc = 0; cc < COLS; cc++) {
                     const uint32_t w = (&d[cc].x)[kk >> 1];
                     const uint32_t dv = (kk & 1) ? (w >> 16) : (w & 0xffffu);
+                    const double dd = FP ? exact_dbl(dv) : 0.0;
 #pragma unroll
-                    for (int v = 0; v < NQ * 2; v++)
-                        acc[cc * NQ * 2 + v] += (uint64_t)av[v] * dv;
+                    for (int v = 0; v < NQ * 2; v++) {
+                        if (on_fp(v)) accd[cc * NQ * 2 + v] = fma(ad[v], dd, accd[cc * NQ * 2 + v]);
+                        else acc[cc * NQ * 2 + v] += (uint64_t)av[v] * dv;
+                    }
                 }
             }
+        }
+        if (FP) {  // exact integers below 2^53 (see above)
+#pragma unroll
+            for (int v = 0; v < NV; v++)
+                if (on_fp(v % (NQ * 2))) acc[v] = (uint64_t)__double2ull_rn(accd[v]);
         }
         // fold lane groups down to NV lanes, then transpose-reduce: lane v (< NV) ends with the
         // warp-wide sum of value v (lanes v + NV, v + 2 NV, ... hold copies)
@@ -188,6 +215,8 @@ __global__ void __launch_bounds__(256, MINB) k_gemv(const uint16_t* __restrict__
         }
     }
 }
+
+constexpr int GF_MAX_ROWS = 4096;  // rows of query residues the FP64 staged form converts into shared memory
 
 // The two-query GEMV with each warp's DB stripes staged through shared memory: a warp owns 8
 // consecutive columns per task (as k_gemv<2, 8>) and streams its (task, stripe) sequence
@@ -279,6 +308,112 @@ __global__ void __launch_bounds__(GS_WARPS * 32, 1)
 }
 constexpr int GS_STAGES = 4;
 constexpr int GS_SMEM = GS_WARPS * GS_STAGES * GS_COLS * 32 * 16;  // 128 KB
+
+// k_gemv_staged with the products on the FP64 pipe.  The ring of DB stripes in shared memory
+// as above is followed by the query residues, converted to doubles once per CTA
+// ([stripe][kk][lane][4]: value v of row k = 256 stripe + 8 lane + kk, so that a warp's 32
+// lanes read 32 consecutive 32-byte groups, no bank conflicts; db_rows <= GF_MAX_ROWS).  Each
+// DB entry becomes the double 2^16 + d by integer operations alone (its 16 bits placed in the
+// mantissa under the exponent of 2^16), so a product is one fused multiply-add.  The offset
+// adds 2^16 x (sum of the lane's residues) to each partial sum; every thread computes that
+// sum once, exactly, and takes it off after the conversion to u64.  Bounds: a product is
+// below 2^28 x 2^17 = 2^45 and a lane sums db_rows / 32 <= 128 of them, below 2^53, so every
+// partial sum is an exact integer.
+template <int STAGES>
+__global__ void __launch_bounds__(GS_WARPS * 32, 1)
+    k_gemv_staged_f64(const uint16_t* __restrict__ db, int db_rows, int64_t db_cols,
+                      const uint32_t* __restrict__ a_il, uint64_t* __restrict__ c) {
+    constexpr int NV = GS_COLS * 4;  // 32 values per lane
+    extern __shared__ uint4 gs_ring[];  // [warp][stage][column][lane], then the residues
+    double* gf_a = reinterpret_cast<double*>(gs_ring + GS_WARPS * STAGES * GS_COLS * 32);
+    for (int i = threadIdx.x; i < db_rows * 4; i += blockDim.x) {
+        const int k = i >> 2, v = i & 3;
+        gf_a[(((k >> 8) * 8 + (k & 7)) * 32 + ((k >> 3) & 31)) * 4 + v] = (double)__ldg(a_il + i);
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    uint4* ring = gs_ring + (threadIdx.x >> 5) * STAGES * GS_COLS * 32;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t ntasks = db_cols / GS_COLS;
+    const int stripes = db_rows >> 8;
+    uint64_t asum[4] = {0, 0, 0, 0};
+    for (int it = 0; it < stripes; it++)
+#pragma unroll
+        for (int kk = 0; kk < 8; kk++) {
+            const uint4 t = __ldg(reinterpret_cast<const uint4*>(a_il) + (it * 256 + lane * 8 + kk));
+            asum[0] += t.x; asum[1] += t.y; asum[2] += t.z; asum[3] += t.w;
+        }
+    const int64_t my_tasks = warp < ntasks ? (ntasks - 1 - warp) / nwarps + 1 : 0;
+    const int64_t items = my_tasks * stripes;
+    auto issue = [&](int64_t u) {
+        if (u < items) {
+            const int64_t col0 = (warp + (u / stripes) * nwarps) * GS_COLS;
+            const int k0 = (int)(u % stripes) * 256 + lane * 8;
+            uint4* dst = ring + (int)(u % STAGES) * GS_COLS * 32 + lane;
+#pragma unroll
+            for (int cc = 0; cc < GS_COLS; cc++) gs_cp16(dst + cc * 32, db + (col0 + cc) * (int64_t)db_rows + k0);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+#pragma unroll
+    for (int u = 0; u < STAGES - 1; u++) issue(u);
+    double accd[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) accd[v] = 0.0;
+    for (int64_t u = 0; u < items; u++) {
+        asm volatile("cp.async.wait_group %0;" ::"n"(STAGES - 2) : "memory");
+        const uint4* src = ring + (int)(u % STAGES) * GS_COLS * 32 + lane;
+        uint4 d[GS_COLS];
+#pragma unroll
+        for (int cc = 0; cc < GS_COLS; cc++) d[cc] = src[cc * 32];
+        issue(u + STAGES - 1);
+        const int it = (int)(u % stripes);
+#pragma unroll
+        for (int kk = 0; kk < 8; kk++) {
+            const double* ar = gf_a + ((it * 8 + kk) * 32 + lane) * 4;
+            const double2 a01 = *reinterpret_cast<const double2*>(ar);
+            const double2 a23 = *reinterpret_cast<const double2*>(ar + 2);
+            const double ad[4] = {a01.x, a01.y, a23.x, a23.y};
+#pragma unroll
+            for (int cc = 0; cc < GS_COLS; cc++) {
+                const uint32_t w = (&d[cc].x)[kk >> 1];
+                const uint32_t m = (kk & 1) ? ((w >> 12) & 0xffff0u) : ((w << 4) & 0xffff0u);
+                const double dd = __hiloint2double((int)(0x40f00000u | m), 0);
+#pragma unroll
+                for (int v = 0; v < 4; v++) accd[cc * 4 + v] = fma(ad[v], dd, accd[cc * 4 + v]);
+            }
+        }
+        if (it == stripes - 1) {
+            uint64_t acc[NV];
+#pragma unroll
+            for (int v = 0; v < NV; v++) acc[v] = (uint64_t)__double2ull_rn(accd[v]) - (asum[v & 3] << 16);
+#pragma unroll
+            for (int s = 16; s >= 1; s >>= 1) {
+                const bool upper = lane & s;
+#pragma unroll
+                for (int i = 0; i < s; i++) {
+                    const uint64_t send = upper ? acc[i] : acc[i + s];
+                    const uint64_t keep = upper ? acc[i + s] : acc[i];
+                    acc[i] = keep + __shfl_xor_sync(0xffffffffu, send, s);
+                }
+            }
+            const int l = lane & 1;
+            const uint32_t r = modq(acc[0], l);
+            const uint32_t other = __shfl_xor_sync(0xffffffffu, r, 1);
+            if (l == 0) {
+                const int q = (lane >> 1) & 1, cc = lane >> 2;
+                const int64_t col0 = (warp + (u / stripes) * nwarps) * GS_COLS;
+                c[(int64_t)q * db_cols + col0 + cc] = crt2(r, other, c_q0inv, c_br[1]);
+            }
+#pragma unroll
+            for (int v = 0; v < NV; v++) accd[v] = 0.0;
+        }
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+constexpr int GSF_STAGES = 3;  // 96 KB of ring + up to 128 KB of residues
+constexpr int gsf_smem(int db_rows) { return GS_WARPS * GSF_STAGES * GS_COLS * 32 * 16 + db_rows * 4 * 8; }
 
 // ---------------------------------------------------------------------------
 // Packing inner product, rotations fused.  For output j, NTT slot z, limb l:
@@ -674,6 +809,9 @@ __global__ void k_synth_modq(uint64_t* out, int64_t n, uint64_t seed, uint64_t s
 cudaError_t init_device_kernels() {
     cudaError_t e = cudaFuncSetAttribute(k_pack, cudaFuncAttributeMaxDynamicSharedMemorySize, T_EXP * N * 8);
     if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_gemv_staged_f64<GSF_STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             gsf_smem(GF_MAX_ROWS));
+    if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_gemv_staged<GS_STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, GS_SMEM);
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_fold_switch, cudaFuncAttributeMaxDynamicSharedMemorySize, 12 * N * 4);
@@ -727,6 +865,13 @@ cudaError_t launch_gemv(const uint16_t* db, int db_rows, int64_t db_cols, int nq
     else if (nq == 2 && form == 2) k_gemv<2, 2, 3><<<sm_count * 3, 256, 0, st>>>(db, db_rows, db_cols, a_il, c);
     else if (nq == 2 && form == 3)
         k_gemv_staged<GS_STAGES><<<sm_count, GS_WARPS * 32, GS_SMEM, st>>>(db, db_rows, db_cols, a_il, c);
+    else if (nq == 2 && (form == 4 || form == 5) && db_rows > 16384)  // the FP64 sums would pass 2^53
+        return cudaErrorInvalidValue;
+    else if (nq == 2 && form == 4) k_gemv<2, 8, 1, 1><<<blocks, 256, 0, st>>>(db, db_rows, db_cols, a_il, c);
+    else if (nq == 2 && form == 5 && db_rows <= GF_MAX_ROWS)
+        k_gemv_staged_f64<GSF_STAGES><<<sm_count, GS_WARPS * 32, gsf_smem(db_rows), st>>>(db, db_rows, db_cols, a_il,
+                                                                                           c);
+    else if (nq == 2 && form == 5) k_gemv<2, 8, 1, 1><<<blocks, 256, 0, st>>>(db, db_rows, db_cols, a_il, c);
     else if (nq == 1) k_gemv<1, 16><<<blocks, 256, 0, st>>>(db, db_rows, db_cols, a_il, c);
     else return cudaErrorInvalidValue;
     return cudaGetLastError();
