@@ -605,6 +605,9 @@ def main():
                     help="3: fold with the packing post-process fused in, one chain per CTA, two or three CTAs "
                          "per SM by chain count (default); 4 / 5: always three / two per SM; 2: the same on two "
                          "chains per CTA; 1: separate INTT + CRT pass")
+    ap.add_argument("--cuda-core-gemv", type=int, default=None, metavar="FORM",
+                    help="with --batch 1: the first dimension on the CUDA-core GEMV of this IPR_OPT_GEMV_FORM "
+                         "instead of the tensor-core GEMV (a profiling case for that kernel)")
     ap.add_argument("--no-serving", action="store_true", help="skip the Poisson serving measurement")
     ap.add_argument("--serve-rates", type=float, nargs="*", default=[1000.0, 2500.0],
                     help="offered Poisson loads (payloads/s) for the serving measurement")
@@ -672,6 +675,9 @@ def main():
     local = srv.plan  # the rank's share: the whole plan for a replica, a fold-group slice for a shard
     if args.fold_form != 3:
         srv.set_option(pkg.KeywordServer.OPT_FOLD_REGISTER_NTT, args.fold_form)
+    if args.cuda_core_gemv is not None:
+        srv.set_option(pkg.KeywordServer.OPT_TENSOR_GEMV, 0)
+        srv.set_option(pkg.KeywordServer.OPT_GEMV_FORM, args.cuda_core_gemv)
     qbytes = srv.query_bytes(2)
     rbytes = srv.response_bytes(2)
 
