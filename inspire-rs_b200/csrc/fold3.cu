@@ -58,6 +58,30 @@ __device__ __forceinline__ uint32_t bred(uint32_t x, uint32_t q) {
     return x - q * __umulhi(x, q == Q0 ? BM0 : BM1);
 }
 
+// Montgomery reduction with R = 2^32 (Montgomery, "Modular multiplication without trial
+// division", 1985): for x < q R, x R^-1 mod q in [0, 2q) from one 32-bit and one 32x32->64
+// multiply, against about six for a Barrett reduction of a 64-bit value.  The one-chain fold
+// keeps its RGSW bodies and row 0 multiplied by R, so reducing a product with them leaves the
+// plain product.
+constexpr uint32_t neg_inv32(uint32_t q) {  // -q^-1 mod 2^32 for odd q (Newton iteration)
+    uint32_t x = q;
+    for (int i = 0; i < 5; i++) x *= 2u - q * x;
+    return 0u - x;
+}
+constexpr uint32_t QNEG0 = neg_inv32(Q0), QNEG1 = neg_inv32(Q1);
+constexpr uint32_t Q0INV_R = (uint32_t)(((uint64_t)Q0INV << 32) % Q1);  // q0^-1 R mod q1
+__device__ __forceinline__ uint32_t redc(uint64_t x, uint32_t q) {
+    const uint32_t m = (uint32_t)x * (q == Q0 ? QNEG0 : QNEG1);
+    return (uint32_t)((x + (uint64_t)m * q) >> 32);
+}
+// crt2 with the Garner coefficient in Montgomery form: (y - x) q0^-1 mod q1 by one reduction
+__device__ __forceinline__ uint64_t crt2m(uint32_t x, uint32_t y) {
+    const uint32_t xm = x >= Q1 ? x - Q1 : x;            // x < q0 < 2 q1
+    const uint32_t d = y >= xm ? y - xm : y + Q1 - xm;   // (y - x) mod q1
+    const uint32_t k = csub(redc((uint64_t)d * Q0INV_R, Q1), Q1);  // d q0inv R < q1^2 < q1 R
+    return (uint64_t)x + (uint64_t)Q0 * k;
+}
+
 // forward butterfly by stage: MODE 0 leaves x unreduced (the bound grows by 2q), MODE 1
 // first brings x (any 32-bit value) to [0, 2q).  Outputs: x + w*y, x - w*y + 2q, w*y in [0, 2q).
 template <int MODE>
@@ -299,13 +323,13 @@ struct NInv {
 __global__ void __launch_bounds__(256) k_fold_prep(uint32_t* __restrict__ S, int64_t count,
                                                    const uint64_t* __restrict__ zb, const uint64_t* __restrict__ bth,
                                                    int instances, NInv ni, uint32_t* __restrict__ gsw,
-                                                   int64_t gsw_words, int64_t zb_words, int64_t bth_words) {
+                                                   int64_t gsw_words, int64_t zb_words, int64_t bth_words, NInv nb) {
     // the queries' RGSW bodies [query][6 gadget rows][2 limbs][N], scaled by N^-1 in place for
     // the fold form that reads them straight from global memory
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < gsw_words / 4;
          i += (int64_t)gridDim.x * blockDim.x) {
         const int lb = (int)((4 * i / N) & 1);
-        const uint32_t q = lb ? Q1 : Q0, w = ni.w[lb], wq = ni.wp[lb];
+        const uint32_t q = lb ? Q1 : Q0, w = nb.w[lb], wq = nb.wp[lb];
         uint4* g = reinterpret_cast<uint4*>(gsw) + i;
         const uint4 b = *g;
         *g = make_uint4(mul_canon(b.x, w, wq, q), mul_canon(b.y, w, wq, q), mul_canon(b.z, w, wq, q),
@@ -538,7 +562,7 @@ __global__ void __launch_bounds__(F4_THREADS, STAGE ? 2 : 3)
         }
         inverse_limbs<1, 2>(pr, t, xbuf, bar, iwi);
 #pragma unroll
-        for (int m = 0; m < EPT; m++) S_AT(1, m) = add_q(crt2(pr[0][m], pr[1][m], Q0INV, BR1), pc[m]);
+        for (int m = 0; m < EPT; m++) S_AT(1, m) = add_q(crt2m(pr[0][m], pr[1][m]), pc[m]);
     }
 
     for (int step = interp - 2; step >= 0; step--) {
@@ -547,8 +571,9 @@ __global__ void __launch_bounds__(F4_THREADS, STAGE ? 2 : 3)
 #pragma unroll
         for (int l = 0; l < 2; l++) {
             const uint32_t q = l ? Q1 : Q0;
-            const uint64_t br = l ? BR1 : BR0;
-            uint32_t acc0[EPT], acc1[EPT];  // acc1 reduced after every batch of three digits
+            // acc0: the six digit transforms' sum (< 12q); acc1: the packing output plus each
+            // batch's Montgomery-reduced MAC (< q + 2 x 2q = 5q), canonicalised after both batches
+            uint32_t acc0[EPT], acc1[EPT];
 #pragma unroll
             for (int m = 0; m < EPT; m++) acc0[m] = 0;
 #pragma unroll 1
@@ -612,7 +637,7 @@ __global__ void __launch_bounds__(F4_THREADS, STAGE ? 2 : 3)
                 }
                 uint64_t part[EPT];
 #pragma unroll
-                for (int m = 0; m < EPT; m++) part[m] = acc1[m];
+                for (int m = 0; m < EPT; m++) part[m] = 0;
 #pragma unroll
                 for (int k = 0; k < 3; k++) {
                     uint4 b0, b1;
@@ -632,11 +657,11 @@ __global__ void __launch_bounds__(F4_THREADS, STAGE ? 2 : 3)
 #pragma unroll
                     for (int m = 0; m < EPT; m++) {
                         acc0[m] += v[k][m];                    // 6 terms < 12q < 2^32
-                        part[m] += (uint64_t)bv[m] * v[k][m];  // q + 3 terms < q + 6 q^2 < 2^60
+                        part[m] += (uint64_t)bv[m] * v[k][m];  // 3 terms < 6 q^2 < q 2^32
                     }
                 }
 #pragma unroll
-                for (int m = 0; m < EPT; m++) acc1[m] = mod64(part[m], q, br);
+                for (int m = 0; m < EPT; m++) acc1[m] += redc(part[m], q);
             }
             uint32_t r0[EPT];
             if constexpr (STAGE) {
@@ -649,16 +674,16 @@ __global__ void __launch_bounds__(F4_THREADS, STAGE ? 2 : 3)
             }
 #pragma unroll
             for (int m = 0; m < EPT; m++) {
-                pr[2 * l][m] = mod64((uint64_t)r0[m] * acc0[m], q, br);
-                pr[2 * l + 1][m] = acc1[m];
+                pr[2 * l][m] = csub(redc((uint64_t)r0[m] * acc0[m], q), q);  // < 12 q^2 < q 2^32
+                pr[2 * l + 1][m] = csub(bred(acc1[m], q), q);
             }
         }
         inverse_limbs<2, 2>(pr, t, xbuf, bar, iwi);
         cp_wait<0>();  // the packed row j in s's slots
 #pragma unroll
         for (int m = 0; m < EPT; m++) {
-            S_AT(0, m) = add_q(crt2(pr[0][m], pr[2][m], Q0INV, BR1), S_AT(0, m));
-            S_AT(1, m) = add_q(crt2(pr[1][m], pr[3][m], Q0INV, BR1), S_AT(1, m));
+            S_AT(0, m) = add_q(crt2m(pr[0][m], pr[2][m]), S_AT(0, m));
+            S_AT(1, m) = add_q(crt2m(pr[1][m], pr[3][m]), S_AT(1, m));
         }
     }
 
@@ -680,9 +705,12 @@ cudaError_t init_fold3_kernel() {
 }
 
 cudaError_t launch_fold_prep(uint32_t* S, int64_t count, const uint64_t* zb, const uint64_t* bth, int instances,
-                             const uint32_t ninv[4], int sm_count, cudaStream_t st, uint32_t* gsw, int gsw_queries) {
+                             const uint32_t ninv[4], int sm_count, cudaStream_t st, uint32_t* gsw, int gsw_queries,
+                             const uint32_t* ninv_bodies) {
     if (count < 1 || (zb && instances < 1) || (gsw && gsw_queries < 1)) return cudaErrorInvalidValue;
     NInv ni{{ninv[0], ninv[2]}, {ninv[1], ninv[3]}};
+    const uint32_t* nbv = ninv_bodies ? ninv_bodies : ninv;
+    NInv nb{{nbv[0], nbv[2]}, {nbv[1], nbv[3]}};
     const int64_t n4 = count * (N / 4);
     const int64_t blocks = std::min<int64_t>((n4 + 255) / 256, (int64_t)sm_count * 8);
     const int64_t gsw_words = gsw ? (int64_t)gsw_queries * 12 * N : 0;
@@ -695,7 +723,7 @@ cudaError_t launch_fold_prep(uint32_t* S, int64_t count, const uint64_t* zb, con
         (e = check_extent(gsw, (uint64_t)gsw_words * 4, "fold scaling: RGSW bodies")) != cudaSuccess)
         return e;
     k_fold_prep<<<(unsigned)blocks, 256, 0, st>>>(S, count, zb, bth, instances, ni, gsw, gsw_words, zb_words,
-                                                  bth_words);
+                                                  bth_words, nb);
     return cudaGetLastError();
 }
 

@@ -235,10 +235,15 @@ void host_params_init(HostParams& p) {
     p.iwu.assign(2 * kN, 0);
     p.iwup.assign(2 * kN, 0);
     p.row0s.assign(2 * kN, 0);
+    p.row0m.assign(2 * kN, 0);
     for (int l = 0; l < 2; l++) {
         const uint64_t m = p.q[l], ninv = inverse(kN, m);
         p.ninv[2 * l] = (uint32_t)ninv;
         p.ninv[2 * l + 1] = (uint32_t)((ninv << 32) / m);
+        const uint64_t ninvr = mulmod(ninv, (1ull << 32) % m, m);
+        p.ninvr[2 * l] = (uint32_t)ninvr;
+        p.ninvr[2 * l + 1] = (uint32_t)((ninvr << 32) / m);
+        for (int i = 0; i < kN; i++) p.row0m[l * kN + i] = (uint32_t)mulmod(p.row0[l * kN + i], ninvr, m);
         for (int i = 0; i < kN; i++) {
             const uint64_t w = (2 * (uint64_t)p.iw[l * kN + i]) % m;
             p.iwu[l * kN + i] = (uint32_t)w;

@@ -27,6 +27,11 @@ struct HostParams {
     // N^-1, and N^-1 mod q_l with its companion as {w0, wp0, w1, wp1}
     std::vector<uint32_t> iwu, iwup, row0s;
     uint32_t ninv[4];
+    // the one-chain fold's Montgomery operands (R = 2^32): row 0 x N^-1 x R and N^-1 x R
+    // (with its Shoup companion) per limb, so that a Montgomery reduction of a product with
+    // them leaves the product with N^-1
+    std::vector<uint32_t> row0m;
+    uint32_t ninvr[4];
     // the forward and plain inverse twiddles interleaved with their companions: [limb][N][2]
     std::vector<uint32_t> fwi, iwi;
 };

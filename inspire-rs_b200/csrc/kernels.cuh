@@ -87,12 +87,13 @@ cudaError_t launch_fold2(const uint32_t* row0, const uint32_t* gsw, const uint64
 // zb / bth indexed by f / instances and f % instances); launch_fold3 then folds with the forward
 // twiddles fwi and the plain inverse twiddles iwi, both [limb][N] pairs (w, Shoup companion),
 // and row0s = row 0 x N^-1, S of payload p at S + p * s_payload_stride.  With gsw non-null,
-// launch_fold_prep also scales the RGSW bodies of gsw_queries parsed queries by N^-1 in place,
-// as launch_fold4 (one chain per CTA, bodies read from global memory) expects them.
+// launch_fold_prep also scales the RGSW bodies of gsw_queries parsed queries in place by
+// ninv_bodies (N^-1 x 2^32 with its Shoup companion, per limb; the one-chain fold's
+// Montgomery form), as launch_fold4 expects them, and launch_fold4 takes row 0 x N^-1 x 2^32.
 cudaError_t init_fold3_kernel();
 cudaError_t launch_fold_prep(uint32_t* S, int64_t count, const uint64_t* zb, const uint64_t* bth, int instances,
                              const uint32_t ninv[4], int sm_count, cudaStream_t st, uint32_t* gsw = nullptr,
-                             int gsw_queries = 0);
+                             int gsw_queries = 0, const uint32_t* ninv_bodies = nullptr);
 cudaError_t launch_fold3(const uint32_t* row0s, const uint32_t* gsw, const uint64_t* a_hat, const uint32_t* S,
                          int64_t s_payload_stride, const uint64_t* cvec, const uint32_t* fwi, const uint32_t* iwi,
                          const uint32_t ninv[4], int interp, int c_groups,

@@ -173,14 +173,14 @@ int enqueue(ipr_server* s, unsigned nq, const uint8_t* d_query, uint8_t* d_resp,
         if (s->fold_mode >= 2) {
             const bool chain = s->fold_mode >= 3;
             CU(ipr::launch_fold_prep(s->d_S, (int64_t)p.instances, nullptr, nullptr, 1, s->hp.ninv, s->sm_count, st,
-                                     chain ? s->d_gsw : nullptr, (int)nq));
+                                     chain ? s->d_gsw : nullptr, (int)nq, s->hp.ninvr));
             rec(4);
             if (chain) {
                 ipr::FoldExtents ext{(int64_t)p.instances * 2 * kN, (int64_t)nq * 12 * kN,
                                      (int64_t)p.instances * kN, (int64_t)nq * (int64_t)p.db_cols,
                                      (int64_t)s->response_bytes(nq)};
                 if (ipr::kBoundsChecked) ext.s_words -= ipr::g_fold_extent_cut.load();
-                CU(ipr::launch_fold4(s->d_row0s, s->d_gsw, s->d_ahat, s->d_S, 0, s->d_c, s->d_fwi, s->d_iwi,
+                CU(ipr::launch_fold4(s->d_row0m, s->d_gsw, s->d_ahat, s->d_S, 0, s->d_c, s->d_fwi, s->d_iwi,
                                      (int)p.interp, (int)p.c, (int)nq, (int64_t)p.db_cols, (int)nq, d_resp, 0,
                                      (int64_t)(4 + s->per_query_bytes()), ext, st,
                                      fold_staged(s, (int)(nq * p.c))));
@@ -333,13 +333,13 @@ int enqueue_batch(ipr_server* s, int B, const uint8_t* d_queries, uint8_t* d_res
     if (s->fold_mode >= 2) {
         const bool chain = s->fold_mode >= 3;
         CU(ipr::launch_fold_prep(s->d_bS, (int64_t)B * p.instances, s->d_zbs, s->d_bth, (int)p.instances, s->hp.ninv,
-                                 s->sm_count, st, chain ? s->d_gsw : nullptr, nqt));
+                                 s->sm_count, st, chain ? s->d_gsw : nullptr, nqt, s->hp.ninvr));
         rec(4);
         if (chain) {
             ipr::FoldExtents ext{(int64_t)B * (int64_t)p.instances * 2 * kN, (int64_t)nqt * 12 * kN,
                                  (int64_t)p.instances * kN, (int64_t)nqt * (int64_t)p.db_cols, (int64_t)B * rb};
             if (ipr::kBoundsChecked) ext.s_words -= ipr::g_fold_extent_cut.load();
-            CU(ipr::launch_fold4(s->d_row0s, s->d_gsw, s->d_ahat, s->d_bS, (int64_t)(p.instances * 2 * kN), s->d_c,
+            CU(ipr::launch_fold4(s->d_row0m, s->d_gsw, s->d_ahat, s->d_bS, (int64_t)(p.instances * 2 * kN), s->d_c,
                                  s->d_fwi, s->d_iwi, (int)p.interp, (int)p.c, nqt, (int64_t)p.db_cols, 2, d_resps, rb,
                                  (int64_t)(4 + s->per_query_bytes()), ext, st, fold_staged(s, (int)(nqt * p.c))));
         }
@@ -432,11 +432,12 @@ int init_common(ipr_server* s, int device, const ipr_plan* plan) {
     const size_t tb = 2 * kN * 4;
     if ((st = s->alloc(&s->d_fw, tb)) || (st = s->alloc(&s->d_fwp, tb)) || (st = s->alloc(&s->d_iw, tb)) ||
         (st = s->alloc(&s->d_iwp, tb)) || (st = s->alloc(&s->d_row0, tb)) || (st = s->alloc(&s->d_fwi, 2 * tb)) ||
-        (st = s->alloc(&s->d_iwi, 2 * tb)) || (st = s->alloc(&s->d_row0s, tb)))
+        (st = s->alloc(&s->d_iwi, 2 * tb)) || (st = s->alloc(&s->d_row0s, tb)) || (st = s->alloc(&s->d_row0m, tb)))
         return st;
     CU(cudaMemcpy(s->d_fwi, s->hp.fwi.data(), 2 * tb, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(s->d_iwi, s->hp.iwi.data(), 2 * tb, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(s->d_row0s, s->hp.row0s.data(), tb, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(s->d_row0m, s->hp.row0m.data(), tb, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(s->d_fw, s->hp.fw.data(), tb, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(s->d_fwp, s->hp.fwp.data(), tb, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(s->d_iw, s->hp.iw.data(), tb, cudaMemcpyHostToDevice));

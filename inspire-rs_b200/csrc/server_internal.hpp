@@ -56,6 +56,7 @@ struct ipr_server {
     uint64_t stash_count = 0, stash_entry = 0;
     uint32_t *d_fw = nullptr, *d_fwp = nullptr, *d_iw = nullptr, *d_iwp = nullptr, *d_row0 = nullptr;
     uint32_t *d_fwi = nullptr, *d_iwi = nullptr, *d_row0s = nullptr;  // the fused fold's tables
+    uint32_t* d_row0m = nullptr;  // row 0 x N^-1 x 2^32 for the one-chain fold's Montgomery reductions
     // per-request scratch
     unsigned cap_q = 0;
     uint8_t* d_query = nullptr;
