@@ -51,11 +51,10 @@ using nttr::eB;
 using nttr::eC;
 using nttr::eD;
 
-// Barrett reduction with m = floor(2^32 / q): any 32-bit x to [0, 2q) (the quotient estimate
-// umulhi(x, m) is at most one below floor(x / q) because 2^32 - m q < q)
-constexpr uint32_t BM0 = (uint32_t)((1ull << 32) / Q0), BM1 = (uint32_t)((1ull << 32) / Q1);
-__device__ __forceinline__ uint32_t bred(uint32_t x, uint32_t q) {
-    return x - q * __umulhi(x, q == Q0 ? BM0 : BM1);
+// x < 16q (< 2^32) to [0, 2q) by three conditional subtractions on the ALU pipe: the fold is
+// bound by its integer multiplies, so these cost less than a Barrett reduction's two
+__device__ __forceinline__ uint32_t red16(uint32_t x, uint32_t q) {
+    return csub(csub(csub(x, 8 * q), 4 * q), 2 * q);
 }
 
 // Montgomery reduction with R = 2^32 (Montgomery, "Modular multiplication without trial
@@ -83,10 +82,10 @@ __device__ __forceinline__ uint64_t crt2m(uint32_t x, uint32_t y) {
 }
 
 // forward butterfly by stage: MODE 0 leaves x unreduced (the bound grows by 2q), MODE 1
-// first brings x (any 32-bit value) to [0, 2q).  Outputs: x + w*y, x - w*y + 2q, w*y in [0, 2q).
+// first brings x (< 16q) to [0, 2q).  Outputs: x + w*y, x - w*y + 2q, w*y in [0, 2q).
 template <int MODE>
 __device__ __forceinline__ void fwd_b(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wp, uint32_t q) {
-    const uint32_t xx = MODE == 1 ? bred(x, q) : x;
+    const uint32_t xx = MODE == 1 ? red16(x, q) : x;
     const uint32_t qn = shoup_lazy(y, w, wp, q);
     x = xx + qn;
     y = xx + 2 * q - qn;
@@ -184,17 +183,17 @@ __device__ __forceinline__ void forward_digits(uint32_t (&v)[P][EPT], int t, uin
 #pragma unroll
     for (int p = 0; p < P; p++)
 #pragma unroll
-        for (int k = 0; k < EPT; k++) v[p][k] = bred(v[p][k], q);
+        for (int k = 0; k < EPT; k++) v[p][k] = red16(v[p][k], q);
 }
 
 // Gentleman-Sande butterfly with a plain inverse twiddle: x + y, (x - y) * w.  Inputs below
 // OFF * q; the difference is taken as x + OFF q - y (< 2 OFF q <= 16q < 2^32); the product
-// lands in [0, 2q); the sum (< 2 OFF q) is Barrett-reduced to [0, 2q) when RED.
+// lands in [0, 2q); the sum (< 2 OFF q <= 16q) is reduced to [0, 2q) when RED.
 template <int OFF, bool RED>
 __device__ __forceinline__ void inv_b(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wp, uint32_t q) {
     const uint32_t s = x + y;
     const uint32_t d = x + OFF * q - y;
-    x = RED ? bred(s, q) : s;
+    x = RED ? red16(s, q) : s;
     y = shoup_lazy(d, w, wp, q);
 }
 
@@ -675,7 +674,7 @@ __global__ void __launch_bounds__(F4_THREADS, STAGE ? 2 : 3)
 #pragma unroll
             for (int m = 0; m < EPT; m++) {
                 pr[2 * l][m] = csub(redc((uint64_t)r0[m] * acc0[m], q), q);  // < 12 q^2 < q 2^32
-                pr[2 * l + 1][m] = csub(bred(acc1[m], q), q);
+                pr[2 * l + 1][m] = csub(csub(csub(acc1[m], 4 * q), 2 * q), q);  // < 5q -> [0, q)
             }
         }
         inverse_limbs<2, 2>(pr, t, xbuf, bar, iwi);
