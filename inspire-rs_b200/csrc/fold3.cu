@@ -57,30 +57,6 @@ __device__ __forceinline__ uint32_t red16(uint32_t x, uint32_t q) {
     return csub(csub(csub(x, 8 * q), 4 * q), 2 * q);
 }
 
-// Montgomery reduction with R = 2^32 (Montgomery, "Modular multiplication without trial
-// division", 1985): for x < q R, x R^-1 mod q in [0, 2q) from one 32-bit and one 32x32->64
-// multiply, against about six for a Barrett reduction of a 64-bit value.  The one-chain fold
-// keeps its RGSW bodies and row 0 multiplied by R, so reducing a product with them leaves the
-// plain product.
-constexpr uint32_t neg_inv32(uint32_t q) {  // -q^-1 mod 2^32 for odd q (Newton iteration)
-    uint32_t x = q;
-    for (int i = 0; i < 5; i++) x *= 2u - q * x;
-    return 0u - x;
-}
-constexpr uint32_t QNEG0 = neg_inv32(Q0), QNEG1 = neg_inv32(Q1);
-constexpr uint32_t Q0INV_R = (uint32_t)(((uint64_t)Q0INV << 32) % Q1);  // q0^-1 R mod q1
-__device__ __forceinline__ uint32_t redc(uint64_t x, uint32_t q) {
-    const uint32_t m = (uint32_t)x * (q == Q0 ? QNEG0 : QNEG1);
-    return (uint32_t)((x + (uint64_t)m * q) >> 32);
-}
-// crt2 with the Garner coefficient in Montgomery form: (y - x) q0^-1 mod q1 by one reduction
-__device__ __forceinline__ uint64_t crt2m(uint32_t x, uint32_t y) {
-    const uint32_t xm = x >= Q1 ? x - Q1 : x;            // x < q0 < 2 q1
-    const uint32_t d = y >= xm ? y - xm : y + Q1 - xm;   // (y - x) mod q1
-    const uint32_t k = csub(redc((uint64_t)d * Q0INV_R, Q1), Q1);  // d q0inv R < q1^2 < q1 R
-    return (uint64_t)x + (uint64_t)Q0 * k;
-}
-
 // forward butterfly by stage: MODE 0 leaves x unreduced (the bound grows by 2q), MODE 1
 // first brings x (< 16q) to [0, 2q).  Outputs: x + w*y, x - w*y + 2q, w*y in [0, 2q).
 template <int MODE>

@@ -204,9 +204,9 @@ __global__ void __launch_bounds__(G1_THREADS, 1)
                             const int i = (qq * 2 + l) * 4 + b;
                             v += ((uint64_t)p0[i] + ((uint64_t)p1[i] << 8)) << (8 * b);
                         }
-                        r[l] = l ? mod64(v, Q1, BR1) : mod64(v, Q0, BR0);
+                        r[l] = mod64m(v, l ? Q1 : Q0);
                     }
-                    if (q < num_queries) c[(int64_t)q * db_cols + j] = crt2(r[0], r[1], Q0INV, BR1);
+                    if (q < num_queries) c[(int64_t)q * db_cols + j] = crt2m(r[0], r[1]);
                 }
             }
             umma::fence_before();

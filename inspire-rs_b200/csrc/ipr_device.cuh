@@ -57,6 +57,42 @@ __device__ __forceinline__ uint64_t crt2(uint32_t x, uint32_t y, uint32_t q0inv,
     return (uint64_t)x + (uint64_t)Q0 * k;
 }
 
+// Montgomery reduction with R = 2^32 (Montgomery, "Modular multiplication without trial
+// division", 1985): for x < q R, x R^-1 mod q in [0, 2q) from one 32-bit and one 32x32->64
+// multiply, against about six for a Barrett reduction of a 64-bit value.  The one-chain fold
+// keeps its RGSW bodies and row 0 multiplied by R, so reducing a product with them leaves the
+// plain product; the first-dimension GEMM's epilogue reduces its recombined sums the same way.
+constexpr uint32_t neg_inv32(uint32_t q) {  // -q^-1 mod 2^32 for odd q (Newton iteration)
+    uint32_t x = q;
+    for (int i = 0; i < 5; i++) x *= 2u - q * x;
+    return 0u - x;
+}
+constexpr uint32_t QNEG0 = neg_inv32(Q0), QNEG1 = neg_inv32(Q1);
+constexpr uint32_t Q0INV_R = (uint32_t)(((uint64_t)Q0INV << 32) % Q1);  // q0^-1 R mod q1
+__device__ __forceinline__ uint32_t redc(uint64_t x, uint32_t q) {
+    const uint32_t m = (uint32_t)x * (q == Q0 ? QNEG0 : QNEG1);
+    return (uint32_t)((x + (uint64_t)m * q) >> 32);
+}
+// any 64-bit v to [0, q) by one Montgomery reduction: with v = vh 2^32 + vl,
+// x = vh (2^64 mod q) + vl (2^32 mod q) < 2 q 2^32 and redc(x) = v mod q in [0, 3q)
+constexpr uint32_t R1_0 = (uint32_t)((1ull << 32) % Q0), R1_1 = (uint32_t)((1ull << 32) % Q1);
+constexpr uint32_t R2_0 = (uint32_t)((uint64_t)R1_0 * R1_0 % Q0), R2_1 = (uint32_t)((uint64_t)R1_1 * R1_1 % Q1);
+__device__ __forceinline__ uint32_t mod64m(uint64_t v, uint32_t q) {
+    const uint64_t x = (uint64_t)(uint32_t)(v >> 32) * (q == Q0 ? R2_0 : R2_1) +
+                       (uint64_t)(uint32_t)v * (q == Q0 ? R1_0 : R1_1);
+    const uint32_t t = redc(x, q), t1 = min(t, t - 2 * q);
+    return min(t1, t1 - q);
+}
+
+// crt2 with the Garner coefficient in Montgomery form: (y - x) q0^-1 mod q1 by one reduction
+__device__ __forceinline__ uint64_t crt2m(uint32_t x, uint32_t y) {
+    const uint32_t xm = x >= Q1 ? x - Q1 : x;            // x < q0 < 2 q1
+    const uint32_t d = y >= xm ? y - xm : y + Q1 - xm;   // (y - x) mod q1
+    const uint32_t kr = redc((uint64_t)d * Q0INV_R, Q1);  // d q0inv R < q1^2 < q1 R
+    const uint32_t k = min(kr, kr - Q1);
+    return (uint64_t)x + (uint64_t)Q0 * k;
+}
+
 // ---------------------------------------------------------------------------
 // Shared-memory negacyclic NTTs over u32 residues, executed cooperatively by
 // all threads of a CTA on `npoly` independent polynomials laid out at
