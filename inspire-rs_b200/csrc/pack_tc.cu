@@ -285,7 +285,6 @@ __global__ void __launch_bounds__(P_THREADS, 1)
             const int lm = (int)(u >> (LOGN - 1));
             const int l = lm / mt_count, mt = lm % mt_count;
             const uint32_t q = l ? Q1 : Q0;
-            const uint64_t br = l ? BR1 : BR0;
             const uint32_t lane_off = (uint32_t)(b * 32) << 16;
             const uint32_t col0 = (uint32_t)(buf * 2 * nt + t * nt);
             const int j = mt * 32 + lane;
@@ -299,7 +298,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
                         uint64_t v = 0;
 #pragma unroll
                         for (int a = 0; a < 4; a++) v += (uint64_t)d[ci * 4 + a] << (8 * a);
-                        const uint32_t r = mod64(v, q, br);
+                        const uint32_t r = mod64m(v, q);
                         xch[(((g - ch * 4) * 4 + ci) * 4 + b) * 32 + lane] = r;  // r < q: shifted by byte b below
                     }
                 }
@@ -320,7 +319,7 @@ __global__ void __launch_bounds__(P_THREADS, 1)
                                              ((uint64_t)xch[(cl * 4 + 1) * 32 + lane] << 8) +
                                              ((uint64_t)xch[(cl * 4 + 2) * 32 + lane] << 16) +
                                              ((uint64_t)xch[(cl * 4 + 3) * 32 + lane] << 24);
-                        S[(((int64_t)c * instances + j) * 2 + l) * N + z] = mod64(tot, q, br);
+                        S[(((int64_t)c * instances + j) * 2 + l) * N + z] = mod64m(tot, q);
                     }
                 }
                 umma::named_bar(gbar, 128);
@@ -492,7 +491,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Q_THREADS, 1)
             const int lm = (int)(u >> (LOGN - 1));
             const int l = lm / mt_count, mt = lm % mt_count;
             const uint32_t q = l ? Q1 : Q0;
-            const uint64_t br = l ? BR1 : BR0;
             const uint32_t lane_off = (uint32_t)(b * 32) << 16;
             const uint32_t col0 = (uint32_t)(buf * nt);
             const int j = mt * 32 + lane;
@@ -506,7 +504,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Q_THREADS, 1)
                         uint64_t v = 0;
 #pragma unroll
                         for (int a = 0; a < 4; a++) v += (uint64_t)d[ci * 4 + a] << (8 * a);
-                        xch[(((g - ch * 4) * 4 + ci) * 4 + b) * 32 + lane] = mod64(v, q, br);
+                        xch[(((g - ch * 4) * 4 + ci) * 4 + b) * 32 + lane] = mod64m(v, q);
                     }
                 }
                 if (ch == chunks - 1) {  // every TMEM read of this unit is done: free the buffer
@@ -524,7 +522,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(Q_THREADS, 1)
                                              ((uint64_t)xch[(cl * 4 + 1) * 32 + lane] << 8) +
                                              ((uint64_t)xch[(cl * 4 + 2) * 32 + lane] << 16) +
                                              ((uint64_t)xch[(cl * 4 + 3) * 32 + lane] << 24);
-                        S[(((int64_t)c * instances + j) * 2 + l) * N + z] = mod64(tot, q, br);
+                        S[(((int64_t)c * instances + j) * 2 + l) * N + z] = mod64m(tot, q);
                     }
                 }
                 umma::named_bar(1, 128);
