@@ -844,7 +844,8 @@ def main():
         forms = {0: "8 columns per warp, registers", 1: "4 columns per warp, registers",
                  2: "2 columns per warp, registers", 3: "8 columns per warp, cp.async ring in shared memory",
                  4: "8 columns per warp, exact products on the FP64 pipe",
-                 5: "8 columns per warp, cp.async ring, FP64 pipe, residues converted once into shared memory"}
+                 5: "8 columns per warp, cp.async ring, FP64 pipe, residues converted once into shared memory",
+                 6: "a lane per column, 16 warps, TMA-fed stages, FP64 pipe, residues broadcast"}
         for form, name in forms.items():
             srv.set_option(pkg.KeywordServer.OPT_GEMV_FORM, form)
             rate = single_rate()

@@ -213,10 +213,12 @@ int ipr_server_set_profiling(ipr_server *srv, int on);
  * for two queries: 0 / 1 / 2 = 8 / 4 / 2 DB columns per warp loaded into
  * registers (fewer columns, fewer partial sums per thread, more warps per SM); 3 = 8 columns
  * per warp streamed through a 4-stage shared-memory ring by cp.async; 4 = form 0 with the
- * products on the FP64 pipe (exact: every partial sum is an integer below 2^53); 5 (default)
- * = form 3's shared-memory ring with the products on the FP64 pipe, the query residues
- * converted to doubles once per CTA and the DB entries turned into doubles by integer
- * operations (up to 4,096 DB rows; above, form 4).  Forms 4 and 5 run as form 0 above
+ * products on the FP64 pipe (exact: every partial sum is an integer below 2^53); 5 = form
+ * 3's shared-memory ring with the products on the FP64 pipe, the query residues converted to
+ * doubles once per CTA and the DB entries turned into doubles by integer operations (up to
+ * 4,096 DB rows; above, form 4); 6 (default) = a lane per DB column in 16 warps, the DB and
+ * the query residues brought into shared memory in stages by TMA, the products on the FP64
+ * pipe (any number of DB rows that is a multiple of 256).  Forms 4 and 5 run as form 0 above
  * 16,384 DB rows.  Identical results. */
 #define IPR_OPT_GEMV_FORM 5
 int ipr_server_set_option(ipr_server *srv, int option, int64_t value);

@@ -270,6 +270,27 @@ cudaError_t make_u8_tile_map(CUtensorMap* map, const void* base, uint64_t row_by
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
+cudaError_t make_u16_col_map(CUtensorMap* map, const uint16_t* db, int db_rows, int64_t db_cols, uint32_t box_rows,
+                             uint32_t box_cols) {
+    if (!g_encode) {
+        cudaDriverEntryPointQueryResult q;
+        cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", (void**)&g_encode, cudaEnableDefault, &q);
+        if (e != cudaSuccess) return e;
+        if (!g_encode || q != cudaDriverEntryPointSuccess) return cudaErrorNotSupported;
+    }
+    if ((reinterpret_cast<uintptr_t>(db) & 15) || (db_rows & 7) || box_rows * 2 != 32 || box_cols == 0 ||
+        box_cols > 256)
+        return cudaErrorInvalidValue;
+    cuuint64_t dims[2] = {(cuuint64_t)db_rows, (cuuint64_t)db_cols};
+    cuuint64_t strides[1] = {(cuuint64_t)db_rows * 2};
+    cuuint32_t box[2] = {box_rows, box_cols};
+    cuuint32_t elem[2] = {1, 1};
+    CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, const_cast<uint16_t*>(db), dims, strides, box, elem,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
 int gemm1_stages(int nt) {
     const int per = 2 * A_STAGE_BYTES + nt * TILE_K;
     int s = (210 * 1024) / per;

@@ -19,6 +19,7 @@
 #include "ipr_device.cuh"
 #include "kernels.cuh"
 #include "ntt_regs.cuh"
+#include "umma.cuh"
 
 namespace ipr {
 
@@ -414,6 +415,190 @@ __global__ void __launch_bounds__(GS_WARPS * 32, 1)
 }
 constexpr int GSF_STAGES = 3;  // 96 KB of ring + up to 128 KB of residues
 constexpr int gsf_smem(int db_rows) { return GS_WARPS * GSF_STAGES * GS_COLS * 32 * 16 + db_rows * 4 * 8; }
+
+// The two-query GEMV with a lane per DB column and TMA-fed stages (form 6).  A CTA owns a tile
+// of GT_COLS = 128 consecutive columns (a contiguous 128 x db_rows x 2-byte block of the
+// column-major DB) and its 16 warps split the tile's rows: in stage s warp w takes rows
+// 256 s + 16 w .. + 16 of all 128 columns, one 2D TMA box ({16 rows, 128 columns}, 32-byte
+// swizzle) plus a 256-byte bulk copy of those rows' query residues, through a private ring
+// of GT_STAGES stages and one mbarrier per stage.  Lane l owns columns l, l + 32, l + 64,
+// l + 96, so the residues of a row are the same for all lanes (broadcast reads, converted to
+// doubles once per stage by the warp) and each residue read serves 4 columns x 4 values;
+// the swizzle puts the 16-byte row chunks of 8 consecutive columns in 8 distinct bank groups.
+// Products run on the FP64 pipe as in k_gemv_staged_f64 (a DB entry is the double 2^16 + d,
+// built by integer operations; a product is below 2^45) and a lane's double accumulators
+// are flushed after at most 16 stages (256 rows, below 2^53: exact) into 64-bit integer
+// sums in shared memory by atomic adds.  At the tile's end the 16 warps meet at a named
+// barrier and each of the first 256 threads finishes one (column, query) output (16 warps
+// of 122 registers fill the register file; more warps per SM, not deeper rings, is what
+// shortened this kernel, 0.85 against 0.92-0.95 ms at 1M for 8 warps x 5 stages): the offset 2^16 x (sum of
+// the limb's residues over all rows) is taken off, then the Barrett reductions and the CRT.
+// The sums use two buffers (alternating tiles), so one barrier per tile suffices.  A stage
+// wait is bounded by time: after a failed wait the warp stops waiting and issuing, the
+// kernel reports code 31 through err_flag and drains its own copies before it returns.
+constexpr int GT_WARPS = 16, GT_ROWS = 16, GT_COLS = 128, GT_STAGES = 2;
+constexpr int GT_DB_BYTES = GT_ROWS * GT_COLS * 2;  // 4 KB of DB per stage
+constexpr int GT_RES_BYTES = GT_ROWS * 16;          // the stage rows' 4 u32 residues each
+constexpr int gt_smem() {
+    return 1024 + GT_WARPS * GT_STAGES * (GT_DB_BYTES + GT_RES_BYTES + GT_RES_BYTES * 2) + 2 * GT_COLS * 4 * 8 +
+           GT_WARPS * GT_STAGES * 8 + 64;
+}
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* mbar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     umma::smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(umma::smem_addr(mbar))
+                 : "memory");
+}
+
+__global__ void __launch_bounds__(GT_WARPS * 32, 1)
+    k_gemv_tma_f64(const __grid_constant__ CUtensorMap tm_db, int db_rows, int64_t db_cols,
+                   const uint32_t* __restrict__ a_il, uint64_t* __restrict__ c, int* __restrict__ err_flag) {
+    extern __shared__ uint8_t gt_raw[];
+    uint8_t* base = gt_raw + ((1024 - (umma::smem_addr(gt_raw) & 1023)) & 1023);
+    uint8_t* ring_db = base;                                                  // [warp][stage][4 KB]
+    uint32_t* ring_ru = reinterpret_cast<uint32_t*>(base + GT_WARPS * GT_STAGES * GT_DB_BYTES);  // [warp][stage][64]
+    double* ring_rd = reinterpret_cast<double*>(ring_ru + GT_WARPS * GT_STAGES * GT_ROWS * 4);    // [warp][stage][64]
+    uint64_t* red = reinterpret_cast<uint64_t*>(ring_rd + GT_WARPS * GT_STAGES * GT_ROWS * 4);   // [2][128][4]
+    uint64_t* bars = red + 2 * GT_COLS * 4;                                                      // [warp][stage]
+    uint64_t* asum_sh = bars + GT_WARPS * GT_STAGES;                                             // [4]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int i = threadIdx.x; i < 2 * GT_COLS * 4; i += blockDim.x) red[i] = 0;
+    if (threadIdx.x < 4) asum_sh[threadIdx.x] = 0;
+    if (lane == 0)
+        for (int s = 0; s < GT_STAGES; s++) umma::mbar_init(&bars[warp * GT_STAGES + s], 1);
+    umma::fence_mbar_init();
+    __syncthreads();
+    {  // the offset: 2^16 x the sum of each limb's residues over all rows
+        uint64_t a4[4] = {0, 0, 0, 0};
+        for (int r = threadIdx.x; r < db_rows; r += blockDim.x) {
+            const uint4 t = __ldg(reinterpret_cast<const uint4*>(a_il) + r);
+            a4[0] += t.x; a4[1] += t.y; a4[2] += t.z; a4[3] += t.w;
+        }
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+#pragma unroll
+            for (int s = 16; s >= 1; s >>= 1) a4[v] += __shfl_xor_sync(0xffffffffu, a4[v], s);
+            if (lane == 0) atomicAdd(reinterpret_cast<unsigned long long*>(&asum_sh[v]), (unsigned long long)a4[v]);
+        }
+    }
+    __syncthreads();
+    const int oq = (threadIdx.x >> 7) & 1;  // the query of this thread's output (threads below 256)
+    const uint64_t off = asum_sh[oq * 2] << 16, off1 = asum_sh[oq * 2 + 1] << 16;
+    const int nst = db_rows / (GT_WARPS * GT_ROWS);  // stages per tile
+    const int64_t ntiles = (db_cols + GT_COLS - 1) / GT_COLS;
+    const int my_tiles = blockIdx.x < ntiles ? (int)((ntiles - 1 - blockIdx.x) / gridDim.x + 1) : 0;
+    const int items = my_tiles * nst;  // (tile, stage) items of every warp of this CTA, in order
+    uint8_t* my_db = ring_db + warp * GT_STAGES * GT_DB_BYTES;
+    uint32_t* my_ru = ring_ru + warp * GT_STAGES * GT_ROWS * 4;
+    double* my_rd = ring_rd + warp * GT_STAGES * GT_ROWS * 4;
+    uint64_t* my_bars = bars + warp * GT_STAGES;
+    int i_next = 0, i_st = 0, i_slot = 0;  // lane 0's issue position: item, its stage, its slot
+    int64_t i_tile = blockIdx.x;
+    auto issue = [&]() {  // lane 0: the next item into its slot, if any
+        if (i_next < items) {
+            const int row0 = i_st * (GT_WARPS * GT_ROWS) + warp * GT_ROWS;
+            uint64_t* bar = &my_bars[i_slot];
+            umma::mbar_expect_tx(bar, GT_DB_BYTES + GT_RES_BYTES);
+            umma::tma_load_2d(my_db + i_slot * GT_DB_BYTES, &tm_db, row0, (int)(i_tile * GT_COLS), bar);
+            bulk_load(my_ru + i_slot * GT_ROWS * 4, a_il + (int64_t)row0 * 4, GT_RES_BYTES, bar);
+            i_next++;
+            if (++i_slot == GT_STAGES) i_slot = 0;
+            if (++i_st == nst) {
+                i_st = 0;
+                i_tile += gridDim.x;
+            }
+        }
+    };
+    if (lane == 0)
+        for (int u = 0; u < GT_STAGES; u++) issue();
+    double acc[16];
+#pragma unroll
+    for (int v = 0; v < 16; v++) acc[v] = 0.0;
+    bool ok = true;
+    int failed_at = -1, slot = 0, st = 0, b = 0;
+    uint32_t phase = 0;
+    int64_t tile = blockIdx.x;
+    for (int u = 0; u < items; u++) {
+        if (ok) {
+            const bool got = umma::mbar_wait(&my_bars[slot], phase);
+            if (!__all_sync(0xffffffffu, got)) {  // the warp stops together
+                ok = false;
+                failed_at = u;
+                if (lane == 0) atomicExch(err_flag, 31);
+            }
+        }
+        if (ok) {
+            const uint32_t* ru = my_ru + slot * GT_ROWS * 4;
+            double* rd = my_rd + slot * GT_ROWS * 4;
+            rd[lane] = (double)ru[lane];
+            rd[lane + 32] = (double)ru[lane + 32];
+            const uint8_t* sb = my_db + slot * GT_DB_BYTES;
+            uint4 d[4][2];
+#pragma unroll
+            for (int p = 0; p < 4; p++) {
+                const int col = p * 32 + lane;
+#pragma unroll
+                for (int j = 0; j < 2; j++)  // 32-byte swizzle: chunk j of column col at chunk j ^ bit 2 of col
+                    d[p][j] = *reinterpret_cast<const uint4*>(sb + col * 32 + ((j ^ ((col >> 2) & 1)) << 4));
+            }
+            __syncwarp();
+#pragma unroll
+            for (int i = 0; i < GT_ROWS; i++) {
+                const double2 a01 = *reinterpret_cast<const double2*>(rd + i * 4);
+                const double2 a23 = *reinterpret_cast<const double2*>(rd + i * 4 + 2);
+                const double ad[4] = {a01.x, a01.y, a23.x, a23.y};
+#pragma unroll
+                for (int p = 0; p < 4; p++) {
+                    const uint32_t w = (&d[p][i >> 3].x)[(i & 7) >> 1];
+                    const uint32_t m = (i & 1) ? ((w >> 12) & 0xffff0u) : ((w << 4) & 0xffff0u);
+                    const double dd = __hiloint2double((int)(0x40f00000u | m), 0);
+#pragma unroll
+                    for (int v = 0; v < 4; v++) acc[p * 4 + v] = fma(ad[v], dd, acc[p * 4 + v]);
+                }
+            }
+        }
+        __syncwarp();
+        if (ok && lane == 0) issue();  // item u + GT_STAGES into the slot every lane has finished reading
+        if ((st & 15) == 15 || st == nst - 1) {  // flush: at most 256 rows per accumulator
+#pragma unroll
+            for (int p = 0; p < 4; p++)
+#pragma unroll
+                for (int v = 0; v < 4; v++) {
+                    atomicAdd(reinterpret_cast<unsigned long long*>(&red[(b * GT_COLS + p * 32 + lane) * 4 + v]),
+                              (unsigned long long)__double2ull_rn(acc[p * 4 + v]));
+                    acc[p * 4 + v] = 0.0;
+                }
+        }
+        if (st == nst - 1) {  // the tile's last stage: every warp has added its sums
+            umma::named_bar(1, GT_WARPS * 32);
+            if (threadIdx.x < 2 * GT_COLS) {
+                const int col = threadIdx.x & (GT_COLS - 1);
+                uint64_t* sp = &red[(b * GT_COLS + col) * 4 + 2 * oq];
+                const uint64_t s0 = sp[0] - off, s1 = sp[1] - off1;
+                sp[0] = 0;
+                sp[1] = 0;
+                const int64_t gcol = tile * GT_COLS + col;
+                if (gcol < db_cols)
+                    c[(int64_t)oq * db_cols + gcol] = crt2(modq(s0, 0), modq(s1, 1), c_q0inv, c_br[1]);
+            }
+        }
+        if (++slot == GT_STAGES) {
+            slot = 0;
+            phase ^= 1;
+        }
+        if (++st == nst) {
+            st = 0;
+            b ^= 1;
+            tile += gridDim.x;
+        }
+    }
+    if (!ok && lane == 0) {  // drain the copies this warp issued and did not consume
+        const int end = failed_at + GT_STAGES < items ? failed_at + GT_STAGES : items;
+        for (int v = failed_at; v < end; v++)
+            umma::mbar_wait(&my_bars[v % GT_STAGES], (uint32_t)((v / GT_STAGES) & 1), umma::kDrainLimitNs);
+    }
+}
 
 // ---------------------------------------------------------------------------
 // Packing inner product, rotations fused.  For output j, NTT slot z, limb l:
@@ -814,6 +999,8 @@ cudaError_t init_device_kernels() {
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_gemv_staged<GS_STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, GS_SMEM);
     if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_gemv_tma_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, gt_smem());
+    if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_fold_switch, cudaFuncAttributeMaxDynamicSharedMemorySize, 12 * N * 4);
 }
 
@@ -858,9 +1045,21 @@ cudaError_t launch_parse_batch(const uint8_t* qb, int npay, int64_t pstride, int
 }
 
 cudaError_t launch_gemv(const uint16_t* db, int db_rows, int64_t db_cols, int nq, const uint32_t* a_il,
-                        uint64_t* c, int sm_count, cudaStream_t st, int form) {
+                        uint64_t* c, int sm_count, cudaStream_t st, int form, int* err_flag) {
     const int blocks = sm_count * 4;
-    if (nq == 2 && form == 0) k_gemv<2, 8><<<blocks, 256, 0, st>>>(db, db_rows, db_cols, a_il, c);
+    cudaError_t e;
+    if ((e = check_extent(db, (uint64_t)db_rows * db_cols * 2, "GEMV: DB")) != cudaSuccess ||
+        (e = check_extent(a_il, (uint64_t)db_rows * nq * 8, "GEMV: query residues")) != cudaSuccess ||
+        (e = check_extent(c, (uint64_t)nq * db_cols * 8, "GEMV: outputs")) != cudaSuccess)
+        return e;
+    if (nq == 2 && form == 6 && (!err_flag || (db_rows % (GT_WARPS * GT_ROWS)) || db_rows > (1 << 18))) form = 5;
+    if (nq == 2 && form == 6) {
+        CUtensorMap tm;
+        if ((e = make_u16_col_map(&tm, db, db_rows, db_cols, GT_ROWS, GT_COLS)) != cudaSuccess) return e;
+        const int64_t ntiles = (db_cols + GT_COLS - 1) / GT_COLS;
+        const int grid = ntiles < sm_count ? (int)ntiles : sm_count;
+        k_gemv_tma_f64<<<grid, GT_WARPS * 32, gt_smem(), st>>>(tm, db_rows, db_cols, a_il, c, err_flag);
+    } else if (nq == 2 && form == 0) k_gemv<2, 8><<<blocks, 256, 0, st>>>(db, db_rows, db_cols, a_il, c);
     else if (nq == 2 && form == 1) k_gemv<2, 4, 2><<<sm_count * 2, 256, 0, st>>>(db, db_rows, db_cols, a_il, c);
     else if (nq == 2 && form == 2) k_gemv<2, 2, 3><<<sm_count * 3, 256, 0, st>>>(db, db_rows, db_cols, a_il, c);
     else if (nq == 2 && form == 3)

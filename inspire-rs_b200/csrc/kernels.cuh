@@ -16,9 +16,15 @@ cudaError_t launch_parse_query(const uint8_t* qb, int nq, int db_rows, uint64_t*
                                uint32_t* a_il, uint32_t* gsw, uint8_t* qbytes, int qbase, cudaStream_t st);
 // nq must be 1 or 2; a_il points at the pair group, c at [nq][db_cols]; form of the two-query
 // kernel: 0 / 1 / 2 = 8 / 4 / 2 DB columns per warp loaded into registers, 3 = 8 columns per
-// warp staged through shared memory by cp.async (one query always takes 16 columns per warp)
+// warp staged through shared memory by cp.async, 4 / 5 = forms 0 / 3 with FP64-pipe products,
+// 6 = a lane per column with TMA-fed stages and FP64-pipe products (needs err_flag and
+// db_rows a multiple of 128; otherwise form 5 runs).  One query always takes 16 columns per warp.
 cudaError_t launch_gemv(const uint16_t* db, int db_rows, int64_t db_cols, int nq, const uint32_t* a_il,
-                        uint64_t* c, int sm_count, cudaStream_t st, int form = 0);
+                        uint64_t* c, int sm_count, cudaStream_t st, int form = 0, int* err_flag = nullptr);
+// 2D tensor map over the column-major u16 DB ([db_cols][db_rows]), boxes of box_rows x box_cols
+// with the 32-byte swizzle (box_rows = 16)
+cudaError_t make_u16_col_map(CUtensorMap* map, const uint16_t* db, int db_rows, int64_t db_cols, uint32_t box_rows,
+                             uint32_t box_cols);
 cudaError_t launch_pack(const uint64_t* bt, const uint64_t* btb, const uint64_t* bth, const uint64_t* y,
                         const uint64_t* z, uint32_t* S, int num_outputs, cudaStream_t st);
 // R = from_ntt(S) per (client, output) polynomial pair; with z_bodies non-null the

@@ -160,11 +160,12 @@ int enqueue(ipr_server* s, unsigned nq, const uint8_t* d_query, uint8_t* d_resp,
         } else {
             for (unsigned g = 0; 2 * g < nq; g++) {
                 const int ng = nq - 2 * g >= 2 ? 2 : 1;
-                // the FP64-pipe forms hold exact sums only up to 16,384 rows; beyond, form 0
-                const int form = (s->gemv_form >= 4 && p.db_rows > 16384) ? 0 : s->gemv_form;
+                // forms 4 and 5 hold exact sums only up to 16,384 rows; beyond, form 0
+                const int form =
+                    ((s->gemv_form == 4 || s->gemv_form == 5) && p.db_rows > 16384) ? 0 : s->gemv_form;
                 CU(ipr::launch_gemv(s->d_db, (int)p.db_rows, (int64_t)p.db_cols, ng,
                                     s->d_ail + (size_t)g * p.db_rows * 4, s->d_c + (size_t)2 * g * p.db_cols,
-                                    s->sm_count, st, form));
+                                    s->sm_count, st, form, s->d_err));
             }
         }
         rec(2);
@@ -1105,7 +1106,7 @@ int ipr_server_set_option(ipr_server* s, int option, int64_t value) {
             return IPR_OK;
         }
         case IPR_OPT_GEMV_FORM:
-            if (value < 0 || value > 5) return fail(IPR_E_ARGS, "IPR_OPT_GEMV_FORM takes 0 to 5");
+            if (value < 0 || value > 6) return fail(IPR_E_ARGS, "IPR_OPT_GEMV_FORM takes 0 to 6");
             s->gemv_form = (int)value;
             destroy_graphs(s);
             return IPR_OK;

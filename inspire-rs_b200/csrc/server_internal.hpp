@@ -49,7 +49,7 @@ struct ipr_server {
                                // 0 smem fold
     int pack_pair = 2;         // batch packing GEMM on CTA pairs: 0 never, 1 always, 2 from 48 payloads up
     int g1_tile = 0;           // first-dimension GEMM query-byte tile height cap (0 = 256)
-    int gemv_form = 5;         // form of the CUDA-core GEMV (IPR_OPT_GEMV_FORM)
+    int gemv_form = 6;         // form of the CUDA-core GEMV (IPR_OPT_GEMV_FORM)
     std::map<int, CUtensorMap> tm_qb;  // per query-byte tile height
     uint64_t *d_ahat = nullptr, *d_bt = nullptr, *d_btb = nullptr, *d_bth = nullptr;
     uint8_t* d_stash = nullptr;

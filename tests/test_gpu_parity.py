@@ -105,7 +105,7 @@ def test_fold_kernels(pkg, orc, regs, instances, interp):
             assert srv.respond_to_serialized_query(q) == orc.respond(sdb, q)
 
 
-@pytest.mark.parametrize("form", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("form", [0, 1, 2, 3, 4, 5, 6])
 def test_u64_gemv_forms(cfg0, pkg, orc, form):
     """the CUDA-core GEMV forms (8 / 4 / 2 DB columns per warp in registers, 8 columns staged
     through a shared-memory ring, products on the FP64 pipe, limbs split between the integer
@@ -118,7 +118,7 @@ def test_u64_gemv_forms(cfg0, pkg, orc, form):
             q = orc.synth_query(70 + nq + form, plan.db_rows, nq)
             assert srv.respond_to_serialized_query(q) == orc.respond(sdb, q)
     finally:
-        srv.set_option(pkg.KeywordServer.OPT_GEMV_FORM, 5)
+        srv.set_option(pkg.KeywordServer.OPT_GEMV_FORM, 6)
         srv.set_option(pkg.KeywordServer.OPT_TENSOR_GEMV, 1)
 
 
@@ -126,14 +126,15 @@ def test_u64_gemv_forms(cfg0, pkg, orc, form):
 def test_fp64_gemv_forms_at_their_row_limit(pkg, orc, db_rows):
     """the FP64-pipe GEMV forms at their row limits, where a lane's partial sum of full-range
     products can come within a factor 2 of 2^53: form 5 at 4,096 rows (above it, form 4), form 4
-    at 16,384, and past both (32,768 rows, run as form 0)"""
+    at 16,384, and past both (32,768 rows, run as form 0); form 6, which flushes its double sums
+    every 256 rows, at all three"""
     plan = _plan(pkg, 2, 2, db_rows=db_rows)
     with pkg.KeywordServer.synthetic(plan, seed=23) as srv:
         sdb = orc.SynthDB(plan.db_rows, 2, 2, 1, seed=23)
         q = orc.synth_query(6, plan.db_rows, 2)
         want = orc.respond(sdb, q)
         srv.set_option(pkg.KeywordServer.OPT_TENSOR_GEMV, 0)
-        for form in (4, 5):
+        for form in (4, 5, 6):
             srv.set_option(pkg.KeywordServer.OPT_GEMV_FORM, form)
             assert srv.respond_to_serialized_query(q) == want
 
