@@ -206,8 +206,11 @@ int ipr_server_set_profiling(ipr_server *srv, int on);
  * Identical results. */
 #define IPR_OPT_PACK_CTA_PAIR 3
 /* IPR_OPT_GEMV_TILE: cap on the first-dimension GEMM's query-byte tile height
- * (N of each MMA: 16, 32, 64, 128 or 256; 0 = 256, the default).  Up to 128 the
- * two accumulators of a tile are double-buffered in TMEM. */
+ * (16, 32, 64, 128 or 256; 0 = 256, the default).  A query takes 7 byte rows (the bytes
+ * of its CRT-composed value), so the tile height N of each MMA is the smallest multiple of
+ * 16 that holds the call's queries, at most 224 (32 queries), and under a cap of 128 or
+ * more the largest multiple of 112 (16 queries) within it.  Up to 128 the two accumulators
+ * of a tile are double-buffered in TMEM. */
 #define IPR_OPT_GEMV_TILE 4
 /* IPR_OPT_GEMV_FORM: form of the CUDA-core first-dimension GEMV (IPR_OPT_TENSOR_GEMV 0)
  * for two queries: 0 / 1 / 2 = 8 / 4 / 2 DB columns per warp loaded into

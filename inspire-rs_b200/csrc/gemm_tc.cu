@@ -3,12 +3,22 @@
 // c[q][j] = CRT( sum_k a_q,0[k] D[j][k] mod q0 , sum_k a_q,1[k] D[j][k] mod q1 )
 // (native/cuda/gemv_kernel.cu:46-103 of rkdud007/inspire-rs, for many queries).
 // Exact split precision: the DB is kept as two byte planes D = D_0 + 256 D_1
-// ([plane][db_cols][db_rows] u8) and every 28-bit query residue as four bytes
-// a = sum_b 256^b a_b, so the dot products are sums of u8 x u8 products:
-//   sum_k D[j][k] a[k] = sum_{p,b} 256^(p+b) P_pb[j],  P_pb[j] = sum_k D_p[j][k] a_b[k]
+// ([plane][db_cols][db_rows] u8).  A query value arrives as its two residues (a_0 mod q0,
+// a_1 mod q1); the parse composes them by the CRT into X < q0 q1 < 2^56, with X = a_l mod
+// q_l, and stores the 7 bytes X = sum_b 256^b X_b, so the dot products are sums of u8 x u8
+// products:
+//   sum_k D[j][k] X[k] = sum_{p,b} 256^(p+b) P_pb[j],  P_pb[j] = sum_k D_p[j][k] X_b[k]
+// and sum_k D[j][k] a_l[k] = (sum_k D[j][k] X[k]) mod q_l.  Seven bytes per query instead of
+// four per residue take 2 x 7 byte products per DB entry and query, not 2 x 8.
 // Each P_pb is one column of a u8 x u8 -> 32-bit tcgen05.mma (kind::i8) GEMM;
-// P_pb < 255^2 * db_rows < 2^31 for db_rows <= 32768, so accumulation is exact,
-// and the recombination sum_{p,b} 256^(p+b) P_pb < 2^63 fits a u64.
+// P_pb < 255^2 * db_rows < 2^31 for db_rows <= 32768, so accumulation is exact.  The
+// recombination splits at byte 4: W0 = sum_{b<4} 256^b S_b < 2^64 and
+// W1 = sum_{b>=4} 256^(b-4) S_b < 2^56 with S_b = P_0b + 256 P_1b, and the sum is
+// W0 + 2^32 W1, reduced mod q_l by two Montgomery steps.
+//
+// Query-byte layout: row 7 q + b holds byte b of query q's values.  A tile of NT rows (N of
+// the MMA, a multiple of 16) carries floor(NT / 7) whole queries and starts at row
+// 7 floor(NT / 7) n; its last NT mod 7 rows are the next queries' bytes, ignored.
 //
 // Kernel shape: persistent CTAs of 10 warps.  Warp 0 issues TMA loads into a
 // multi-stage shared-memory ring (128-byte swizzle); one stage holds the same
@@ -46,6 +56,47 @@ struct G1Smem {
 };
 
 }  // namespace
+
+// One octet of queries of an accumulator tile (octet 2 sg + ODD: local queries
+// 16 sg + 8 ODD .. + 8, columns 112 sg + 56 ODD .. + 56, inside column groups 7 sg + 3 ODD ..
+// 7 sg + 3 ODD + 3): each thread recombines its DB column's byte sums of the 8 queries and
+// writes their CRT-composed residue pairs.
+template <int ODD>
+__device__ __forceinline__ void epilogue_octet(uint32_t acc0, uint32_t acc1, int sg, int nt, int qpt, int q0,
+                                               int num_queries, uint64_t* __restrict__ c, int64_t db_cols,
+                                               int64_t j) {
+    uint64_t w0[8], w1[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) w0[i] = w1[i] = 0;
+#pragma unroll
+    for (int g = 3 * ODD; g < 3 * ODD + 4; g++) {
+        const int col0 = sg * 112 + g * 16;
+        if (col0 >= nt) break;
+        uint32_t p0[16], p1[16];
+        umma::tmem_ld16(acc0 + (uint32_t)col0, p0);
+        umma::tmem_ld16(acc1 + (uint32_t)col0, p1);
+        umma::tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            const int cl = g * 16 + i, ql = cl / 7 - 8 * ODD, b = cl % 7;
+            if (ql >= 0 && ql < 8) {
+                const uint64_t sb = (uint64_t)p0[i] + ((uint64_t)p1[i] << 8);
+                if (b < 4) w0[ql] += sb << (8 * b);
+                else w1[ql] += sb << (8 * (b - 4));
+            }
+        }
+    }
+#pragma unroll
+    for (int ql = 0; ql < 8; ql++) {
+        const int qloc = sg * 16 + 8 * ODD + ql, q = q0 + qloc;
+        if (qloc < qpt && q < num_queries) {
+            const uint64_t t = w1[ql] + (w0[ql] >> 32), lo = w0[ql] & 0xffffffffull;
+            const uint32_t r0 = mod64m(((uint64_t)mod64m(t, Q0) << 32) + lo, Q0);
+            const uint32_t r1 = mod64m(((uint64_t)mod64m(t, Q1) << 32) + lo, Q1);
+            c[(int64_t)q * db_cols + j] = crt2m(r0, r1);
+        }
+    }
+}
 
 __global__ void __launch_bounds__(G1_THREADS, 1)
     k_gemm1(const __grid_constant__ CUtensorMap tm_db, const __grid_constant__ CUtensorMap tm_qb, int db_rows,
@@ -107,7 +158,8 @@ __global__ void __launch_bounds__(G1_THREADS, 1)
                     umma::tma_load_2d(at, &tm_db, ks * TILE_K, (int)(m * TILE_M), &sh->full[stage]);
                     umma::tma_load_2d(at + A_STAGE_BYTES, &tm_db, ks * TILE_K, (int)(db_cols + m * TILE_M),
                                       &sh->full[stage]);
-                    umma::tma_load_2d(b_tiles + stage * b_stage_bytes, &tm_qb, ks * TILE_K, n * nt, &sh->full[stage]);
+                    umma::tma_load_2d(b_tiles + stage * b_stage_bytes, &tm_qb, ks * TILE_K, n * (nt / 7) * 7,
+                                      &sh->full[stage]);
                     last_phase[stage] = (int)phase;
                     if (++stage == stages) {
                         stage = 0;
@@ -186,28 +238,14 @@ __global__ void __launch_bounds__(G1_THREADS, 1)
             const int n_tile = (int)(t % n_tiles);
             const int64_t j = m * TILE_M + row;
             const uint32_t lane_off = (uint32_t)(quarter * 32) << 16;
-            for (int g = half; g < nt / 16; g += 2) {
-                uint32_t p0[16], p1[16];
-                umma::tmem_ld16(tmem + lane_off + (uint32_t)((buf * 2 + 0) * nt + g * 16), p0);
-                umma::tmem_ld16(tmem + lane_off + (uint32_t)((buf * 2 + 1) * nt + g * 16), p1);
-                umma::tmem_wait_ld();
-                // 16 columns = 2 queries x 2 limbs x 4 bytes: column (q*2 + l)*4 + b
-#pragma unroll
-                for (int qq = 0; qq < 2; qq++) {
-                    const int q = (n_tile * nt + g * 16) / 8 + qq;
-                    uint32_t r[2];
-#pragma unroll
-                    for (int l = 0; l < 2; l++) {
-                        uint64_t v = 0;
-#pragma unroll
-                        for (int b = 0; b < 4; b++) {
-                            const int i = (qq * 2 + l) * 4 + b;
-                            v += ((uint64_t)p0[i] + ((uint64_t)p1[i] << 8)) << (8 * b);
-                        }
-                        r[l] = mod64m(v, l ? Q1 : Q0);
-                    }
-                    if (q < num_queries) c[(int64_t)q * db_cols + j] = crt2m(r[0], r[1]);
-                }
+            // queries in octets (8 queries = 56 columns); half 0 takes the even octets, half 1
+            // the odd ones, so the column -> (query, byte) map of each is known at compile time
+            const int qpt = nt / 7;
+            const uint32_t acc0 = tmem + lane_off + (uint32_t)(buf * 2 * nt), acc1 = acc0 + (uint32_t)nt;
+            const int q0 = n_tile * qpt;
+            for (int o = half; o < (qpt + 7) / 8; o += 2) {
+                if (half) epilogue_octet<1>(acc0, acc1, o >> 1, nt, qpt, q0, num_queries, c, db_cols, j);
+                else epilogue_octet<0>(acc0, acc1, o >> 1, nt, qpt, q0, num_queries, c, db_cols, j);
             }
             umma::fence_before();
             __syncwarp();

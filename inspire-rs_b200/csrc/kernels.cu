@@ -86,13 +86,13 @@ __global__ void k_parse_query(const uint8_t* __restrict__ qb_all, int nq, int db
                     dst[0] = lo;
                     dst[1] = hi;
                 }
-                if (qbytes) {  // tensor-core operand: row (query*2 + limb)*4 + byte, column r
-                    uint8_t* qrow = qbytes + (int64_t)(qbase + q) * 8 * db_rows + r;
+                if (qbytes) {  // tensor-core operand: row query*7 + byte of X, column r, where
+                    // X = crt(lo, hi) < q0 q1 < 2^56 is congruent to lo mod q0 and to hi mod q1
+                    // (for any lo, hi below 2^28)
+                    const uint64_t x = crt2m(lo, hi);
+                    uint8_t* qrow = qbytes + (int64_t)(qbase + q) * 7 * db_rows + r;
 #pragma unroll
-                    for (int b = 0; b < 4; b++) {
-                        qrow[(int64_t)b * db_rows] = (uint8_t)(lo >> (8 * b));
-                        qrow[(int64_t)(4 + b) * db_rows] = (uint8_t)(hi >> (8 * b));
-                    }
+                    for (int b = 0; b < 7; b++) qrow[(int64_t)b * db_rows] = (uint8_t)(x >> (8 * b));
                 }
             } else {
                 const int64_t rr = r - db_rows;  // poly c = rr / N, coeff z = rr % N
@@ -1021,7 +1021,7 @@ cudaError_t parse_extents(const uint8_t* qb, int npay, int64_t pstride, int nq, 
     if (a_il && (e = check_extent(a_il, (uint64_t)(nq + 1) / 2 * db_rows * 4 * 4, "parse: GEMV operand")) != cudaSuccess)
         return e;
     if (qbytes &&
-        (e = check_extent(qbytes, ((uint64_t)qbase + (uint64_t)npay * nq) * 8 * db_rows, "parse: query byte rows")) !=
+        (e = check_extent(qbytes, ((uint64_t)qbase + (uint64_t)npay * nq) * 7 * db_rows, "parse: query byte rows")) !=
             cudaSuccess)
         return e;
     return cudaSuccess;

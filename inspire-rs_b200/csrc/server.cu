@@ -69,22 +69,22 @@ void destroy_graphs(ipr_server* s) {
     s->graphs.clear();
 }
 
-// query-byte tile height for nq queries (8 byte-rows per query) and the padded row count
-int qb_tile(unsigned nq) {
-    int n = (int)(8 * nq + 15) / 16 * 16;
-    return n > 256 ? 256 : n;
-}
-unsigned qb_rows(unsigned nq) {
-    const unsigned nt = (unsigned)qb_tile(nq);
-    return (8 * nq + nt - 1) / nt * nt;
-}
+// query-byte rows: 7 per query (the bytes of its CRT-composed value); a tile of nt rows
+// (the MMA's N, a multiple of 16) carries nt / 7 whole queries.  The buffer holds 256 rows
+// beyond the queries, so that every tile box lies inside it.
+constexpr unsigned kQbPadRows = 256;
+unsigned qb_rows(unsigned nq) { return 7 * nq + kQbPadRows; }
 
-// the GEMM's tile height: the query-byte tile, capped by the server option where the cap
-// divides it (then it also divides qb_rows)
+// the GEMM's tile height: the smallest multiple of 16 that holds all nq queries, at most 224
+// (32 queries), lowered under the server option's cap to a multiple of 112 (16 queries, no
+// unused rows) when the cap allows one, else to a multiple of 16
 int g1_nt(const ipr_server* s, unsigned nq) {
-    const int nt = qb_tile(nq);
-    return s->g1_tile && s->g1_tile < nt && nt % s->g1_tile == 0 ? s->g1_tile : nt;
+    int nt = (int)(7 * nq + 15) / 16 * 16;
+    if (nt > 224) nt = 224;
+    if (s->g1_tile && s->g1_tile < nt) nt = s->g1_tile >= 112 ? s->g1_tile / 112 * 112 : s->g1_tile / 16 * 16;
+    return nt < 16 ? 16 : nt;
 }
+int g1_tiles(unsigned nq, int nt) { return (int)((nq + nt / 7 - 1) / (nt / 7)); }
 
 int qb_map(ipr_server* s, int nt, const CUtensorMap** out) {
     auto it = s->tm_qb.find(nt);
@@ -155,7 +155,7 @@ int enqueue(ipr_server* s, unsigned nq, const uint8_t* d_query, uint8_t* d_resp,
             const CUtensorMap* tq;
             int e = qb_map(s, nt, &tq);
             if (e) return e;
-            CU(ipr::launch_gemm1(&s->tm_db, tq, (int)p.db_rows, (int64_t)p.db_cols, nt, (int)(qb_rows(nq) / nt),
+            CU(ipr::launch_gemm1(&s->tm_db, tq, (int)p.db_rows, (int64_t)p.db_cols, nt, g1_tiles(nq, nt),
                                  (int)nq, s->d_c, s->d_err, s->sm_count, st));
         } else {
             for (unsigned g = 0; 2 * g < nq; g++) {
@@ -312,7 +312,7 @@ int enqueue_batch(ipr_server* s, int B, const uint8_t* d_queries, uint8_t* d_res
         const CUtensorMap* tq;
         int e = qb_map(s, nt, &tq);
         if (e) return e;
-        CU(ipr::launch_gemm1(&s->tm_db, tq, (int)p.db_rows, (int64_t)p.db_cols, nt, (int)(qb_rows((unsigned)nqt) / nt),
+        CU(ipr::launch_gemm1(&s->tm_db, tq, (int)p.db_rows, (int64_t)p.db_cols, nt, g1_tiles((unsigned)nqt, nt),
                              nqt, s->d_c, s->d_err, s->sm_count, st));
     }
     rec(2);

@@ -64,7 +64,7 @@ struct ipr_server {
     uint32_t *d_ail = nullptr, *d_gsw = nullptr, *d_S = nullptr;
     uint64_t *d_R = nullptr, *d_c = nullptr;
     uint8_t* d_resp = nullptr;
-    uint8_t* d_qb = nullptr;  // query bytes [(q*2 + limb)*4 + byte][db_rows]
+    uint8_t* d_qb = nullptr;  // query bytes [q*7 + byte][db_rows], bytes of the CRT-composed values
     int* d_err = nullptr;     // device-side wait failures (bounded waits)
     uint8_t *h_query = nullptr, *h_resp = nullptr;
     int* h_err = nullptr;
