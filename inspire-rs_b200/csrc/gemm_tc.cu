@@ -27,7 +27,7 @@
 // (M = 128 DB columns, N = NT query-byte columns, K = 32 bytes each) into
 // TMEM accumulators, one per plane, double buffered when they fit; warps 2-5
 // read the accumulators, recombine, reduce mod q0 / q1 and CRT-compose.
-// Eight epilogue warps (two per TMEM lane quarter) keep the drain short while
+// Sixteen epilogue warps (four per TMEM lane quarter) keep the drain short while
 // both accumulators of a tile occupy all of TMEM.
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -43,7 +43,8 @@ namespace ipr {
 
 namespace {
 
-constexpr int G1_THREADS = 320;  // producer, MMA, 8 epilogue warps
+constexpr int G1_THREADS = 576;  // producer, MMA, 16 epilogue warps
+constexpr int G1_EPI_WARPS = 16;
 constexpr int TILE_M = 128;
 constexpr int TILE_K = 128;  // bytes per stage along K (one 128-byte swizzle row)
 constexpr int A_STAGE_BYTES = TILE_M * TILE_K;
@@ -90,10 +91,7 @@ __device__ __forceinline__ void epilogue_octet(uint32_t acc0, uint32_t acc1, int
     for (int ql = 0; ql < 8; ql++) {
         const int qloc = sg * 16 + 8 * ODD + ql, q = q0 + qloc;
         if (qloc < qpt && q < num_queries) {
-            const uint64_t t = w1[ql] + (w0[ql] >> 32), lo = w0[ql] & 0xffffffffull;
-            const uint32_t r0 = mod64m(((uint64_t)mod64m(t, Q0) << 32) + lo, Q0);
-            const uint32_t r1 = mod64m(((uint64_t)mod64m(t, Q1) << 32) + lo, Q1);
-            c[(int64_t)q * db_cols + j] = crt2m(r0, r1);
+            c[(int64_t)q * db_cols + j] = crt2m(mod96m(w0[ql], w1[ql], Q0), mod96m(w0[ql], w1[ql], Q1));
         }
     }
 }
@@ -124,7 +122,7 @@ __global__ void __launch_bounds__(G1_THREADS, 1)
         }
         for (int b = 0; b < 2; b++) {
             umma::mbar_init(&sh->acc_full[b], 1);
-            umma::mbar_init(&sh->acc_empty[b], 8);
+            umma::mbar_init(&sh->acc_empty[b], G1_EPI_WARPS);
         }
         *err = 0;
         umma::fence_mbar_init();
@@ -221,10 +219,10 @@ __global__ void __launch_bounds__(G1_THREADS, 1)
             if (last_stage >= 0) umma::mbar_wait(&sh->empty[last_stage], last_parity, umma::kDrainLimitNs);
         }
     } else {
-        // epilogue: warps 2..9 -> TMEM lane quarters 2,3,0,1 (twice); the two warps of a quarter
-        // split the accumulator's column groups between them
+        // epilogue: warps 2..17 -> TMEM lane quarters 2,3,0,1 (four times); the four warps of a
+        // quarter split the accumulator's query octets between them
         const int quarter = warp & 3;
-        const int half = (warp - 2) >> 2;
+        const int sub = (warp - 2) >> 2;  // 0..3: the octets sub, sub + 4, ...
         const int row = quarter * 32 + lane;
         int buf = 0;
         uint32_t acc_phase = 0;
@@ -238,13 +236,13 @@ __global__ void __launch_bounds__(G1_THREADS, 1)
             const int n_tile = (int)(t % n_tiles);
             const int64_t j = m * TILE_M + row;
             const uint32_t lane_off = (uint32_t)(quarter * 32) << 16;
-            // queries in octets (8 queries = 56 columns); half 0 takes the even octets, half 1
-            // the odd ones, so the column -> (query, byte) map of each is known at compile time
+            // queries in octets (8 queries = 56 columns); warps with sub even take even octets,
+            // the others odd ones, so the column -> (query, byte) map is known at compile time
             const int qpt = nt / 7;
             const uint32_t acc0 = tmem + lane_off + (uint32_t)(buf * 2 * nt), acc1 = acc0 + (uint32_t)nt;
             const int q0 = n_tile * qpt;
-            for (int o = half; o < (qpt + 7) / 8; o += 2) {
-                if (half) epilogue_octet<1>(acc0, acc1, o >> 1, nt, qpt, q0, num_queries, c, db_cols, j);
+            for (int o = sub; o < (qpt + 7) / 8; o += G1_EPI_WARPS / 4) {
+                if (sub & 1) epilogue_octet<1>(acc0, acc1, o >> 1, nt, qpt, q0, num_queries, c, db_cols, j);
                 else epilogue_octet<0>(acc0, acc1, o >> 1, nt, qpt, q0, num_queries, c, db_cols, j);
             }
             umma::fence_before();

@@ -84,6 +84,18 @@ __device__ __forceinline__ uint32_t mod64m(uint64_t v, uint32_t q) {
     return min(t1, t1 - q);
 }
 
+// w0 + 2^32 w1 (w0 < 2^64, w1 < 2^56) to [0, q) by one Montgomery reduction: with
+// t = w1 + (w0 >> 32) = th 2^32 + tl, x = (w0 mod 2^32)(2^32 mod q) + tl (2^64 mod q)
+// + th (2^96 mod q) < 2^62 and redc(x) = (w0 + 2^32 w1) mod q in [0, 4q)
+constexpr uint32_t R3_0 = (uint32_t)((uint64_t)R2_0 * R1_0 % Q0), R3_1 = (uint32_t)((uint64_t)R2_1 * R1_1 % Q1);
+__device__ __forceinline__ uint32_t mod96m(uint64_t w0, uint64_t w1, uint32_t q) {
+    const uint64_t t = w1 + (w0 >> 32);
+    const uint64_t x = (uint64_t)(uint32_t)w0 * (q == Q0 ? R1_0 : R1_1) +
+                       (uint64_t)(uint32_t)t * (q == Q0 ? R2_0 : R2_1) + (t >> 32) * (q == Q0 ? R3_0 : R3_1);
+    const uint32_t r = redc(x, q), r1 = min(r, r - 2 * q);
+    return min(r1, r1 - q);
+}
+
 // crt2 with the Garner coefficient in Montgomery form: (y - x) q0^-1 mod q1 by one reduction
 __device__ __forceinline__ uint64_t crt2m(uint32_t x, uint32_t y) {
     const uint32_t xm = x >= Q1 ? x - Q1 : x;            // x < q0 < 2 q1
