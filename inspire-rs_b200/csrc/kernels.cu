@@ -429,13 +429,14 @@ constexpr int gsf_smem(int db_rows) { return GS_WARPS * GSF_STAGES * GS_COLS * 3
 // built by integer operations; a product is below 2^45) and a lane's double accumulators
 // are flushed after at most 16 stages (256 rows, below 2^53: exact) into 64-bit integer
 // sums in shared memory by atomic adds.  At the tile's end the 16 warps meet at a named
-// barrier and each of the first 256 threads finishes one (column, query) output (16 warps
-// of 122 registers fill the register file; more warps per SM, not deeper rings, is what
-// shortened this kernel, 0.85 against 0.92-0.95 ms at 1M for 8 warps x 5 stages): the offset 2^16 x (sum of
-// the limb's residues over all rows) is taken off, then the Barrett reductions and the CRT.
-// The sums use two buffers (alternating tiles), so one barrier per tile suffices.  A stage
-// wait is bounded by time: after a failed wait the warp stops waiting and issuing, the
-// kernel reports code 31 through err_flag and drains its own copies before it returns.
+// barrier and each of the first 256 threads finishes one (column, query) output: the offset
+// 2^16 x (sum of the limb's residues over all rows) is taken off, then the Barrett
+// reductions and the CRT.  The sums use two buffers (alternating tiles), so one barrier per
+// tile suffices.  Sixteen warps of 122 registers fill the register file; more warps per SM,
+// not deeper rings, is what shortened this kernel (0.85 ms at 1M against 0.92-0.95 ms for
+// 8 warps with 5-stage rings).  A stage wait is bounded by time: after a failed wait the
+// warp stops waiting and issuing, the kernel reports code 31 through err_flag and drains
+// its own copies before it returns.
 constexpr int GT_WARPS = 16, GT_ROWS = 16, GT_COLS = 128, GT_STAGES = 2;
 constexpr int GT_DB_BYTES = GT_ROWS * GT_COLS * 2;  // 4 KB of DB per stage
 constexpr int GT_RES_BYTES = GT_ROWS * 16;          // the stage rows' 4 u32 residues each
