@@ -18,7 +18,8 @@ cudaError_t launch_parse_query(const uint8_t* qb, int nq, int db_rows, uint64_t*
 // kernel: 0 / 1 / 2 = 8 / 4 / 2 DB columns per warp loaded into registers, 3 = 8 columns per
 // warp staged through shared memory by cp.async, 4 / 5 = forms 0 / 3 with FP64-pipe products,
 // 6 = a lane per column with TMA-fed stages and FP64-pipe products (needs err_flag and
-// db_rows a multiple of 128; otherwise form 5 runs).  One query always takes 16 columns per warp.
+// db_rows a multiple of 256, at most 2^18; otherwise form 5 runs, or form 0 above 16,384
+// rows).  One query always takes 16 columns per warp.
 cudaError_t launch_gemv(const uint16_t* db, int db_rows, int64_t db_cols, int nq, const uint32_t* a_il,
                         uint64_t* c, int sm_count, cudaStream_t st, int form = 0, int* err_flag = nullptr);
 // 2D tensor map over the column-major u16 DB ([db_cols][db_rows]), boxes of box_rows x box_cols
